@@ -1,0 +1,529 @@
+// C ABI of the B200-native tetrahedral volume-rendering path (see
+// include/difftetvr_b200.h).  Host orchestration: buffers, stage order, the
+// one host synchronisation per render (the exact fragment count from the scan
+// sizes the record buffer), error reporting.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include "difftetvr_b200.h"
+#include "dtv_internal.h"
+
+extern "C" int32_t dtv_build_hex_mesh_impl(const float* mn, const float* mx, uint32_t xs, uint32_t ys,
+                                           uint32_t zs, uint32_t* cells, float* positions);
+
+namespace {
+
+using u64 = unsigned long long;
+
+thread_local std::string g_last_error;
+
+struct DtvError : std::runtime_error {
+    int32_t code;
+    DtvError(int32_t c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define DTV_CK(expr)                                                                                   \
+    do {                                                                                               \
+        cudaError_t err__ = (expr);                                                                    \
+        if (err__ != cudaSuccess)                                                                      \
+            throw DtvError(DTV_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(err__));       \
+    } while (0)
+
+inline void check_launch(const char* what) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) throw DtvError(DTV_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <class F>
+int32_t guarded(F&& fn) {
+    try {
+        fn();
+        return DTV_OK;
+    } catch (const DtvError& e) {
+        g_last_error = e.what();
+        return e.code;
+    } catch (const std::invalid_argument& e) {
+        g_last_error = e.what();
+        return DTV_ERR_ARG;
+    } catch (const std::bad_alloc&) {
+        g_last_error = "host allocation failed";
+        return DTV_ERR_BUDGET;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return DTV_ERR_STATE;
+    }
+}
+
+inline void require(bool cond, const char* msg) {
+    if (!cond) throw DtvError(DTV_ERR_ARG, msg);
+}
+
+// Grow-only device buffer.
+template <class T>
+struct DevBuf {
+    T* ptr = nullptr;
+    size_t cap = 0;
+    bool ensure(size_t n, cudaStream_t s, bool zero_new = false, double headroom = 1.0) {
+        if (n <= cap && ptr) return false;
+        if (ptr) {
+            DTV_CK(cudaStreamSynchronize(s));
+            DTV_CK(cudaFree(ptr));
+            ptr = nullptr;
+            cap = 0;
+        }
+        size_t want = size_t(double(n) * headroom);
+        if (want < n) want = n;
+        if (want == 0) want = 1;
+        cudaError_t e = cudaMalloc(&ptr, want * sizeof(T));
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            ptr = nullptr;
+            throw DtvError(DTV_ERR_BUDGET, "device allocation of " + std::to_string(want * sizeof(T)) +
+                                               " bytes failed: " + cudaGetErrorString(e));
+        }
+        cap = want;
+        if (zero_new) DTV_CK(cudaMemsetAsync(ptr, 0, want * sizeof(T), s));
+        return true;
+    }
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        cap = 0;
+    }
+};
+
+dtv::CamDev make_cam(const dtv_camera& c) {
+    dtv::CamDev k;
+    std::memcpy(k.V, c.view, sizeof(k.V));
+    const double tanh = std::tan(0.5 * double(c.fovy));
+    k.f = float(0.5 * double(c.height) / tanh);
+    k.cx = 0.5f * float(c.width);
+    k.cy = 0.5f * float(c.height);
+    k.znear = c.znear;
+    k.zfar = c.zfar;
+    k.W = c.width;
+    k.H = c.height;
+    return k;
+}
+
+dtv::ShadeDev make_shade(const dtv_render_params& p) {
+    dtv::ShadeDev s;
+    s.atten = p.attenuation;
+    s.ert_thresh = p.early_ray_out_thresh;
+    s.use_ert = p.use_early_ray_termination ? 1 : 0;
+    s.use_abs_grad = p.use_abs_grad ? 1 : 0;
+    for (int k = 0; k < 4; ++k) s.clear[k] = p.clear_color[k];
+    return s;
+}
+
+enum Stage { kProject = 0, kCount, kScan, kFill, kSort, kComposite, kAdjoint, kNumStages };
+
+}  // namespace
+
+struct dtv_mesh {
+    dtv::MeshHost host;
+    uint4* d_faces = nullptr;
+    uint32_t* d_vertex_boundary = nullptr;
+    uint32_t* d_face_to_tet = nullptr;
+    uint32_t* d_cells = nullptr;
+};
+
+struct dtv_renderer {
+    int32_t type = DTV_RENDERER_PPLL;
+    DevBuf<float4> vproj;
+    DevBuf<int2> vfix;
+    DevBuf<uint32_t> counts;
+    DevBuf<u64> offsets;
+    DevBuf<u64> records;
+    DevBuf<u64> scan_scratch;
+    DevBuf<float> tfinal;
+    DevBuf<uint32_t> term;
+    DevBuf<uint32_t> long_list;
+    DevBuf<uint32_t> flags;
+    u64* h_nf = nullptr;          // pinned
+    uint32_t* h_flags = nullptr;  // pinned
+    bool flags_pending = false;
+    cudaEvent_t flags_event = nullptr;
+    // State of the last render.
+    bool have_render = false;
+    const dtv_mesh* mesh = nullptr;
+    dtv::CamDev cam{};
+    dtv::ShadeDev sh{};
+    uint64_t P = 0, V = 0, nf = 0;
+    // Stage timing.
+    bool timing = false;
+    cudaEvent_t ev[kNumStages + 2] = {};  // render: 0..6, adjoint: 7..8
+    float stage_ms[kNumStages] = {};
+    bool adjoint_timed = false;
+};
+
+namespace {
+
+void check_pending_flags(dtv_renderer* r) {
+    if (!r->flags_pending) return;
+    DTV_CK(cudaEventSynchronize(r->flags_event));
+    r->flags_pending = false;
+    if (r->h_flags[1] != 0u)
+        throw DtvError(DTV_ERR_BUDGET, "a per-pixel fragment list exceeded " +
+                                           std::to_string(dtv::kSortBlockCap) +
+                                           " entries in the previous render; its order is undefined");
+}
+
+void rec_event(dtv_renderer* r, int idx, cudaStream_t s) {
+    if (r->timing) DTV_CK(cudaEventRecord(r->ev[idx], s));
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t dtv_version(void) { return 100; }
+
+const char* dtv_last_error_string(void) { return g_last_error.c_str(); }
+
+int32_t dtv_build_hex_mesh(const float* aabb_min3, const float* aabb_max3, uint32_t xs, uint32_t ys, uint32_t zs,
+                           uint32_t* h_cells, float* h_positions) {
+    return guarded([&] {
+        require(aabb_min3 && aabb_max3 && h_cells && h_positions, "null pointer");
+        require(xs >= 2 && ys >= 2 && zs >= 2, "xs, ys, zs must be >= 2 (vertex counts per axis)");
+        require(uint64_t(xs) * ys * zs < (1ull << 32), "grid too large for u32 vertex indices");
+        dtv_build_hex_mesh_impl(aabb_min3, aabb_max3, xs, ys, zs, h_cells, h_positions);
+    });
+}
+
+int32_t dtv_mesh_build_faces_host(const uint32_t* h_cells, uint64_t num_cells, uint64_t num_vertices,
+                                  uint32_t* h_tri, uint32_t* h_fb, uint32_t* h_f2t, uint32_t* h_vb,
+                                  uint64_t* num_faces) {
+    return guarded([&] {
+        require(h_cells != nullptr || num_cells == 0, "cells is null");
+        require(h_tri && h_fb && h_f2t && h_vb && num_faces, "null output pointer");
+        dtv::MeshHost mh;
+        dtv::build_faces(h_cells, num_cells, num_vertices, mh);
+        std::memcpy(h_tri, mh.tri.data(), sizeof(uint32_t) * mh.tri.size());
+        std::memcpy(h_fb, mh.face_boundary.data(), sizeof(uint32_t) * mh.face_boundary.size());
+        std::memcpy(h_f2t, mh.face_to_tet.data(), sizeof(uint32_t) * mh.face_to_tet.size());
+        std::memcpy(h_vb, mh.vertex_boundary.data(), sizeof(uint32_t) * mh.vertex_boundary.size());
+        *num_faces = mh.num_faces;
+    });
+}
+
+int32_t dtv_mesh_create(const uint32_t* h_cells, uint64_t num_cells, uint64_t num_vertices, dtv_mesh** out) {
+    return guarded([&] {
+        require(out != nullptr, "out is null");
+        require(h_cells != nullptr || num_cells == 0, "cells is null");
+        require(num_vertices < (1ull << 32), "too many vertices");
+        require(num_cells < (1ull << 28), "too many cells (face index must fit in 30 bits)");
+        *out = nullptr;
+        auto* m = new dtv_mesh();
+        try {
+            dtv::build_faces(h_cells, num_cells, num_vertices, m->host);
+            const uint64_t F = m->host.num_faces;
+            std::vector<uint4> faces(F);
+            for (uint64_t f = 0; f < F; ++f)
+                faces[f] = make_uint4(m->host.tri[3 * f], m->host.tri[3 * f + 1], m->host.tri[3 * f + 2],
+                                      m->host.face_boundary[f]);
+            DTV_CK(cudaMalloc(&m->d_faces, sizeof(uint4) * (F ? F : 1)));
+            DTV_CK(cudaMalloc(&m->d_vertex_boundary, sizeof(uint32_t) * (num_vertices ? num_vertices : 1)));
+            DTV_CK(cudaMalloc(&m->d_face_to_tet, sizeof(uint32_t) * (2 * F ? 2 * F : 1)));
+            DTV_CK(cudaMalloc(&m->d_cells, sizeof(uint32_t) * (4 * num_cells ? 4 * num_cells : 1)));
+            if (F) {
+                DTV_CK(cudaMemcpy(m->d_faces, faces.data(), sizeof(uint4) * F, cudaMemcpyHostToDevice));
+                DTV_CK(cudaMemcpy(m->d_face_to_tet, m->host.face_to_tet.data(), sizeof(uint32_t) * 2 * F,
+                                  cudaMemcpyHostToDevice));
+            }
+            if (num_vertices)
+                DTV_CK(cudaMemcpy(m->d_vertex_boundary, m->host.vertex_boundary.data(),
+                                  sizeof(uint32_t) * num_vertices, cudaMemcpyHostToDevice));
+            if (num_cells)
+                DTV_CK(cudaMemcpy(m->d_cells, h_cells, sizeof(uint32_t) * 4 * num_cells, cudaMemcpyHostToDevice));
+        } catch (...) {
+            dtv_mesh_destroy(m);
+            throw;
+        }
+        *out = m;
+    });
+}
+
+int32_t dtv_mesh_destroy(dtv_mesh* m) {
+    if (!m) return DTV_OK;
+    cudaFree(m->d_faces);
+    cudaFree(m->d_vertex_boundary);
+    cudaFree(m->d_face_to_tet);
+    cudaFree(m->d_cells);
+    delete m;
+    return DTV_OK;
+}
+
+int32_t dtv_mesh_get_info(const dtv_mesh* m, uint64_t* nc, uint64_t* nv, uint64_t* nfaces) {
+    return guarded([&] {
+        require(m != nullptr, "mesh is null");
+        if (nc) *nc = m->host.num_cells;
+        if (nv) *nv = m->host.num_vertices;
+        if (nfaces) *nfaces = m->host.num_faces;
+    });
+}
+
+int32_t dtv_mesh_copy_faces(const dtv_mesh* m, uint32_t* tri, uint32_t* fb, uint32_t* f2t, uint32_t* vb) {
+    return guarded([&] {
+        require(m != nullptr, "mesh is null");
+        const auto& h = m->host;
+        if (tri) std::memcpy(tri, h.tri.data(), sizeof(uint32_t) * h.tri.size());
+        if (fb) std::memcpy(fb, h.face_boundary.data(), sizeof(uint32_t) * h.face_boundary.size());
+        if (f2t) std::memcpy(f2t, h.face_to_tet.data(), sizeof(uint32_t) * h.face_to_tet.size());
+        if (vb) std::memcpy(vb, h.vertex_boundary.data(), sizeof(uint32_t) * h.vertex_boundary.size());
+    });
+}
+
+int32_t dtv_mesh_vertex_boundary_device(const dtv_mesh* m, const uint32_t** d_vb) {
+    return guarded([&] {
+        require(m != nullptr && d_vb != nullptr, "null pointer");
+        *d_vb = m->d_vertex_boundary;
+    });
+}
+
+int32_t dtv_renderer_create(int32_t type, dtv_renderer** out) {
+    return guarded([&] {
+        require(out != nullptr, "out is null");
+        require(type == DTV_RENDERER_PPLL,
+                "renderer type not provided by this library (PPLL = 0 is available)");
+        *out = nullptr;
+        auto* r = new dtv_renderer();
+        r->type = type;
+        try {
+            DTV_CK(cudaMallocHost(&r->h_nf, sizeof(u64)));
+            DTV_CK(cudaMallocHost(&r->h_flags, 2 * sizeof(uint32_t)));
+            DTV_CK(cudaEventCreateWithFlags(&r->flags_event, cudaEventDisableTiming));
+            for (auto& e : r->ev) DTV_CK(cudaEventCreate(&e));
+        } catch (...) {
+            dtv_renderer_destroy(r);
+            throw;
+        }
+        *out = r;
+    });
+}
+
+int32_t dtv_renderer_destroy(dtv_renderer* r) {
+    if (!r) return DTV_OK;
+    cudaDeviceSynchronize();
+    r->vproj.release();
+    r->vfix.release();
+    r->counts.release();
+    r->offsets.release();
+    r->records.release();
+    r->scan_scratch.release();
+    r->tfinal.release();
+    r->term.release();
+    r->long_list.release();
+    r->flags.release();
+    if (r->h_nf) cudaFreeHost(r->h_nf);
+    if (r->h_flags) cudaFreeHost(r->h_flags);
+    if (r->flags_event) cudaEventDestroy(r->flags_event);
+    for (auto& e : r->ev)
+        if (e) cudaEventDestroy(e);
+    delete r;
+    return DTV_OK;
+}
+
+int32_t dtv_renderer_render(dtv_renderer* r, const dtv_mesh* mesh, const float* d_positions, const float* d_colors,
+                            const dtv_camera* camera, const dtv_render_params* params, float* d_image,
+                            dtv_stream stream) {
+    return guarded([&] {
+        require(r && mesh && camera && params, "null handle or struct");
+        require(d_positions && d_colors && d_image, "null device pointer");
+        require((reinterpret_cast<uintptr_t>(d_colors) & 15u) == 0, "colors must be 16-byte aligned");
+        require((reinterpret_cast<uintptr_t>(d_image) & 15u) == 0, "image must be 16-byte aligned");
+        require(camera->width > 0 && camera->height > 0 && camera->width <= 16384 && camera->height <= 16384,
+                "viewport size must be in [1, 16384]");
+        require(camera->znear > 0.f && camera->zfar > camera->znear, "need 0 < znear < zfar");
+        require(camera->fovy > 0.f && camera->fovy < 3.14159f, "fovy must be in (0, pi)");
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        check_pending_flags(r);
+        r->have_render = false;
+        const uint64_t V = mesh->host.num_vertices, F = mesh->host.num_faces;
+        const int W = camera->width, H = camera->height;
+        const uint64_t P = uint64_t(W) * H;
+        dtv::CamDev cam = make_cam(*camera);
+        dtv::ShadeDev sh = make_shade(*params);
+
+        r->vproj.ensure(V ? V : 1, s);
+        r->vfix.ensure(V ? V : 1, s);
+        r->counts.ensure(P, s, /*zero_new=*/true);
+        r->offsets.ensure(P + 1, s);
+        r->scan_scratch.ensure(dtv::scan_scratch_elems(P), s);
+        r->tfinal.ensure(P, s);
+        r->term.ensure(P, s);
+        r->long_list.ensure(P, s);
+        r->flags.ensure(2, s);
+
+        rec_event(r, 0, s);
+        dtv::launch_project(d_positions, uint32_t(V), cam, r->vproj.ptr, r->vfix.ptr, s);
+        check_launch("project");
+        rec_event(r, 1, s);
+        dtv::launch_raster_count(mesh->d_faces, uint32_t(F), r->vproj.ptr, r->vfix.ptr, W, H, r->counts.ptr, s);
+        check_launch("raster count");
+        rec_event(r, 2, s);
+        dtv::launch_scan(r->counts.ptr, P, r->offsets.ptr, r->scan_scratch.ptr, s);
+        check_launch("scan");
+        DTV_CK(cudaMemcpyAsync(r->h_nf, r->offsets.ptr + P, sizeof(u64), cudaMemcpyDeviceToHost, s));
+        DTV_CK(cudaStreamSynchronize(s));
+        const uint64_t nf = *r->h_nf;
+        if (params->fragment_budget_bytes && nf * sizeof(u64) > params->fragment_budget_bytes) {
+            // Leave counts zeroed for the next render.
+            DTV_CK(cudaMemsetAsync(r->counts.ptr, 0, P * sizeof(uint32_t), s));
+            throw DtvError(DTV_ERR_BUDGET, "render needs " + std::to_string(nf) + " fragments (" +
+                                               std::to_string(nf * sizeof(u64)) + " bytes), over the budget of " +
+                                               std::to_string(params->fragment_budget_bytes) + " bytes");
+        }
+        try {
+            r->records.ensure(nf ? nf : 1, s, false, 1.25);
+        } catch (...) {
+            cudaMemsetAsync(r->counts.ptr, 0, P * sizeof(uint32_t), s);
+            throw;
+        }
+        rec_event(r, 3, s);
+        dtv::launch_raster_fill(mesh->d_faces, uint32_t(F), r->vproj.ptr, r->vfix.ptr, W, H, r->counts.ptr,
+                                r->offsets.ptr, r->records.ptr, s);
+        check_launch("raster fill");
+        rec_event(r, 4, s);
+        DTV_CK(cudaMemsetAsync(r->flags.ptr, 0, 2 * sizeof(uint32_t), s));
+        dtv::launch_sort(r->offsets.ptr, r->records.ptr, uint32_t(P), r->long_list.ptr, r->flags.ptr, s);
+        check_launch("sort");
+        dtv::launch_sort_long(r->offsets.ptr, r->records.ptr, r->long_list.ptr, 0, r->flags.ptr, s);
+        check_launch("sort long lists");
+        DTV_CK(cudaMemcpyAsync(r->h_flags, r->flags.ptr, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        DTV_CK(cudaEventRecord(r->flags_event, s));
+        r->flags_pending = true;
+        rec_event(r, 5, s);
+        dtv::launch_composite(r->offsets.ptr, r->records.ptr, mesh->d_faces, r->vproj.ptr,
+                              reinterpret_cast<const float4*>(d_colors), W, H, sh,
+                              reinterpret_cast<float4*>(d_image), r->tfinal.ptr, r->term.ptr, s);
+        check_launch("composite");
+        rec_event(r, 6, s);
+        r->adjoint_timed = false;
+        r->have_render = true;
+        r->mesh = mesh;
+        r->cam = cam;
+        r->sh = sh;
+        r->P = P;
+        r->V = V;
+        r->nf = nf;
+    });
+}
+
+int32_t dtv_renderer_render_adjoint(dtv_renderer* r, const dtv_mesh* mesh, const float* d_positions,
+                                    const float* d_colors, const float* d_image_adjoint, int32_t use_abs_grad,
+                                    float* d_grad_positions, float* d_grad_colors, dtv_stream stream) {
+    return guarded([&] {
+        require(r && mesh, "null handle");
+        require(d_positions && d_colors && d_image_adjoint && d_grad_positions && d_grad_colors,
+                "null device pointer");
+        require((reinterpret_cast<uintptr_t>(d_colors) & 15u) == 0, "colors must be 16-byte aligned");
+        require((reinterpret_cast<uintptr_t>(d_grad_colors) & 15u) == 0, "grad colors must be 16-byte aligned");
+        require((reinterpret_cast<uintptr_t>(d_image_adjoint) & 15u) == 0,
+                "image adjoint must be 16-byte aligned");
+        if (!r->have_render) throw DtvError(DTV_ERR_STATE, "render_adjoint called before render");
+        if (r->mesh != mesh) throw DtvError(DTV_ERR_STATE, "render_adjoint called with a different mesh");
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        check_pending_flags(r);
+        dtv::ShadeDev sh = r->sh;
+        sh.use_abs_grad = use_abs_grad ? 1 : 0;
+        rec_event(r, 7, s);
+        dtv::launch_adjoint(r->offsets.ptr, r->records.ptr, mesh->d_faces, r->vproj.ptr,
+                            reinterpret_cast<const float4*>(d_colors), r->cam, sh,
+                            reinterpret_cast<const float4*>(d_image_adjoint), r->tfinal.ptr, r->term.ptr,
+                            d_grad_positions, reinterpret_cast<float4*>(d_grad_colors), s);
+        check_launch("adjoint");
+        rec_event(r, 8, s);
+        r->adjoint_timed = true;
+    });
+}
+
+int32_t dtv_renderer_get_num_fragments(const dtv_renderer* r, uint64_t* nf) {
+    return guarded([&] {
+        require(r && nf, "null pointer");
+        *nf = r->have_render ? r->nf : 0;
+    });
+}
+
+int32_t dtv_renderer_copy_fragments(const dtv_renderer* r, uint64_t* h_offsets, uint64_t* h_records,
+                                    uint64_t cap, dtv_stream stream) {
+    return guarded([&] {
+        require(r != nullptr, "renderer is null");
+        if (!r->have_render) throw DtvError(DTV_ERR_STATE, "no render to copy from");
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        if (h_offsets)
+            DTV_CK(cudaMemcpyAsync(h_offsets, r->offsets.ptr, sizeof(u64) * (r->P + 1), cudaMemcpyDeviceToHost, s));
+        if (h_records) {
+            require(cap >= r->nf, "records capacity too small");
+            if (r->nf)
+                DTV_CK(cudaMemcpyAsync(h_records, r->records.ptr, sizeof(u64) * r->nf, cudaMemcpyDeviceToHost, s));
+        }
+        DTV_CK(cudaStreamSynchronize(s));
+    });
+}
+
+int32_t dtv_renderer_copy_pixel_state(const dtv_renderer* r, float* h_t, uint32_t* h_term, dtv_stream stream) {
+    return guarded([&] {
+        require(r != nullptr, "renderer is null");
+        if (!r->have_render) throw DtvError(DTV_ERR_STATE, "no render to copy from");
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        if (h_t) DTV_CK(cudaMemcpyAsync(h_t, r->tfinal.ptr, sizeof(float) * r->P, cudaMemcpyDeviceToHost, s));
+        if (h_term)
+            DTV_CK(cudaMemcpyAsync(h_term, r->term.ptr, sizeof(uint32_t) * r->P, cudaMemcpyDeviceToHost, s));
+        DTV_CK(cudaStreamSynchronize(s));
+    });
+}
+
+int32_t dtv_renderer_set_timing(dtv_renderer* r, int32_t enable) {
+    return guarded([&] {
+        require(r != nullptr, "renderer is null");
+        r->timing = enable != 0;
+    });
+}
+
+int32_t dtv_renderer_stage_times(const dtv_renderer* r, float* h_ms, int32_t n) {
+    return guarded([&] {
+        require(r && h_ms, "null pointer");
+        if (!r->timing || !r->have_render) throw DtvError(DTV_ERR_STATE, "timing not enabled or no render");
+        const int stages = r->adjoint_timed ? 7 : 6;
+        for (int i = 0; i < n && i < kNumStages; ++i) {
+            h_ms[i] = 0.f;
+            if (i < stages) {
+                const int a = i < 6 ? i : 7;
+                DTV_CK(cudaEventSynchronize(r->ev[a + 1]));
+                DTV_CK(cudaEventElapsedTime(&h_ms[i], r->ev[a], r->ev[a + 1]));
+            }
+        }
+    });
+}
+
+int32_t dtv_loss_l2(const float* d_image, const float* d_target, uint64_t n, float scale, float* d_adjoint,
+                    float* d_loss, dtv_stream stream) {
+    return guarded([&] {
+        require(d_image && d_target, "null device pointer");
+        dtv::launch_loss_l2(d_image, d_target, n, scale, d_adjoint, d_loss, static_cast<cudaStream_t>(stream));
+        check_launch("loss");
+    });
+}
+
+int32_t dtv_adam_step(float* d_param, const float* d_grad, float* d_m, float* d_v, uint64_t n, float lr,
+                      float beta1, float beta2, float eps, int32_t step, int32_t clamp_mode,
+                      const uint32_t* d_fixed_mask, int32_t fixed_mode, int32_t stride, dtv_stream stream) {
+    return guarded([&] {
+        require(d_param && d_grad && d_m && d_v, "null device pointer");
+        require(step >= 1, "step must be >= 1");
+        require(clamp_mode >= 0 && clamp_mode <= 2, "clamp_mode must be 0, 1 or 2");
+        require(fixed_mode >= 0 && fixed_mode <= 2, "fixed_mode must be 0, 1 or 2");
+        require(stride >= 1, "stride must be >= 1");
+        require(clamp_mode != 2 || stride == 4 || n % 4 == 0, "clamp_mode 2 needs RGBA groups");
+        const double bc1 = 1.0 - std::pow(double(beta1), double(step));
+        const double bc2 = 1.0 - std::pow(double(beta2), double(step));
+        dtv::launch_adam(d_param, d_grad, d_m, d_v, n, lr, beta1, beta2, eps, float(bc1), float(bc2), clamp_mode,
+                         d_fixed_mask, fixed_mode, stride, static_cast<cudaStream_t>(stream));
+        check_launch("adam");
+    });
+}
+
+}  // extern "C"

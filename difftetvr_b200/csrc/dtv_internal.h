@@ -1,0 +1,60 @@
+// Internal host-side declarations shared by the C-ABI layer and the kernel
+// launch wrappers.  Not part of the public interface (include/difftetvr_b200.h).
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+#include <cuda_runtime.h>
+#include "dtv_types.h"
+
+namespace dtv {
+
+// Face record on the device: three vertex indices (winding of the lowest
+// faceId copy, TetMesh.cpp:1249-1252) and the boundary bit in .w.
+struct MeshHost {
+    uint64_t num_cells = 0, num_vertices = 0, num_faces = 0;
+    std::vector<uint32_t> tri;            // 3F
+    std::vector<uint32_t> face_boundary;  // F
+    std::vector<uint32_t> face_to_tet;    // 2F
+    std::vector<uint32_t> vertex_boundary;// V
+    std::vector<uint32_t> cells;          // 4T
+};
+
+// Builds faces from cells (restates buildFacesSlim, TetMesh.cpp:1218-1268).
+void build_faces(const uint32_t* cells, uint64_t T, uint64_t V, MeshHost& out);
+
+// Launch wrappers (dtv_kernels.cu).  All run on `s`.
+void launch_project(const float* pos, uint32_t V, const CamDev& cam, float4* vproj, int2* vfix, cudaStream_t s);
+void launch_raster_count(const uint4* faces, uint32_t F, const float4* vproj, const int2* vfix, int W, int H,
+                         uint32_t* counts, cudaStream_t s);
+void launch_raster_fill(const uint4* faces, uint32_t F, const float4* vproj, const int2* vfix, int W, int H,
+                        uint32_t* counts, const unsigned long long* offsets, unsigned long long* records,
+                        cudaStream_t s);
+// Exclusive scan of counts[n] into offsets[n+1]; scratch must hold scan_scratch_elems(n) u64.
+size_t scan_scratch_elems(uint64_t n);
+void launch_scan(const uint32_t* counts, uint64_t n, unsigned long long* offsets, unsigned long long* scratch,
+                 cudaStream_t s);
+// Per-pixel sort.  long_list holds up to P entries; flags[0] = number of long lists,
+// flags[1] = error (list longer than the block sort capacity).
+void launch_sort(const unsigned long long* offsets, unsigned long long* records, uint32_t P, uint32_t* long_list,
+                 uint32_t* flags, cudaStream_t s);
+void launch_sort_long(const unsigned long long* offsets, unsigned long long* records, const uint32_t* long_list,
+                      uint32_t num_long, uint32_t* flags, cudaStream_t s);
+constexpr uint32_t kSortWarpCap = 1024;    // elements per warp list sorted in shared memory
+constexpr uint32_t kSortBlockCap = 16384;  // elements per block-sorted list (128 KiB shared memory)
+
+void launch_composite(const unsigned long long* offsets, const unsigned long long* records, const uint4* faces,
+                      const float4* vproj, const float4* colors, int W, int H, const ShadeDev& sh, float4* image,
+                      float* tfinal, uint32_t* term, cudaStream_t s);
+void launch_adjoint(const unsigned long long* offsets, const unsigned long long* records, const uint4* faces,
+                    const float4* vproj, const float4* colors, const CamDev& cam, const ShadeDev& sh,
+                    const float4* dimage, const float* tfinal, const uint32_t* term, float* grad_pos,
+                    float4* grad_col, cudaStream_t s);
+
+void launch_loss_l2(const float* image, const float* target, uint64_t n, float scale, float* adjoint,
+                    float* loss_accum, cudaStream_t s);
+void launch_adam(float* param, const float* grad, float* m, float* v, uint64_t n, float lr, float beta1,
+                 float beta2, float eps, float bc1, float bc2, int clamp_mode, const uint32_t* fixed_mask,
+                 int fixed_mode, int stride, cudaStream_t s);
+
+}  // namespace dtv

@@ -1,0 +1,230 @@
+"""Renderer: the renderer object of the `difftetvr` module
+(TetMeshVolumeRenderer, src/Renderer/TetMeshVolumeRenderer.hpp:84-280, bound in
+src/Module/Module.cpp:838-981), backed by the CUDA library through the C ABI.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+
+import numpy as np
+import torch
+
+from . import _lib
+from .tet_mesh import TetMesh
+from .types import RendererType, vec4
+
+
+def default_view_matrix() -> list[float]:
+    """Camera at (0, 0, 0.8) with identity orientation (Module.cpp:458-463), column-major."""
+    m = np.eye(4, dtype=np.float64)
+    m[2, 3] = -0.8
+    return [float(m[j, i]) for i in range(4) for j in range(4)]
+
+
+class Renderer:
+    STAGES = ("project", "count", "scan", "fill", "sort", "composite", "adjoint")
+
+    def __init__(self, renderer_type: RendererType = RendererType.PPLL):
+        renderer_type = RendererType(renderer_type)
+        if renderer_type != RendererType.PPLL:
+            raise RuntimeError(f"RendererType.{renderer_type.name} is not provided by difftetvr_b200")
+        self._type = renderer_type
+        h = ctypes.c_void_p()
+        _lib.call("dtv_renderer_create", int(renderer_type), ctypes.byref(h))
+        self._handle = h
+        self._owner = True
+        self._tet_mesh: TetMesh | None = None
+        # Defaults of the reference (TetMeshVolumeRenderer.hpp:237-244, Module.cpp:458-463).
+        self._attenuation = 100.0
+        self._use_ert = True
+        self._ert_thresh = 1e-4
+        self._clear = (0.0, 0.0, 0.0, 0.0)
+        self._width, self._height = 1, 1
+        self._fovy = math.atan(1.0 / 2.0) * 2.0
+        self._znear, self._zfar = 0.01, 100.0
+        self._view = default_view_matrix()
+        self._fragment_budget = 0
+        self._coarse_to_fine_target = 0
+        self._export_lists = False
+        self._last_image: torch.Tensor | None = None
+
+    def __del__(self):
+        h = getattr(self, "_handle", None)
+        if h is not None and getattr(self, "_owner", False) and h.value and _lib._lib is not None:
+            _lib.load().dtv_renderer_destroy(h)
+            self._handle = None
+
+    # -- settings (Module.cpp:862-911) -----------------------------------
+    def get_renderer_type(self) -> RendererType:
+        return self._type
+
+    def set_tet_mesh(self, tet_mesh: TetMesh) -> None:
+        self._tet_mesh = tet_mesh
+
+    def get_tet_mesh(self) -> TetMesh:
+        return self._tet_mesh
+
+    def get_attenuation(self) -> float:
+        return self._attenuation
+
+    def set_attenuation(self, attenuation_coefficient: float) -> None:
+        self._attenuation = float(attenuation_coefficient)
+
+    def set_coarse_to_fine_target_num_tets(self, target_num_tets: int) -> None:
+        self._coarse_to_fine_target = int(target_num_tets)
+
+    def set_use_early_ray_termination(self, use_early_ray_termination: bool) -> None:
+        self._use_ert = bool(use_early_ray_termination)
+
+    def set_early_ray_out_thresh(self, threshold: float) -> None:
+        self._ert_thresh = float(threshold)
+
+    def set_early_ray_out_alpha(self, alpha: float) -> None:
+        self._ert_thresh = 1.0 - float(alpha)
+
+    def set_clear_color(self, color: vec4) -> None:
+        self._clear = tuple(float(c) for c in color)
+
+    def set_viewport_size(self, image_width: int, image_height: int, recreate_swapchain: bool = True) -> None:
+        self._width, self._height = int(image_width), int(image_height)
+
+    def get_viewport_size(self) -> tuple[int, int]:
+        return self._width, self._height
+
+    def reuse_intermediate_buffers_from(self, renderer_other: "Renderer") -> None:
+        """Share the other renderer's fragment storage (Module.cpp:888-899)."""
+        if self._owner and self._handle is not None and self._handle.value:
+            _lib.load().dtv_renderer_destroy(self._handle)
+        self._handle = renderer_other._handle
+        self._owner = False
+        self._keepalive = renderer_other
+
+    def set_camera_fovy(self, fovy: float) -> None:
+        self._fovy = float(fovy)
+
+    def set_camera_clip(self, znear: float, zfar: float) -> None:
+        self._znear, self._zfar = float(znear), float(zfar)
+
+    def set_view_matrix(self, view_matrix_array) -> None:
+        """16 floats, column-major (Module.cpp:904-911)."""
+        arr = [float(v) for v in np.asarray(view_matrix_array, dtype=np.float64).reshape(-1)]
+        if len(arr) != 16:
+            raise RuntimeError("Error in set_view_matrix: expected 16 values.")
+        self._view = arr
+
+    def set_fragment_budget_bytes(self, budget: int) -> None:
+        """Bound on stored fragment records; renders beyond it raise DTV_ERR_BUDGET."""
+        self._fragment_budget = int(budget)
+
+    # -- render / adjoint (Module.cpp:912-959) ----------------------------
+    def _camera(self) -> _lib.Camera:
+        cam = _lib.Camera()
+        cam.view[:] = self._view
+        cam.fovy = self._fovy
+        cam.znear = self._znear
+        cam.zfar = self._zfar
+        cam.width = self._width
+        cam.height = self._height
+        return cam
+
+    def _params(self, use_abs_grad: bool = False) -> _lib.RenderParams:
+        p = _lib.RenderParams()
+        p.attenuation = self._attenuation
+        # Early ray termination only when gradients are on, as in the reference
+        # (USE_TERMINATION_INDEX, TetMeshVolumeRenderer.cpp:417-419).
+        mesh = self._tet_mesh
+        p.use_early_ray_termination = int(self._use_ert and mesh is not None and mesh._use_gradients)
+        p.early_ray_out_thresh = self._ert_thresh
+        p.clear_color[:] = self._clear
+        p.use_abs_grad = int(use_abs_grad)
+        p.fragment_budget_bytes = self._fragment_budget
+        return p
+
+    def render(self) -> torch.Tensor:
+        mesh = self._tet_mesh
+        if mesh is None or mesh.get_is_empty():
+            raise RuntimeError("Missing valid tet mesh in Renderer.render.")
+        pos = mesh.get_vertex_positions().detach()
+        col = mesh.get_vertex_colors().detach()
+        image = torch.empty((self._height, self._width, 4), dtype=torch.float32, device=pos.device)
+        stream = torch.cuda.current_stream(pos.device).cuda_stream
+        cam, prm = self._camera(), self._params()
+        _lib.call("dtv_renderer_render", self._handle, mesh.native.handle, pos.data_ptr(), col.data_ptr(),
+                  ctypes.byref(cam), ctypes.byref(prm), image.data_ptr(), stream)
+        self._last_image = image
+        return image
+
+    def render_adjoint(self, image_adjoint: torch.Tensor, use_abs_grad: bool = False) -> None:
+        mesh = self._tet_mesh
+        if mesh is None or mesh.get_is_empty():
+            raise RuntimeError("Missing valid tet mesh in Renderer.render_adjoint.")
+        pos = mesh.get_vertex_positions()
+        col = mesh.get_vertex_colors()
+        if not torch.is_tensor(image_adjoint) or image_adjoint.device != pos.device:
+            raise RuntimeError(
+                "Error in render_adjoint: The tensors must be on the device used at initialization time.")
+        if image_adjoint.dim() != 3:
+            raise RuntimeError("Error in render_adjoint: imageAdjointTensor.sizes().size() != 3.")
+        if image_adjoint.shape[2] != 4:
+            raise RuntimeError("Error in render_adjoint: The number of image channels is not equal to 4.")
+        if image_adjoint.dtype != torch.float32:
+            raise RuntimeError("Error in render_adjoint: The only data type currently supported is 32-bit float.")
+        if tuple(image_adjoint.shape[:2]) != (self._height, self._width):
+            raise RuntimeError("Error in render_adjoint: image size does not match the viewport.")
+        image_adjoint = image_adjoint.contiguous()
+        if pos.grad is None:
+            pos.grad = torch.zeros_like(pos)
+        if col.grad is None:
+            col.grad = torch.zeros_like(col)
+        stream = torch.cuda.current_stream(pos.device).cuda_stream
+        _lib.call("dtv_renderer_render_adjoint", self._handle, mesh.native.handle, pos.detach().data_ptr(),
+                  col.detach().data_ptr(), image_adjoint.data_ptr(), int(bool(use_abs_grad)),
+                  pos.grad.data_ptr(), col.grad.data_ptr(), stream)
+
+    # -- fragment list export (Module.cpp:960-981) -------------------------
+    def set_export_linked_list_data(self) -> None:
+        self._export_lists = True
+
+    def get_num_fragments(self) -> int:
+        n = ctypes.c_uint64()
+        _lib.call("dtv_renderer_get_num_fragments", self._handle, ctypes.byref(n))
+        return int(n.value)
+
+    def get_fragment_lists(self) -> tuple[np.ndarray, np.ndarray]:
+        """(offsets u64[H*W+1], records u64[Nf]) of the last render, sorted per pixel."""
+        nf = self.get_num_fragments()
+        offsets = np.empty(self._width * self._height + 1, dtype=np.uint64)
+        records = np.empty(max(nf, 1), dtype=np.uint64)
+        stream = torch.cuda.current_stream().cuda_stream
+        _lib.call("dtv_renderer_copy_fragments", self._handle, offsets.ctypes.data, records.ctypes.data,
+                  records.shape[0], stream)
+        return offsets, records[:nf]
+
+    def get_fragment_buffer(self) -> torch.Tensor:
+        """Sorted fragment records as int64 [Nf]:
+        (fp32 view-depth bits << 32) | (faceIndex << 2) | (boundary << 1) | frontFacing."""
+        _, rec = self.get_fragment_lists()
+        return torch.from_numpy(rec.view(np.int64).copy())
+
+    def get_start_offset_buffer(self) -> torch.Tensor:
+        """Per-pixel list offsets as int64 [H*W+1] (pixel p owns records [o[p], o[p+1]))."""
+        off, _ = self.get_fragment_lists()
+        return torch.from_numpy(off.view(np.int64).copy())
+
+    def get_pixel_state(self) -> tuple[np.ndarray, np.ndarray]:
+        """(final transmittance f32[H,W], termination index u32[H,W]) of the last render."""
+        t = np.empty(self._width * self._height, dtype=np.float32)
+        term = np.empty(self._width * self._height, dtype=np.uint32)
+        _lib.call("dtv_renderer_copy_pixel_state", self._handle, t.ctypes.data, term.ctypes.data,
+                  torch.cuda.current_stream().cuda_stream)
+        return t.reshape(self._height, self._width), term.reshape(self._height, self._width)
+
+    # -- tracing -----------------------------------------------------------
+    def set_stage_timing(self, enable: bool = True) -> None:
+        _lib.call("dtv_renderer_set_timing", self._handle, int(bool(enable)))
+
+    def get_stage_times(self) -> dict[str, float]:
+        ms = (ctypes.c_float * len(self.STAGES))()
+        _lib.call("dtv_renderer_stage_times", self._handle, ms, len(self.STAGES))
+        return {k: float(v) for k, v in zip(self.STAGES, ms)}

@@ -1,0 +1,254 @@
+"""TetMesh: the mesh object of the `difftetvr` module (src/Tet/TetMesh.hpp:89-286,
+bound in src/Module/Module.cpp:775-837), holding cells, per-vertex positions
+and RGBA as CUDA tensors and the face topology on the device.
+
+As in the reference, ``get_vertex_positions()`` / ``get_vertex_colors()``
+return the same leaf tensors every call, with ``.grad`` attached; the renderer
+adds gradients into those ``.grad`` buffers in place (TetMesh.cpp:236-308), so
+``torch.optim`` updates the tensors the renderer reads.  Gradient buffers start
+at zero (the reference fills them with a copy of the values,
+TetMesh.cpp:661-675; callers zero them before use either way).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+from .types import AABB3, ColorStorage, TestCase, vec3, vec4
+
+# HEX_TO_TET_TABLE, src/Tet/TetMesh.cpp:104-117 (Kuhn split around diagonal 0-6).
+HEX_TO_TET_TABLE = np.array([[0, 4, 7, 6], [0, 4, 6, 5], [0, 3, 6, 7], [0, 3, 2, 6], [0, 1, 5, 6], [0, 1, 6, 2]],
+                            dtype=np.int64)
+
+
+def convert_hex_to_tet_indices(hex_indices: np.ndarray) -> np.ndarray:
+    """convertHexToTetIndices (TetMesh.cpp:119-132): 8 vertex ids per hex -> 6 tets."""
+    hexes = np.asarray(hex_indices, dtype=np.uint32).reshape(-1, 8)
+    return hexes[:, HEX_TO_TET_TABLE].reshape(-1, 4).astype(np.uint32)
+
+
+def build_hex_mesh(aabb_min, aabb_max, xs: int, ys: int, zs: int):
+    """Vertex grid and Kuhn tets of TetMesh::setHexMeshConst (C ABI dtv_build_hex_mesh).
+
+    Returns (cells u32[T,4], positions f32[V,3]) on the host."""
+    nv = xs * ys * zs
+    nt = 6 * (xs - 1) * (ys - 1) * (zs - 1)
+    cells = np.empty((nt, 4), dtype=np.uint32)
+    pos = np.empty((nv, 3), dtype=np.float32)
+    mn = (ctypes.c_float * 3)(*aabb_min)
+    mx = (ctypes.c_float * 3)(*aabb_max)
+    _lib.call("dtv_build_hex_mesh", mn, mx, xs, ys, zs, cells.ctypes.data, pos.ctypes.data)
+    return cells, pos
+
+
+def build_faces_host(cells: np.ndarray, num_vertices: int):
+    """Unique faces (C ABI dtv_mesh_build_faces_host; buildFacesSlim, TetMesh.cpp:1218-1268).
+
+    Returns (tri u32[F,3], face_boundary u32[F], face_to_tet u32[F,2], vertex_boundary u32[V])."""
+    cells = np.ascontiguousarray(cells, dtype=np.uint32).reshape(-1, 4)
+    T = cells.shape[0]
+    tri = np.empty((4 * T, 3), dtype=np.uint32)
+    fb = np.empty(4 * T, dtype=np.uint32)
+    f2t = np.empty((4 * T, 2), dtype=np.uint32)
+    vb = np.empty(num_vertices, dtype=np.uint32)
+    nf = ctypes.c_uint64(0)
+    _lib.call("dtv_mesh_build_faces_host", cells.ctypes.data, T, num_vertices, tri.ctypes.data, fb.ctypes.data,
+              f2t.ctypes.data, vb.ctypes.data, ctypes.byref(nf))
+    F = nf.value
+    return tri[:F].copy(), fb[:F].copy(), f2t[:F].copy(), vb
+
+
+class NativeMesh:
+    """Owner of a dtv_mesh handle (device face topology)."""
+
+    def __init__(self, cells: np.ndarray, num_vertices: int):
+        cells = np.ascontiguousarray(cells, dtype=np.uint32).reshape(-1, 4)
+        h = ctypes.c_void_p()
+        _lib.call("dtv_mesh_create", cells.ctypes.data, cells.shape[0], num_vertices, ctypes.byref(h))
+        self.handle = h
+        nc, nv, nf = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+        _lib.call("dtv_mesh_get_info", h, ctypes.byref(nc), ctypes.byref(nv), ctypes.byref(nf))
+        self.num_cells, self.num_vertices, self.num_faces = nc.value, nv.value, nf.value
+
+    def copy_faces(self):
+        F, V = self.num_faces, self.num_vertices
+        tri = np.empty((F, 3), dtype=np.uint32)
+        fb = np.empty(F, dtype=np.uint32)
+        f2t = np.empty((F, 2), dtype=np.uint32)
+        vb = np.empty(V, dtype=np.uint32)
+        _lib.call("dtv_mesh_copy_faces", self.handle, tri.ctypes.data, fb.ctypes.data, f2t.ctypes.data,
+                  vb.ctypes.data)
+        return tri, fb, f2t, vb
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value and _lib._lib is not None:
+            _lib.load().dtv_mesh_destroy(h)
+            self.handle = None
+
+
+def _device() -> torch.device:
+    if not torch.cuda.is_available():
+        raise RuntimeError("difftetvr_b200 runs on CUDA devices only (no CPU fallback)")
+    return torch.device("cuda", torch.cuda.current_device())
+
+
+class TetMesh:
+    """Tetrahedral mesh with per-vertex RGBA (A = extinction density)."""
+
+    def __init__(self):
+        self._cells: np.ndarray | None = None
+        self._positions: torch.Tensor | None = None
+        self._colors: torch.Tensor | None = None
+        self._cell_colors: torch.Tensor | None = None
+        self._use_gradients = False
+        self._color_storage = ColorStorage.PER_VERTEX
+        self._native: NativeMesh | None = None
+        self._vertex_boundary: torch.Tensor | None = None
+
+    # -- construction ------------------------------------------------------
+    def set_use_gradients(self, use_gradients: bool = True) -> None:
+        """TetMesh::setUseGradients (Module.cpp:785)."""
+        self._use_gradients = bool(use_gradients)
+        if self._positions is not None:
+            self._attach_grads()
+
+    def set_tet_mesh_data(self, cells, vertex_positions, vertex_colors) -> None:
+        """TetMesh::setTetMeshData(cells, positions, colors) (TetMesh.hpp:93-95)."""
+        cells = np.ascontiguousarray(np.asarray(cells, dtype=np.uint32).reshape(-1, 4))
+        pos = torch.as_tensor(np.asarray(vertex_positions, dtype=np.float32).reshape(-1, 3))
+        col = torch.as_tensor(np.asarray(vertex_colors, dtype=np.float32).reshape(-1, 4))
+        if col.shape[0] != pos.shape[0]:
+            raise RuntimeError("Error in TetMesh.set_tet_mesh_data: #colors != #vertices.")
+        if cells.size and int(cells.max()) >= pos.shape[0]:
+            raise RuntimeError("Error in TetMesh.set_tet_mesh_data: cell index out of range.")
+        dev = _device()
+        self._cells = cells
+        self._color_storage = ColorStorage.PER_VERTEX
+        self._positions = pos.to(dev).contiguous()
+        self._colors = col.to(dev).contiguous()
+        self._cell_colors = None
+        self._native = NativeMesh(cells, pos.shape[0])
+        _, _, _, vb = self._native.copy_faces()
+        self._vertex_boundary = torch.as_tensor(vb.astype(np.int32)).to(dev)
+        self._attach_grads()
+
+    def _attach_grads(self) -> None:
+        for t in (self._positions, self._colors):
+            if t is None:
+                continue
+            t.requires_grad_(self._use_gradients)
+            if self._use_gradients:
+                if t.grad is None:
+                    t.grad = torch.zeros_like(t)
+            else:
+                t.grad = None
+
+    def load_test_data(self, test_case: TestCase) -> None:
+        """TetMesh::loadTestData (TetMesh.cpp:1016-1077)."""
+        if test_case == TestCase.SINGLE_TETRAHEDRON:
+            cells = np.array([[0, 1, 2, 3]], dtype=np.uint32)
+            pos = np.array([[-0.1, -0.1, 0.1], [0.1, -0.1, 0.1], [0.0, 0.3, 0.0], [0.1, -0.1, -0.1]],
+                           dtype=np.float32)
+            col = np.array([[1.0, 1.0, 1.0, 0.1], [1.0, 1.0, 1.0, 0.1], [0.0, 1.0, 0.0, 0.1],
+                            [1.0, 1.0, 1.0, 0.8]], dtype=np.float32)
+            self.set_tet_mesh_data(cells, pos, col)
+        elif test_case == TestCase.CUBE_CENTRAL_GRADIENT:
+            cells, pos, col = cube_central_gradient_data()
+            self.set_tet_mesh_data(cells, pos, col)
+        else:
+            raise RuntimeError(f"Unknown test case {test_case}")
+
+    def set_hex_mesh_const(self, aabb: AABB3, xs: int, ys: int, zs: int, const_color: vec4,
+                           color_storage: ColorStorage = ColorStorage.PER_VERTEX) -> None:
+        """TetMesh::setHexMeshConst (TetMesh.cpp:1882-1936); xs, ys, zs are vertex counts."""
+        if color_storage != ColorStorage.PER_VERTEX:
+            raise RuntimeError("ColorStorage.PER_CELL is not provided by difftetvr_b200")
+        cells, pos = build_hex_mesh(tuple(aabb.min), tuple(aabb.max), xs, ys, zs)
+        col = np.tile(np.array(tuple(const_color), dtype=np.float32), (pos.shape[0], 1))
+        self.set_tet_mesh_data(cells, pos, col)
+
+    # -- accessors ---------------------------------------------------------
+    def get_num_cells(self) -> int:
+        return 0 if self._cells is None else int(self._cells.shape[0])
+
+    def get_num_vertices(self) -> int:
+        return 0 if self._positions is None else int(self._positions.shape[0])
+
+    def get_num_faces(self) -> int:
+        return 0 if self._native is None else int(self._native.num_faces)
+
+    def get_vertex_positions(self) -> torch.Tensor:
+        return self._positions
+
+    def get_vertex_colors(self) -> torch.Tensor:
+        return self._colors
+
+    def get_cell_colors(self) -> torch.Tensor:
+        raise RuntimeError("ColorStorage.PER_CELL is not provided by difftetvr_b200")
+
+    def get_cells(self) -> np.ndarray:
+        return self._cells
+
+    def get_vertex_boundary_bit_tensor(self) -> torch.Tensor:
+        return self._vertex_boundary
+
+    def get_color_storage(self) -> ColorStorage:
+        return self._color_storage
+
+    def get_bounding_box(self) -> AABB3:
+        p = self._positions.detach()
+        mn = p.min(dim=0).values.tolist()
+        mx = p.max(dim=0).values.tolist()
+        return AABB3(vec3(*mn), vec3(*mx))
+
+    def get_is_empty(self) -> bool:
+        return self._cells is None or self._cells.shape[0] == 0
+
+    def set_vertices_changed(self, vertices_changed: bool = True) -> None:
+        """No-op: renders read the position / colour tensors directly."""
+
+    def on_zero_grad(self) -> None:
+        """No-op on CUDA (the reference uses it for its CPU device path)."""
+
+    def check_is_any_tet_degenerate(self) -> bool:
+        """TetMesh::checkIsAnyTetDegenerate (TetMesh.cpp:544-558): valid tets have
+        dot(cross(p1-p0, p2-p0), p3-p0) < 0."""
+        p = self._positions.detach().double()
+        c = torch.as_tensor(self._cells.astype(np.int64), device=p.device)
+        p0, p1, p2, p3 = (p[c[:, k]] for k in range(4))
+        vol = torch.sum(torch.cross(p1 - p0, p2 - p0, dim=1) * (p3 - p0), dim=1)
+        return bool((vol >= 0).any().item())
+
+    @property
+    def native(self) -> NativeMesh:
+        if self._native is None:
+            raise RuntimeError("Missing valid tet mesh.")
+        return self._native
+
+
+def cube_central_gradient_data():
+    """CUBE_CENTRAL_GRADIENT fixture (createBaseCubeHex, TetMesh.cpp:969-1014, scaled
+    by 1/16 in loadTestData :1066-1076): 4 hexes, red denser central slab."""
+    width = 4.0
+    ml, mr = -width * 0.5, width * 0.5
+    pos = np.array([
+        [-4, -4, 4], [ml, -4, 4], [0, -4, 4], [mr, -4, 4], [4, -4, 4],
+        [4, -4, -4], [mr, -4, -4], [0, -4, -4], [ml, -4, -4], [-4, -4, -4],
+        [-4, 4, 4], [ml, 4, 4], [0, 4, 4], [mr, 4, 4], [4, 4, 4],
+        [4, 4, -4], [mr, 4, -4], [0, 4, -4], [ml, 4, -4], [-4, 4, -4],
+    ], dtype=np.float32) * np.float32(1.0 / 16.0)
+    alpha_scale = 0.25
+    c0 = [0.5, 0.5, 0.5, 0.0625 * alpha_scale]
+    c1 = [1.0, 0.0, 0.0, 0.125 * alpha_scale]
+    col = np.array([c0, c0, c1, c0, c0] * 4, dtype=np.float32)
+    hexes = np.array([
+        9, 8, 18, 19, 0, 1, 11, 10,
+        8, 7, 17, 18, 1, 2, 12, 11,
+        7, 6, 16, 17, 2, 3, 13, 12,
+        6, 5, 15, 16, 3, 4, 14, 13,
+    ], dtype=np.uint32)
+    return convert_hex_to_tet_indices(hexes), pos, col

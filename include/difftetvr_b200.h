@@ -1,0 +1,168 @@
+/*
+ * difftetvr_b200 — C ABI of the B200-native differentiable tetrahedral
+ * volume-rendering path.
+ *
+ * Plain pointers and sizes only.  Device pointers ("d_") are CUDA device
+ * memory on the current device; host pointers ("h_") are host memory.  Every
+ * function returns a status code (DTV_OK on success); the message of the last
+ * failure on the calling thread is returned by dtv_last_error_string().
+ *
+ * Each entry point names the reference interface it replaces (paths inside
+ * chrismile/DiffTetVR).  The Python module difftetvr_b200 binds this ABI with
+ * ctypes and mirrors the reference module `difftetvr` (src/Module/Module.cpp).
+ */
+#ifndef DIFFTETVR_B200_H
+#define DIFFTETVR_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DTV_OK 0
+#define DTV_ERR_ARG 1      /* invalid argument (bad pointer, size, alignment, enum) */
+#define DTV_ERR_BUDGET 2   /* fragment storage exceeds the configured memory budget or a list cap */
+#define DTV_ERR_CUDA 3     /* CUDA runtime error */
+#define DTV_ERR_TIMEOUT 4  /* a bounded device-side wait gave up */
+#define DTV_ERR_STATE 5    /* call out of order (e.g. adjoint before render) */
+
+/* Renderer types, numbered as RendererType in src/Renderer/TetMeshRendererType.hpp:32-37. */
+#define DTV_RENDERER_PPLL 0
+#define DTV_RENDERER_PROJECTION 1   /* not provided; dtv_renderer_create returns DTV_ERR_ARG */
+#define DTV_RENDERER_INTERSECTION 2
+
+typedef struct dtv_mesh dtv_mesh;
+typedef struct dtv_renderer dtv_renderer;
+typedef void* dtv_stream; /* cudaStream_t; NULL = legacy default stream */
+
+/* Camera: Renderer.set_view_matrix (16 floats, column-major, Module.cpp:904-911),
+ * Renderer.set_camera_fovy (radians, Module.cpp:900-903), near/far clip
+ * (Module.cpp:458-460 defaults 0.01 / 100) and the viewport size
+ * (Renderer.set_viewport_size, Module.cpp:874-887). */
+typedef struct dtv_camera {
+    float view[16];
+    float fovy;
+    float znear;
+    float zfar;
+    int32_t width;
+    int32_t height;
+} dtv_camera;
+
+/* Per-render settings: Renderer.set_attenuation (Module.cpp:866),
+ * set_use_early_ray_termination / set_early_ray_out_thresh (:868-870),
+ * set_clear_color (:871-873); use_abs_grad is render_adjoint's flag (:922).
+ * fragment_budget_bytes bounds the stored fragment records (0 = no bound). */
+typedef struct dtv_render_params {
+    float attenuation;
+    int32_t use_early_ray_termination;
+    float early_ray_out_thresh;
+    float clear_color[4];
+    int32_t use_abs_grad;
+    int32_t reserved0;
+    uint64_t fragment_budget_bytes;
+} dtv_render_params;
+
+/* Library version (major*10000 + minor*100 + patch). */
+int32_t dtv_version(void);
+
+/* Message of the last failed call on this thread ("" if none). */
+const char* dtv_last_error_string(void);
+
+/* Tetrahedralised hex grid: replaces TetMesh::setHexMeshConst
+ * (src/Tet/TetMesh.cpp:1882-1936; HEX_TO_TET_TABLE :104-117).  xs, ys, zs are
+ * vertex counts per axis (>= 2).  h_cells receives 24*(xs-1)(ys-1)(zs-1) u32,
+ * h_positions 3*xs*ys*zs floats. */
+int32_t dtv_build_hex_mesh(const float* aabb_min3, const float* aabb_max3, uint32_t xs, uint32_t ys, uint32_t zs,
+                           uint32_t* h_cells, float* h_positions);
+
+/* Topology upload: replaces TetMesh::setTetMeshData (src/Tet/TetMesh.hpp:93-95)
+ * with buildFacesSlim (TetMesh.cpp:1218-1268) and uploadDataToDevice
+ * (TetMesh.cpp:560-778) for the face arrays.  Positions and colours stay
+ * caller-owned device memory passed to each render. */
+/* Host-only face build (same arrays and face order as dtv_mesh_create, no
+ * device work): replaces buildFacesSlim (TetMesh.cpp:1218-1268).  h_tri needs
+ * room for 3*4T entries, h_face_boundary 4T, h_face_to_tet 2*4T, h_vertex_boundary V;
+ * *num_faces receives F. */
+int32_t dtv_mesh_build_faces_host(const uint32_t* h_cells, uint64_t num_cells, uint64_t num_vertices,
+                                  uint32_t* h_tri, uint32_t* h_face_boundary, uint32_t* h_face_to_tet,
+                                  uint32_t* h_vertex_boundary, uint64_t* num_faces);
+int32_t dtv_mesh_create(const uint32_t* h_cells, uint64_t num_cells, uint64_t num_vertices, dtv_mesh** out);
+int32_t dtv_mesh_destroy(dtv_mesh* mesh);
+/* TetMesh::getNumCells / getNumVertices (Module.cpp get_num_cells/get_num_vertices) and the face count. */
+int32_t dtv_mesh_get_info(const dtv_mesh* mesh, uint64_t* num_cells, uint64_t* num_vertices, uint64_t* num_faces);
+/* Host copies of the face arrays (triangleIndices u32[3F], faceBoundaryBit u32[F],
+ * faceToTetMap u32[2F], vertexBoundaryBit u32[V]); any pointer may be NULL. */
+int32_t dtv_mesh_copy_faces(const dtv_mesh* mesh, uint32_t* h_tri, uint32_t* h_face_boundary,
+                            uint32_t* h_face_to_tet, uint32_t* h_vertex_boundary);
+/* Device pointer of the per-vertex boundary bits (TetMesh::getVertexBoundaryBitTensor). */
+int32_t dtv_mesh_vertex_boundary_device(const dtv_mesh* mesh, const uint32_t** d_vertex_boundary);
+
+/* Renderer object: replaces the TetMeshVolumeRenderer subclasses
+ * (TetMeshRendererPPLL.hpp:61-178, TetMeshRendererIntersection.hpp:41-135);
+ * it owns the per-view fragment storage (the reference's fragment / start
+ * offset buffers, TetMeshRendererPPLL.cpp:518-654). */
+int32_t dtv_renderer_create(int32_t renderer_type, dtv_renderer** out);
+int32_t dtv_renderer_destroy(dtv_renderer* r);
+
+/* Forward render: replaces TetMeshRendererPPLL::render (TetMeshRendererPPLL.cpp:671-716)
+ * / TetMeshRendererIntersection::render (:603-707) plus copyOutputImageToBuffer.
+ * d_positions f32[3V], d_colors f32[4V] (16-byte aligned), d_image f32[H*W*4]
+ * premultiplied RGBA over the clear colour.  Keeps the state the adjoint needs. */
+int32_t dtv_renderer_render(dtv_renderer* r, const dtv_mesh* mesh, const float* d_positions,
+                            const float* d_colors, const dtv_camera* camera, const dtv_render_params* params,
+                            float* d_image, dtv_stream stream);
+
+/* Adjoint: replaces TetMeshRendererPPLL::renderAdjoint (TetMeshRendererPPLL.cpp:718-724)
+ * behind Renderer.render_adjoint (Module.cpp:922-959).  Gradients are ADDED to
+ * d_grad_positions f32[3V] and d_grad_colors f32[4V] (16-byte aligned), as
+ * the reference adds into the aliased .grad buffers.  Uses the camera and
+ * parameters of the last dtv_renderer_render on this renderer (same mesh,
+ * positions and colours).  use_abs_grad overrides params.use_abs_grad. */
+int32_t dtv_renderer_render_adjoint(dtv_renderer* r, const dtv_mesh* mesh, const float* d_positions,
+                                    const float* d_colors, const float* d_image_adjoint, int32_t use_abs_grad,
+                                    float* d_grad_positions, float* d_grad_colors, dtv_stream stream);
+
+/* Total fragments of the last render (exact, from the scan). */
+int32_t dtv_renderer_get_num_fragments(const dtv_renderer* r, uint64_t* num_fragments);
+
+/* Sorted fragment lists of the last render: replaces get_fragment_buffer /
+ * get_start_offset_buffer (Module.cpp:960-981) with an offsets + records
+ * layout: h_offsets u64[H*W+1], h_records u64[Nf] where
+ * record = (fp32 view-depth bits << 32) | (faceIndex << 2) | (boundary << 1) | frontFacing.
+ * Either pointer may be NULL; records_capacity is the element count of h_records. */
+int32_t dtv_renderer_copy_fragments(const dtv_renderer* r, uint64_t* h_offsets, uint64_t* h_records,
+                                    uint64_t records_capacity, dtv_stream stream);
+
+/* Per-pixel state of the last render: final transmittance f32[H*W] and the
+ * termination index u32[H*W] (terminationIndexImage, Forward.glsl:256-259). */
+int32_t dtv_renderer_copy_pixel_state(const dtv_renderer* r, float* h_transmittance, uint32_t* h_termination,
+                                      dtv_stream stream);
+
+/* Device time of each stage of the last render / adjoint, in ms:
+ * [project, count, scan, fill, sort, composite, adjoint].  Stage timing is
+ * recorded only after dtv_renderer_set_timing(r, 1). */
+int32_t dtv_renderer_set_timing(dtv_renderer* r, int32_t enable);
+int32_t dtv_renderer_stage_times(const dtv_renderer* r, float* h_ms, int32_t n);
+
+/* L2 loss: replaces Loss.glsl:242-248 / torch.nn.MSELoss (pytests/train.py:321-326).
+ * d_adjoint[i] = 2*scale*(d_image[i]-d_target[i]) (may be NULL);
+ * *d_loss += scale * sum (d_image-d_target)^2 (may be NULL). */
+int32_t dtv_loss_l2(const float* d_image, const float* d_target, uint64_t n, float scale, float* d_adjoint,
+                    float* d_loss, dtv_stream stream);
+
+/* Adam step: replaces Optimizer.glsl Compute.Adam (:88-169) and the
+ * torch.optim.Adam step of pytests/train.py:318,351.  step >= 1 is the
+ * 1-based time step.  clamp_mode: 0 none, 1 max(p,0) (train.py:352-356),
+ * 2 rgb in [0,1] / alpha >= 0 (Optimizer.glsl:161-167).  d_fixed_mask (u32
+ * per group of `stride` values, may be NULL) with fixed_mode 1 = zero the
+ * gradient (train.py:349-350), 2 = skip the update (Optimizer.glsl:141-145). */
+int32_t dtv_adam_step(float* d_param, const float* d_grad, float* d_m, float* d_v, uint64_t n, float lr,
+                      float beta1, float beta2, float eps, int32_t step, int32_t clamp_mode,
+                      const uint32_t* d_fixed_mask, int32_t fixed_mode, int32_t stride, dtv_stream stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DIFFTETVR_B200_H */

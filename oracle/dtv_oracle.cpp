@@ -1,0 +1,794 @@
+// CPU oracle for the differentiable tetrahedral volume-rendering hot path.
+//
+// TEST INFRASTRUCTURE ONLY.  Nothing in the product (difftetvr_b200/) links,
+// loads or calls this file; only tests/, __graft_entry__.smoke() and the
+// cpu_baseline / --impl reference legs of bench.py use it, always as the
+// checker or as the timed CPU baseline, never as the thing shipped.
+//
+// It is a plain C++ restatement of the reference's algorithm (GLSL shaders and
+// C++ host code of DiffTetVR), instantiated in double (the FP64 oracle) and in
+// float (the timed CPU port).  Every function cites the reference file:line it
+// follows.  Discrete decisions (which pixel a face covers, the per-pixel depth
+// order) are computed with integer / explicitly-ordered FP32 arithmetic that
+// the CUDA path reproduces bit for bit; everything continuous (depth used for
+// segment lengths, barycentrics, colours, the segment integral, the adjoint)
+// runs in the template precision R.
+//
+// Parity status: the reference cannot run here (Vulkan only), and it ships no
+// golden vectors.  This oracle is pinned by closed-form known answers
+// (single-tet optical depth, empty pixels, a->0 limit of the segment
+// integral), by FP64 central differences of its own forward, and by the mesh
+// fixtures of TetMesh::loadTestData; see tests/test_oracle_*.py.
+
+#include <cstdint>
+#include <cstring>
+#include <cmath>
+#include <vector>
+#include <algorithm>
+#include <atomic>
+#include <type_traits>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+// Face table, src/Tet/TetMesh.cpp:1175-1181 (also Data/Shaders/Common/TetFaceTable.glsl:29-34):
+// consistent outward winding for each of the four faces of a tet.
+const int kTetFace[4][4] = {
+    {0, 1, 2, 3}, {1, 0, 3, 2}, {0, 2, 3, 1}, {2, 1, 3, 0},
+};
+
+constexpr int kNumSubdivs = 4;             // Data/Shaders/Common/RayCommon.glsl:1-2
+constexpr float kGuardPx = 1048576.0f;     // |screen coord| limit (2^20 px) for the int64 edge functions
+
+struct Camera {
+    float view[16];   // column-major, as Renderer.set_view_matrix (src/Module/Module.cpp:904-911)
+    float fovy;       // radians
+    float znear, zfar;
+    int32_t width, height;
+};
+
+struct Params {
+    float attenuation;        // TetMeshVolumeRenderer::attenuationCoefficient
+    int32_t use_ert;          // USE_TERMINATION_INDEX (TetMeshVolumeRenderer.cpp:417-419)
+    float ert_thresh;         // earlyRayOutThresh = 1 - earlyRayTerminationAlpha
+    float clear_color[4];     // blended under the premultiplied result (BACK_TO_FRONT_PREMUL_ALPHA)
+    int32_t use_abs_grad;     // Backward.glsl:449-468
+    int32_t row_begin, row_end;  // pixel rows to process (bounded CPU samples); row_end<=0 means all
+};
+
+// Camera constants.  Perspective RH, depth [0,1], y flipped for a top-left
+// origin (TetMeshRendererPPLL.cpp:675-681 shows the same perspectiveRH_ZO with
+// [1][1] negated).  Screen x = cx + f * xv/ze, y = cy - f * yv/ze, ze = -zv.
+struct CamConst {
+    float V[16];
+    float f, cx, cy, znear, zfar;
+    double fd, cxd, cyd;
+    int W, H;
+};
+
+CamConst make_cam(const Camera& c) {
+    CamConst k;
+    std::memcpy(k.V, c.view, sizeof(k.V));
+    const double tanh = std::tan(0.5 * double(c.fovy));
+    k.fd = 0.5 * double(c.height) / tanh;
+    k.f = float(k.fd);
+    k.cx = 0.5f * float(c.width);
+    k.cy = 0.5f * float(c.height);
+    k.cxd = k.cx;
+    k.cyd = k.cy;
+    k.znear = c.znear;
+    k.zfar = c.zfar;
+    k.W = c.width;
+    k.H = c.height;
+    return k;
+}
+
+// FP32 projection with a fixed operation order (the CUDA path uses the same
+// sequence with __fmul_rn/__fadd_rn, so the snapped coordinates, the coverage
+// and the sort keys agree bit for bit).  LinkedListGather.glsl:55-68 projects
+// with viewProjectionMatrix; here the projection is split into view transform
+// and perspective divide.
+struct ProjF {
+    float sx, sy, iz, ze;
+    int32_t X, Y;     // 1/256-pixel fixed point
+    bool valid;
+};
+
+ProjF project_f(const CamConst& c, float x, float y, float z) {
+    ProjF p;
+    const float* V = c.V;
+    float xv = ((V[0] * x + V[4] * y) + V[8] * z) + V[12];
+    float yv = ((V[1] * x + V[5] * y) + V[9] * z) + V[13];
+    float zv = ((V[2] * x + V[6] * y) + V[10] * z) + V[14];
+    p.ze = -zv;
+    p.iz = 1.0f / p.ze;
+    p.sx = c.cx + c.f * (xv * p.iz);
+    p.sy = c.cy - c.f * (yv * p.iz);
+    p.valid = (p.ze >= c.znear) && (p.ze <= c.zfar) && std::fabs(p.sx) <= kGuardPx &&
+              std::fabs(p.sy) <= kGuardPx;
+    if (p.valid) {
+        p.X = int32_t(std::nearbyint(p.sx * 256.0f));
+        p.Y = int32_t(std::nearbyint(p.sy * 256.0f));
+    } else {
+        p.X = p.Y = 0;
+    }
+    return p;
+}
+
+template <class R>
+struct ProjR {
+    R sx, sy, iz, ze, xv, yv;
+};
+
+template <class R>
+ProjR<R> project_r(const CamConst& c, R x, R y, R z) {
+    ProjR<R> p;
+    const float* V = c.V;
+    p.xv = ((R(V[0]) * x + R(V[4]) * y) + R(V[8]) * z) + R(V[12]);
+    p.yv = ((R(V[1]) * x + R(V[5]) * y) + R(V[9]) * z) + R(V[13]);
+    R zv = ((R(V[2]) * x + R(V[6]) * y) + R(V[10]) * z) + R(V[14]);
+    p.ze = -zv;
+    p.iz = R(1) / p.ze;
+    const R f = std::is_same<R, float>::value ? R(c.f) : R(c.fd);
+    p.sx = R(c.cx) + f * (p.xv * p.iz);
+    p.sy = R(c.cy) - f * (p.yv * p.iz);
+    return p;
+}
+
+inline int64_t floor_div(int64_t a, int64_t b) {  // b > 0
+    int64_t q = a / b;
+    if ((a % b) != 0 && (a < 0)) --q;
+    return q;
+}
+inline int64_t ceil_div(int64_t a, int64_t b) { return -floor_div(-a, b); }
+
+// Top-left style tie rule: a sample exactly on an edge a->b (of a triangle
+// oriented so that the interior has E > 0) belongs to the triangle iff the
+// sample point nudged by (eps, eps^2) lies inside.  Shared edges are then
+// owned by exactly one of the two triangles, so interior faces tile the screen
+// without gaps or double hits (the rule of a hardware rasteriser, written out
+// so the CPU and the GPU agree exactly).
+inline bool edge_inside(int64_t E, int64_t dx, int64_t dy) {
+    if (E > 0) return true;
+    if (E < 0) return false;
+    return (dy < 0) || (dy == 0 && dx > 0);
+}
+
+// FP32 depth key of a fragment: perspective-correct view depth at the pixel
+// centre from the face's projected vertices.  Fixed operation order; the CUDA
+// kernel computes the same bits.  (The reference stores gl_FragCoord.z,
+// LinkedListGather.glsl:97; view depth is used here so the segment length
+// keeps full FP32 precision.)
+inline float depth_key_f(const ProjF& a, const ProjF& b, const ProjF& c, float qx, float qy) {
+    float d0x = a.sx - qx, d0y = a.sy - qy;
+    float d1x = b.sx - qx, d1y = b.sy - qy;
+    float d2x = c.sx - qx, d2y = c.sy - qy;
+    float E0 = d1x * d2y - d1y * d2x;
+    float E1 = d2x * d0y - d2y * d0x;
+    float E2 = d0x * d1y - d0y * d1x;
+    float w = ((E0 * a.iz + E1 * b.iz) + E2 * c.iz) / ((E0 + E1) + E2);
+    float z = 1.0f / w;
+    float zmin = std::fmin(std::fmin(a.ze, b.ze), c.ze);
+    float zmax = std::fmax(std::fmax(a.ze, b.ze), c.ze);
+    return std::fmin(std::fmax(z, zmin), zmax);
+}
+
+inline uint32_t f2u(float f) {
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    return u;
+}
+inline float u2f(uint32_t u) {
+    float f;
+    std::memcpy(&f, &u, 4);
+    return f;
+}
+
+struct FragLists {
+    std::vector<int64_t> offsets;   // P+1
+    std::vector<uint64_t> records;  // (depth bits << 32) | (face << 2) | (boundary << 1) | front
+};
+
+// Rasterise every face into per-pixel fragment lists and sort each list.
+// LinkedListGather.glsl:84-121 (one node per covered pixel per face, faceBits =
+// faceIndex<<2 | boundary<<1 | frontFacing) and LinkedListSort.glsl:189-216 /
+// Forward.glsl:107-114 (front-to-back order).  The order here is total: depth
+// key, then face index.  Only rows [row_begin, row_end) are emitted.
+FragLists build_fragments(const uint32_t* tri, const uint32_t* face_boundary, int64_t F,
+                          const std::vector<ProjF>& proj, const CamConst& cam, int row_begin,
+                          int row_end) {
+    const int W = cam.W, H = cam.H;
+    const int64_t P = int64_t(W) * H;
+    int nthreads = 1;
+#ifdef _OPENMP
+    nthreads = omp_get_max_threads();
+#endif
+    std::vector<std::vector<std::pair<uint32_t, uint64_t>>> per_thread(nthreads);
+#pragma omp parallel
+    {
+        int tid = 0;
+#ifdef _OPENMP
+        tid = omp_get_thread_num();
+#endif
+        auto& out = per_thread[tid];
+#pragma omp for schedule(dynamic, 256)
+        for (int64_t f = 0; f < F; ++f) {
+            const ProjF& p0 = proj[tri[3 * f + 0]];
+            const ProjF& p1 = proj[tri[3 * f + 1]];
+            const ProjF& p2 = proj[tri[3 * f + 2]];
+            if (!(p0.valid && p1.valid && p2.valid)) continue;
+            int64_t X0 = p0.X, Y0 = p0.Y, X1 = p1.X, Y1 = p1.Y, X2 = p2.X, Y2 = p2.Y;
+            int64_t area2 = (X1 - X0) * (Y2 - Y0) - (Y1 - Y0) * (X2 - X0);
+            if (area2 == 0) continue;
+            const uint32_t front = area2 < 0 ? 1u : 0u;
+            const uint32_t bits = (uint32_t(f) << 2) | ((face_boundary[f] & 1u) << 1) | front;
+            // Orient so the interior has positive edge functions.
+            int64_t ax[3] = {X0, X1, X2}, ay[3] = {Y0, Y1, Y2};
+            if (area2 < 0) {
+                std::swap(ax[1], ax[2]);
+                std::swap(ay[1], ay[2]);
+            }
+            int64_t minX = std::min({X0, X1, X2}), maxX = std::max({X0, X1, X2});
+            int64_t minY = std::min({Y0, Y1, Y2}), maxY = std::max({Y0, Y1, Y2});
+            int64_t px0 = std::max<int64_t>(0, ceil_div(minX - 128, 256));
+            int64_t px1 = std::min<int64_t>(W - 1, floor_div(maxX - 128, 256));
+            int64_t py0 = std::max<int64_t>(std::max(0, row_begin), ceil_div(minY - 128, 256));
+            int64_t py1 = std::min<int64_t>(std::min(H, row_end) - 1, floor_div(maxY - 128, 256));
+            for (int64_t py = py0; py <= py1; ++py) {
+                const int64_t Yc = 256 * py + 128;
+                for (int64_t px = px0; px <= px1; ++px) {
+                    const int64_t Xc = 256 * px + 128;
+                    bool in = true;
+                    for (int e = 0; e < 3 && in; ++e) {
+                        int a = (e + 1) % 3, b = (e + 2) % 3;
+                        int64_t dx = ax[b] - ax[a], dy = ay[b] - ay[a];
+                        int64_t E = dx * (Yc - ay[a]) - dy * (Xc - ax[a]);
+                        in = edge_inside(E, dx, dy);
+                    }
+                    if (!in) continue;
+                    float qx = float(px) + 0.5f, qy = float(py) + 0.5f;
+                    float z = depth_key_f(p0, p1, p2, qx, qy);
+                    uint64_t rec = (uint64_t(f2u(z)) << 32) | bits;
+                    out.emplace_back(uint32_t(py * W + px), rec);
+                }
+            }
+        }
+    }
+    FragLists fl;
+    fl.offsets.assign(P + 1, 0);
+    for (auto& v : per_thread)
+        for (auto& pr : v) fl.offsets[pr.first + 1]++;
+    for (int64_t i = 0; i < P; ++i) fl.offsets[i + 1] += fl.offsets[i];
+    fl.records.resize(fl.offsets[P]);
+    std::vector<int64_t> cursor(fl.offsets.begin(), fl.offsets.end() - 1);
+    for (auto& v : per_thread)
+        for (auto& pr : v) fl.records[cursor[pr.first]++] = pr.second;
+#pragma omp parallel for schedule(dynamic, 1024)
+    for (int64_t p = 0; p < P; ++p)
+        std::sort(fl.records.begin() + fl.offsets[p], fl.records.begin() + fl.offsets[p + 1]);
+    return fl;
+}
+
+// ---------------------------------------------------------------------------
+// Continuous per-fragment values in precision R.
+template <class R>
+struct Frag {
+    R z;
+    R col[4];
+    uint32_t face;
+    bool boundary, front;
+};
+
+template <class R>
+struct MeshR {
+    const uint32_t* tri;
+    const R* pos;
+    const R* col;
+    std::vector<ProjR<R>> proj;
+};
+
+// Perspective-correct barycentrics of the pixel centre on the face (screen
+// space), which equal the world-space barycentrics of the point where the pixel
+// ray meets the face plane.  Forward.glsl:80-103 computes the same point by
+// unprojecting gl_FragCoord.z and takes unsigned cross-product ratios; here
+// the signed ratios are used (they agree inside the face and stay linear at
+// its edges).
+template <class R>
+void face_bary(const ProjR<R>& a, const ProjR<R>& b, const ProjR<R>& c, R qx, R qy, R lam[3], R bary[3],
+               R& z) {
+    R d0x = a.sx - qx, d0y = a.sy - qy;
+    R d1x = b.sx - qx, d1y = b.sy - qy;
+    R d2x = c.sx - qx, d2y = c.sy - qy;
+    R E0 = d1x * d2y - d1y * d2x;
+    R E1 = d2x * d0y - d2y * d0x;
+    R E2 = d0x * d1y - d0y * d1x;
+    R A = (E0 + E1) + E2;
+    lam[0] = E0 / A;
+    lam[1] = E1 / A;
+    lam[2] = E2 / A;
+    R u0 = lam[0] * a.iz, u1 = lam[1] * b.iz, u2 = lam[2] * c.iz;
+    R w = (u0 + u1) + u2;
+    z = R(1) / w;
+    bary[0] = u0 * z;
+    bary[1] = u1 * z;
+    bary[2] = u2 * z;
+}
+
+template <class R>
+Frag<R> eval_frag(const MeshR<R>& m, uint64_t rec, int px, int py) {
+    Frag<R> fr;
+    uint32_t bits = uint32_t(rec & 0xffffffffu);
+    fr.face = bits >> 2;
+    fr.boundary = (bits >> 1) & 1u;
+    fr.front = bits & 1u;
+    uint32_t i0 = m.tri[3 * fr.face], i1 = m.tri[3 * fr.face + 1], i2 = m.tri[3 * fr.face + 2];
+    R lam[3], b[3];
+    face_bary(m.proj[i0], m.proj[i1], m.proj[i2], R(px) + R(0.5), R(py) + R(0.5), lam, b, fr.z);
+    for (int k = 0; k < 4; ++k)
+        fr.col[k] = b[0] * m.col[4 * i0 + k] + b[1] * m.col[4 * i1 + k] + b[2] * m.col[4 * i2 + k];
+    return fr;
+}
+
+// accumulateLinearConst, Data/Shaders/Common/ForwardCommon.glsl:42-49.
+template <class R>
+inline bool seg_integral(R t, const R c0[3], const R c1[3], R a, R cacc[3], R& A) {
+    if (a < R(1e-6)) {
+        A = R(1);
+        cacc[0] = cacc[1] = cacc[2] = R(0);
+        return false;
+    }
+    A = std::exp(-a * t);
+    R K = (t + R(1) / a) * A - R(1) / a;
+    for (int k = 0; k < 3; ++k) cacc[k] = (R(1) - A) * c0[k] + K * (c0[k] - c1[k]);
+    return true;
+}
+
+template <class R>
+inline bool skip_pair(const Frag<R>& f0, const Frag<R>& f1) {
+    // Forward.glsl:183-185: gap between a back-facing and a front-facing boundary face.
+    return (f0.boundary && !f0.front) && (f1.boundary && f1.front);
+}
+
+template <class R>
+void sub_inputs(const Frag<R>& f0, const Frag<R>& f1, int s, R atten, R c0[3], R c1[3], R& a) {
+    const R inv = R(1) / R(kNumSubdivs);
+    R fb = R(s) * inv, fm = (R(s) + R(0.5)) * inv, fe = (R(s) + R(1)) * inv;
+    for (int k = 0; k < 3; ++k) {
+        c0[k] = f0.col[k] + (f1.col[k] - f0.col[k]) * fb;
+        c1[k] = f0.col[k] + (f1.col[k] - f0.col[k]) * fe;
+    }
+    a = (f0.col[3] + (f1.col[3] - f0.col[3]) * fm) * atten;
+}
+
+// Front-to-back compositing of one pixel, Forward.glsl:159-211 and :250-261.
+// State is (premultiplied colour C, transmittance T); alpha = 1 - T.  Early ray
+// termination (Forward.glsl:169-173) stops before segment i once T < thresh.
+template <class R>
+void composite_pixel(const MeshR<R>& m, const Params& prm, const uint64_t* recs, int64_t n, int px, int py,
+                     R out[4], R& Tfinal, uint32_t& term) {
+    R C[3] = {0, 0, 0};
+    R T = 1;
+    uint32_t i = 1;
+    if (n >= 2) {
+        Frag<R> f1 = eval_frag(m, recs[0], px, py), f0;
+        for (i = 1; i < uint32_t(n); ++i) {
+            if (prm.use_ert && T < R(prm.ert_thresh)) break;
+            f0 = f1;
+            f1 = eval_frag(m, recs[i], px, py);
+            if (skip_pair(f0, f1)) continue;
+            R t = f1.z - f0.z;
+            R tSeg = t / R(kNumSubdivs);
+            for (int s = 0; s < kNumSubdivs; ++s) {
+                R c0[3], c1[3], a, cacc[3], A;
+                sub_inputs(f0, f1, s, R(prm.attenuation), c0, c1, a);
+                if (!seg_integral(tSeg, c0, c1, a, cacc, A)) continue;
+                for (int k = 0; k < 3; ++k) C[k] += T * cacc[k];
+                T *= A;
+            }
+        }
+    } else {
+        i = uint32_t(n);
+    }
+    term = (n >= 2) ? i : uint32_t(n);
+    Tfinal = T;
+    for (int k = 0; k < 3; ++k) out[k] = C[k] + T * R(prm.clear_color[k]);
+    out[3] = (R(1) - T) + T * R(prm.clear_color[3]);
+}
+
+// Adjoint of seg_integral w.r.t. (tSeg, a, c0, c1); BackwardCommon.glsl:116-133
+// (accumulateLinearConstAdjoint) including its a->0 branch.
+template <class R>
+void seg_integral_adjoint(R tSeg, const R c0[3], const R c1[3], R a, R A, const R gc[3], R gA, R& g_t,
+                          R& g_a, R g_c0[3], R g_c1[3]) {
+    if (a < R(1e-6)) {
+        // Derivative of the exact integral at a = 0 (the forward drops the term).
+        g_t = 0;
+        g_a = R(0);
+        for (int k = 0; k < 3; ++k) {
+            g_a += gc[k] * (tSeg * c0[k] + R(0.5) * tSeg * tSeg * (c1[k] - c0[k]));
+            g_c0[k] = g_c1[k] = R(0);
+        }
+        g_a += -gA * tSeg;  // alpha_acc = 1 - A ~ a t  =>  d alpha/da = t, gA = -g_alpha
+        return;
+    }
+    R inva = R(1) / a;
+    R K = (tSeg + inva) * A - inva;
+    R dot_t = 0, dot_a = 0;
+    for (int k = 0; k < 3; ++k) {
+        dot_t += gc[k] * (a * A * (c0[k] + tSeg * (c1[k] - c0[k])));
+        dot_a += gc[k] * (tSeg * A * c0[k] + (inva * inva - (tSeg * tSeg + inva * inva + tSeg * inva) * A) *
+                                                    (c0[k] - c1[k]));
+        g_c0[k] = ((R(1) - A) + K) * gc[k];
+        g_c1[k] = -K * gc[k];
+    }
+    g_t = dot_t + gA * (-a * A);
+    g_a = dot_a + gA * (-tSeg * A);
+}
+
+// Back-propagate (dL/dz, dL/dcolour) of one fragment to its face's three
+// vertex positions and colours (exact derivative of face_bary + projection).
+template <class R>
+void frag_vertex_grads(const MeshR<R>& m, const CamConst& cam, uint32_t face, int px, int py, R gz,
+                       const R gcol[4], bool use_abs, R* grad_pos, R* grad_col) {
+    const uint32_t vi[3] = {m.tri[3 * face], m.tri[3 * face + 1], m.tri[3 * face + 2]};
+    const ProjR<R>* P[3] = {&m.proj[vi[0]], &m.proj[vi[1]], &m.proj[vi[2]]};
+    const R qx = R(px) + R(0.5), qy = R(py) + R(0.5);
+    R dx[3], dy[3];
+    for (int j = 0; j < 3; ++j) {
+        dx[j] = P[j]->sx - qx;
+        dy[j] = P[j]->sy - qy;
+    }
+    R E[3] = {dx[1] * dy[2] - dy[1] * dx[2], dx[2] * dy[0] - dy[2] * dx[0], dx[0] * dy[1] - dy[0] * dx[1]};
+    R A = (E[0] + E[1]) + E[2];
+    R lam[3], u[3], w = 0;
+    for (int j = 0; j < 3; ++j) {
+        lam[j] = E[j] / A;
+        u[j] = lam[j] * P[j]->iz;
+        w += u[j];
+    }
+    R z = R(1) / w;
+    R b[3], gb[3], sb = 0;
+    for (int j = 0; j < 3; ++j) {
+        b[j] = u[j] * z;
+        gb[j] = 0;
+        for (int k = 0; k < 4; ++k) gb[j] += gcol[k] * m.col[4 * vi[j] + k];
+        sb += gb[j] * b[j];
+    }
+    R glam[3], giz[3], sl = 0;
+    for (int j = 0; j < 3; ++j) {
+        R gu = z * (gb[j] - sb) - gz * z * z;
+        glam[j] = gu * P[j]->iz;
+        giz[j] = gu * lam[j];
+        sl += glam[j] * lam[j];
+    }
+    R gE[3];
+    for (int j = 0; j < 3; ++j) gE[j] = (glam[j] - sl) / A;
+    // dE0/d(d1) = (d2y, -d2x), dE0/d(d2) = (-d1y, d1x); cyclic for E1, E2.
+    R gsx[3], gsy[3];
+    gsx[0] = gE[1] * (-dy[2]) + gE[2] * dy[1];
+    gsy[0] = gE[1] * dx[2] + gE[2] * (-dx[1]);
+    gsx[1] = gE[0] * dy[2] + gE[2] * (-dy[0]);
+    gsy[1] = gE[0] * (-dx[2]) + gE[2] * dx[0];
+    gsx[2] = gE[0] * (-dy[1]) + gE[1] * dy[0];
+    gsy[2] = gE[0] * dx[1] + gE[1] * (-dx[0]);
+    const R f = std::is_same<R, float>::value ? R(cam.f) : R(cam.fd);
+    const float* V = cam.V;
+    for (int j = 0; j < 3; ++j) {
+        const ProjR<R>& p = *P[j];
+        R gxv = gsx[j] * f * p.iz;
+        R gyv = -gsy[j] * f * p.iz;
+        R giz_t = giz[j] + gsx[j] * f * p.xv - gsy[j] * f * p.yv;
+        R gzv = giz_t * p.iz * p.iz;  // iz = -1/zv  =>  d iz/d zv = iz^2
+        R gp[3] = {R(V[0]) * gxv + R(V[1]) * gyv + R(V[2]) * gzv, R(V[4]) * gxv + R(V[5]) * gyv + R(V[6]) * gzv,
+                   R(V[8]) * gxv + R(V[9]) * gyv + R(V[10]) * gzv};
+        R gc[4];
+        for (int k = 0; k < 4; ++k) gc[k] = b[j] * gcol[k];
+        if (use_abs) {
+            for (int k = 0; k < 3; ++k) gp[k] = std::fabs(gp[k]);
+            for (int k = 0; k < 4; ++k) gc[k] = std::fabs(gc[k]);
+        }
+        for (int k = 0; k < 3; ++k) grad_pos[3 * vi[j] + k] += gp[k];
+        for (int k = 0; k < 4; ++k) grad_col[4 * vi[j] + k] += gc[k];
+    }
+}
+
+// Adjoint of one pixel, back to front from the termination index.
+// Backward.glsl:107-512 restated as the exact derivative of composite_pixel:
+// transmittance is rebuilt from the final value by T_in = T_out / A (the
+// inversion of Weiss et al. that Backward.glsl:231-246 applies to alpha), all
+// four sub-segments are differentiated, and segment length / barycentric
+// adjoints follow the screen-space construction of face_bary.
+template <class R>
+void adjoint_pixel(const MeshR<R>& m, const CamConst& cam, const Params& prm, const uint64_t* recs, int64_t n,
+                   int px, int py, R Tfinal, uint32_t term, const R g[4], R* grad_pos, R* grad_col) {
+    if (n < 2) return;
+    const R atten = R(prm.attenuation);
+    R gC[3] = {g[0], g[1], g[2]};
+    R gT = g[0] * R(prm.clear_color[0]) + g[1] * R(prm.clear_color[1]) + g[2] * R(prm.clear_color[2]) +
+           g[3] * (R(prm.clear_color[3]) - R(1));
+    R T = Tfinal;
+    int64_t last = prm.use_ert ? int64_t(term) - 1 : n - 1;  // last composited segment index
+    if (last < 1) return;
+    // Fragment accumulators: fragment i (back of segment i) and i-1 (front).
+    Frag<R> fb = eval_frag(m, recs[last], px, py);
+    R gz_b = 0, gcol_b[4] = {0, 0, 0, 0};
+    for (int64_t i = last; i >= 1; --i) {
+        Frag<R> ff = eval_frag(m, recs[i - 1], px, py);
+        R gz_f = 0, gcol_f[4] = {0, 0, 0, 0};
+        if (!skip_pair(ff, fb)) {
+            R t = fb.z - ff.z;
+            R tSeg = t / R(kNumSubdivs);
+            R g_tot = 0;
+            const R inv = R(1) / R(kNumSubdivs);
+            for (int s = kNumSubdivs - 1; s >= 0; --s) {
+                R c0[3], c1[3], a, cacc[3], A;
+                sub_inputs(ff, fb, s, atten, c0, c1, a);
+                bool active = seg_integral(tSeg, c0, c1, a, cacc, A);
+                R Tin = active ? T / A : T;
+                R gcacc[3] = {Tin * gC[0], Tin * gC[1], Tin * gC[2]};
+                R gA = Tin * gT;
+                if (active) {
+                    gT = (gC[0] * cacc[0] + gC[1] * cacc[1] + gC[2] * cacc[2]) + gT * A;
+                } else {
+                    gA = Tin * gT;  // A == 1 in the forward; derivative through the a->0 limit
+                }
+                T = Tin;
+                R g_t, g_a, g_c0[3], g_c1[3];
+                seg_integral_adjoint(tSeg, c0, c1, a, A, gcacc, gA, g_t, g_a, g_c0, g_c1);
+                g_tot += g_t * inv;
+                R fbg = R(s) * inv, fm = (R(s) + R(0.5)) * inv, fe = (R(s) + R(1)) * inv;
+                for (int k = 0; k < 3; ++k) {
+                    gcol_f[k] += (R(1) - fbg) * g_c0[k] + (R(1) - fe) * g_c1[k];
+                    gcol_b[k] += fbg * g_c0[k] + fe * g_c1[k];
+                }
+                gcol_f[3] += (R(1) - fm) * g_a * atten;
+                gcol_b[3] += fm * g_a * atten;
+            }
+            gz_f -= g_tot;
+            gz_b += g_tot;
+        }
+        // Fragment i is complete.
+        frag_vertex_grads(m, cam, fb.face, px, py, gz_b, gcol_b, prm.use_abs_grad != 0, grad_pos, grad_col);
+        fb = ff;
+        gz_b = gz_f;
+        for (int k = 0; k < 4; ++k) gcol_b[k] = gcol_f[k];
+    }
+    frag_vertex_grads(m, cam, fb.face, px, py, gz_b, gcol_b, prm.use_abs_grad != 0, grad_pos, grad_col);
+}
+
+template <class R>
+MeshR<R> make_mesh(const uint32_t* tri, const R* pos, const R* col, int64_t V, const CamConst& cam) {
+    MeshR<R> m;
+    m.tri = tri;
+    m.pos = pos;
+    m.col = col;
+    m.proj.resize(V);
+    for (int64_t v = 0; v < V; ++v) m.proj[v] = project_r<R>(cam, pos[3 * v], pos[3 * v + 1], pos[3 * v + 2]);
+    return m;
+}
+
+template <class R>
+std::vector<ProjF> project_all_f(const R* pos, int64_t V, const CamConst& cam) {
+    std::vector<ProjF> pf(V);
+    for (int64_t v = 0; v < V; ++v)
+        pf[v] = project_f(cam, float(pos[3 * v]), float(pos[3 * v + 1]), float(pos[3 * v + 2]));
+    return pf;
+}
+
+inline void row_range(const Params& prm, int H, int& r0, int& r1) {
+    r0 = std::max(0, prm.row_begin);
+    r1 = prm.row_end > 0 ? std::min(H, prm.row_end) : H;
+}
+
+template <class R>
+int render_impl(const uint32_t* tri, const uint32_t* fbits, int64_t F, const R* pos, const R* col, int64_t V,
+                const Camera* camp, const Params* prm, R* image, R* tfinal, uint32_t* term, int64_t* nfrag,
+                const float* pos_coverage = nullptr) {
+    CamConst cam = make_cam(*camp);
+    int r0, r1;
+    row_range(*prm, cam.H, r0, r1);
+    // Coverage and depth order come from pos_coverage when given (frozen
+    // fragment lists for smooth finite differences), else from pos.
+    auto pf = pos_coverage ? project_all_f(pos_coverage, V, cam) : project_all_f(pos, V, cam);
+    FragLists fl = build_fragments(tri, fbits, F, pf, cam, r0, r1);
+    MeshR<R> m = make_mesh(tri, pos, col, V, cam);
+    const int W = cam.W;
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int py = r0; py < r1; ++py) {
+        for (int px = 0; px < W; ++px) {
+            int64_t p = int64_t(py) * W + px;
+            R out[4], Tf;
+            uint32_t tm;
+            composite_pixel(m, *prm, fl.records.data() + fl.offsets[p], fl.offsets[p + 1] - fl.offsets[p], px,
+                            py, out, Tf, tm);
+            for (int k = 0; k < 4; ++k) image[4 * p + k] = out[k];
+            if (tfinal) tfinal[p] = Tf;
+            if (term) term[p] = tm;
+        }
+    }
+    if (nfrag) *nfrag = int64_t(fl.records.size());
+    return 0;
+}
+
+template <class R>
+int adjoint_impl(const uint32_t* tri, const uint32_t* fbits, int64_t F, const R* pos, const R* col, int64_t V,
+                 const Camera* camp, const Params* prm, const R* image_adj, R* grad_pos, R* grad_col) {
+    CamConst cam = make_cam(*camp);
+    int r0, r1;
+    row_range(*prm, cam.H, r0, r1);
+    auto pf = project_all_f(pos, V, cam);
+    FragLists fl = build_fragments(tri, fbits, F, pf, cam, r0, r1);
+    MeshR<R> m = make_mesh(tri, pos, col, V, cam);
+    const int W = cam.W;
+    int nthreads = 1;
+#ifdef _OPENMP
+    nthreads = omp_get_max_threads();
+#endif
+    std::vector<std::vector<R>> gp(nthreads, std::vector<R>(3 * V, R(0)));
+    std::vector<std::vector<R>> gc(nthreads, std::vector<R>(4 * V, R(0)));
+#pragma omp parallel
+    {
+        int tid = 0;
+#ifdef _OPENMP
+        tid = omp_get_thread_num();
+#endif
+#pragma omp for schedule(dynamic, 4)
+        for (int py = r0; py < r1; ++py) {
+            for (int px = 0; px < W; ++px) {
+                int64_t p = int64_t(py) * W + px;
+                const uint64_t* recs = fl.records.data() + fl.offsets[p];
+                int64_t n = fl.offsets[p + 1] - fl.offsets[p];
+                R out[4], Tf;
+                uint32_t tm;
+                composite_pixel(m, *prm, recs, n, px, py, out, Tf, tm);
+                R g[4] = {image_adj[4 * p], image_adj[4 * p + 1], image_adj[4 * p + 2], image_adj[4 * p + 3]};
+                adjoint_pixel(m, cam, *prm, recs, n, px, py, Tf, tm, g, gp[tid].data(), gc[tid].data());
+            }
+        }
+    }
+    for (int t = 0; t < nthreads; ++t) {
+        for (int64_t i = 0; i < 3 * V; ++i) grad_pos[i] += gp[t][i];
+        for (int64_t i = 0; i < 4 * V; ++i) grad_col[i] += gc[t][i];
+    }
+    return 0;
+}
+
+struct TempFace {
+    uint32_t v[3];
+    uint32_t face_id;
+    uint32_t tet_id;
+    bool operator<(const TempFace& o) const {
+        for (int i = 0; i < 3; ++i)
+            if (v[i] != o.v[i]) return v[i] < o.v[i];
+        return face_id < o.face_id;
+    }
+    bool same(const TempFace& o) const { return v[0] == o.v[0] && v[1] == o.v[1] && v[2] == o.v[2]; }
+};
+
+}  // namespace
+
+extern "C" {
+
+// buildFacesSlim, src/Tet/TetMesh.cpp:1218-1268 (with TempFace ordering
+// :1183-1216 and the device arrays of uploadDataToDevice :560-576): unique
+// faces in sorted-vertex-triple order, each keeping the winding of its lowest
+// faceId copy; boundary bit per face and per vertex; face -> (tet0, tet1).
+// Returns the number of faces F (arrays must hold 4T faces).
+int64_t orc_build_faces(const uint32_t* cells, int64_t T, int64_t V, uint32_t* tri_out, uint32_t* face_boundary,
+                        uint32_t* face_to_tet, uint32_t* vertex_boundary) {
+    std::vector<TempFace> tf(size_t(T) * 4);
+    std::vector<uint32_t> wound(size_t(T) * 12);
+    for (int64_t c = 0; c < T; ++c) {
+        for (int j = 0; j < 4; ++j) {
+            uint32_t fid = uint32_t(4 * c + j);
+            uint32_t v[3];
+            for (int k = 0; k < 3; ++k) v[k] = cells[4 * c + kTetFace[j][k]];
+            for (int k = 0; k < 3; ++k) wound[3 * size_t(fid) + k] = v[k];
+            std::sort(v, v + 3);
+            tf[fid] = TempFace{{v[0], v[1], v[2]}, fid, uint32_t(c)};
+        }
+    }
+    std::sort(tf.begin(), tf.end());
+    int64_t F = 0;
+    for (size_t i = 0; i < tf.size(); ++i) {
+        if (i == 0 || !tf[i].same(tf[i - 1])) {
+            for (int k = 0; k < 3; ++k) tri_out[3 * F + k] = wound[3 * size_t(tf[i].face_id) + k];
+            face_to_tet[2 * F] = tf[i].tet_id;
+            face_to_tet[2 * F + 1] = 0xffffffffu;
+            face_boundary[F] = 1;
+            ++F;
+        } else {
+            face_boundary[F - 1] = 0;
+            face_to_tet[2 * (F - 1) + 1] = tf[i].tet_id;
+        }
+    }
+    std::memset(vertex_boundary, 0, sizeof(uint32_t) * size_t(V));
+    for (int64_t f = 0; f < F; ++f)
+        if (face_boundary[f])
+            for (int k = 0; k < 3; ++k) vertex_boundary[tri_out[3 * f + k]] = 1;
+    return F;
+}
+
+// Per-pixel sorted fragment lists (exported like Renderer.get_fragment_buffer /
+// get_start_offset_buffer, Module.cpp:960-981, in offsets+records layout).
+// Returns Nf; writes offsets[P+1] and records[Nf] when the pointers are non-null
+// and records_cap >= Nf.
+int64_t orc_fragments(const uint32_t* tri, const uint32_t* fbits, int64_t F, const float* pos, int64_t V,
+                      const Camera* camp, int64_t* offsets, uint64_t* records, int64_t records_cap) {
+    CamConst cam = make_cam(*camp);
+    auto pf = project_all_f(pos, V, cam);
+    FragLists fl = build_fragments(tri, fbits, F, pf, cam, 0, cam.H);
+    int64_t nf = int64_t(fl.records.size());
+    if (offsets) std::memcpy(offsets, fl.offsets.data(), sizeof(int64_t) * fl.offsets.size());
+    if (records && records_cap >= nf) std::memcpy(records, fl.records.data(), sizeof(uint64_t) * size_t(nf));
+    return nf;
+}
+
+// FP32 projection of vertices (sx, sy, ze per vertex) and the snapped coords.
+void orc_project_f32(const float* pos, int64_t V, const Camera* camp, float* sxsyze, int32_t* XY,
+                     uint8_t* valid) {
+    CamConst cam = make_cam(*camp);
+    for (int64_t v = 0; v < V; ++v) {
+        ProjF p = project_f(cam, pos[3 * v], pos[3 * v + 1], pos[3 * v + 2]);
+        sxsyze[3 * v] = p.sx;
+        sxsyze[3 * v + 1] = p.sy;
+        sxsyze[3 * v + 2] = p.ze;
+        XY[2 * v] = p.X;
+        XY[2 * v + 1] = p.Y;
+        valid[v] = p.valid ? 1 : 0;
+    }
+}
+
+int orc_render_f64(const uint32_t* tri, const uint32_t* fbits, int64_t F, const double* pos, const double* col,
+                   int64_t V, const Camera* cam, const Params* prm, double* image, double* tfinal, uint32_t* term,
+                   int64_t* nfrag) {
+    return render_impl<double>(tri, fbits, F, pos, col, V, cam, prm, image, tfinal, term, nfrag);
+}
+
+// Forward with the fragment lists (coverage and order) of pos_coverage and
+// every continuous quantity from pos: the function whose derivative the
+// adjoint computes, smooth in pos, for finite-difference checks.
+int orc_render_frozen_f64(const uint32_t* tri, const uint32_t* fbits, int64_t F, const float* pos_coverage,
+                          const double* pos, const double* col, int64_t V, const Camera* cam, const Params* prm,
+                          double* image) {
+    return render_impl<double>(tri, fbits, F, pos, col, V, cam, prm, image, nullptr, nullptr, nullptr,
+                               pos_coverage);
+}
+
+int orc_render_f32(const uint32_t* tri, const uint32_t* fbits, int64_t F, const float* pos, const float* col,
+                   int64_t V, const Camera* cam, const Params* prm, float* image, float* tfinal, uint32_t* term,
+                   int64_t* nfrag) {
+    return render_impl<float>(tri, fbits, F, pos, col, V, cam, prm, image, tfinal, term, nfrag);
+}
+
+int orc_adjoint_f64(const uint32_t* tri, const uint32_t* fbits, int64_t F, const double* pos, const double* col,
+                    int64_t V, const Camera* cam, const Params* prm, const double* image_adj, double* grad_pos,
+                    double* grad_col) {
+    return adjoint_impl<double>(tri, fbits, F, pos, col, V, cam, prm, image_adj, grad_pos, grad_col);
+}
+
+int orc_adjoint_f32(const uint32_t* tri, const uint32_t* fbits, int64_t F, const float* pos, const float* col,
+                    int64_t V, const Camera* cam, const Params* prm, const float* image_adj, float* grad_pos,
+                    float* grad_col) {
+    return adjoint_impl<float>(tri, fbits, F, pos, col, V, cam, prm, image_adj, grad_pos, grad_col);
+}
+
+// Segment integral for closed-form checks (ForwardCommon.glsl:42-49).
+void orc_segment_integral(double t, const double* c0, const double* c1, double a, double* out4) {
+    double cacc[3], A;
+    bool active = seg_integral<double>(t, c0, c1, a, cacc, A);
+    for (int k = 0; k < 3; ++k) out4[k] = cacc[k];
+    out4[3] = active ? 1.0 - A : 0.0;
+}
+
+int orc_num_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+}  // extern "C"
