@@ -1,0 +1,398 @@
+#!/usr/bin/env python
+"""Benchmark: forward + adjoint + Adam iterations of the plain method on a
+Kuhn 64^3 grid (1,572,864 tets, 274,625 vertices) at 1024x1024, one camera per
+step, fitting RGBA and positions to target images of a different-seed mesh
+of the same topology (seeded synthetic inputs; no dataset is involved).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  `value` is device-timed iterations/s with all
+inputs resident in HBM; `e2e` is the same loop through the public Python API
+(DifferentiableRenderer + l2_loss + optim.Adam) with each step's target image
+copied from pinned host memory and the loss read back.  Under torchrun each
+rank runs an independent replica (the path has no data-path collective).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "fwd+adj iter/s at 1.57M tets 1024²"
+LR_COL, LR_POS = 1e-2, 1e-4
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=64, help="Kuhn grid cubes per axis")
+    ap.add_argument("--res", type=int, default=1024)
+    ap.add_argument("--views", type=int, default=16)
+    ap.add_argument("--cpu-rows", type=int, default=32, help="rows of the CPU baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.gpu)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[4:8]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            pk = json.load(f)
+        return float(pk["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def ncu_traffic_per_unit():
+    """Per-launch DRAM traffic of the dominant kernels per fragment, from one ncu
+    capture summarised in profiles/roofline_traffic.json (None if absent)."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "roofline_traffic.json")) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+# ---------------------------------------------------------------------------
+def build_scene(args, device):
+    import numpy as np
+    import torch
+
+    import difftetvr_b200 as d
+    from difftetvr_b200 import synthetic as S
+
+    cells, pos = S.kuhn_mesh(args.n, seed=0)
+    col = S.gaussian_colors(pos, seed=0)
+    _, pos_t = S.kuhn_mesh(args.n, seed=1)
+    col_t = S.gaussian_colors(pos_t, seed=1)
+    views = [S.sphere_camera(100 + i) for i in range(args.views)]
+
+    def make(cells, pos, col):
+        mesh = d.TetMesh()
+        mesh.set_use_gradients(True)
+        mesh.set_tet_mesh_data(cells, pos, col)
+        r = d.Renderer(d.RendererType.PPLL)
+        r.set_tet_mesh(mesh)
+        r.set_viewport_size(args.res, args.res)
+        r.set_camera_fovy(S.FOVY_45)
+        r.set_attenuation(1.0)
+        r.set_clear_color(d.vec4(0, 0, 0, 0))
+        return mesh, r
+
+    mesh_t, r_t = make(cells, pos_t, col_t)
+    targets = []
+    with torch.no_grad():
+        for v in views:
+            r_t.set_view_matrix(v)
+            targets.append(r_t.render().clone())
+    del r_t, mesh_t
+    mesh, r = make(cells, pos, col)
+    return {"cells": cells, "pos": pos, "col": col, "views": views, "targets": targets, "mesh": mesh,
+            "renderer": r, "np": np}
+
+
+def run_ours(args, rank, world):
+    import torch
+
+    import difftetvr_b200 as d
+    from difftetvr_b200 import _lib
+    from difftetvr_b200.optim import CLAMP_NONNEGATIVE, Adam, l2_loss
+
+    device = torch.device("cuda", torch.cuda.current_device())
+    sc = build_scene(args, device)
+    mesh, r, views, targets = sc["mesh"], sc["renderer"], sc["views"], sc["targets"]
+    pos, col = mesh.get_vertex_positions(), mesh.get_vertex_colors()
+    opt = Adam([{"params": [col], "lr": LR_COL, "clamp": CLAMP_NONNEGATIVE},
+                {"params": [pos], "lr": LR_POS}], betas=(0.9, 0.999), eps=1e-8)
+    n_img = targets[0].numel()
+    adj = torch.empty_like(targets[0])
+    loss_acc = torch.zeros(1, device=device)
+    stream = torch.cuda.current_stream(device)
+
+    def step(i):
+        # Device-resident step: render, fused loss + image adjoint, adjoint, Adam.
+        pos.grad.zero_()
+        col.grad.zero_()
+        r.set_view_matrix(views[i % len(views)])
+        image = r.render()
+        _lib.call("dtv_loss_l2", image.data_ptr(), targets[i % len(views)].data_ptr(), n_img,
+                  1.0 / n_img, adj.data_ptr(), loss_acc.data_ptr(), stream.cuda_stream)
+        r.render_adjoint(adj)
+        opt.step()
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    for i in range(args.warmup):
+        step(i)
+    # Stage breakdown (CUDA events on the launching stream) over the timed steps.
+    r.set_stage_timing(True)
+    stage_sum = {k: 0.0 for k in r.STAGES}
+    nf_sum = 0
+    clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")) if world > 1 else torch.cuda.current_device())
+    barrier()
+    clocks.start()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for i in range(args.steps):
+        step(args.warmup + i)
+        st = r.get_stage_times()  # reads events of this step (host waits for them)
+        for k, v in st.items():
+            stage_sum[k] += v
+        nf_sum += r.get_num_fragments()
+    t1.record(stream)
+    barrier()
+    clk = clocks.stop()
+    ms = t0.elapsed_time(t1)
+    r.set_stage_timing(False)
+    if world > 1:
+        tt = torch.tensor([ms], device=device)
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        ms = float(tt.item())
+    value = world * args.steps / (ms / 1e3)
+
+    # End-to-end through the public API, host buffers in the timed region.
+    e2e = None
+    if not args.no_e2e:
+        diff = d.DifferentiableRenderer(r)
+        opt2 = Adam([{"params": [col], "lr": LR_COL, "clamp": CLAMP_NONNEGATIVE},
+                     {"params": [pos], "lr": LR_POS}])
+        host_targets = [t.cpu().pin_memory() for t in targets]
+        h2d = host_targets[0].numel() * 4
+        dev_target = torch.empty_like(targets[0])
+
+        def e2e_step(i):
+            opt2.zero_grad(set_to_none=False)
+            dev_target.copy_(host_targets[i % len(views)], non_blocking=True)
+            r.set_view_matrix(views[i % len(views)])
+            image = diff()
+            loss = l2_loss(image, dev_target)
+            loss.backward()
+            opt2.step()
+            return loss.item()
+
+        for i in range(args.warmup):
+            e2e_step(i)
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for i in range(args.steps):
+            e2e_step(i)
+        e1.record(stream)
+        barrier()
+        ems = e0.elapsed_time(e1)
+        if world > 1:
+            tt = torch.tensor([ems], device=device)
+            torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+            ems = float(tt.item())
+        e2e = {"value": world * args.steps / (ems / 1e3), "unit": "iter/s", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": 4, "ms_per_step": ems / args.steps,
+               "api": "DifferentiableRenderer + optim.l2_loss + optim.Adam"}
+
+    # Roofline of the dominant kernel (algorithmic bytes per launch / its event time).
+    K = args.steps
+    avg = {k: v / K for k, v in stage_sum.items()}
+    nf = nf_sum / K
+    P = args.res * args.res
+    V = mesh.get_num_vertices()
+    F = mesh.get_num_faces()
+    algo = {
+        "composite": 8 * nf + 16 * P + 4 * P + 4 * P + 28 * V + 16 * F,
+        "adjoint": 8 * nf + 36 * P + 16 * F + 28 * V + 28 * V,
+        "fill": 8 * nf + 16 * F + 24 * V + 16 * P,
+        "sort": 16 * nf + 16 * P,
+        "count": 4 * P + 16 * F + 24 * V,
+    }
+    dominant = max(algo, key=lambda k: avg.get(k, 0.0))
+    peak, peak_kind = measured_peaks()
+    achieved = algo[dominant] / (avg[dominant] / 1e3) / 1e9
+    tr = ncu_traffic_per_unit().get(dominant)
+    traffic = None if tr is None else float(tr["bytes_per_fragment"]) * nf + float(tr.get("bytes_per_pixel", 0)) * P
+    roofline = {"bound": "hbm", "kernel": dominant, "achieved": round(achieved, 1), "peak": peak,
+                "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                "traffic": traffic, "algorithmic_bytes": algo[dominant], "kernel_ms": avg[dominant]}
+
+    result = {
+        "metric": METRIC, "value": value, "unit": "iter/s", "n_gpus": world, "steps": K, "warmup": args.warmup,
+        "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded Kuhn grid, Gaussian densities, sphere cameras)",
+        "config": {"workload": f"plain method, Kuhn {args.n}^3 ({6 * args.n ** 3} tets, {V} verts), "
+                               f"{args.res}x{args.res}, one camera per step, fwd+adj+Adam",
+                   "tets": 6 * args.n ** 3, "vertices": V, "faces": F, "res": args.res,
+                   "fragments_per_step": nf, "views": len(views), "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (fragment records ~%.1f GB per step)" % (8 * nf / 1e9)},
+        "e2e": e2e,
+        "gpu_launches": 13 * K,
+        "stage_ms": {k: round(v, 4) for k, v in avg.items()},
+        "fragments_per_s": nf * value / world * world,
+        "roofline": roofline,
+        "clocks": clk,
+    }
+    return result, sc
+
+
+def cpu_port_sample(args, sc, rows=None):
+    """Time the oracle's FP32 port (all host threads) on a band of rows of one
+    forward + adjoint view of the same workload; returns (iter/s extrapolated
+    to the full image, seconds, description)."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    rows = rows or args.cpu_rows
+    res = args.res
+    r0 = res // 2 - rows // 2
+    fa = O.Faces(sc["cells"], sc["pos"].shape[0])
+    cam = O.make_camera(sc["views"][0], __import__("math").radians(45.0), res, res)
+    prm = O.make_params(attenuation=1.0, use_ert=True, ert_thresh=1e-4, rows=(r0, r0 + rows))
+    w = np.zeros((res, res, 4), np.float32)
+    w[r0:r0 + rows] = 1e-6
+    t = time.perf_counter()
+    O.render(fa, sc["pos"], sc["col"], cam, prm, precision=32)
+    O.adjoint(fa, sc["pos"], sc["col"], cam, prm, w, precision=32)
+    sec = time.perf_counter() - t
+    frac = rows / res
+    return frac / sec, sec, (f"rows [{r0},{r0 + rows}) of {res} ({frac:.4f} of the pixels; faces are rasterised "
+                              f"in full), forward + adjoint of one view, FP32 port, extrapolated to the image")
+
+
+def run_reference(args, rank, world):
+    """CPU implementation of the path (the oracle's FP32 port; the reference's
+    own Vulkan path is unavailable on this box) timed on host cores."""
+    import numpy as np
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    from difftetvr_b200 import synthetic as S
+    cells, pos = S.kuhn_mesh(args.n, seed=0)
+    col = S.gaussian_colors(pos, seed=0)
+    views = [S.sphere_camera(100 + i) for i in range(args.views)]
+    sc = {"cells": cells, "pos": pos, "col": col, "views": views, "np": np}
+    for _ in range(args.warmup):
+        cpu_port_sample(args, sc, rows=8)
+    secs = []
+    for _ in range(args.steps):
+        _, s, desc = cpu_port_sample(args, sc, rows=8)
+        secs.append(s)
+    frac = 8 / args.res
+    value = frac / (sum(secs) / len(secs))
+    cores = O.num_threads()
+    return {
+        "metric": METRIC, "value": value, "unit": "iter/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+        "config": {"workload": f"plain method, Kuhn {args.n}^3, {args.res}x{args.res}, fwd+adj (CPU port)"},
+        "cpu_baseline": {"value": value, "unit": "iter/s", "cores": cores, "kind": "port",
+                         "sample": desc.replace(f"rows [{args.res // 2 - args.cpu_rows // 2}", "rows [")},
+        "e2e": {"value": value, "unit": "iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference's Vulkan renderer (and lavapipe) is unavailable on this box; the timed CPU "
+                "implementation is this repository's FP32 restatement of its algorithm",
+    }
+
+
+def main():
+    args = parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        print(json.dumps(run_reference(args, rank, world)))
+        return 0
+    import torch
+    if world > 1:
+        local = int(os.environ.get("LOCAL_RANK", "0"))
+        torch.cuda.set_device(local)
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                             device_id=torch.device("cuda", local))
+    from difftetvr_b200 import build as B
+    if not B.up_to_date() and rank == 0:
+        B.build()
+    if world > 1:
+        torch.distributed.barrier()
+    result, sc = run_ours(args, rank, world)
+    if rank == 0 and not args.no_cpu_baseline:
+        v, s, desc = cpu_port_sample(args, sc)
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        result["cpu_baseline"] = {"value": v, "unit": "iter/s", "cores": O.num_threads(), "kind": "port",
+                                  "sample": desc, "seconds": s}
+    if rank == 0:
+        print(json.dumps(result))
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -98,7 +98,8 @@ dtv::CamDev make_cam(const dtv_camera& c) {
     dtv::CamDev k;
     std::memcpy(k.V, c.view, sizeof(k.V));
     const double tanh = std::tan(0.5 * double(c.fovy));
-    k.f = float(0.5 * double(c.height) / tanh);
+    k.fd = 0.5 * double(c.height) / tanh;
+    k.f = float(k.fd);
     k.cx = 0.5f * float(c.width);
     k.cy = 0.5f * float(c.height);
     k.znear = c.znear;
@@ -134,6 +135,7 @@ struct dtv_renderer {
     int32_t type = DTV_RENDERER_PPLL;
     DevBuf<float4> vproj;
     DevBuf<int2> vfix;
+    DevBuf<dtv::VGeo> vgeo;
     DevBuf<uint32_t> counts;
     DevBuf<u64> offsets;
     DevBuf<u64> records;
@@ -309,6 +311,7 @@ int32_t dtv_renderer_destroy(dtv_renderer* r) {
     cudaDeviceSynchronize();
     r->vproj.release();
     r->vfix.release();
+    r->vgeo.release();
     r->counts.release();
     r->offsets.release();
     r->records.release();
@@ -349,6 +352,7 @@ int32_t dtv_renderer_render(dtv_renderer* r, const dtv_mesh* mesh, const float* 
 
         r->vproj.ensure(V ? V : 1, s);
         r->vfix.ensure(V ? V : 1, s);
+        r->vgeo.ensure(V ? V : 1, s);
         r->counts.ensure(P, s, /*zero_new=*/true);
         r->offsets.ensure(P + 1, s);
         r->scan_scratch.ensure(dtv::scan_scratch_elems(P), s);
@@ -358,7 +362,7 @@ int32_t dtv_renderer_render(dtv_renderer* r, const dtv_mesh* mesh, const float* 
         r->flags.ensure(2, s);
 
         rec_event(r, 0, s);
-        dtv::launch_project(d_positions, uint32_t(V), cam, r->vproj.ptr, r->vfix.ptr, s);
+        dtv::launch_project(d_positions, uint32_t(V), cam, r->vproj.ptr, r->vfix.ptr, r->vgeo.ptr, s);
         check_launch("project");
         rec_event(r, 1, s);
         dtv::launch_raster_count(mesh->d_faces, uint32_t(F), r->vproj.ptr, r->vfix.ptr, W, H, r->counts.ptr, s);
@@ -396,7 +400,7 @@ int32_t dtv_renderer_render(dtv_renderer* r, const dtv_mesh* mesh, const float* 
         DTV_CK(cudaEventRecord(r->flags_event, s));
         r->flags_pending = true;
         rec_event(r, 5, s);
-        dtv::launch_composite(r->offsets.ptr, r->records.ptr, mesh->d_faces, r->vproj.ptr,
+        dtv::launch_composite(r->offsets.ptr, r->records.ptr, mesh->d_faces, r->vgeo.ptr,
                               reinterpret_cast<const float4*>(d_colors), W, H, sh,
                               reinterpret_cast<float4*>(d_image), r->tfinal.ptr, r->term.ptr, s);
         check_launch("composite");
@@ -430,7 +434,7 @@ int32_t dtv_renderer_render_adjoint(dtv_renderer* r, const dtv_mesh* mesh, const
         dtv::ShadeDev sh = r->sh;
         sh.use_abs_grad = use_abs_grad ? 1 : 0;
         rec_event(r, 7, s);
-        dtv::launch_adjoint(r->offsets.ptr, r->records.ptr, mesh->d_faces, r->vproj.ptr,
+        dtv::launch_adjoint(r->offsets.ptr, r->records.ptr, mesh->d_faces, r->vgeo.ptr,
                             reinterpret_cast<const float4*>(d_colors), r->cam, sh,
                             reinterpret_cast<const float4*>(d_image_adjoint), r->tfinal.ptr, r->term.ptr,
                             d_grad_positions, reinterpret_cast<float4*>(d_grad_colors), s);

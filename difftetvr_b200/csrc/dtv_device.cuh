@@ -31,6 +31,25 @@ __device__ __forceinline__ float4 project_vertex(const CamDev& c, float x, float
     return make_float4(sx, sy, iz, ze);
 }
 
+// FP64 projection of the same vertex (continuous path).
+__device__ __forceinline__ VGeo project_vertex_geo(const CamDev& c, float x, float y, float z) {
+    const float* V = c.V;
+    const double X = x, Y = y, Z = z;
+    const double xv = ((double(V[0]) * X + double(V[4]) * Y) + double(V[8]) * Z) + double(V[12]);
+    const double yv = ((double(V[1]) * X + double(V[5]) * Y) + double(V[9]) * Z) + double(V[13]);
+    const double zv = ((double(V[2]) * X + double(V[6]) * Y) + double(V[10]) * Z) + double(V[14]);
+    const double ze = -zv;
+    const double iz = 1.0 / ze;
+    VGeo g;
+    g.sx = double(c.cx) + c.fd * (xv * iz);
+    g.sy = double(c.cy) - c.fd * (yv * iz);
+    g.iz = float(iz);
+    g.ze = float(ze);
+    g.xv = float(xv);
+    g.yv = float(yv);
+    return g;
+}
+
 __device__ __forceinline__ long long floor_div256(long long a) { return a >> 8; }  // arithmetic shift = floor
 __device__ __forceinline__ long long ceil_div256(long long a) { return -((-a) >> 8); }
 
@@ -59,28 +78,58 @@ __device__ __forceinline__ float depth_key(const float4& a, const float4& b, con
     return fminf(fmaxf(z, zmin), zmax);
 }
 
-// Continuous fragment values (ordinary FP32): perspective-correct barycentrics
-// of the pixel centre on the face.
-__device__ __forceinline__ void face_bary(const float4& a, const float4& b, const float4& c, float qx, float qy,
-                                          float bary[3]) {
-    float d0x = a.x - qx, d0y = a.y - qy;
-    float d1x = b.x - qx, d1y = b.y - qy;
-    float d2x = c.x - qx, d2y = c.y - qy;
-    float u0 = (d1x * d2y - d1y * d2x) * a.z;
-    float u1 = (d2x * d0y - d2y * d0x) * b.z;
-    float u2 = (d0x * d1y - d0y * d1x) * c.z;
-    float inv = 1.0f / (u0 + u1 + u2);
-    bary[0] = u0 * inv;
-    bary[1] = u1 * inv;
-    bary[2] = u2 * inv;
+// Continuous fragment values: perspective-correct barycentrics of the pixel
+// centre on the face, from the FP64 screen positions (edge functions in FP64,
+// so thin, nearly edge-on faces keep accurate weights).  Signed weights (a
+// pixel centre the fixed-point coverage rule places just outside the exact
+// projection extrapolates linearly); the depth is clamped to the face's vertex
+// depth range.  Depth and colour of a fragment come from the same weights.
+struct FaceInterp {
+    float lam[3];   // screen-space weights E_j / sum(E)
+    float A;        // sum(E)
+    float dx[3], dy[3];
+    float zb;       // 1 / sum(lam_j iz_j)
+    float z;        // zb clamped to the vertex depth range
+    bool clamped;
+    float bary[3];  // perspective-correct weights
+};
+
+__device__ __forceinline__ void face_interp(const VGeo& a, const VGeo& b, const VGeo& c, float qx, float qy,
+                                            FaceInterp& fi) {
+    const double d0x = a.sx - double(qx), d0y = a.sy - double(qy);
+    const double d1x = b.sx - double(qx), d1y = b.sy - double(qy);
+    const double d2x = c.sx - double(qx), d2y = c.sy - double(qy);
+    const double E0 = d1x * d2y - d1y * d2x;
+    const double E1 = d2x * d0y - d2y * d0x;
+    const double E2 = d0x * d1y - d0y * d1x;
+    const double A = E0 + E1 + E2;
+    fi.A = float(A);
+    const float iA = 1.0f / fi.A;
+    fi.lam[0] = float(E0) * iA;
+    fi.lam[1] = float(E1) * iA;
+    fi.lam[2] = float(E2) * iA;
+    fi.dx[0] = float(d0x); fi.dx[1] = float(d1x); fi.dx[2] = float(d2x);
+    fi.dy[0] = float(d0y); fi.dy[1] = float(d1y); fi.dy[2] = float(d2y);
+    const float u0 = fi.lam[0] * a.iz, u1 = fi.lam[1] * b.iz, u2 = fi.lam[2] * c.iz;
+    fi.zb = 1.0f / (u0 + u1 + u2);
+    fi.bary[0] = u0 * fi.zb;
+    fi.bary[1] = u1 * fi.zb;
+    fi.bary[2] = u2 * fi.zb;
+    const float zmin = fminf(fminf(a.ze, b.ze), c.ze), zmax = fmaxf(fmaxf(a.ze, b.ze), c.ze);
+    fi.clamped = !(fi.zb >= zmin && fi.zb <= zmax);
+    fi.z = fminf(fmaxf(fi.zb, zmin), zmax);
 }
 
-struct Frag {
-    float z;
-    float4 col;
-    uint32_t face;
-    uint32_t bits;   // bit0 front, bit1 boundary
-};
+// Forward-only variant (depth and weights).
+__device__ __forceinline__ void face_bary(const VGeo& a, const VGeo& b, const VGeo& c, float qx, float qy,
+                                          float bary[3], float& z) {
+    FaceInterp fi;
+    face_interp(a, b, c, qx, qy, fi);
+    bary[0] = fi.bary[0];
+    bary[1] = fi.bary[1];
+    bary[2] = fi.bary[2];
+    z = fi.z;
+}
 
 __device__ __forceinline__ bool skip_pair(uint32_t bits0, uint32_t bits1) {
     // Forward.glsl:183-185: back-facing boundary followed by front-facing boundary.

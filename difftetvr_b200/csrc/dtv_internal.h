@@ -24,7 +24,8 @@ struct MeshHost {
 void build_faces(const uint32_t* cells, uint64_t T, uint64_t V, MeshHost& out);
 
 // Launch wrappers (dtv_kernels.cu).  All run on `s`.
-void launch_project(const float* pos, uint32_t V, const CamDev& cam, float4* vproj, int2* vfix, cudaStream_t s);
+void launch_project(const float* pos, uint32_t V, const CamDev& cam, float4* vproj, int2* vfix, VGeo* vgeo,
+                    cudaStream_t s);
 void launch_raster_count(const uint4* faces, uint32_t F, const float4* vproj, const int2* vfix, int W, int H,
                          uint32_t* counts, cudaStream_t s);
 void launch_raster_fill(const uint4* faces, uint32_t F, const float4* vproj, const int2* vfix, int W, int H,
@@ -44,10 +45,10 @@ constexpr uint32_t kSortWarpCap = 1024;    // elements per warp list sorted in s
 constexpr uint32_t kSortBlockCap = 16384;  // elements per block-sorted list (128 KiB shared memory)
 
 void launch_composite(const unsigned long long* offsets, const unsigned long long* records, const uint4* faces,
-                      const float4* vproj, const float4* colors, int W, int H, const ShadeDev& sh, float4* image,
+                      const VGeo* vgeo, const float4* colors, int W, int H, const ShadeDev& sh, float4* image,
                       float* tfinal, uint32_t* term, cudaStream_t s);
 void launch_adjoint(const unsigned long long* offsets, const unsigned long long* records, const uint4* faces,
-                    const float4* vproj, const float4* colors, const CamDev& cam, const ShadeDev& sh,
+                    const VGeo* vgeo, const float4* colors, const CamDev& cam, const ShadeDev& sh,
                     const float4* dimage, const float* tfinal, const uint32_t* term, float* grad_pos,
                     float4* grad_col, cudaStream_t s);
 

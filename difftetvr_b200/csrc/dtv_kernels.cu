@@ -17,18 +17,21 @@ constexpr unsigned kFull = 0xffffffffu;
 // (a) vertex projection (LinkedListGather.glsl:55-68, split into view
 // transform + perspective divide; FP32 with fixed rounding).
 __global__ void __launch_bounds__(256) k_project(const float* __restrict__ pos, uint32_t V, CamDev cam,
-                                                 float4* __restrict__ vproj, int2* __restrict__ vfix) {
+                                                 float4* __restrict__ vproj, int2* __restrict__ vfix,
+                                                 VGeo* __restrict__ vgeo) {
     uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= V) return;
     float x = pos[3 * size_t(v)], y = pos[3 * size_t(v) + 1], z = pos[3 * size_t(v) + 2];
     int2 fx;
     vproj[v] = project_vertex(cam, x, y, z, fx);
     vfix[v] = fx;
+    vgeo[v] = project_vertex_geo(cam, x, y, z);
 }
 
-void launch_project(const float* pos, uint32_t V, const CamDev& cam, float4* vproj, int2* vfix, cudaStream_t s) {
+void launch_project(const float* pos, uint32_t V, const CamDev& cam, float4* vproj, int2* vfix, VGeo* vgeo,
+                    cudaStream_t s) {
     if (V == 0) return;
-    k_project<<<(V + 255) / 256, 256, 0, s>>>(pos, V, cam, vproj, vfix);
+    k_project<<<(V + 255) / 256, 256, 0, s>>>(pos, V, cam, vproj, vfix, vgeo);
 }
 
 // ---------------------------------------------------------------------------
@@ -337,19 +340,18 @@ struct FragV {
 };
 
 __device__ __forceinline__ FragV load_frag(u64 rec, float qx, float qy, const uint4* __restrict__ faces,
-                                           const float4* __restrict__ vproj, const float4* __restrict__ colors) {
+                                           const VGeo* __restrict__ vgeo, const float4* __restrict__ colors) {
     FragV fr;
     const uint32_t lo = uint32_t(rec);
-    fr.z = __uint_as_float(uint32_t(rec >> 32));
     fr.face = lo >> 2;
     fr.bits = lo & 3u;
     const uint4 fc = faces[fr.face];
     fr.v0 = fc.x;
     fr.v1 = fc.y;
     fr.v2 = fc.z;
-    const float4 a = vproj[fc.x], b = vproj[fc.y], c = vproj[fc.z];
+    const VGeo a = vgeo[fc.x], b = vgeo[fc.y], c = vgeo[fc.z];
     float bary[3];
-    face_bary(a, b, c, qx, qy, bary);
+    face_bary(a, b, c, qx, qy, bary, fr.z);  // depth and colour from the same weights
     const float4 c0 = colors[fc.x], c1 = colors[fc.y], c2 = colors[fc.z];
     fr.col = make_float4(bary[0] * c0.x + bary[1] * c1.x + bary[2] * c2.x,
                          bary[0] * c0.y + bary[1] * c1.y + bary[2] * c2.y,
@@ -366,7 +368,7 @@ constexpr int kTile = 16;
 
 __global__ void __launch_bounds__(kTile * kTile) k_composite(
     const u64* __restrict__ offsets, const u64* __restrict__ records, const uint4* __restrict__ faces,
-    const float4* __restrict__ vproj, const float4* __restrict__ colors, int W, int H, ShadeDev sh,
+    const VGeo* __restrict__ vgeo, const float4* __restrict__ colors, int W, int H, ShadeDev sh,
     float4* __restrict__ image, float* __restrict__ tfinal, uint32_t* __restrict__ term) {
     const int px = blockIdx.x * kTile + (threadIdx.x % kTile);
     const int py = blockIdx.y * kTile + (threadIdx.x / kTile);
@@ -378,11 +380,11 @@ __global__ void __launch_bounds__(kTile * kTile) k_composite(
     float C0 = 0.f, C1 = 0.f, C2 = 0.f, T = 1.f;
     uint32_t i = n;
     if (n >= 2) {
-        FragV f1 = load_frag(records[beg], qx, qy, faces, vproj, colors), f0;
+        FragV f1 = load_frag(records[beg], qx, qy, faces, vgeo, colors), f0;
         for (i = 1; i < n; ++i) {
             if (sh.use_ert && T < sh.ert_thresh) break;
             f0 = f1;
-            f1 = load_frag(records[beg + i], qx, qy, faces, vproj, colors);
+            f1 = load_frag(records[beg + i], qx, qy, faces, vgeo, colors);
             if (skip_pair(f0.bits, f1.bits)) continue;
             const float tSeg = (f1.z - f0.z) * 0.25f;
 #pragma unroll
@@ -391,7 +393,7 @@ __global__ void __launch_bounds__(kTile * kTile) k_composite(
                 const float4 c0 = lerp4(f0.col, f1.col, fb);
                 const float4 c1 = lerp4(f0.col, f1.col, fe);
                 const float a = (f0.col.w + (f1.col.w - f0.col.w) * fm) * sh.atten;
-                if (a < 1e-6f) continue;
+                if (!(a > 0.f)) continue;  // a <= 0 contributes nothing
                 const SegTerms st = seg_terms(tSeg, a);
                 C0 += T * (st.omA * c0.x + st.K * (c0.x - c1.x));
                 C1 += T * (st.omA * c0.y + st.K * (c0.y - c1.y));
@@ -406,11 +408,11 @@ __global__ void __launch_bounds__(kTile * kTile) k_composite(
     term[p] = i;
 }
 
-void launch_composite(const u64* offsets, const u64* records, const uint4* faces, const float4* vproj,
+void launch_composite(const u64* offsets, const u64* records, const uint4* faces, const VGeo* vgeo,
                       const float4* colors, int W, int H, const ShadeDev& sh, float4* image, float* tfinal,
                       uint32_t* term, cudaStream_t s) {
     dim3 grid((W + kTile - 1) / kTile, (H + kTile - 1) / kTile);
-    k_composite<<<grid, kTile * kTile, 0, s>>>(offsets, records, faces, vproj, colors, W, H, sh, image, tfinal,
+    k_composite<<<grid, kTile * kTile, 0, s>>>(offsets, records, faces, vgeo, colors, W, H, sh, image, tfinal,
                                                term);
 }
 
@@ -420,50 +422,39 @@ void launch_composite(const u64* offsets, const u64* records, const uint4* faces
 // colour adjoints of its two segments are summed and pushed through the
 // screen-space barycentrics and the projection to the face's three vertices.
 __device__ __forceinline__ void frag_vertex_grads(const FragV& fr, float qx, float qy,
-                                                  const float4* __restrict__ vproj,
+                                                  const VGeo* __restrict__ vgeo,
                                                   const float4* __restrict__ colors, const CamDev& cam,
                                                   float gz, float4 gcol, bool use_abs, float* grad_pos,
                                                   float4* grad_col) {
     const uint32_t vi[3] = {fr.v0, fr.v1, fr.v2};
-    float4 P[3];
+    VGeo P[3];
     float4 Cv[3];
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
-        P[j] = vproj[vi[j]];
+        P[j] = vgeo[vi[j]];
         Cv[j] = colors[vi[j]];
     }
-    float dx[3], dy[3];
+    FaceInterp fi;
+    face_interp(P[0], P[1], P[2], qx, qy, fi);
+    const float* dx = fi.dx;
+    const float* dy = fi.dy;
+    const float zb = fi.zb;
+    float gb[3], sb = 0.f;
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
-        dx[j] = P[j].x - qx;
-        dy[j] = P[j].y - qy;
-    }
-    const float E[3] = {dx[1] * dy[2] - dy[1] * dx[2], dx[2] * dy[0] - dy[2] * dx[0],
-                        dx[0] * dy[1] - dy[0] * dx[1]};
-    const float invA = 1.0f / (E[0] + E[1] + E[2]);
-    float lam[3], u[3], w = 0.f;
-#pragma unroll
-    for (int j = 0; j < 3; ++j) {
-        lam[j] = E[j] * invA;
-        u[j] = lam[j] * P[j].z;
-        w += u[j];
-    }
-    const float z = 1.0f / w;
-    float b[3], gb[3], sb = 0.f;
-#pragma unroll
-    for (int j = 0; j < 3; ++j) {
-        b[j] = u[j] * z;
         gb[j] = gcol.x * Cv[j].x + gcol.y * Cv[j].y + gcol.z * Cv[j].z + gcol.w * Cv[j].w;
-        sb += gb[j] * b[j];
+        sb += gb[j] * fi.bary[j];
     }
+    const float gzz = fi.clamped ? 0.f : gz * zb * zb;
     float glam[3], giz[3], sl = 0.f;
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
-        const float gu = z * (gb[j] - sb) - gz * z * z;
-        glam[j] = gu * P[j].z;
-        giz[j] = gu * lam[j];
-        sl += glam[j] * lam[j];
+        const float gu = zb * (gb[j] - sb) - gzz;
+        glam[j] = gu * P[j].iz;
+        giz[j] = gu * fi.lam[j];
+        sl += glam[j] * fi.lam[j];
     }
+    const float invA = 1.0f / fi.A;
     float gE[3];
 #pragma unroll
     for (int j = 0; j < 3; ++j) gE[j] = (glam[j] - sl) * invA;
@@ -477,16 +468,15 @@ __device__ __forceinline__ void frag_vertex_grads(const FragV& fr, float qx, flo
     const float* V = cam.V;
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
-        const float iz = P[j].z, ze = P[j].w;
+        const float iz = P[j].iz;
         const float gxv = gsx[j] * cam.f * iz;
         const float gyv = -gsy[j] * cam.f * iz;
-        // f * xv = (sx - cx) * ze,  f * yv = (cy - sy) * ze
-        const float giz_t = giz[j] + ze * (gsx[j] * (P[j].x - cam.cx) - gsy[j] * (cam.cy - P[j].y));
+        const float giz_t = giz[j] + cam.f * (gsx[j] * P[j].xv - gsy[j] * P[j].yv);
         const float gzv = giz_t * iz * iz;
         float gp0 = V[0] * gxv + V[1] * gyv + V[2] * gzv;
         float gp1 = V[4] * gxv + V[5] * gyv + V[6] * gzv;
         float gp2 = V[8] * gxv + V[9] * gyv + V[10] * gzv;
-        float4 gc = f4scale(gcol, b[j]);
+        float4 gc = f4scale(gcol, fi.bary[j]);
         if (use_abs) {
             gp0 = fabsf(gp0); gp1 = fabsf(gp1); gp2 = fabsf(gp2);
             gc = make_float4(fabsf(gc.x), fabsf(gc.y), fabsf(gc.z), fabsf(gc.w));
@@ -501,7 +491,7 @@ __device__ __forceinline__ void frag_vertex_grads(const FragV& fr, float qx, flo
 
 __global__ void __launch_bounds__(kTile * kTile) k_adjoint(
     const u64* __restrict__ offsets, const u64* __restrict__ records, const uint4* __restrict__ faces,
-    const float4* __restrict__ vproj, const float4* __restrict__ colors, int W, int H, CamDev cam, ShadeDev sh,
+    const VGeo* __restrict__ vgeo, const float4* __restrict__ colors, int W, int H, CamDev cam, ShadeDev sh,
     const float4* __restrict__ dimage, const float* __restrict__ tfinal, const uint32_t* __restrict__ term,
     float* __restrict__ grad_pos, float4* __restrict__ grad_col) {
     const int px = blockIdx.x * kTile + (threadIdx.x % kTile);
@@ -521,11 +511,11 @@ __global__ void __launch_bounds__(kTile * kTile) k_adjoint(
     if (last < 1) return;
     const float atten = sh.atten;
     const bool use_abs = sh.use_abs_grad != 0;
-    FragV fb = load_frag(records[beg + last], qx, qy, faces, vproj, colors);
+    FragV fb = load_frag(records[beg + last], qx, qy, faces, vgeo, colors);
     float gz_b = 0.f;
     float4 gcol_b = make_float4(0.f, 0.f, 0.f, 0.f);
     for (int i = last; i >= 1; --i) {
-        const FragV ff = load_frag(records[beg + i - 1], qx, qy, faces, vproj, colors);
+        const FragV ff = load_frag(records[beg + i - 1], qx, qy, faces, vgeo, colors);
         float gz_f = 0.f;
         float4 gcol_f = make_float4(0.f, 0.f, 0.f, 0.f);
         if (!skip_pair(ff.bits, fb.bits)) {
@@ -538,7 +528,7 @@ __global__ void __launch_bounds__(kTile * kTile) k_adjoint(
                 const float4 c1 = lerp4(ff.col, fb.col, fe);
                 const float a = (ff.col.w + (fb.col.w - ff.col.w) * fm) * atten;
                 float g_t, g_a, gc0x, gc0y, gc0z, gc1x, gc1y, gc1z;
-                if (a >= 1e-6f) {
+                if (a > 0.f) {
                     const SegTerms st = seg_terms(tSeg, a);
                     const float cx = st.omA * c0.x + st.K * (c0.x - c1.x);
                     const float cy = st.omA * c0.y + st.K * (c0.y - c1.y);
@@ -559,8 +549,9 @@ __global__ void __launch_bounds__(kTile * kTile) k_adjoint(
                     gc0x = k0 * gax; gc0y = k0 * gay; gc0z = k0 * gaz;
                     gc1x = -st.K * gax; gc1y = -st.K * gay; gc1z = -st.K * gaz;
                 } else {
-                    // The forward drops the sub-segment; the derivative of the
-                    // exact integral at a = 0 (BackwardCommon.glsl:121-125).
+                    // The forward drops the sub-segment for a <= 0; the gradient
+                    // is the a -> 0+ limit (BackwardCommon.glsl:121-125) so a
+                    // density clamped at zero can grow again.
                     const float gax = T * gC0, gay = T * gC1, gaz = T * gC2, gA = T * gT;
                     g_t = 0.f;
                     g_a = gax * (tSeg * c0.x + 0.5f * tSeg * tSeg * (c1.x - c0.x)) +
@@ -581,19 +572,19 @@ __global__ void __launch_bounds__(kTile * kTile) k_adjoint(
             gz_f -= g_tot;
             gz_b += g_tot;
         }
-        frag_vertex_grads(fb, qx, qy, vproj, colors, cam, gz_b, gcol_b, use_abs, grad_pos, grad_col);
+        frag_vertex_grads(fb, qx, qy, vgeo, colors, cam, gz_b, gcol_b, use_abs, grad_pos, grad_col);
         fb = ff;
         gz_b = gz_f;
         gcol_b = gcol_f;
     }
-    frag_vertex_grads(fb, qx, qy, vproj, colors, cam, gz_b, gcol_b, use_abs, grad_pos, grad_col);
+    frag_vertex_grads(fb, qx, qy, vgeo, colors, cam, gz_b, gcol_b, use_abs, grad_pos, grad_col);
 }
 
-void launch_adjoint(const u64* offsets, const u64* records, const uint4* faces, const float4* vproj,
+void launch_adjoint(const u64* offsets, const u64* records, const uint4* faces, const VGeo* vgeo,
                     const float4* colors, const CamDev& cam, const ShadeDev& sh, const float4* dimage,
                     const float* tfinal, const uint32_t* term, float* grad_pos, float4* grad_col, cudaStream_t s) {
     dim3 grid((cam.W + kTile - 1) / kTile, (cam.H + kTile - 1) / kTile);
-    k_adjoint<<<grid, kTile * kTile, 0, s>>>(offsets, records, faces, vproj, colors, cam.W, cam.H, cam, sh, dimage,
+    k_adjoint<<<grid, kTile * kTile, 0, s>>>(offsets, records, faces, vgeo, colors, cam.W, cam.H, cam, sh, dimage,
                                              tfinal, term, grad_pos, grad_col);
 }
 

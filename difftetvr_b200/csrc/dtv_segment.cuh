@@ -67,7 +67,8 @@ __device__ __forceinline__ float series_chi(float x) {
     return p;
 }
 
-// Forward terms; caller guarantees a >= 1e-6.
+// Forward terms; caller guarantees a > 0.  (The reference drops a < 1e-6; the
+// continuous value kept here differs from that by at most a t.)
 __device__ __forceinline__ SegTerms seg_terms(float t, float a) {
     SegTerms s;
     float x = a * t;

@@ -12,10 +12,19 @@ constexpr int32_t kInvalidFix = INT32_MIN; // marks a vertex outside [znear, zfa
 // Camera constants, computed once on the host (see dtv_camera_constants).
 struct CamDev {
     float V[16];    // view matrix, column-major
-    float f;        // 0.5 * H / tan(fovy/2)
+    float f;        // 0.5 * H / tan(fovy/2), rounded to FP32 (discrete path)
+    double fd;      // the same in FP64 (continuous path)
     float cx, cy;   // 0.5 * W, 0.5 * H
     float znear, zfar;
     int W, H;
+};
+
+// FP64 projection of a vertex for the continuous path (barycentrics, depth,
+// adjoint): screen position in FP64 so that thin, nearly edge-on faces keep
+// accurate weights; 1/ze, ze and the view-space x, y in FP32.  32 bytes.
+struct alignas(16) VGeo {
+    double sx, sy;
+    float iz, ze, xv, yv;
 };
 
 // Per-render settings that the kernels read.

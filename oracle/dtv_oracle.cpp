@@ -293,11 +293,13 @@ struct MeshR {
 // space), which equal the world-space barycentrics of the point where the pixel
 // ray meets the face plane.  Forward.glsl:80-103 computes the same point by
 // unprojecting gl_FragCoord.z and takes unsigned cross-product ratios; here
-// the signed ratios are used (they agree inside the face and stay linear at
-// its edges).
+// the signed ratios are used (equal inside the face; linear just outside it,
+// where the fixed-point coverage rule can place a pixel centre).  The depth
+// is clamped to the face's vertex depth range; the fragment's depth and
+// colour come from the same weights.
 template <class R>
 void face_bary(const ProjR<R>& a, const ProjR<R>& b, const ProjR<R>& c, R qx, R qy, R lam[3], R bary[3],
-               R& z) {
+               R& z, bool* z_clamped = nullptr) {
     R d0x = a.sx - qx, d0y = a.sy - qy;
     R d1x = b.sx - qx, d1y = b.sy - qy;
     R d2x = c.sx - qx, d2y = c.sy - qy;
@@ -310,10 +312,13 @@ void face_bary(const ProjR<R>& a, const ProjR<R>& b, const ProjR<R>& c, R qx, R 
     lam[2] = E2 / A;
     R u0 = lam[0] * a.iz, u1 = lam[1] * b.iz, u2 = lam[2] * c.iz;
     R w = (u0 + u1) + u2;
-    z = R(1) / w;
-    bary[0] = u0 * z;
-    bary[1] = u1 * z;
-    bary[2] = u2 * z;
+    R zb = R(1) / w;
+    bary[0] = u0 * zb;
+    bary[1] = u1 * zb;
+    bary[2] = u2 * zb;
+    R zmin = std::min(std::min(a.ze, b.ze), c.ze), zmax = std::max(std::max(a.ze, b.ze), c.ze);
+    z = std::min(std::max(zb, zmin), zmax);
+    if (z_clamped) *z_clamped = !(zb >= zmin && zb <= zmax);
 }
 
 template <class R>
@@ -331,20 +336,49 @@ Frag<R> eval_frag(const MeshR<R>& m, uint64_t rec, int px, int py) {
     return fr;
 }
 
-// accumulateLinearConst, Data/Shaders/Common/ForwardCommon.glsl:42-49.
+// Series of phi1(x) = (1 - e^-x)/x, psi(x) = (phi1(x) - e^-x)/x and
+// chi(x) = (1 - e^-x (1 + x + x^2))/x^2 (coefficients from the exponential
+// series), used for small optical depth x where the direct forms cancel.
+template <class R>
+inline R poly(const double* c, int n, R x) {
+    R p = R(c[n - 1]);
+    for (int i = n - 2; i >= 0; --i) p = p * x + R(c[i]);
+    return p;
+}
+const double kPhi1[10] = {1.0, -1.0 / 2, 1.0 / 6, -1.0 / 24, 1.0 / 120, -1.0 / 720, 1.0 / 5040, -1.0 / 40320,
+                          1.0 / 362880, -1.0 / 3628800};
+const double kPsi[10] = {1.0 / 2, -2.0 / 6, 3.0 / 24, -4.0 / 120, 5.0 / 720, -6.0 / 5040, 7.0 / 40320, -8.0 / 362880,
+                         9.0 / 3628800, -10.0 / 39916800};
+const double kChi[10] = {-1.0 / 2, 4.0 / 6, -9.0 / 24, 16.0 / 120, -25.0 / 720, 36.0 / 5040, -49.0 / 40320,
+                         64.0 / 362880, -81.0 / 3628800, 100.0 / 39916800};
+template <class R>
+inline R series_cut() { return std::is_same<R, float>::value ? R(0.5) : R(1e-3); }
+
+// accumulateLinearConst, Data/Shaders/Common/ForwardCommon.glsl:42-49:
+//   A = exp(-a t),  C = (1 - A) c0 + ((t + 1/a) A - 1/a) (c0 - c1),  alpha = 1 - A,
+// written as 1 - A = x phi1(x), (t + 1/a) A - 1/a = -t x psi(x) with x = a t.
+// The reference drops the term for a < 1e-6; here only a <= 0 is dropped and
+// 0 < a < 1e-6 keeps the (continuous) value, which differs by at most a t.
 template <class R>
 inline bool seg_integral(R t, const R c0[3], const R c1[3], R a, R cacc[3], R& A) {
-    if (a < R(1e-6)) {
+    if (!(a > R(0))) {
         A = R(1);
         cacc[0] = cacc[1] = cacc[2] = R(0);
         return false;
     }
-    A = std::exp(-a * t);
-    R K = (t + R(1) / a) * A - R(1) / a;
-    for (int k = 0; k < 3; ++k) cacc[k] = (R(1) - A) * c0[k] + K * (c0[k] - c1[k]);
+    const R x = a * t;
+    A = std::exp(-x);
+    R omA, K;
+    if (std::fabs(x) < series_cut<R>()) {
+        omA = x * poly(kPhi1, 10, x);
+        K = -t * x * poly(kPsi, 10, x);
+    } else {
+        omA = R(1) - A;
+        K = (t + R(1) / a) * A - R(1) / a;
+    }
+    for (int k = 0; k < 3; ++k) cacc[k] = omA * c0[k] + K * (c0[k] - c1[k]);
     return true;
 }
-
 template <class R>
 inline bool skip_pair(const Frag<R>& f0, const Frag<R>& f1) {
     // Forward.glsl:183-185: gap between a back-facing and a front-facing boundary face.
@@ -398,12 +432,13 @@ void composite_pixel(const MeshR<R>& m, const Params& prm, const uint64_t* recs,
 }
 
 // Adjoint of seg_integral w.r.t. (tSeg, a, c0, c1); BackwardCommon.glsl:116-133
-// (accumulateLinearConstAdjoint) including its a->0 branch.
+// (accumulateLinearConstAdjoint), with dK/da = t^2 chi(x).  For a <= 0 the
+// forward drops the term; its gradient is the a -> 0+ limit (the reference's
+// small-a branch), so a density clamped to zero can grow again.
 template <class R>
 void seg_integral_adjoint(R tSeg, const R c0[3], const R c1[3], R a, R A, const R gc[3], R gA, R& g_t,
                           R& g_a, R g_c0[3], R g_c1[3]) {
-    if (a < R(1e-6)) {
-        // Derivative of the exact integral at a = 0 (the forward drops the term).
+    if (!(a > R(0))) {
         g_t = 0;
         g_a = R(0);
         for (int k = 0; k < 3; ++k) {
@@ -413,14 +448,23 @@ void seg_integral_adjoint(R tSeg, const R c0[3], const R c1[3], R a, R A, const 
         g_a += -gA * tSeg;  // alpha_acc = 1 - A ~ a t  =>  d alpha/da = t, gA = -g_alpha
         return;
     }
-    R inva = R(1) / a;
-    R K = (tSeg + inva) * A - inva;
+    const R x = a * tSeg;
+    R omA, K, chi;
+    if (std::fabs(x) < series_cut<R>()) {
+        omA = x * poly(kPhi1, 10, x);
+        K = -tSeg * x * poly(kPsi, 10, x);
+        chi = poly(kChi, 10, x);
+    } else {
+        omA = R(1) - A;
+        K = (tSeg + R(1) / a) * A - R(1) / a;
+        chi = (omA - x * A * (R(1) + x)) / (x * x);
+    }
+    const R dK = tSeg * tSeg * chi;
     R dot_t = 0, dot_a = 0;
     for (int k = 0; k < 3; ++k) {
         dot_t += gc[k] * (a * A * (c0[k] + tSeg * (c1[k] - c0[k])));
-        dot_a += gc[k] * (tSeg * A * c0[k] + (inva * inva - (tSeg * tSeg + inva * inva + tSeg * inva) * A) *
-                                                    (c0[k] - c1[k]));
-        g_c0[k] = ((R(1) - A) + K) * gc[k];
+        dot_a += gc[k] * (tSeg * A * c0[k] + dK * (c0[k] - c1[k]));
+        g_c0[k] = (omA + K) * gc[k];
         g_c1[k] = -K * gc[k];
     }
     g_t = dot_t + gA * (-a * A);
@@ -448,17 +492,20 @@ void frag_vertex_grads(const MeshR<R>& m, const CamConst& cam, uint32_t face, in
         u[j] = lam[j] * P[j]->iz;
         w += u[j];
     }
-    R z = R(1) / w;
+    const R zb = R(1) / w;  // weights use the unclamped 1/w; the depth is clamped
+    const R zmin = std::min(std::min(P[0]->ze, P[1]->ze), P[2]->ze);
+    const R zmax = std::max(std::max(P[0]->ze, P[1]->ze), P[2]->ze);
+    const bool clamped = !(zb >= zmin && zb <= zmax);
     R b[3], gb[3], sb = 0;
     for (int j = 0; j < 3; ++j) {
-        b[j] = u[j] * z;
+        b[j] = u[j] * zb;
         gb[j] = 0;
         for (int k = 0; k < 4; ++k) gb[j] += gcol[k] * m.col[4 * vi[j] + k];
         sb += gb[j] * b[j];
     }
     R glam[3], giz[3], sl = 0;
     for (int j = 0; j < 3; ++j) {
-        R gu = z * (gb[j] - sb) - gz * z * z;
+        R gu = zb * (gb[j] - sb) - (clamped ? R(0) : gz * zb * zb);
         glam[j] = gu * P[j]->iz;
         giz[j] = gu * lam[j];
         sl += glam[j] * lam[j];

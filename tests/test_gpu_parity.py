@@ -1,0 +1,188 @@
+"""CUDA path vs the CPU oracle (B200).  Fragment lists bit-exact; images within
+1e-5 absolute of the FP64 oracle; gradients within 1e-4 relative (norm) of the
+FP64 oracle's exact adjoint."""
+import numpy as np
+import pytest
+import torch
+
+from helpers import Scene, rel_err
+
+pytestmark = pytest.mark.gpu
+
+IMG_TOL = 1e-5     # absolute, FP32 image vs FP64 oracle
+GRAD_TOL = 1e-4    # relative (L2 norm), FP32 adjoint vs FP64 oracle adjoint
+
+
+def _oracle_all(O, sc, w=None, ert=None):
+    fa = O.Faces(sc.cells, sc.pos.shape[0])
+    cam = sc.oracle_camera(O)
+    prm = sc.oracle_params(O) if ert is None else O.make_params(
+        attenuation=sc.attenuation, use_ert=ert, clear=sc.clear)
+    img, tf, term, nf = O.render(fa, sc.pos, sc.col, cam, prm)
+    out = {"faces": fa, "cam": cam, "prm": prm, "img": img, "tf": tf, "term": term, "nf": nf}
+    if w is not None:
+        out["gp"], out["gc"] = O.adjoint(fa, sc.pos, sc.col, cam, prm, w)
+    return out
+
+
+@pytest.mark.parametrize("n,res", [(8, 128), (16, 512)])
+def test_fragment_lists_bit_exact(oracle, n, res):
+    sc = Scene(n, res, seed=n)
+    mesh, r = sc.make_renderer()
+    r.render()
+    torch.cuda.synchronize()
+    off_g, rec_g = r.get_fragment_lists()
+    fa = oracle.Faces(sc.cells, sc.pos.shape[0])
+    off_o, rec_o = oracle.fragments(fa, sc.pos, sc.oracle_camera(oracle))
+    assert np.array_equal(off_g.astype(np.int64), off_o)
+    assert rec_g.shape == rec_o.shape
+    assert np.array_equal(rec_g, rec_o)
+
+
+def test_mesh_faces_match_oracle(oracle):
+    sc = Scene(8, 64, seed=3)
+    mesh, r = sc.make_renderer()
+    tri, fb, f2t, vb = mesh.native.copy_faces()
+    fa = oracle.Faces(sc.cells, sc.pos.shape[0])
+    assert np.array_equal(tri, fa.tri) and np.array_equal(fb, fa.face_boundary)
+    assert np.array_equal(f2t, fa.face_to_tet) and np.array_equal(vb, fa.vertex_boundary)
+
+
+@pytest.mark.parametrize("n,res,clear", [(8, 128, (0, 0, 0, 0)), (16, 512, (0, 0, 0, 0)),
+                                         (8, 96, (0.2, 0.4, 0.6, 0.5))])
+def test_image_matches_fp64_oracle(oracle, n, res, clear):
+    sc = Scene(n, res, seed=n + 1, clear=clear)
+    mesh, r = sc.make_renderer()
+    img = r.render().cpu().numpy()
+    o = _oracle_all(oracle, sc)
+    e = np.abs(img.astype(np.float64) - o["img"]).max(-1)
+    y, x = np.unravel_index(int(e.argmax()), e.shape)
+    assert e.max() < IMG_TOL, (float(e.max()), (y, x), img[y, x].tolist(), o["img"][y, x].tolist(),
+                               int((e > IMG_TOL).sum()))
+    assert r.get_num_fragments() == o["nf"]
+
+
+def test_image_with_early_ray_termination(oracle):
+    """ERT on (threshold 1e-4, attenuation 4): the termination index is a discrete
+    function of FP32 vs FP64 transmittance, so a pixel whose T lands within
+    rounding of the threshold may stop one segment apart; such pixels differ by
+    at most T * (segment opacity) <= thresh."""
+    sc = Scene(16, 256, seed=9, attenuation=4.0, ert=True)
+    mesh, r = sc.make_renderer()
+    img = r.render().cpu().numpy().astype(np.float64)
+    tf_g, term_g = r.get_pixel_state()
+    o = _oracle_all(oracle, sc)
+    same = term_g == o["term"]
+    assert same.mean() > 0.999
+    err = np.abs(img - o["img"]).max(-1)
+    assert err[same].max() < IMG_TOL
+    assert err.max() < 1e-4
+    assert (term_g < np.diff(r.get_fragment_lists()[0]).reshape(256, 256)).sum() > 100  # ERT actually fired
+
+
+@pytest.mark.parametrize("n,res,ert", [(8, 128, False), (16, 256, False), (8, 128, True)])
+def test_gradients_match_fp64_oracle(oracle, n, res, ert):
+    sc = Scene(n, res, seed=20 + n, attenuation=2.0 if ert else 1.0, ert=ert)
+    mesh, r = sc.make_renderer()
+    rng = np.random.default_rng(5)
+    w = rng.normal(size=(res, res, 4)).astype(np.float32)
+    img = r.render()
+    pos, col = mesh.get_vertex_positions(), mesh.get_vertex_colors()
+    pos.grad.zero_()
+    col.grad.zero_()
+    r.render_adjoint(torch.from_numpy(w).cuda())
+    gp = pos.grad.cpu().numpy()
+    gc = col.grad.cpu().numpy()
+    o = _oracle_all(oracle, sc, w=w.astype(np.float64))
+    if ert:
+        _, term_g = r.get_pixel_state()
+        assert (term_g == o["term"]).mean() > 0.999
+    assert rel_err(gp, o["gp"]) < GRAD_TOL, rel_err(gp, o["gp"])
+    assert rel_err(gc, o["gc"]) < GRAD_TOL, rel_err(gc, o["gc"])
+
+
+def test_gradients_vs_fp64_central_differences(oracle):
+    """CUDA adjoint vs FP64 central differences (step 1e-4, Richardson-refined)
+    of the forward with frozen fragment lists: 64 position coordinates + 64
+    RGBA values of an 8^3 mesh at 128^2."""
+    from test_oracle import _fd_pairs
+    sc = Scene(8, 128, seed=11)
+    mesh, r = sc.make_renderer()
+    rng = np.random.default_rng(11)
+    w = rng.normal(size=(128, 128, 4))
+    r.render()
+    pos, col = mesh.get_vertex_positions(), mesh.get_vertex_colors()
+    pos.grad.zero_()
+    col.grad.zero_()
+    r.render_adjoint(torch.from_numpy(w.astype(np.float32)).cuda())
+    gp = pos.grad.cpu().numpy().astype(np.float64)
+    gc = col.grad.cpu().numpy().astype(np.float64)
+    fa = oracle.Faces(sc.cells, sc.pos.shape[0])
+    cam, prm = sc.oracle_camera(oracle), sc.oracle_params(oracle)
+    loss = lambda p, c: float((oracle.render_frozen(fa, sc.pos, p, c, cam, prm) * w).sum())  # noqa: E731
+    fd, an, rel = _fd_pairs(oracle, loss, gp, gc, sc.pos.astype(np.float64), sc.col.astype(np.float64),
+                            np.random.default_rng(3), richardson=True)
+    assert np.median(rel) < 1e-5
+    assert rel.max() < 1e-3, np.sort(rel)[-5:]
+    assert rel_err(fd, an) < 1e-4
+
+
+def test_deterministic_lists_and_images():
+    sc = Scene(16, 256, seed=2)
+    mesh, r = sc.make_renderer()
+    a = r.render().clone()
+    la = r.get_fragment_lists()
+    b = r.render().clone()
+    lb = r.get_fragment_lists()
+    assert torch.equal(a, b)
+    assert np.array_equal(la[0], lb[0]) and np.array_equal(la[1], lb[1])
+
+
+def test_empty_view_and_tiny_viewports(oracle):
+    import difftetvr_b200 as d
+    from difftetvr_b200 import synthetic as S
+    sc = Scene(4, 32, seed=1)
+    mesh, r = sc.make_renderer()
+    # Camera looking away from the mesh: no fragments, image = clear colour.
+    # Camera at (0, 0, 3) looking along +z, away from the mesh (rotation of 180
+    # degrees about y): every vertex lies behind it.
+    r.set_view_matrix([-1, 0, 0, 0, 0, 1, 0, 0, 0, 0, -1, 0, 0, 0, 3, 1])
+    r.set_clear_color(d.vec4(0.25, 0.5, 0.75, 1.0))
+    img = r.render()
+    assert r.get_num_fragments() == 0
+    assert torch.allclose(img, torch.tensor([0.25, 0.5, 0.75, 1.0], device=img.device).expand_as(img))
+    # 1x1 and non-square viewports agree with the oracle.
+    for (w, h) in [(1, 1), (37, 5), (5, 61)]:
+        sc2 = Scene(4, 1, seed=4)
+        mesh2, r2 = sc2.make_renderer()
+        r2.set_viewport_size(w, h)
+        img2 = r2.render().cpu().numpy().astype(np.float64)
+        fa = oracle.Faces(sc2.cells, sc2.pos.shape[0])
+        cam = oracle.make_camera(sc2.view, sc2.fovy, w, h)
+        o = oracle.render(fa, sc2.pos, sc2.col, cam, sc2.oracle_params(oracle))[0]
+        assert np.abs(img2 - o).max() < IMG_TOL
+
+
+def test_budget_error_is_reported():
+    from difftetvr_b200._lib import DTV_ERR_BUDGET, DtvError
+    sc = Scene(8, 128, seed=1)
+    mesh, r = sc.make_renderer()
+    r.set_fragment_budget_bytes(1024)
+    with pytest.raises(DtvError) as e:
+        r.render()
+    assert e.value.code == DTV_ERR_BUDGET
+    r.set_fragment_budget_bytes(0)
+    r.render()  # recovers: counters were reset
+    assert r.get_num_fragments() > 0
+
+
+def test_render_adjoint_argument_checks():
+    sc = Scene(4, 32, seed=1)
+    mesh, r = sc.make_renderer()
+    r.render()
+    with pytest.raises(RuntimeError):
+        r.render_adjoint(torch.zeros(32, 32, 3, device="cuda"))
+    with pytest.raises(RuntimeError):
+        r.render_adjoint(torch.zeros(32, 32, 4, device="cuda", dtype=torch.float64))
+    with pytest.raises(RuntimeError):
+        r.render_adjoint(torch.zeros(32, 32, 4))

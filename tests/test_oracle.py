@@ -91,8 +91,15 @@ def test_segment_integral_limits(oracle):
         lin = a * (t * c0 + 0.5 * t * t * (c1 - c0))
         np.testing.assert_allclose(out[:3], lin, rtol=2 * a * t + 1e-9)
         np.testing.assert_allclose(out[3], 1 - np.exp(-a * t), rtol=1e-12)
-    # below 1e-6 the contribution is dropped (ForwardCommon.glsl:43-46)
-    assert np.all(oracle.segment_integral(t, c0, c1, 5e-7) == 0)
+    # The reference drops a < 1e-6 (ForwardCommon.glsl:43-46); here the value
+    # stays continuous down to a = 0 (a difference of at most a t) ...
+    a = 5e-7
+    out = oracle.segment_integral(t, c0, c1, a)
+    np.testing.assert_allclose(out[:3], a * (t * c0 + 0.5 * t * t * (c1 - c0)), rtol=1e-6)
+    assert np.abs(out).max() < a * t
+    # ... and a <= 0 contributes nothing.
+    assert np.all(oracle.segment_integral(t, c0, c1, 0.0) == 0)
+    assert np.all(oracle.segment_integral(t, c0, c1, -0.3) == 0)
     # constant colour: C = (1 - A) c
     out = oracle.segment_integral(t, c0, c0, 3.0)
     np.testing.assert_allclose(out[:3], (1 - np.exp(-3 * t)) * c0, rtol=1e-12)
@@ -150,12 +157,17 @@ def _fd_pairs(oracle, loss, gp, gc, pos, col, rng, h=1e-4, n=64, richardson=Fals
         d1 = cd(f, x, idx, h)
         return (4 * cd(f, x, idx, h / 2) - d1) / 3 if richardson else d1
 
+    # Densities within 1e-3 of zero sit next to the kink at a = 0 (a <= 0
+    # contributes nothing), so their alpha coordinates are not sampled.
+    cand_a = cand[col[cand, 3] > 1e-3]
     out = []
     for k in rng.choice(cand.size * 3, size=n, replace=False):
         idx = (cand[k // 3], k % 3)
         out.append((deriv(lambda p: loss(p, col), pos, idx), gp[idx]))
     for k in rng.choice(cand.size * 4, size=n, replace=False):
         idx = (cand[k // 4], k % 4)
+        if idx[1] == 3 and col[idx] <= 1e-3:
+            idx = (cand_a[k % cand_a.size], 3)
         out.append((deriv(lambda c: loss(pos, c), col, idx), gc[idx]))
     fd, an = np.array(out).T
     scale = np.abs(an).max()
