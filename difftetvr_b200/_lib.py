@@ -89,6 +89,8 @@ SIGNATURES = {
     "dtv_renderer_copy_pixel_state": (ctypes.c_int32, [c_vp, c_vp, c_vp, c_vp]),
     "dtv_renderer_set_timing": (ctypes.c_int32, [c_vp, ctypes.c_int32]),
     "dtv_renderer_stage_times": (ctypes.c_int32, [c_vp, c_f32p, ctypes.c_int32]),
+    "dtv_render_noalloc": (ctypes.c_int32, [c_vp, c_vp, c_vp, ctypes.POINTER(Camera), ctypes.POINTER(RenderParams),
+                                            c_vp, c_vp]),
     "dtv_loss_l2": (ctypes.c_int32, [c_vp, c_vp, ctypes.c_uint64, ctypes.c_float, c_vp, c_vp, c_vp]),
     "dtv_adam_step": (ctypes.c_int32, [c_vp, c_vp, c_vp, c_vp, ctypes.c_uint64, ctypes.c_float, ctypes.c_float,
                                        ctypes.c_float, ctypes.c_float, ctypes.c_int32, ctypes.c_int32, c_vp,

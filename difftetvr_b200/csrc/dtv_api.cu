@@ -531,3 +531,12 @@ int32_t dtv_adam_step(float* d_param, const float* d_grad, float* d_m, float* d_
 }
 
 }  // extern "C"
+
+// Helpers for the allocation-free entry point (dtv_noalloc.cu).
+namespace dtv {
+MeshView mesh_view(const dtv_mesh* m) { return MeshView{m->d_faces, m->host.num_faces, m->host.num_vertices}; }
+CamDev camera_constants(const dtv_camera& c) { return make_cam(c); }
+ShadeDev shade_constants(const dtv_render_params& p) { return make_shade(p); }
+}  // namespace dtv
+
+void dtv_set_last_error(const std::string& msg) { g_last_error = msg; }

@@ -58,4 +58,25 @@ void launch_adam(float* param, const float* grad, float* m, float* v, uint64_t n
                  float beta2, float eps, float bc1, float bc2, int clamp_mode, const uint32_t* fixed_mask,
                  int fixed_mode, int stride, cudaStream_t s);
 
+// Accessors used by the allocation-free entry point (dtv_noalloc.cu); they
+// expose what dtv_renderer_render derives from its arguments.
+struct MeshView {
+    const uint4* faces;
+    uint64_t num_faces;
+    uint64_t num_vertices;
+};
+
 }  // namespace dtv
+
+struct dtv_mesh;
+struct dtv_camera;
+struct dtv_render_params;
+
+namespace dtv {
+MeshView mesh_view(const dtv_mesh* m);
+CamDev camera_constants(const dtv_camera& c);
+ShadeDev shade_constants(const dtv_render_params& p);
+}  // namespace dtv
+
+// Sets the message returned by dtv_last_error_string() on this thread.
+void dtv_set_last_error(const std::string& msg);

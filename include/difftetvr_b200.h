@@ -145,6 +145,21 @@ int32_t dtv_renderer_copy_pixel_state(const dtv_renderer* r, float* h_transmitta
 int32_t dtv_renderer_set_timing(dtv_renderer* r, int32_t enable);
 int32_t dtv_renderer_stage_times(const dtv_renderer* r, float* h_ms, int32_t n);
 
+/* Allocation-free forward render.  No counterpart in the reference: it is for
+ * callers that cannot allocate device memory while rendering (a host
+ * framework that owns the device heap, or a serving loop that must not call
+ * cudaMalloc/cudaFree, which synchronise the device).  Same kernels and output
+ * as dtv_renderer_render, with all scratch in one fixed file-scope device
+ * array (about 37 MiB, held by every GPU that loads the library until exit).
+ * Limits: <= 65,536 vertices, <= 65,536 pixels, <= 4,194,304 fragments; larger
+ * requests return DTV_ERR_ARG / DTV_ERR_BUDGET.  The first call on a device
+ * looks up the array's address (make it before any stream capture).  Calls
+ * share the array, so calls that overlap on the GPU race; serialise them.
+ * The call synchronises `stream` (it reads the exact fragment count). */
+int32_t dtv_render_noalloc(const dtv_mesh* mesh, const float* d_positions, const float* d_colors,
+                           const dtv_camera* camera, const dtv_render_params* params, float* d_image,
+                           dtv_stream stream);
+
 /* L2 loss: replaces Loss.glsl:242-248 / torch.nn.MSELoss (pytests/train.py:321-326).
  * d_adjoint[i] = 2*scale*(d_image[i]-d_target[i]) (may be NULL);
  * *d_loss += scale * sum (d_image-d_target)^2 (may be NULL). */
