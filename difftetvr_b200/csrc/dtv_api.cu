@@ -144,6 +144,7 @@ struct dtv_renderer {
     DevBuf<uint32_t> term;
     DevBuf<uint32_t> long_list;
     DevBuf<uint32_t> flags;
+    DevBuf<float4> grad_rows;     // [V][2] interleaved vertex gradient accumulator
     u64* h_nf = nullptr;          // pinned
     uint32_t* h_flags = nullptr;  // pinned
     bool flags_pending = false;
@@ -320,6 +321,7 @@ int32_t dtv_renderer_destroy(dtv_renderer* r) {
     r->term.release();
     r->long_list.release();
     r->flags.release();
+    r->grad_rows.release();
     if (r->h_nf) cudaFreeHost(r->h_nf);
     if (r->h_flags) cudaFreeHost(r->h_flags);
     if (r->flags_event) cudaEventDestroy(r->flags_event);
@@ -433,11 +435,13 @@ int32_t dtv_renderer_render_adjoint(dtv_renderer* r, const dtv_mesh* mesh, const
         check_pending_flags(r);
         dtv::ShadeDev sh = r->sh;
         sh.use_abs_grad = use_abs_grad ? 1 : 0;
+        r->grad_rows.ensure(2 * (r->V ? r->V : 1), s);
         rec_event(r, 7, s);
         dtv::launch_adjoint(r->offsets.ptr, r->records.ptr, mesh->d_faces, r->vgeo.ptr,
                             reinterpret_cast<const float4*>(d_colors), r->cam, sh,
                             reinterpret_cast<const float4*>(d_image_adjoint), r->tfinal.ptr, r->term.ptr,
-                            d_grad_positions, reinterpret_cast<float4*>(d_grad_colors), s);
+                            uint32_t(r->V), r->grad_rows.ptr, d_grad_positions,
+                            reinterpret_cast<float4*>(d_grad_colors), s);
         check_launch("adjoint");
         rec_event(r, 8, s);
         r->adjoint_timed = true;

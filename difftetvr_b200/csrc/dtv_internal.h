@@ -49,8 +49,8 @@ void launch_composite(const unsigned long long* offsets, const unsigned long lon
                       float* tfinal, uint32_t* term, cudaStream_t s);
 void launch_adjoint(const unsigned long long* offsets, const unsigned long long* records, const uint4* faces,
                     const VGeo* vgeo, const float4* colors, const CamDev& cam, const ShadeDev& sh,
-                    const float4* dimage, const float* tfinal, const uint32_t* term, float* grad_pos,
-                    float4* grad_col, cudaStream_t s);
+                    const float4* dimage, const float* tfinal, const uint32_t* term, uint32_t V,
+                    float4* grad_rows, float* grad_pos, float4* grad_col, cudaStream_t s);
 
 void launch_loss_l2(const float* image, const float* target, uint64_t n, float scale, float* adjoint,
                     float* loss_accum, cudaStream_t s);

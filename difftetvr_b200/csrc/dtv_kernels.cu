@@ -231,6 +231,60 @@ __device__ __forceinline__ u64 bitonic32(u64 v, int lane) {
     return v;
 }
 
+// Bitonic sort of N = 32*K records held in registers, K consecutive records
+// per lane (record i lives in lane i / K, register i % K).  Stages with
+// partner distance j < K stay inside a lane; the others exchange registers
+// with lane ^ (j / K) through shuffles.
+template <int K>
+__device__ __forceinline__ void warp_sort_regs(u64 (&v)[K], int lane) {
+#pragma unroll
+    for (int k = 2; k <= 32 * K; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            if (j < K) {
+#pragma unroll
+                for (int r = 0; r < K; ++r) {
+                    const int l = r ^ j;
+                    if (l > r) {
+                        const int i = lane * K + r;
+                        const bool up = (i & k) == 0;
+                        const u64 a = v[r], b = v[l];
+                        const bool sw = (a > b) == up;
+                        v[r] = sw ? b : a;
+                        v[l] = sw ? a : b;
+                    }
+                }
+            } else {
+                const int lm = j / K;
+                const bool lower = (lane & lm) == 0;
+#pragma unroll
+                for (int r = 0; r < K; ++r) {
+                    const int i = lane * K + r;
+                    const bool up = (i & k) == 0;
+                    const u64 o = __shfl_xor_sync(kFull, v[r], lm);
+                    v[r] = (lower == up) ? umin64(v[r], o) : umax64(v[r], o);
+                }
+            }
+        }
+    }
+}
+
+template <int K>
+__device__ __forceinline__ void warp_sort_list(u64* r, uint32_t n, int lane) {
+    u64 v[K];
+#pragma unroll
+    for (int q = 0; q < K; ++q) {
+        const uint32_t i = uint32_t(lane) * K + q;
+        v[q] = i < n ? r[i] : ~0ull;
+    }
+    warp_sort_regs<K>(v, lane);
+#pragma unroll
+    for (int q = 0; q < K; ++q) {
+        const uint32_t i = uint32_t(lane) * K + q;
+        if (i < n) r[i] = v[q];
+    }
+}
+
 template <bool BLOCK>
 __device__ __forceinline__ void bitonic_smem(u64* s, uint32_t N, uint32_t tid, uint32_t nthr) {
     for (uint32_t k = 2; k <= N; k <<= 1) {
@@ -269,6 +323,10 @@ __global__ void __launch_bounds__(kSortWarps * 32) k_sort_warp(const u64* __rest
         if (lane < int(n)) r[lane] = v;
         return;
     }
+    if (n <= 64) { warp_sort_list<2>(r, n, lane); return; }
+    if (n <= 128) { warp_sort_list<4>(r, n, lane); return; }
+    if (n <= 256) { warp_sort_list<8>(r, n, lane); return; }
+    if (n <= 512) { warp_sort_list<16>(r, n, lane); return; }
     if (n > kSortWarpCap) {
         if (lane == 0) {
             uint32_t idx = atomicAdd(&flags[0], 1u);
@@ -421,11 +479,23 @@ void launch_composite(const u64* offsets, const u64* records, const uint4* faces
 // rebuilt from the final value (T_in = T_out / A); per fragment the depth and
 // colour adjoints of its two segments are summed and pushed through the
 // screen-space barycentrics and the projection to the face's three vertices.
+// Vertex gradient accumulation: the 7 values of a vertex (position xyz, pad,
+// colour rgba) share one 32-byte row of an interleaved buffer and are added
+// with two float4 vector atomics, so each vertex update touches one L2 sector
+// (scalar atomics into the [V,3] / [V,4] layout touch about three).
+struct GradAcc {
+    float4* rows;   // [V][2]
+
+    __device__ __forceinline__ void add(uint32_t v, float gp0, float gp1, float gp2, float4 gc) const {
+        atomicAdd(rows + 2 * size_t(v), make_float4(gp0, gp1, gp2, 0.f));
+        atomicAdd(rows + 2 * size_t(v) + 1, gc);
+    }
+};
+
 __device__ __forceinline__ void frag_vertex_grads(const FragV& fr, float qx, float qy,
                                                   const VGeo* __restrict__ vgeo,
                                                   const float4* __restrict__ colors, const CamDev& cam,
-                                                  float gz, float4 gcol, bool use_abs, float* grad_pos,
-                                                  float4* grad_col) {
+                                                  float gz, float4 gcol, bool use_abs, const GradAcc& acc) {
     const uint32_t vi[3] = {fr.v0, fr.v1, fr.v2};
     VGeo P[3];
     float4 Cv[3];
@@ -481,22 +551,15 @@ __device__ __forceinline__ void frag_vertex_grads(const FragV& fr, float qx, flo
             gp0 = fabsf(gp0); gp1 = fabsf(gp1); gp2 = fabsf(gp2);
             gc = make_float4(fabsf(gc.x), fabsf(gc.y), fabsf(gc.z), fabsf(gc.w));
         }
-        float* gpp = grad_pos + 3 * size_t(vi[j]);
-        atomicAdd(gpp, gp0);
-        atomicAdd(gpp + 1, gp1);
-        atomicAdd(gpp + 2, gp2);
-        atomicAdd(grad_col + vi[j], gc);
+        acc.add(vi[j], gp0, gp1, gp2, gc);
     }
 }
 
-__global__ void __launch_bounds__(kTile * kTile) k_adjoint(
-    const u64* __restrict__ offsets, const u64* __restrict__ records, const uint4* __restrict__ faces,
-    const VGeo* __restrict__ vgeo, const float4* __restrict__ colors, int W, int H, CamDev cam, ShadeDev sh,
+__device__ __forceinline__ void adjoint_pixel(
+    int px, int py, const u64* __restrict__ offsets, const u64* __restrict__ records, const uint4* __restrict__ faces,
+    const VGeo* __restrict__ vgeo, const float4* __restrict__ colors, int W, const CamDev& cam, const ShadeDev& sh,
     const float4* __restrict__ dimage, const float* __restrict__ tfinal, const uint32_t* __restrict__ term,
-    float* __restrict__ grad_pos, float4* __restrict__ grad_col) {
-    const int px = blockIdx.x * kTile + (threadIdx.x % kTile);
-    const int py = blockIdx.y * kTile + (threadIdx.x / kTile);
-    if (px >= W || py >= H) return;
+    const GradAcc& acc) {
     const size_t p = size_t(py) * W + px;
     const u64 beg = offsets[p];
     const uint32_t n = uint32_t(offsets[p + 1] - beg);
@@ -572,20 +635,51 @@ __global__ void __launch_bounds__(kTile * kTile) k_adjoint(
             gz_f -= g_tot;
             gz_b += g_tot;
         }
-        frag_vertex_grads(fb, qx, qy, vgeo, colors, cam, gz_b, gcol_b, use_abs, grad_pos, grad_col);
+        frag_vertex_grads(fb, qx, qy, vgeo, colors, cam, gz_b, gcol_b, use_abs, acc);
         fb = ff;
         gz_b = gz_f;
         gcol_b = gcol_f;
     }
-    frag_vertex_grads(fb, qx, qy, vgeo, colors, cam, gz_b, gcol_b, use_abs, grad_pos, grad_col);
+    frag_vertex_grads(fb, qx, qy, vgeo, colors, cam, gz_b, gcol_b, use_abs, acc);
+}
+
+
+__global__ void __launch_bounds__(kTile * kTile) k_adjoint(
+    const u64* __restrict__ offsets, const u64* __restrict__ records, const uint4* __restrict__ faces,
+    const VGeo* __restrict__ vgeo, const float4* __restrict__ colors, int W, int H, CamDev cam, ShadeDev sh,
+    const float4* __restrict__ dimage, const float* __restrict__ tfinal, const uint32_t* __restrict__ term,
+    float4* __restrict__ grad_rows) {
+    const int px = blockIdx.x * kTile + (threadIdx.x % kTile);
+    const int py = blockIdx.y * kTile + (threadIdx.x / kTile);
+    if (px >= W || py >= H) return;
+    adjoint_pixel(px, py, offsets, records, faces, vgeo, colors, W, cam, sh, dimage, tfinal, term,
+                  GradAcc{grad_rows});
+}
+
+// Adds the interleaved rows into the caller's gradient buffers.
+__global__ void __launch_bounds__(256) k_scatter_grads(const float4* __restrict__ rows, uint32_t V,
+                                                       float* __restrict__ grad_pos,
+                                                       float4* __restrict__ grad_col) {
+    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= V) return;
+    const float4 a = rows[2 * size_t(v)], b = rows[2 * size_t(v) + 1];
+    float* gp = grad_pos + 3 * size_t(v);
+    gp[0] += a.x;
+    gp[1] += a.y;
+    gp[2] += a.z;
+    float4 c = grad_col[v];
+    grad_col[v] = make_float4(c.x + b.x, c.y + b.y, c.z + b.z, c.w + b.w);
 }
 
 void launch_adjoint(const u64* offsets, const u64* records, const uint4* faces, const VGeo* vgeo,
                     const float4* colors, const CamDev& cam, const ShadeDev& sh, const float4* dimage,
-                    const float* tfinal, const uint32_t* term, float* grad_pos, float4* grad_col, cudaStream_t s) {
+                    const float* tfinal, const uint32_t* term, uint32_t V, float4* grad_rows, float* grad_pos,
+                    float4* grad_col, cudaStream_t s) {
+    cudaMemsetAsync(grad_rows, 0, sizeof(float4) * 2 * size_t(V), s);
     dim3 grid((cam.W + kTile - 1) / kTile, (cam.H + kTile - 1) / kTile);
     k_adjoint<<<grid, kTile * kTile, 0, s>>>(offsets, records, faces, vgeo, colors, cam.W, cam.H, cam, sh, dimage,
-                                             tfinal, term, grad_pos, grad_col);
+                                             tfinal, term, grad_rows);
+    if (V) k_scatter_grads<<<(V + 255) / 256, 256, 0, s>>>(grad_rows, V, grad_pos, grad_col);
 }
 
 // ---------------------------------------------------------------------------
