@@ -8,6 +8,7 @@
 #include <stdexcept>
 #include <string>
 #include "difftetvr_b200.h"
+#include "dtv_host.h"
 #include "dtv_internal.h"
 
 extern "C" int32_t dtv_build_hex_mesh_impl(const float* mn, const float* mx, uint32_t xs, uint32_t ys,
@@ -15,84 +16,10 @@ extern "C" int32_t dtv_build_hex_mesh_impl(const float* mn, const float* mx, uin
 
 namespace {
 
+using namespace dtv_host;
 using u64 = unsigned long long;
 
 thread_local std::string g_last_error;
-
-struct DtvError : std::runtime_error {
-    int32_t code;
-    DtvError(int32_t c, const std::string& m) : std::runtime_error(m), code(c) {}
-};
-
-#define DTV_CK(expr)                                                                                   \
-    do {                                                                                               \
-        cudaError_t err__ = (expr);                                                                    \
-        if (err__ != cudaSuccess)                                                                      \
-            throw DtvError(DTV_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(err__));       \
-    } while (0)
-
-inline void check_launch(const char* what) {
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) throw DtvError(DTV_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
-}
-
-template <class F>
-int32_t guarded(F&& fn) {
-    try {
-        fn();
-        return DTV_OK;
-    } catch (const DtvError& e) {
-        g_last_error = e.what();
-        return e.code;
-    } catch (const std::invalid_argument& e) {
-        g_last_error = e.what();
-        return DTV_ERR_ARG;
-    } catch (const std::bad_alloc&) {
-        g_last_error = "host allocation failed";
-        return DTV_ERR_BUDGET;
-    } catch (const std::exception& e) {
-        g_last_error = e.what();
-        return DTV_ERR_STATE;
-    }
-}
-
-inline void require(bool cond, const char* msg) {
-    if (!cond) throw DtvError(DTV_ERR_ARG, msg);
-}
-
-// Grow-only device buffer.
-template <class T>
-struct DevBuf {
-    T* ptr = nullptr;
-    size_t cap = 0;
-    bool ensure(size_t n, cudaStream_t s, bool zero_new = false, double headroom = 1.0) {
-        if (n <= cap && ptr) return false;
-        if (ptr) {
-            DTV_CK(cudaStreamSynchronize(s));
-            DTV_CK(cudaFree(ptr));
-            ptr = nullptr;
-            cap = 0;
-        }
-        size_t want = size_t(double(n) * headroom);
-        if (want < n) want = n;
-        if (want == 0) want = 1;
-        cudaError_t e = cudaMalloc(&ptr, want * sizeof(T));
-        if (e != cudaSuccess) {
-            cudaGetLastError();
-            ptr = nullptr;
-            throw DtvError(DTV_ERR_BUDGET, "device allocation of " + std::to_string(want * sizeof(T)) +
-                                               " bytes failed: " + cudaGetErrorString(e));
-        }
-        cap = want;
-        if (zero_new) DTV_CK(cudaMemsetAsync(ptr, 0, want * sizeof(T), s));
-        return true;
-    }
-    void release() {
-        if (ptr) cudaFree(ptr);
-        ptr = nullptr;
-        cap = 0;
-    }
-};
 
 dtv::CamDev make_cam(const dtv_camera& c) {
     dtv::CamDev k;

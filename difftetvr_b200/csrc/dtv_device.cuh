@@ -71,8 +71,7 @@ __device__ __forceinline__ float depth_key(const float4& a, const float4& b, con
     float E2 = __fsub_rn(__fmul_rn(d0x, d1y), __fmul_rn(d0y, d1x));
     float num = __fadd_rn(__fadd_rn(__fmul_rn(E0, a.z), __fmul_rn(E1, b.z)), __fmul_rn(E2, c.z));
     float den = __fadd_rn(__fadd_rn(E0, E1), E2);
-    float w = __fdiv_rn(num, den);
-    float z = __fdiv_rn(1.0f, w);
+    float z = __fdiv_rn(den, num);  // z = 1 / sum(lam_j / ze_j)
     float zmin = fminf(fminf(a.w, b.w), c.w);
     float zmax = fmaxf(fmaxf(a.w, b.w), c.w);
     return fminf(fmaxf(z, zmin), zmax);

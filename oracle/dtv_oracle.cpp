@@ -168,8 +168,7 @@ inline float depth_key_f(const ProjF& a, const ProjF& b, const ProjF& c, float q
     float E0 = d1x * d2y - d1y * d2x;
     float E1 = d2x * d0y - d2y * d0x;
     float E2 = d0x * d1y - d0y * d1x;
-    float w = ((E0 * a.iz + E1 * b.iz) + E2 * c.iz) / ((E0 + E1) + E2);
-    float z = 1.0f / w;
+    float z = ((E0 + E1) + E2) / ((E0 * a.iz + E1 * b.iz) + E2 * c.iz);  // 1 / sum(lam_j / ze_j)
     float zmin = std::fmin(std::fmin(a.ze, b.ze), c.ze);
     float zmax = std::fmax(std::fmax(a.ze, b.ze), c.ze);
     return std::fmin(std::fmax(z, zmin), zmax);
