@@ -57,6 +57,33 @@ class RenderParams(ctypes.Structure):
     ]
 
 
+class BatchView(ctypes.Structure):
+    _fields_ = [
+        ("mesh", ctypes.c_int32),
+        ("grad_slot", ctypes.c_int32),
+        ("camera", Camera),
+        ("d_image", ctypes.c_void_p),
+        ("d_target", ctypes.c_void_p),
+        ("d_image_adjoint", ctypes.c_void_p),
+    ]
+
+
+class BatchGradSlot(ctypes.Structure):
+    _fields_ = [("mesh", ctypes.c_int32), ("d_grad_positions", ctypes.c_void_p), ("d_grad_colors", ctypes.c_void_p)]
+
+
+class BatchOptim(ctypes.Structure):
+    _fields_ = [
+        ("lr_positions", ctypes.c_float),
+        ("lr_colors", ctypes.c_float),
+        ("beta1", ctypes.c_float),
+        ("beta2", ctypes.c_float),
+        ("eps", ctypes.c_float),
+        ("clamp_colors", ctypes.c_int32),
+        ("fixed_boundary", ctypes.c_int32),
+    ]
+
+
 class DtvError(RuntimeError):
     """Raised when a C-ABI call returns a non-zero status."""
 
@@ -91,6 +118,17 @@ SIGNATURES = {
     "dtv_renderer_stage_times": (ctypes.c_int32, [c_vp, c_f32p, ctypes.c_int32]),
     "dtv_render_noalloc": (ctypes.c_int32, [c_vp, c_vp, c_vp, ctypes.POINTER(Camera), ctypes.POINTER(RenderParams),
                                             c_vp, c_vp]),
+    "dtv_batch_create": (ctypes.c_int32, [ctypes.POINTER(c_vp)]),
+    "dtv_batch_destroy": (ctypes.c_int32, [c_vp]),
+    "dtv_batch_set_meshes": (ctypes.c_int32, [c_vp, ctypes.c_int32, c_vp, c_vp, c_vp]),
+    "dtv_batch_render": (ctypes.c_int32, [c_vp, ctypes.c_int32, ctypes.POINTER(BatchView), ctypes.POINTER(RenderParams),
+                                          c_vp]),
+    "dtv_batch_render_adjoint": (ctypes.c_int32, [c_vp, ctypes.c_int32, ctypes.POINTER(BatchView), ctypes.c_int32,
+                                                  ctypes.POINTER(BatchGradSlot), ctypes.c_int32, c_vp]),
+    "dtv_batch_train_step": (ctypes.c_int32, [c_vp, ctypes.c_int32, ctypes.POINTER(BatchView),
+                                              ctypes.POINTER(RenderParams), ctypes.POINTER(BatchOptim), c_vp, c_vp]),
+    "dtv_batch_set_graph": (ctypes.c_int32, [c_vp, ctypes.c_int32]),
+    "dtv_batch_get_info": (ctypes.c_int32, [c_vp, c_u64p, c_u64p, c_u64p, ctypes.POINTER(ctypes.c_int32)]),
     "dtv_loss_l2": (ctypes.c_int32, [c_vp, c_vp, ctypes.c_uint64, ctypes.c_float, c_vp, c_vp, c_vp]),
     "dtv_adam_step": (ctypes.c_int32, [c_vp, c_vp, c_vp, c_vp, ctypes.c_uint64, ctypes.c_float, ctypes.c_float,
                                        ctypes.c_float, ctypes.c_float, ctypes.c_int32, ctypes.c_int32, c_vp,

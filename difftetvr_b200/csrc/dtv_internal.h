@@ -37,10 +37,12 @@ void launch_scan(const uint32_t* counts, uint64_t n, unsigned long long* offsets
                  cudaStream_t s);
 // Per-pixel sort.  long_list holds up to P entries; flags[0] = number of long lists,
 // flags[1] = error (list longer than the block sort capacity).
+// With a non-null `ok`, the sorts do nothing when *ok == 0 (batched steps
+// whose records overflowed the buffer).
 void launch_sort(const unsigned long long* offsets, unsigned long long* records, uint32_t P, uint32_t* long_list,
-                 uint32_t* flags, cudaStream_t s);
+                 uint32_t* flags, cudaStream_t s, const uint32_t* ok = nullptr);
 void launch_sort_long(const unsigned long long* offsets, unsigned long long* records, const uint32_t* long_list,
-                      uint32_t num_long, uint32_t* flags, cudaStream_t s);
+                      uint32_t num_long, uint32_t* flags, cudaStream_t s, const uint32_t* ok = nullptr);
 constexpr uint32_t kSortWarpCap = 1024;    // elements per warp list sorted in shared memory
 constexpr uint32_t kSortBlockCap = 16384;  // elements per block-sorted list (128 KiB shared memory)
 

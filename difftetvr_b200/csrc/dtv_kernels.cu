@@ -247,7 +247,9 @@ constexpr int kSortWarps = 8;
 
 __global__ void __launch_bounds__(kSortWarps * 32) k_sort_warp(const u64* __restrict__ offsets, u64* records,
                                                                 uint32_t P, uint32_t* __restrict__ long_list,
-                                                                uint32_t* __restrict__ flags) {
+                                                                uint32_t* __restrict__ flags,
+                                                                const uint32_t* __restrict__ ok) {
+    if (ok && *ok == 0u) return;
     extern __shared__ u64 sm_sort[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t p = blockIdx.x * kSortWarps + warp;
@@ -284,7 +286,8 @@ __global__ void __launch_bounds__(kSortWarps * 32) k_sort_warp(const u64* __rest
 
 __global__ void __launch_bounds__(1024) k_sort_long(const u64* __restrict__ offsets, u64* records,
                                                     const uint32_t* __restrict__ long_list,
-                                                    uint32_t* __restrict__ flags) {
+                                                    uint32_t* __restrict__ flags, const uint32_t* __restrict__ ok) {
+    if (ok && *ok == 0u) return;
     extern __shared__ u64 sm_sort[];
     const uint32_t num_long = flags[0];
     for (uint32_t li = blockIdx.x; li < num_long; li += gridDim.x) {
@@ -307,7 +310,7 @@ __global__ void __launch_bounds__(1024) k_sort_long(const u64* __restrict__ offs
 }
 
 void launch_sort(const u64* offsets, u64* records, uint32_t P, uint32_t* long_list, uint32_t* flags,
-                 cudaStream_t s) {
+                 cudaStream_t s, const uint32_t* ok) {
     static bool attr_set = false;
     const size_t smem = size_t(kSortWarps) * kSortWarpCap * sizeof(u64);
     if (!attr_set) {
@@ -318,12 +321,12 @@ void launch_sort(const u64* offsets, u64* records, uint32_t P, uint32_t* long_li
     }
     if (P == 0) return;
     k_sort_warp<<<(P + kSortWarps - 1) / kSortWarps, kSortWarps * 32, smem, s>>>(offsets, records, P, long_list,
-                                                                                 flags);
+                                                                                 flags, ok);
 }
 
 void launch_sort_long(const u64* offsets, u64* records, const uint32_t* long_list, uint32_t /*num_long*/,
-                      uint32_t* flags, cudaStream_t s) {
-    k_sort_long<<<296, 1024, kSortBlockCap * sizeof(u64), s>>>(offsets, records, long_list, flags);
+                      uint32_t* flags, cudaStream_t s, const uint32_t* ok) {
+    k_sort_long<<<296, 1024, kSortBlockCap * sizeof(u64), s>>>(offsets, records, long_list, flags, ok);
 }
 
 // ---------------------------------------------------------------------------

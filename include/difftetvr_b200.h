@@ -160,6 +160,66 @@ int32_t dtv_render_noalloc(const dtv_mesh* mesh, const float* d_positions, const
                            const dtv_camera* camera, const dtv_render_params* params, float* d_image,
                            dtv_stream stream);
 
+/* ---- Batched views (many cameras, several meshes, one launch per stage) ----
+ * The reference renders one view per call; the batch renders and
+ * differentiates many views of meshes of uneven size together.  A batch
+ * holds a mesh table (dtv_batch_set_meshes); each view names its mesh. */
+typedef struct dtv_batch dtv_batch;
+
+typedef struct dtv_batch_view {
+    int32_t mesh;              /* index into the batch's mesh table */
+    int32_t grad_slot;         /* dtv_batch_render_adjoint: slot receiving this view's gradient, -1 = none */
+    dtv_camera camera;         /* view matrix, fovy, clip planes, viewport size (may differ per view) */
+    float* d_image;            /* out: f32[H*W*4], 16-byte aligned */
+    const float* d_target;     /* dtv_batch_train_step: target image f32[H*W*4] */
+    float* d_image_adjoint;    /* render_adjoint: dL/dimage (in); train step: written (NULL = internal) */
+} dtv_batch_view;
+
+typedef struct dtv_batch_grad_slot {
+    int32_t mesh;              /* mesh of the views mapped to this slot */
+    float* d_grad_positions;   /* f32[V*3]: gradients are ADDED */
+    float* d_grad_colors;      /* f32[V*4], 16-byte aligned: gradients are ADDED */
+} dtv_batch_grad_slot;
+
+/* Adam of dtv_batch_train_step (torch.optim.Adam semantics, pytests/train.py:310-318,
+ * 349-356): clamp_colors 0 none / 1 max(0) / 2 rgb in [0,1] alpha >= 0;
+ * fixed_boundary 0 none / 1 zero boundary position gradients / 2 skip them. */
+typedef struct dtv_batch_optim {
+    float lr_positions;
+    float lr_colors;
+    float beta1;
+    float beta2;
+    float eps;
+    int32_t clamp_colors;
+    int32_t fixed_boundary;
+} dtv_batch_optim;
+
+int32_t dtv_batch_create(dtv_batch** out);
+int32_t dtv_batch_destroy(dtv_batch* batch);
+/* Mesh table: topology handles plus device positions f32[V*3] and colours f32[V*4]
+ * (updated in place by dtv_batch_train_step). */
+int32_t dtv_batch_set_meshes(dtv_batch* batch, int32_t num_meshes, const dtv_mesh* const* meshes,
+                             float* const* d_positions, float* const* d_colors);
+/* Forward render of all views (one synchronisation for the exact fragment count). */
+int32_t dtv_batch_render(dtv_batch* batch, int32_t num_views, const dtv_batch_view* views,
+                         const dtv_render_params* params, dtv_stream stream);
+/* Adjoint of the last dtv_batch_render (same views, in the same order): each
+ * view with grad_slot >= 0 reads its d_image_adjoint and adds its vertex
+ * gradients into that slot. */
+int32_t dtv_batch_render_adjoint(dtv_batch* batch, int32_t num_views, const dtv_batch_view* views,
+                                 int32_t num_slots, const dtv_batch_grad_slot* slots, int32_t use_abs_grad,
+                                 dtv_stream stream);
+/* One training step over all views: render, L2 loss against each view's target
+ * (torch.nn.MSELoss per view, summed into *d_loss), adjoint, Adam of every mesh. */
+int32_t dtv_batch_train_step(dtv_batch* batch, int32_t num_views, const dtv_batch_view* views,
+                             const dtv_render_params* params, const dtv_batch_optim* optim, float* d_loss,
+                             dtv_stream stream);
+/* Capture dtv_batch_train_step in a CUDA graph and replay it (1) or run eagerly (0). */
+int32_t dtv_batch_set_graph(dtv_batch* batch, int32_t enable);
+/* Fragments of the last step, record capacity, steps rerun after an overflow, graph in use. */
+int32_t dtv_batch_get_info(const dtv_batch* batch, uint64_t* num_fragments, uint64_t* capacity,
+                           uint64_t* steps_rerun, int32_t* graph_active);
+
 /* L2 loss: replaces Loss.glsl:242-248 / torch.nn.MSELoss (pytests/train.py:321-326).
  * d_adjoint[i] = 2*scale*(d_image[i]-d_target[i]) (may be NULL);
  * *d_loss += scale * sum (d_image-d_target)^2 (may be NULL). */
