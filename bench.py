@@ -41,6 +41,12 @@ def parse_args():
     ap.add_argument("--cpu-rows", type=int, default=32, help="rows of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--batched-res", type=str, default="512,1024")
+    ap.add_argument("--batched-steps", type=int, default=3)
+    ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--serving-rates", type=str, default="50,200,500,1000,2000")
+    ap.add_argument("--serving-requests", type=int, default=150)
     return ap.parse_args()
 
 
@@ -299,6 +305,187 @@ def run_ours(args, rank, world):
     return result, sc
 
 
+def run_batched(args, res: int, steps: int, warmup: int = 2):
+    """Batching config: meshes Kuhn 64^3 / 24^3 / 40^3, 32 views per step on a
+    Fibonacci sphere split 16 / 10 / 6, all at res x res; forward + adjoint +
+    Adam per step.  Batched (one launch per stage, CUDA graph) vs the plain
+    one-view-per-launch loop on the same GPU, both device-timed."""
+    import torch
+
+    import difftetvr_b200 as d
+    from difftetvr_b200 import _lib
+    from difftetvr_b200 import synthetic as S
+    from difftetvr_b200.batch import BatchRenderer, View
+    from difftetvr_b200.optim import CLAMP_NONNEGATIVE, Adam
+
+    sizes = [64, 24, 40]
+    counts = [16, 10, 6]
+
+    def mk(n, seed):
+        cells, pos = S.kuhn_mesh(n, seed=seed)
+        m = d.TetMesh()
+        m.set_use_gradients(True)
+        m.set_tet_mesh_data(cells, pos, S.gaussian_colors(pos, seed=seed))
+        return m
+
+    cams = S.fibonacci_cameras(sum(counts))
+    views, k = [], 0
+    for mi, c in enumerate(counts):
+        for _ in range(c):
+            views.append(View(mesh=mi, view_matrix=cams[k], width=res, height=res))
+            k += 1
+    # Targets from seed+1 meshes of the same topology.
+    tgt_meshes = [mk(n, 11 + i) for i, n in enumerate(sizes)]
+    tr = BatchRenderer(tgt_meshes, attenuation=1.0)
+    for v, img in zip(views, tr.render(views)):
+        v.target = img.clone()
+        v.image = None
+    del tr, tgt_meshes
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+
+    def timed(fn, n):
+        for i in range(warmup):
+            fn(i)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for i in range(n):
+            fn(warmup + i)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / n
+
+    meshes = [mk(n, 1 + i) for i, n in enumerate(sizes)]
+    br = BatchRenderer(meshes, attenuation=1.0)
+    br.set_graph(True)
+    ms_batched = timed(lambda i: br.train_step(views, lr_positions=LR_POS, lr_colors=LR_COL, clamp_colors=1), steps)
+    info = br.info()
+    del br
+
+    meshes_p = [mk(n, 1 + i) for i, n in enumerate(sizes)]
+    rends = []
+    for m in meshes_p:
+        r = d.Renderer(d.RendererType.PPLL)
+        r.set_tet_mesh(m)
+        r.set_viewport_size(res, res)
+        r.set_camera_fovy(S.FOVY_45)
+        r.set_attenuation(1.0)
+        rends.append(r)
+    opts = [Adam([{"params": [m.get_vertex_colors()], "lr": LR_COL, "clamp": CLAMP_NONNEGATIVE},
+                  {"params": [m.get_vertex_positions()], "lr": LR_POS}]) for m in meshes_p]
+    adj = torch.empty((res, res, 4), device="cuda")
+    loss = torch.zeros(1, device="cuda")
+    n_img = res * res * 4
+
+    def plain_step(i):
+        for o in opts:
+            o.zero_grad(set_to_none=False)
+        for v in views:
+            r = rends[v.mesh]
+            r.set_view_matrix(v.view_matrix)
+            img = r.render()
+            _lib.call("dtv_loss_l2", img.data_ptr(), v.target.data_ptr(), n_img, 1.0 / n_img, adj.data_ptr(),
+                      loss.data_ptr(), stream.cuda_stream)
+            r.render_adjoint(adj)
+        for o in opts:
+            o.step()
+
+    ms_plain = timed(plain_step, steps)
+    nv = len(views)
+    return {"res": res, "views": nv, "views_per_mesh": counts, "meshes": [f"{n}^3" for n in sizes],
+            "batched_views_per_s": nv / (ms_batched / 1e3), "plain_views_per_s": nv / (ms_plain / 1e3),
+            "batched_ms_per_step": ms_batched, "plain_ms_per_step": ms_plain,
+            "speedup": ms_plain / ms_batched, "fragments_per_step": info["fragments"],
+            "graph": info["graph"], "steps": steps, "warmup": warmup}
+
+
+def run_serving(args):
+    """Serving config: Kuhn 16^3 / 32^3 / 64^3 meshes resident; Poisson arrivals
+    at each rate; resolution 256^2 / 512^2 / 1024^2 with weights 0.5 / 0.3 / 0.2;
+    70 % forward-only, 30 % forward + adjoint against a supplied target image.
+    Continuous batching over 2 slots, admission by fragment storage.  Reports
+    p50 / p99 latency and throughput per rate beside the latency of the same
+    kind of requests served alone (serial plain solves)."""
+    import numpy as np
+    import torch
+
+    import difftetvr_b200 as d
+    from difftetvr_b200 import synthetic as S
+    from difftetvr_b200.serve import GpuBackend, Request, ServingEngine
+
+    names = {"16^3": 16, "32^3": 32, "64^3": 64}
+    meshes = {}
+    for i, (k, n) in enumerate(names.items()):
+        cells, pos = S.kuhn_mesh(n, seed=20 + i)
+        m = d.TetMesh()
+        m.set_use_gradients(True)
+        m.set_tet_mesh_data(cells, pos, S.gaussian_colors(pos, seed=20 + i))
+        meshes[k] = m
+    be = GpuBackend(meshes, slots=2)
+    be.calibrate(S.sphere_camera(0), res=256)
+    res_choices, res_w = [256, 512, 1024], [0.5, 0.3, 0.2]
+    targets = {r: torch.rand(r, r, 4, device="cuda", generator=torch.Generator(device="cuda").manual_seed(r))
+               for r in res_choices}
+
+    def make_requests(rng, n):
+        out = []
+        for i in range(n):
+            res = int(rng.choice(res_choices, p=res_w))
+            mode = "gradient" if rng.random() < 0.3 else "forward"
+            out.append(Request(mesh=str(rng.choice(list(names))), view_matrix=S.sphere_camera(int(rng.integers(1 << 30))),
+                               width=res, height=res, mode=mode, target=targets[res] if mode == "gradient" else None))
+        return out
+
+    # Isolated latency: each request alone through the plain path.
+    rends = {}
+    for k, m in meshes.items():
+        r = d.Renderer(d.RendererType.PPLL)
+        r.set_tet_mesh(m)
+        r.set_camera_fovy(S.FOVY_45)
+        r.set_attenuation(1.0)
+        rends[k] = r
+    iso = []
+    for j, q in enumerate(make_requests(np.random.default_rng(7), 60)):
+        r = rends[q.mesh]
+        r.set_viewport_size(q.width, q.height)
+        r.set_view_matrix(q.view_matrix)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        img = r.render()
+        if q.mode == "gradient":
+            r.render_adjoint(((img - q.target) * (2.0 / img.numel())).contiguous())
+        torch.cuda.synchronize()
+        if j >= 5:
+            iso.append((time.perf_counter() - t0) * 1e3)
+    iso = np.array(iso)
+    out = {"meshes": list(names), "resolutions": res_choices, "resolution_weights": res_w, "gradient_fraction": 0.3,
+           "slots": be.slots, "isolated": {"p50_ms": float(np.percentile(iso, 50)),
+                                            "p99_ms": float(np.percentile(iso, 99))}, "rates": []}
+    budget = int(max(be.fragments_per_pixel(k) for k in names) * 1024 * 1024 * 4)
+    for rate in [float(x) for x in args.serving_rates.split(",") if x]:
+        rng = np.random.default_rng(int(rate))
+        reqs = make_requests(rng, args.serving_requests)
+        gaps = rng.exponential(1.0 / rate, size=len(reqs))
+        eng = ServingEngine(be, budget_fragments=budget, max_batch=32)
+        eng.start()
+        t = time.perf_counter()
+        futs = []
+        for q, g in zip(reqs, gaps):
+            t += g
+            dt = t - time.perf_counter()
+            if dt > 0:
+                time.sleep(dt)  # sleeping (not spinning) keeps the GIL free for the engine thread
+            futs.append(eng.submit(q))
+        for f in futs:
+            f.result(timeout=600)
+        eng.stop()
+        st = eng.latency_stats()
+        st["rate_rps"] = rate
+        out["rates"].append(st)
+    return out
+
+
 def cpu_port_sample(args, sc, rows=None):
     """Time the oracle's FP32 port (all host threads) on a band of rows of one
     forward + adjoint view of the same workload; returns (iter/s extrapolated
@@ -381,6 +568,15 @@ def main():
     if world > 1:
         torch.distributed.barrier()
     result, sc = run_ours(args, rank, world)
+    if not args.no_batched:
+        import torch
+        del sc["renderer"], sc["mesh"], sc["targets"]
+        torch.cuda.empty_cache()
+        result["batched"] = [run_batched(args, int(r), args.batched_steps) for r in args.batched_res.split(",") if r]
+    if not args.no_serving:
+        import torch
+        torch.cuda.empty_cache()
+        result["served"] = run_serving(args)
     if rank == 0 and not args.no_cpu_baseline:
         v, s, desc = cpu_port_sample(args, sc)
         sys.path.insert(0, os.path.join(ROOT, "oracle"))

@@ -75,11 +75,23 @@ __device__ __forceinline__ int find_index(u64 g, int n, Getter base) {
 
 __device__ __forceinline__ bool batch_ok(const uint32_t* ok) { return ok == nullptr || *ok != 0u; }
 
+// View of item g for kernels with one item per thread: one search for the
+// block's first item (the same loads for every thread of the block), then a
+// forward walk for the few threads past a view boundary.
+template <typename Getter>
+__device__ __forceinline__ int view_of_item(u64 g, u64 block_first, int n, Getter base) {
+    int v = find_index(block_first, n, base);
+    while (v + 1 < n && base(v + 1) <= g) ++v;
+    return v;
+}
+
 __global__ void __launch_bounds__(256) kb_project(const BatchView* __restrict__ views, int nviews, u64 total,
                                                   float4* __restrict__ vproj, int2* __restrict__ vfix,
                                                   VGeo* __restrict__ vgeo) {
-    for (u64 g = u64(blockIdx.x) * blockDim.x + threadIdx.x; g < total; g += u64(gridDim.x) * blockDim.x) {
-        const int v = find_index(g, nviews, [&](int i) { return views[i].vert_base; });
+    const u64 first = u64(blockIdx.x) * blockDim.x;
+    const u64 g = first + threadIdx.x;
+    if (g < total) {
+        const int v = view_of_item(g, first, nviews, [&](int i) { return views[i].vert_base; });
         const BatchView& bv = views[v];
         const u64 k = g - bv.vert_base;
         const float x = bv.positions[3 * k], y = bv.positions[3 * k + 1], z = bv.positions[3 * k + 2];
@@ -96,8 +108,10 @@ __global__ void __launch_bounds__(128) kb_raster(const BatchView* __restrict__ v
                                                  uint32_t* __restrict__ counts, const u64* __restrict__ offsets,
                                                  u64* __restrict__ records, const uint32_t* __restrict__ ok) {
     if (FILL && !batch_ok(ok)) return;
-    for (u64 g = u64(blockIdx.x) * blockDim.x + threadIdx.x; g < total; g += u64(gridDim.x) * blockDim.x) {
-        const int v = find_index(g, nviews, [&](int i) { return views[i].face_base; });
+    const u64 first = u64(blockIdx.x) * blockDim.x;
+    const u64 g = first + threadIdx.x;
+    if (g < total) {
+        const int v = view_of_item(g, first, nviews, [&](int i) { return views[i].face_base; });
         const BatchView& bv = views[v];
         raster_face<FILL>(uint32_t(g - bv.face_base), bv.faces, vproj + bv.vert_base, vfix + bv.vert_base,
                           int(bv.W), int(bv.H), counts + bv.pix_base, offsets + bv.pix_base, records);
@@ -430,16 +444,16 @@ void upload_views(dtv_batch* b, cudaStream_t s) {
 void enqueue_forward(dtv_batch* b, const dtv::ShadeDev& sh, bool guarded, cudaStream_t s) {
     using namespace dtv;
     const uint32_t* okp = guarded ? b->ok.ptr : nullptr;
-    kb_project<<<grid_for(b->tot_verts, 256, 148 * 16), 256, 0, s>>>(b->d_views.ptr, b->nviews, b->tot_verts,
-                                                                     b->vproj.ptr, b->vfix.ptr, b->vgeo.ptr);
-    kb_raster<false><<<grid_for(b->tot_faces, 128, 148 * 64), 128, 0, s>>>(
+    kb_project<<<grid_for(b->tot_verts, 256, 0x7fffffffu), 256, 0, s>>>(b->d_views.ptr, b->nviews, b->tot_verts,
+                                                                        b->vproj.ptr, b->vfix.ptr, b->vgeo.ptr);
+    kb_raster<false><<<grid_for(b->tot_faces, 128, 0x7fffffffu), 128, 0, s>>>(
         b->d_views.ptr, b->nviews, b->tot_faces, b->vproj.ptr, b->vfix.ptr, b->counts.ptr, nullptr, nullptr, nullptr);
     launch_scan(b->counts.ptr, b->tot_pixels, b->offsets.ptr, b->scan.ptr, s);
     if (guarded) {
         kb_check_capacity<<<1, 1, 0, s>>>(b->offsets.ptr + b->tot_pixels, b->capacity, b->ok.ptr, b->total.ptr);
         kb_clear_counts<<<grid_for(b->tot_pixels, 256, 148 * 16), 256, 0, s>>>(b->counts.ptr, b->tot_pixels, okp);
     }
-    kb_raster<true><<<grid_for(b->tot_faces, 128, 148 * 64), 128, 0, s>>>(
+    kb_raster<true><<<grid_for(b->tot_faces, 128, 0x7fffffffu), 128, 0, s>>>(
         b->d_views.ptr, b->nviews, b->tot_faces, b->vproj.ptr, b->vfix.ptr, b->counts.ptr, b->offsets.ptr,
         b->records.ptr, okp);
     DTV_CK(cudaMemsetAsync(b->sort_flags.ptr, 0, 2 * sizeof(uint32_t), s));
@@ -558,9 +572,10 @@ int32_t dtv_batch_render(dtv_batch* b, int32_t num_views, const dtv_batch_view* 
         upload_views(b, s);
         // Count and scan, then size the record buffer exactly (one host sync).
         using namespace dtv;
-        kb_project<<<grid_for(b->tot_verts, 256, 148 * 16), 256, 0, s>>>(b->d_views.ptr, b->nviews, b->tot_verts,
-                                                                         b->vproj.ptr, b->vfix.ptr, b->vgeo.ptr);
-        kb_raster<false><<<grid_for(b->tot_faces, 128, 148 * 64), 128, 0, s>>>(
+        kb_project<<<grid_for(b->tot_verts, 256, 0x7fffffffu), 256, 0, s>>>(b->d_views.ptr, b->nviews,
+                                                                            b->tot_verts, b->vproj.ptr, b->vfix.ptr,
+                                                                            b->vgeo.ptr);
+        kb_raster<false><<<grid_for(b->tot_faces, 128, 0x7fffffffu), 128, 0, s>>>(
             b->d_views.ptr, b->nviews, b->tot_faces, b->vproj.ptr, b->vfix.ptr, b->counts.ptr, nullptr, nullptr,
             nullptr);
         launch_scan(b->counts.ptr, b->tot_pixels, b->offsets.ptr, b->scan.ptr, s);
@@ -578,7 +593,7 @@ int32_t dtv_batch_render(dtv_batch* b, int32_t num_views, const dtv_batch_view* 
             cudaMemsetAsync(b->counts.ptr, 0, sizeof(uint32_t) * b->tot_pixels, s);
             throw;
         }
-        kb_raster<true><<<grid_for(b->tot_faces, 128, 148 * 64), 128, 0, s>>>(
+        kb_raster<true><<<grid_for(b->tot_faces, 128, 0x7fffffffu), 128, 0, s>>>(
             b->d_views.ptr, b->nviews, b->tot_faces, b->vproj.ptr, b->vfix.ptr, b->counts.ptr, b->offsets.ptr,
             b->records.ptr, nullptr);
         DTV_CK(cudaMemsetAsync(b->sort_flags.ptr, 0, 2 * sizeof(uint32_t), s));

@@ -1,0 +1,273 @@
+"""Serving: a request loop over meshes kept resident on the device.
+
+Requests (forward renders, or forward + adjoint against a supplied target
+image) of mixed resolution arrive at any time.  The engine batches them with
+continuous batching: it keeps a small number of execution slots (each a CUDA
+stream with its own batch renderer and fragment storage); whenever a slot is
+free it admits queued requests in arrival order while their estimated
+fragment storage fits the slot's budget, launches the batch asynchronously,
+and goes back to admitting - so requests that arrive while other batches run
+on the GPU start as soon as a slot and memory are free, and the batches of
+different slots overlap on the device.  Results are delivered through
+futures; each request records its arrival, start and finish times.
+
+The fragment-storage estimate per request is (pixels) x (fragments per pixel
+of its mesh), where the per-mesh figure is learned from the exact counts of
+completed batches (seeded from one probe render per mesh).
+"""
+from __future__ import annotations
+
+import itertools
+import math
+import threading
+import time
+from collections import deque
+from concurrent.futures import Future
+from dataclasses import dataclass, field
+
+import numpy as np
+
+
+@dataclass
+class Request:
+    mesh: str
+    view_matrix: list
+    width: int
+    height: int
+    mode: str = "forward"            # "forward" or "gradient"
+    target: object = None            # gradient: target image [H, W, 4] (torch CUDA tensor)
+    fovy: float = math.radians(45.0)
+    id: int = -1
+    t_arrival: float = 0.0
+    t_start: float = 0.0
+    t_finish: float = 0.0
+    future: Future = field(default_factory=Future, repr=False)
+
+    @property
+    def pixels(self) -> int:
+        return self.width * self.height
+
+
+@dataclass
+class Result:
+    request_id: int
+    image: object                    # [H, W, 4]
+    grad_positions: object = None    # gradient mode: [V, 3]
+    grad_colors: object = None       # gradient mode: [V, 4]
+    loss: float | None = None
+
+
+class ServingEngine:
+    """Continuous-batching request loop.
+
+    backend: object with
+      - slots (int): number of execution slots
+      - launch(slot, requests) -> handle (asynchronous)
+      - done(handle) -> bool
+      - finish(handle) -> list[Result] (in request order)
+      - fragments_per_pixel(mesh) -> float
+      - observe(mesh, pixels, fragments) (optional; refines the estimate)
+    """
+
+    def __init__(self, backend, budget_fragments: int, max_batch: int = 32, poll_s: float = 5e-5):
+        self.backend = backend
+        self.budget = int(budget_fragments)
+        self.max_batch = int(max_batch)
+        self.poll_s = poll_s
+        self.queue: deque[Request] = deque()
+        self.lock = threading.Lock()
+        self.cv = threading.Condition(self.lock)
+        self.ids = itertools.count()
+        self.busy: dict[int, tuple[object, list[Request]]] = {}
+        self.completed: list[Request] = []
+        self.rejected = 0
+        self.batches = 0
+        self.running = False
+        self.thread: threading.Thread | None = None
+
+    # -- client side -------------------------------------------------------
+    def submit(self, req: Request) -> Future:
+        req.id = next(self.ids)
+        req.t_arrival = time.perf_counter()
+        if self.estimate(req) > self.budget:
+            self.rejected += 1
+            req.future.set_exception(RuntimeError(
+                f"request {req.id} needs about {self.estimate(req):.0f} fragments, over the slot budget "
+                f"of {self.budget}"))
+            return req.future
+        with self.cv:
+            self.queue.append(req)
+            self.cv.notify()
+        return req.future
+
+    def cancel_pending(self) -> int:
+        """Cancel every request still waiting in the queue."""
+        with self.cv:
+            n = 0
+            while self.queue:
+                r = self.queue.popleft()
+                r.future.cancel()
+                n += 1
+        return n
+
+    def estimate(self, req: Request) -> float:
+        return req.pixels * self.backend.fragments_per_pixel(req.mesh)
+
+    # -- engine ------------------------------------------------------------
+    def admit(self) -> list[Request]:
+        """Requests for the next batch: arrival order, within the budget."""
+        batch, frags = [], 0.0
+        while self.queue and len(batch) < self.max_batch:
+            e = self.estimate(self.queue[0])
+            if batch and frags + e > self.budget:
+                break
+            batch.append(self.queue.popleft())
+            frags += e
+        return batch
+
+    def step(self) -> bool:
+        """One scheduling pass: finish completed batches, launch on free slots.
+        Returns True if anything happened."""
+        progressed = False
+        for slot, (handle, reqs) in list(self.busy.items()):
+            if self.backend.done(handle):
+                results = self.backend.finish(handle)
+                t = time.perf_counter()
+                for r, res in zip(reqs, results):
+                    r.t_finish = t
+                    if not r.future.cancelled():
+                        r.future.set_result(res)
+                    self.completed.append(r)
+                del self.busy[slot]
+                progressed = True
+        for slot in range(self.backend.slots):
+            if slot in self.busy:
+                continue
+            with self.lock:
+                batch = self.admit()
+            if not batch:
+                break
+            t = time.perf_counter()
+            for r in batch:
+                r.t_start = t
+            self.busy[slot] = (self.backend.launch(slot, batch), batch)
+            self.batches += 1
+            progressed = True
+        return progressed
+
+    def _loop(self):
+        while self.running or self.busy or self.queue:
+            if not self.step():
+                with self.cv:
+                    if not self.queue and self.running:
+                        self.cv.wait(timeout=self.poll_s if self.busy else 0.01)
+                if self.busy:
+                    time.sleep(self.poll_s)
+
+    def start(self):
+        self.running = True
+        self.thread = threading.Thread(target=self._loop, daemon=True)
+        self.thread.start()
+
+    def stop(self, timeout: float = 60.0):
+        self.running = False
+        with self.cv:
+            self.cv.notify_all()
+        if self.thread:
+            self.thread.join(timeout=timeout)
+
+    # -- statistics ------------------------------------------------------------
+    def latency_stats(self) -> dict:
+        lat = np.array([(r.t_finish - r.t_arrival) * 1e3 for r in self.completed]) if self.completed else np.zeros(0)
+        if lat.size == 0:
+            return {"requests": 0}
+        span = max(r.t_finish for r in self.completed) - min(r.t_arrival for r in self.completed)
+        return {"requests": int(lat.size), "p50_ms": float(np.percentile(lat, 50)),
+                "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(lat.mean()),
+                "throughput_rps": float(lat.size / span) if span > 0 else float("nan"),
+                "batches": self.batches, "rejected": self.rejected}
+
+
+class GpuBackend:
+    """Executes request batches with the batched CUDA path; one CUDA stream and
+    one batch renderer (own fragment storage) per slot, meshes shared."""
+
+    def __init__(self, meshes: dict, slots: int = 2, attenuation: float = 1.0):
+        import torch
+
+        from .batch import BatchRenderer
+        self.torch = torch
+        self.names = list(meshes)
+        self.meshes = [meshes[n] for n in self.names]
+        self.index = {n: i for i, n in enumerate(self.names)}
+        self.slots = int(slots)
+        self.streams = [torch.cuda.Stream() for _ in range(self.slots)]
+        self.renderers = [BatchRenderer(self.meshes, attenuation=attenuation, use_early_ray_termination=True)
+                          for _ in range(self.slots)]
+        self.fpp = {n: 64.0 for n in self.names}
+
+    def fragments_per_pixel(self, mesh: str) -> float:
+        return self.fpp[mesh]
+
+    def observe(self, mesh: str, pixels: int, fragments: int) -> None:
+        self.fpp[mesh] = 0.7 * self.fpp[mesh] + 0.3 * max(fragments / max(pixels, 1), 1.0)
+
+    def calibrate(self, view_matrix, res: int = 256) -> None:
+        """One probe render per mesh to seed the fragments-per-pixel estimate."""
+        from .batch import View
+        for n in self.names:
+            br = self.renderers[0]
+            br.render([View(mesh=self.index[n], view_matrix=view_matrix, width=res, height=res)])
+            self.fpp[n] = max(br.info()["fragments"] / float(res * res), 1.0)
+
+    def launch(self, slot: int, reqs: list[Request]):
+        torch = self.torch
+        from .batch import View
+        br = self.renderers[slot]
+        stream = self.streams[slot]
+        views = [View(mesh=self.index[r.mesh], view_matrix=r.view_matrix, width=r.width, height=r.height,
+                      fovy=r.fovy) for r in reqs]
+        grads = []
+        with torch.cuda.stream(stream):
+            br.render(views)
+            slots = []
+            for i, (r, v) in enumerate(zip(reqs, views)):
+                if r.mode == "gradient":
+                    n = float(v.width * v.height * 4)
+                    v.image_adjoint = (v.image - r.target) * (2.0 / n)
+                    v.grad_slot = len(slots)
+                    m = self.meshes[v.mesh]
+                    gp = torch.zeros_like(m.get_vertex_positions(), memory_format=torch.contiguous_format)
+                    gc = torch.zeros_like(m.get_vertex_colors(), memory_format=torch.contiguous_format)
+                    slots.append((v.mesh, gp.detach(), gc.detach()))
+                    grads.append((i, gp, gc))
+            if slots:
+                br.render_adjoint([(m, gp, gc) for (m, gp, gc) in slots])
+            ev = torch.cuda.Event()
+            ev.record(stream)
+        fr = br.info()["fragments"]
+        px = sum(r.pixels for r in reqs)
+        return {"event": ev, "views": views, "reqs": reqs, "grads": grads, "fragments": fr, "pixels": px}
+
+    def done(self, handle) -> bool:
+        return handle["event"].query()
+
+    def finish(self, handle) -> list[Result]:
+        handle["event"].synchronize()
+        reqs, views = handle["reqs"], handle["views"]
+        # Per-mesh fragments-per-pixel estimate from the exact batch count.
+        by_mesh = {}
+        for r in reqs:
+            by_mesh[r.mesh] = by_mesh.get(r.mesh, 0) + r.pixels
+        if len(by_mesh) == 1:
+            (m, px), = by_mesh.items()
+            self.observe(m, px, handle["fragments"])
+        g = {i: (gp, gc) for i, gp, gc in handle["grads"]}
+        out = []
+        for i, (r, v) in enumerate(zip(reqs, views)):
+            gp, gc = g.get(i, (None, None))
+            loss = None
+            if r.mode == "gradient":
+                loss = float(((v.image - r.target) ** 2).mean())
+            out.append(Result(r.id, v.image, gp, gc, loss))
+        return out

@@ -185,6 +185,32 @@ inline float u2f(uint32_t u) {
     return f;
 }
 
+// Exact fixed-point coverage of pixel (px, py) by face f (the rule of
+// build_fragments); *area2 receives the signed doubled area in the stored winding.
+inline bool face_covers(const std::vector<ProjF>& proj, const uint32_t* tri, uint32_t f, int64_t px, int64_t py,
+                        int64_t* area2_out) {
+    const ProjF& p0 = proj[tri[3 * f]];
+    const ProjF& p1 = proj[tri[3 * f + 1]];
+    const ProjF& p2 = proj[tri[3 * f + 2]];
+    *area2_out = 0;
+    if (!(p0.valid && p1.valid && p2.valid)) return false;
+    int64_t ax[3] = {p0.X, p1.X, p2.X}, ay[3] = {p0.Y, p1.Y, p2.Y};
+    const int64_t area2 = (ax[1] - ax[0]) * (ay[2] - ay[0]) - (ay[1] - ay[0]) * (ax[2] - ax[0]);
+    *area2_out = area2;
+    if (area2 == 0) return false;
+    if (area2 < 0) {
+        std::swap(ax[1], ax[2]);
+        std::swap(ay[1], ay[2]);
+    }
+    const int64_t Xc = 256 * px + 128, Yc = 256 * py + 128;
+    for (int e = 0; e < 3; ++e) {
+        const int a = (e + 1) % 3, b = (e + 2) % 3;
+        const int64_t dx = ax[b] - ax[a], dy = ay[b] - ay[a];
+        if (!edge_inside(dx * (Yc - ay[a]) - dy * (Xc - ax[a]), dx, dy)) return false;
+    }
+    return true;
+}
+
 struct FragLists {
     std::vector<int64_t> offsets;   // P+1
     std::vector<uint64_t> records;  // (depth bits << 32) | (face << 2) | (boundary << 1) | front
@@ -701,6 +727,254 @@ int adjoint_impl(const uint32_t* tri, const uint32_t* fbits, int64_t F, const R*
     return 0;
 }
 
+// ---------------------------------------------------------------------------
+// Ray-tet path (intersection renderer).  The reference draws the camera-facing
+// faces of every tet sorted by depth and intersects each pixel ray with the
+// whole tet (Intersect/IntersectRasterization.glsl:139-273,
+// RayIntersectionTests.glsl:77-106): one segment per (pixel, tet), Euclidean
+// length along the normalised ray, the same 4-sub-segment integral.  Here the
+// tets a pixel ray crosses are found by walking through face adjacency: the
+// entries come from the pixel's boundary fragments (front-facing boundary
+// faces, depth order); from a tet entered through face fe the ray leaves
+// through the back face that covers the pixel (the exact fixed-point rule of
+// the rasteriser), and continues into the tet on the other side until it
+// leaves through a boundary face.
+struct WalkTopo {
+    const uint32_t* tri;
+    const uint32_t* fbits;
+    const uint32_t* f2t;
+    const uint32_t* tet_faces;
+};
+
+constexpr uint32_t kNoTet = 0xffffffffu;
+
+// Face of tet t (other than `skip`) that covers the pixel and faces the camera
+// (want_front) or away from it, with respect to t's outward normal.
+inline uint32_t tet_face_at(const WalkTopo& tp, const std::vector<ProjF>& pf, uint32_t t, uint32_t skip,
+                            bool want_front, int px, int py) {
+    for (int j = 0; j < 4; ++j) {
+        const uint32_t f = tp.tet_faces[4 * size_t(t) + j];
+        if (f == skip) continue;
+        int64_t a2;
+        if (!face_covers(pf, tp.tri, f, px, py, &a2)) continue;
+        const bool front_stored = a2 < 0;
+        const bool owner = tp.f2t[2 * size_t(f)] == t;  // stored winding is outward for tetId0
+        if ((front_stored == owner) == want_front) return f;
+    }
+    return kNoTet;
+}
+
+inline uint32_t other_tet(const WalkTopo& tp, uint32_t f, uint32_t t) {
+    const uint32_t a = tp.f2t[2 * size_t(f)], b = tp.f2t[2 * size_t(f) + 1];
+    return a == t ? b : a;
+}
+
+struct WalkState {
+    uint32_t last_tet = kNoTet, last_entry = kNoTet, last_b = 0, nseg = 0;
+};
+
+template <class R>
+inline R ray_len_scale(const CamConst& cam, int px, int py) {
+    const R f = std::is_same<R, float>::value ? R(cam.f) : R(cam.fd);
+    const R dx = (R(px) + R(0.5) - R(cam.cx)) / f, dy = (R(py) + R(0.5) - R(cam.cy)) / f;
+    return std::sqrt(R(1) + dx * dx + dy * dy);
+}
+
+template <class R>
+Frag<R> face_frag(const MeshR<R>& m, uint32_t f, int px, int py) {
+    return eval_frag(m, uint64_t(f) << 2, px, py);
+}
+
+template <class R>
+void walk_composite_pixel(const MeshR<R>& m, const WalkTopo& tp, const std::vector<ProjF>& pf, const CamConst& cam,
+                          const Params& prm, const uint64_t* recs, int64_t n, int px, int py, R out[4], R& Tfinal,
+                          WalkState& st) {
+    R C[3] = {0, 0, 0};
+    R T = 1;
+    const R scale = ray_len_scale<R>(cam, px, py);
+    bool stop = false;
+    const uint64_t max_steps = 1ull << 24;
+    for (int64_t b = 0; b < n && !stop; ++b) {
+        const uint32_t bits = uint32_t(recs[b] & 0xffffffffu);
+        const uint32_t fe0 = bits >> 2;
+        if (!tp.fbits[fe0] || !(bits & 1u)) continue;  // intervals start at front-facing boundary faces
+        uint32_t fe = fe0, t = tp.f2t[2 * size_t(fe0)];
+        Frag<R> f0 = face_frag(m, fe, px, py);
+        for (uint64_t step = 0; step < max_steps; ++step) {
+            const uint32_t fx = tet_face_at(tp, pf, t, fe, /*want_front=*/false, px, py);
+            if (fx == kNoTet) break;
+            if (prm.use_ert && T < R(prm.ert_thresh)) {
+                stop = true;
+                break;
+            }
+            const Frag<R> f1 = face_frag(m, fx, px, py);
+            const R tSeg = (f1.z - f0.z) * scale / R(kNumSubdivs);
+            for (int s = 0; s < kNumSubdivs; ++s) {
+                R c0[3], c1[3], a, cacc[3], A;
+                sub_inputs(f0, f1, s, R(prm.attenuation), c0, c1, a);
+                if (!seg_integral(tSeg, c0, c1, a, cacc, A)) continue;
+                for (int k = 0; k < 3; ++k) C[k] += T * cacc[k];
+                T *= A;
+            }
+            st.last_tet = t;
+            st.last_entry = fe;
+            st.last_b = uint32_t(b);
+            st.nseg++;
+            if (tp.fbits[fx]) break;
+            const uint32_t tn = other_tet(tp, fx, t);
+            if (tn == kNoTet) break;
+            t = tn;
+            fe = fx;
+            f0 = f1;
+        }
+    }
+    Tfinal = T;
+    for (int k = 0; k < 3; ++k) out[k] = C[k] + T * R(prm.clear_color[k]);
+    out[3] = (R(1) - T) + T * R(prm.clear_color[3]);
+}
+
+template <class R>
+void walk_adjoint_pixel(const MeshR<R>& m, const WalkTopo& tp, const std::vector<ProjF>& pf, const CamConst& cam,
+                        const Params& prm, const uint64_t* recs, int64_t n, int px, int py, R Tfinal,
+                        const WalkState& st, const R g[4], R* grad_pos, R* grad_col) {
+    if (st.last_tet == kNoTet) return;
+    const R atten = R(prm.attenuation);
+    const R scale = ray_len_scale<R>(cam, px, py);
+    R gC[3] = {g[0], g[1], g[2]};
+    R gT = g[0] * R(prm.clear_color[0]) + g[1] * R(prm.clear_color[1]) + g[2] * R(prm.clear_color[2]) +
+           g[3] * (R(prm.clear_color[3]) - R(1));
+    R T = Tfinal;
+    uint32_t t = st.last_tet, fe = st.last_entry;
+    int64_t b = st.last_b;
+    // Exit face of the current tet and its accumulated (dL/dz, dL/dcolour).
+    uint32_t fx = tet_face_at(tp, pf, t, fe, false, px, py);
+    R gz_x = 0, gcol_x[4] = {0, 0, 0, 0};
+    const uint64_t max_steps = 1ull << 24;
+    for (uint64_t step = 0; step < max_steps; ++step) {
+        const Frag<R> f0 = face_frag(m, fe, px, py), f1 = face_frag(m, fx, px, py);
+        const R tSeg = (f1.z - f0.z) * scale / R(kNumSubdivs);
+        R gz_e = 0, gcol_e[4] = {0, 0, 0, 0};
+        R g_tot = 0;
+        const R inv = R(1) / R(kNumSubdivs);
+        for (int s = kNumSubdivs - 1; s >= 0; --s) {
+            R c0[3], c1[3], a, cacc[3], A;
+            sub_inputs(f0, f1, s, atten, c0, c1, a);
+            const bool active = seg_integral(tSeg, c0, c1, a, cacc, A);
+            const R Tin = active ? T / A : T;
+            R gcacc[3] = {Tin * gC[0], Tin * gC[1], Tin * gC[2]};
+            const R gA = Tin * gT;
+            if (active) gT = (gC[0] * cacc[0] + gC[1] * cacc[1] + gC[2] * cacc[2]) + gT * A;
+            T = Tin;
+            R g_t, g_a, g_c0[3], g_c1[3];
+            seg_integral_adjoint(tSeg, c0, c1, a, A, gcacc, gA, g_t, g_a, g_c0, g_c1);
+            g_tot += g_t * inv;
+            const R fbg = R(s) * inv, fm = (R(s) + R(0.5)) * inv, fen = (R(s) + R(1)) * inv;
+            for (int k = 0; k < 3; ++k) {
+                gcol_e[k] += (R(1) - fbg) * g_c0[k] + (R(1) - fen) * g_c1[k];
+                gcol_x[k] += fbg * g_c0[k] + fen * g_c1[k];
+            }
+            gcol_e[3] += (R(1) - fm) * g_a * atten;
+            gcol_x[3] += fm * g_a * atten;
+        }
+        gz_e -= g_tot * scale;
+        gz_x += g_tot * scale;
+        frag_vertex_grads(m, cam, fx, px, py, gz_x, gcol_x, prm.use_abs_grad != 0, grad_pos, grad_col);
+        if (tp.fbits[fe]) {
+            frag_vertex_grads(m, cam, fe, px, py, gz_e, gcol_e, prm.use_abs_grad != 0, grad_pos, grad_col);
+            // Previous interval: its exit is the last back-facing boundary fragment before b.
+            int64_t bb = b - 1;
+            while (bb >= 0) {
+                const uint32_t bits = uint32_t(recs[bb] & 0xffffffffu);
+                if (tp.fbits[bits >> 2] && !(bits & 1u)) break;
+                --bb;
+            }
+            if (bb < 0) return;
+            fx = uint32_t(recs[bb] & 0xffffffffu) >> 2;
+            t = tp.f2t[2 * size_t(fx)];
+            fe = tet_face_at(tp, pf, t, fx, /*want_front=*/true, px, py);
+            if (fe == kNoTet) return;
+            // Entry fragment of the previous interval: the last front boundary fragment before bb.
+            int64_t be = bb - 1;
+            while (be >= 0) {
+                const uint32_t bits = uint32_t(recs[be] & 0xffffffffu);
+                if (tp.fbits[bits >> 2] && (bits & 1u)) break;
+                --be;
+            }
+            b = be < 0 ? 0 : be;
+            gz_x = 0;
+            for (int k = 0; k < 4; ++k) gcol_x[k] = 0;
+            continue;
+        }
+        const uint32_t tp_prev = other_tet(tp, fe, t);
+        if (tp_prev == kNoTet) return;
+        const uint32_t fe_prev = tet_face_at(tp, pf, tp_prev, fe, /*want_front=*/true, px, py);
+        if (fe_prev == kNoTet) return;
+        fx = fe;
+        gz_x = gz_e;
+        for (int k = 0; k < 4; ++k) gcol_x[k] = gcol_e[k];
+        t = tp_prev;
+        fe = fe_prev;
+    }
+}
+
+template <class R>
+int raytet_impl(const uint32_t* tri, const uint32_t* fbits, const uint32_t* f2t, const uint32_t* tet_faces,
+                int64_t F, const R* pos, const R* col, int64_t V, const Camera* camp, const Params* prm, R* image,
+                R* tfinal, uint32_t* nseg, const R* image_adj, R* grad_pos, R* grad_col, const float* pos_cov) {
+    CamConst cam = make_cam(*camp);
+    int r0, r1;
+    row_range(*prm, cam.H, r0, r1);
+    auto pf = pos_cov ? project_all_f(pos_cov, V, cam) : project_all_f(pos, V, cam);
+    FragLists fl = build_fragments(tri, fbits, F, pf, cam, r0, r1);
+    MeshR<R> m = make_mesh(tri, pos, col, V, cam);
+    const WalkTopo tp{tri, fbits, f2t, tet_faces};
+    const int W = cam.W;
+    int nthreads = 1;
+#ifdef _OPENMP
+    nthreads = omp_get_max_threads();
+#endif
+    std::vector<std::vector<R>> gp, gc;
+    if (image_adj) {
+        gp.assign(nthreads, std::vector<R>(3 * V, R(0)));
+        gc.assign(nthreads, std::vector<R>(4 * V, R(0)));
+    }
+#pragma omp parallel
+    {
+        int tid = 0;
+#ifdef _OPENMP
+        tid = omp_get_thread_num();
+#endif
+#pragma omp for schedule(dynamic, 4)
+        for (int py = r0; py < r1; ++py) {
+            for (int px = 0; px < W; ++px) {
+                const int64_t p = int64_t(py) * W + px;
+                const uint64_t* recs = fl.records.data() + fl.offsets[p];
+                const int64_t n = fl.offsets[p + 1] - fl.offsets[p];
+                R out[4], Tf;
+                WalkState st;
+                walk_composite_pixel(m, tp, pf, cam, *prm, recs, n, px, py, out, Tf, st);
+                if (image)
+                    for (int k = 0; k < 4; ++k) image[4 * p + k] = out[k];
+                if (tfinal) tfinal[p] = Tf;
+                if (nseg) nseg[p] = st.nseg;
+                if (image_adj) {
+                    const R g[4] = {image_adj[4 * p], image_adj[4 * p + 1], image_adj[4 * p + 2],
+                                    image_adj[4 * p + 3]};
+                    walk_adjoint_pixel(m, tp, pf, cam, *prm, recs, n, px, py, Tf, st, g, gp[tid].data(),
+                                       gc[tid].data());
+                }
+            }
+        }
+    }
+    if (image_adj) {
+        for (int t = 0; t < nthreads; ++t) {
+            for (int64_t i = 0; i < 3 * V; ++i) grad_pos[i] += gp[t][i];
+            for (int64_t i = 0; i < 4 * V; ++i) grad_col[i] += gc[t][i];
+        }
+    }
+    return 0;
+}
+
 struct TempFace {
     uint32_t v[3];
     uint32_t face_id;
@@ -819,6 +1093,44 @@ int orc_adjoint_f32(const uint32_t* tri, const uint32_t* fbits, int64_t F, const
                     int64_t V, const Camera* cam, const Params* prm, const float* image_adj, float* grad_pos,
                     float* grad_col) {
     return adjoint_impl<float>(tri, fbits, F, pos, col, V, cam, prm, image_adj, grad_pos, grad_col);
+}
+
+// tet -> its four unique face indices, in TetFaceTable order (the face of tet
+// c opposite vertex tetFaceTable[j][3] is tet_faces[4c + j]).
+void orc_tet_faces(const uint32_t* cells, int64_t T, uint32_t* tet_faces) {
+    std::vector<TempFace> tf(size_t(T) * 4);
+    for (int64_t c = 0; c < T; ++c)
+        for (int j = 0; j < 4; ++j) {
+            uint32_t v[3];
+            for (int k = 0; k < 3; ++k) v[k] = cells[4 * c + kTetFace[j][k]];
+            std::sort(v, v + 3);
+            tf[4 * c + j] = TempFace{{v[0], v[1], v[2]}, uint32_t(4 * c + j), uint32_t(c)};
+        }
+    std::sort(tf.begin(), tf.end());
+    int64_t F = -1;
+    for (size_t i = 0; i < tf.size(); ++i) {
+        if (i == 0 || !tf[i].same(tf[i - 1])) ++F;
+        tet_faces[tf[i].face_id] = uint32_t(F);
+    }
+}
+
+// Ray-tet path: forward (image, T_final, segments per pixel) and, with
+// image_adj non-null, the exact adjoint added into grad_pos / grad_col.
+// pos_cov (nullable): coverage and walk from these float positions (frozen).
+int orc_raytet_f64(const uint32_t* tri, const uint32_t* fbits, const uint32_t* f2t, const uint32_t* tet_faces,
+                   int64_t F, const double* pos, const double* col, int64_t V, const Camera* cam, const Params* prm,
+                   double* image, double* tfinal, uint32_t* nseg, const double* image_adj, double* grad_pos,
+                   double* grad_col, const float* pos_cov) {
+    return raytet_impl<double>(tri, fbits, f2t, tet_faces, F, pos, col, V, cam, prm, image, tfinal, nseg, image_adj,
+                               grad_pos, grad_col, pos_cov);
+}
+
+int orc_raytet_f32(const uint32_t* tri, const uint32_t* fbits, const uint32_t* f2t, const uint32_t* tet_faces,
+                   int64_t F, const float* pos, const float* col, int64_t V, const Camera* cam, const Params* prm,
+                   float* image, float* tfinal, uint32_t* nseg, const float* image_adj, float* grad_pos,
+                   float* grad_col, const float* pos_cov) {
+    return raytet_impl<float>(tri, fbits, f2t, tet_faces, F, pos, col, V, cam, prm, image, tfinal, nseg, image_adj,
+                              grad_pos, grad_col, pos_cov);
 }
 
 // Segment integral for closed-form checks (ForwardCommon.glsl:42-49).

@@ -66,6 +66,13 @@ def load():
         lib.orc_render_frozen_f64.restype = ctypes.c_int
         lib.orc_render_frozen_f64.argtypes = [_vp, _vp, ctypes.c_int64, _vp, _vp, _vp, ctypes.c_int64,
                                               ctypes.POINTER(Camera), ctypes.POINTER(Params), _vp]
+        lib.orc_tet_faces.restype = None
+        lib.orc_tet_faces.argtypes = [_vp, ctypes.c_int64, _vp]
+        for name in ("orc_raytet_f64", "orc_raytet_f32"):
+            fn = getattr(lib, name)
+            fn.restype = ctypes.c_int
+            fn.argtypes = [_vp, _vp, _vp, _vp, ctypes.c_int64, _vp, _vp, ctypes.c_int64, ctypes.POINTER(Camera),
+                           ctypes.POINTER(Params), _vp, _vp, _vp, _vp, _vp, _vp, _vp]
         lib.orc_segment_integral.restype = None
         lib.orc_segment_integral.argtypes = [ctypes.c_double, _vp, _vp, ctypes.c_double, _vp]
         lib.orc_num_threads.restype = ctypes.c_int
@@ -114,6 +121,8 @@ class Faces:
         self.face_to_tet = f2t[:2 * F].reshape(F, 2).copy()
         self.vertex_boundary = vb
         self.num_faces = F
+        self.tet_faces = np.empty(4 * T, np.uint32)
+        lib.orc_tet_faces(_p(cells), T, _p(self.tet_faces))
 
 
 def fragments(faces: Faces, positions: np.ndarray, cam: Camera):
@@ -184,6 +193,32 @@ def adjoint(faces: Faces, positions, colors, cam: Camera, prm: Params, image_adj
     fn(_p(faces.tri), _p(faces.face_boundary), faces.num_faces, _p(pos), _p(col), pos.shape[0],
        ctypes.byref(cam), ctypes.byref(prm), _p(gimg), _p(gp), _p(gc))
     return gp, gc
+
+
+def raytet(faces: Faces, positions, colors, cam: Camera, prm: Params, image_adjoint=None, precision: int = 64,
+           positions_coverage=None):
+    """Ray-tet (intersection) path: returns (image [H,W,4], T_final [H,W], segments [H,W]) and, with
+    image_adjoint, also (grad_positions [V,3], grad_colors [V,4])."""
+    lib = load()
+    dt = np.float64 if precision == 64 else np.float32
+    pos = np.ascontiguousarray(positions, dtype=dt)
+    col = np.ascontiguousarray(colors, dtype=dt)
+    P = cam.width * cam.height
+    img = np.zeros((P, 4), dt)
+    tf = np.ones(P, dt)
+    nseg = np.zeros(P, np.uint32)
+    V = pos.shape[0]
+    gp = np.zeros((V, 3), dt)
+    gc = np.zeros((V, 4), dt)
+    gimg = None if image_adjoint is None else np.ascontiguousarray(image_adjoint, dtype=dt).reshape(-1, 4)
+    pc = None if positions_coverage is None else np.ascontiguousarray(positions_coverage, dtype=np.float32)
+    fn = lib.orc_raytet_f64 if precision == 64 else lib.orc_raytet_f32
+    fn(_p(faces.tri), _p(faces.face_boundary), _p(faces.face_to_tet), _p(faces.tet_faces), faces.num_faces,
+       _p(pos), _p(col), V, ctypes.byref(cam), ctypes.byref(prm), _p(img), _p(tf), _p(nseg),
+       None if gimg is None else _p(gimg), _p(gp), _p(gc), None if pc is None else _p(pc))
+    H, W = cam.height, cam.width
+    out = (img.reshape(H, W, 4), tf.reshape(H, W), nseg.reshape(H, W))
+    return out if gimg is None else out + (gp, gc)
 
 
 def segment_integral(t, c0, c1, a):

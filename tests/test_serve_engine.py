@@ -1,0 +1,101 @@
+"""Continuous-batching request loop (host logic, fake backend; no GPU)."""
+import threading
+import time
+
+import pytest
+
+from difftetvr_b200.serve import Request, Result, ServingEngine
+
+
+class FakeBackend:
+    """Completes a batch `delay` seconds after launch; records what it saw."""
+
+    def __init__(self, slots=2, delay=0.02, fpp=10.0):
+        self.slots = slots
+        self.delay = delay
+        self.fpp = fpp
+        self.launched = []
+        self.max_concurrent = 0
+        self.active = 0
+        self.lock = threading.Lock()
+
+    def fragments_per_pixel(self, mesh):
+        return self.fpp
+
+    def launch(self, slot, reqs):
+        with self.lock:
+            self.active += 1
+            self.max_concurrent = max(self.max_concurrent, self.active)
+        self.launched.append((slot, [r.id for r in reqs]))
+        return {"t": time.perf_counter() + self.delay, "reqs": reqs}
+
+    def done(self, h):
+        return time.perf_counter() >= h["t"]
+
+    def finish(self, h):
+        with self.lock:
+            self.active -= 1
+        return [Result(r.id, image=("img", r.id)) for r in h["reqs"]]
+
+
+def req(w=16, h=16, mode="forward"):
+    return Request(mesh="m", view_matrix=[0.0] * 16, width=w, height=h, mode=mode)
+
+
+def test_all_requests_complete_in_arrival_order_within_budget():
+    be = FakeBackend(delay=0.005)
+    eng = ServingEngine(be, budget_fragments=10 * 16 * 16 * 3, max_batch=8)  # 3 requests per batch
+    eng.start()
+    futs = [eng.submit(req()) for _ in range(20)]
+    res = [f.result(timeout=10) for f in futs]
+    eng.stop()
+    assert [r.request_id for r in res] == list(range(20))
+    launched = [i for _, ids in be.launched for i in ids]
+    assert launched == list(range(20))  # FIFO admission
+    assert max(len(ids) for _, ids in be.launched) <= 3  # memory budget respected
+    st = eng.latency_stats()
+    assert st["requests"] == 20 and st["p99_ms"] >= st["p50_ms"] > 0
+
+
+def test_requests_arriving_during_a_batch_start_on_the_free_slot():
+    be = FakeBackend(slots=2, delay=0.05)
+    eng = ServingEngine(be, budget_fragments=10 * 16 * 16, max_batch=1)
+    eng.start()
+    f1 = eng.submit(req())
+    time.sleep(0.01)
+    f2 = eng.submit(req())  # arrives while the first batch is on the "GPU"
+    f1.result(timeout=5)
+    f2.result(timeout=5)
+    eng.stop()
+    assert be.max_concurrent == 2
+    assert {s for s, _ in be.launched} == {0, 1}
+
+
+def test_over_budget_request_is_rejected_and_others_proceed():
+    be = FakeBackend(delay=0.001)
+    eng = ServingEngine(be, budget_fragments=10 * 32 * 32)
+    eng.start()
+    bad = eng.submit(req(64, 64))
+    good = eng.submit(req(32, 32))
+    with pytest.raises(RuntimeError):
+        bad.result(timeout=5)
+    assert good.result(timeout=5).request_id == good_id(good, eng)
+    eng.stop()
+    assert eng.rejected == 1
+
+
+def good_id(fut, eng):
+    return [r.id for r in eng.completed][-1]
+
+
+def test_cancel_pending_requests():
+    be = FakeBackend(slots=1, delay=0.05)
+    eng = ServingEngine(be, budget_fragments=10 * 16 * 16, max_batch=1)
+    eng.start()
+    futs = [eng.submit(req()) for _ in range(5)]
+    time.sleep(0.01)
+    n = eng.cancel_pending()
+    eng.stop()
+    assert n >= 3
+    assert sum(f.cancelled() for f in futs) == n
+    assert all(f.done() for f in futs)
