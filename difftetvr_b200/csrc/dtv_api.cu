@@ -56,6 +56,12 @@ struct dtv_mesh {
     uint32_t* d_vertex_boundary = nullptr;
     uint32_t* d_face_to_tet = nullptr;
     uint32_t* d_cells = nullptr;
+    // Ray-tet path: per-tet face ids and the boundary faces as their own
+    // face set (rasterised alone; record face field k -> global face bf_global[k]).
+    uint32_t* d_tet_faces = nullptr;   // 4T
+    uint4* d_bfaces = nullptr;         // Nb
+    uint32_t* d_bf_global = nullptr;   // Nb
+    std::vector<uint32_t> bf_global;   // host copy
 };
 
 struct dtv_renderer {
@@ -72,6 +78,7 @@ struct dtv_renderer {
     DevBuf<uint32_t> long_list;
     DevBuf<uint32_t> flags;
     DevBuf<float4> grad_rows;     // [V][2] interleaved vertex gradient accumulator
+    DevBuf<uint4> wstate;         // ray-tet path: (last tet, its entry face, boundary entry index, segments)
     u64* h_nf = nullptr;          // pinned
     uint32_t* h_flags = nullptr;  // pinned
     bool flags_pending = false;
@@ -158,6 +165,24 @@ int32_t dtv_mesh_create(const uint32_t* h_cells, uint64_t num_cells, uint64_t nu
             DTV_CK(cudaMalloc(&m->d_vertex_boundary, sizeof(uint32_t) * (num_vertices ? num_vertices : 1)));
             DTV_CK(cudaMalloc(&m->d_face_to_tet, sizeof(uint32_t) * (2 * F ? 2 * F : 1)));
             DTV_CK(cudaMalloc(&m->d_cells, sizeof(uint32_t) * (4 * num_cells ? 4 * num_cells : 1)));
+            std::vector<uint4> bfaces;
+            for (uint64_t f = 0; f < F; ++f)
+                if (m->host.face_boundary[f]) {
+                    m->bf_global.push_back(uint32_t(f));
+                    bfaces.push_back(faces[f]);
+                }
+            const uint64_t Nb = m->bf_global.size();
+            DTV_CK(cudaMalloc(&m->d_tet_faces, sizeof(uint32_t) * (4 * num_cells ? 4 * num_cells : 1)));
+            DTV_CK(cudaMalloc(&m->d_bfaces, sizeof(uint4) * (Nb ? Nb : 1)));
+            DTV_CK(cudaMalloc(&m->d_bf_global, sizeof(uint32_t) * (Nb ? Nb : 1)));
+            if (Nb) {
+                DTV_CK(cudaMemcpy(m->d_bfaces, bfaces.data(), sizeof(uint4) * Nb, cudaMemcpyHostToDevice));
+                DTV_CK(cudaMemcpy(m->d_bf_global, m->bf_global.data(), sizeof(uint32_t) * Nb,
+                                  cudaMemcpyHostToDevice));
+            }
+            if (num_cells)
+                DTV_CK(cudaMemcpy(m->d_tet_faces, m->host.tet_faces.data(), sizeof(uint32_t) * 4 * num_cells,
+                                  cudaMemcpyHostToDevice));
             if (F) {
                 DTV_CK(cudaMemcpy(m->d_faces, faces.data(), sizeof(uint4) * F, cudaMemcpyHostToDevice));
                 DTV_CK(cudaMemcpy(m->d_face_to_tet, m->host.face_to_tet.data(), sizeof(uint32_t) * 2 * F,
@@ -182,6 +207,9 @@ int32_t dtv_mesh_destroy(dtv_mesh* m) {
     cudaFree(m->d_vertex_boundary);
     cudaFree(m->d_face_to_tet);
     cudaFree(m->d_cells);
+    cudaFree(m->d_tet_faces);
+    cudaFree(m->d_bfaces);
+    cudaFree(m->d_bf_global);
     delete m;
     return DTV_OK;
 }
@@ -216,8 +244,8 @@ int32_t dtv_mesh_vertex_boundary_device(const dtv_mesh* m, const uint32_t** d_vb
 int32_t dtv_renderer_create(int32_t type, dtv_renderer** out) {
     return guarded([&] {
         require(out != nullptr, "out is null");
-        require(type == DTV_RENDERER_PPLL,
-                "renderer type not provided by this library (PPLL = 0 is available)");
+        require(type == DTV_RENDERER_PPLL || type == DTV_RENDERER_INTERSECTION,
+                "renderer type not provided by this library (PPLL = 0 and INTERSECTION = 2 are available)");
         *out = nullptr;
         auto* r = new dtv_renderer();
         r->type = type;
@@ -249,6 +277,7 @@ int32_t dtv_renderer_destroy(dtv_renderer* r) {
     r->long_list.release();
     r->flags.release();
     r->grad_rows.release();
+    r->wstate.release();
     if (r->h_nf) cudaFreeHost(r->h_nf);
     if (r->h_flags) cudaFreeHost(r->h_flags);
     if (r->flags_event) cudaEventDestroy(r->flags_event);
@@ -273,7 +302,11 @@ int32_t dtv_renderer_render(dtv_renderer* r, const dtv_mesh* mesh, const float* 
         cudaStream_t s = static_cast<cudaStream_t>(stream);
         check_pending_flags(r);
         r->have_render = false;
-        const uint64_t V = mesh->host.num_vertices, F = mesh->host.num_faces;
+        const bool raytet = r->type == DTV_RENDERER_INTERSECTION;
+        const uint64_t V = mesh->host.num_vertices;
+        // The ray-tet path rasterises only the boundary faces (interval entries and exits).
+        const uint64_t F = raytet ? mesh->bf_global.size() : mesh->host.num_faces;
+        const uint4* rfaces = raytet ? mesh->d_bfaces : mesh->d_faces;
         const int W = camera->width, H = camera->height;
         const uint64_t P = uint64_t(W) * H;
         dtv::CamDev cam = make_cam(*camera);
@@ -286,7 +319,10 @@ int32_t dtv_renderer_render(dtv_renderer* r, const dtv_mesh* mesh, const float* 
         r->offsets.ensure(P + 1, s);
         r->scan_scratch.ensure(dtv::scan_scratch_elems(P), s);
         r->tfinal.ensure(P, s);
-        r->term.ensure(P, s);
+        if (raytet)
+            r->wstate.ensure(P, s);
+        else
+            r->term.ensure(P, s);
         r->long_list.ensure(P, s);
         r->flags.ensure(2, s);
 
@@ -294,7 +330,7 @@ int32_t dtv_renderer_render(dtv_renderer* r, const dtv_mesh* mesh, const float* 
         dtv::launch_project(d_positions, uint32_t(V), cam, r->vproj.ptr, r->vfix.ptr, r->vgeo.ptr, s);
         check_launch("project");
         rec_event(r, 1, s);
-        dtv::launch_raster_count(mesh->d_faces, uint32_t(F), r->vproj.ptr, r->vfix.ptr, W, H, r->counts.ptr, s);
+        dtv::launch_raster_count(rfaces, uint32_t(F), r->vproj.ptr, r->vfix.ptr, W, H, r->counts.ptr, s);
         check_launch("raster count");
         rec_event(r, 2, s);
         dtv::launch_scan(r->counts.ptr, P, r->offsets.ptr, r->scan_scratch.ptr, s);
@@ -316,7 +352,7 @@ int32_t dtv_renderer_render(dtv_renderer* r, const dtv_mesh* mesh, const float* 
             throw;
         }
         rec_event(r, 3, s);
-        dtv::launch_raster_fill(mesh->d_faces, uint32_t(F), r->vproj.ptr, r->vfix.ptr, W, H, r->counts.ptr,
+        dtv::launch_raster_fill(rfaces, uint32_t(F), r->vproj.ptr, r->vfix.ptr, W, H, r->counts.ptr,
                                 r->offsets.ptr, r->records.ptr, s);
         check_launch("raster fill");
         rec_event(r, 4, s);
@@ -329,10 +365,18 @@ int32_t dtv_renderer_render(dtv_renderer* r, const dtv_mesh* mesh, const float* 
         DTV_CK(cudaEventRecord(r->flags_event, s));
         r->flags_pending = true;
         rec_event(r, 5, s);
-        dtv::launch_composite(r->offsets.ptr, r->records.ptr, mesh->d_faces, r->vgeo.ptr,
-                              reinterpret_cast<const float4*>(d_colors), W, H, sh,
-                              reinterpret_cast<float4*>(d_image), r->tfinal.ptr, r->term.ptr, s);
-        check_launch("composite");
+        if (raytet) {
+            dtv::launch_walk_composite(r->offsets.ptr, r->records.ptr, mesh->d_bf_global, mesh->d_faces,
+                                       mesh->d_face_to_tet, mesh->d_tet_faces, uint32_t(mesh->host.num_cells),
+                                       r->vfix.ptr, r->vgeo.ptr, reinterpret_cast<const float4*>(d_colors), cam, sh,
+                                       reinterpret_cast<float4*>(d_image), r->tfinal.ptr, r->wstate.ptr, s);
+            check_launch("ray-tet walk");
+        } else {
+            dtv::launch_composite(r->offsets.ptr, r->records.ptr, mesh->d_faces, r->vgeo.ptr,
+                                  reinterpret_cast<const float4*>(d_colors), W, H, sh,
+                                  reinterpret_cast<float4*>(d_image), r->tfinal.ptr, r->term.ptr, s);
+            check_launch("composite");
+        }
         rec_event(r, 6, s);
         r->adjoint_timed = false;
         r->have_render = true;
@@ -364,12 +408,22 @@ int32_t dtv_renderer_render_adjoint(dtv_renderer* r, const dtv_mesh* mesh, const
         sh.use_abs_grad = use_abs_grad ? 1 : 0;
         r->grad_rows.ensure(2 * (r->V ? r->V : 1), s);
         rec_event(r, 7, s);
-        dtv::launch_adjoint(r->offsets.ptr, r->records.ptr, mesh->d_faces, r->vgeo.ptr,
-                            reinterpret_cast<const float4*>(d_colors), r->cam, sh,
-                            reinterpret_cast<const float4*>(d_image_adjoint), r->tfinal.ptr, r->term.ptr,
-                            uint32_t(r->V), r->grad_rows.ptr, d_grad_positions,
-                            reinterpret_cast<float4*>(d_grad_colors), s);
-        check_launch("adjoint");
+        if (r->type == DTV_RENDERER_INTERSECTION) {
+            dtv::launch_walk_adjoint(r->offsets.ptr, r->records.ptr, mesh->d_bf_global, mesh->d_faces,
+                                     mesh->d_face_to_tet, mesh->d_tet_faces, uint32_t(mesh->host.num_cells),
+                                     r->vfix.ptr, r->vgeo.ptr, reinterpret_cast<const float4*>(d_colors), r->cam, sh,
+                                     reinterpret_cast<const float4*>(d_image_adjoint), r->tfinal.ptr,
+                                     r->wstate.ptr, uint32_t(r->V), r->grad_rows.ptr, d_grad_positions,
+                                     reinterpret_cast<float4*>(d_grad_colors), s);
+            check_launch("ray-tet adjoint walk");
+        } else {
+            dtv::launch_adjoint(r->offsets.ptr, r->records.ptr, mesh->d_faces, r->vgeo.ptr,
+                                reinterpret_cast<const float4*>(d_colors), r->cam, sh,
+                                reinterpret_cast<const float4*>(d_image_adjoint), r->tfinal.ptr, r->term.ptr,
+                                uint32_t(r->V), r->grad_rows.ptr, d_grad_positions,
+                                reinterpret_cast<float4*>(d_grad_colors), s);
+            check_launch("adjoint");
+        }
         rec_event(r, 8, s);
         r->adjoint_timed = true;
     });
@@ -396,6 +450,15 @@ int32_t dtv_renderer_copy_fragments(const dtv_renderer* r, uint64_t* h_offsets, 
                 DTV_CK(cudaMemcpyAsync(h_records, r->records.ptr, sizeof(u64) * r->nf, cudaMemcpyDeviceToHost, s));
         }
         DTV_CK(cudaStreamSynchronize(s));
+        if (h_records && r->type == DTV_RENDERER_INTERSECTION) {
+            // Boundary-list records name faces of the boundary subset; report global face ids.
+            const auto& bg = r->mesh->bf_global;
+            for (uint64_t i = 0; i < r->nf; ++i) {
+                const uint32_t lo = uint32_t(h_records[i]);
+                const uint32_t g = bg[lo >> 2];
+                h_records[i] = (h_records[i] & 0xffffffff00000000ull) | (uint64_t(g) << 2) | (lo & 3u);
+            }
+        }
     });
 }
 
@@ -405,9 +468,16 @@ int32_t dtv_renderer_copy_pixel_state(const dtv_renderer* r, float* h_t, uint32_
         if (!r->have_render) throw DtvError(DTV_ERR_STATE, "no render to copy from");
         cudaStream_t s = static_cast<cudaStream_t>(stream);
         if (h_t) DTV_CK(cudaMemcpyAsync(h_t, r->tfinal.ptr, sizeof(float) * r->P, cudaMemcpyDeviceToHost, s));
-        if (h_term)
+        std::vector<uint4> ws;
+        if (h_term && r->type == DTV_RENDERER_INTERSECTION) {
+            // Ray-tet path: the per-pixel value is the number of tet segments composited.
+            ws.resize(r->P);
+            DTV_CK(cudaMemcpyAsync(ws.data(), r->wstate.ptr, sizeof(uint4) * r->P, cudaMemcpyDeviceToHost, s));
+        } else if (h_term) {
             DTV_CK(cudaMemcpyAsync(h_term, r->term.ptr, sizeof(uint32_t) * r->P, cudaMemcpyDeviceToHost, s));
+        }
         DTV_CK(cudaStreamSynchronize(s));
+        for (uint64_t p = 0; p < ws.size(); ++p) h_term[p] = ws[p].w;
     });
 }
 

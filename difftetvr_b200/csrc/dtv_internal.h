@@ -18,6 +18,7 @@ struct MeshHost {
     std::vector<uint32_t> face_to_tet;    // 2F
     std::vector<uint32_t> vertex_boundary;// V
     std::vector<uint32_t> cells;          // 4T
+    std::vector<uint32_t> tet_faces;      // 4T: unique face index of face j of tet c (TetFaceTable order)
 };
 
 // Builds faces from cells (restates buildFacesSlim, TetMesh.cpp:1218-1268).
@@ -53,12 +54,27 @@ void launch_adjoint(const unsigned long long* offsets, const unsigned long long*
                     const VGeo* vgeo, const float4* colors, const CamDev& cam, const ShadeDev& sh,
                     const float4* dimage, const float* tfinal, const uint32_t* term, uint32_t V,
                     float4* grad_rows, float* grad_pos, float4* grad_col, cudaStream_t s);
+// Adds the interleaved [V][2] gradient rows into grad_pos [V,3] / grad_col [V,4].
+void launch_scatter_grads(const float4* grad_rows, uint32_t V, float* grad_pos, float4* grad_col, cudaStream_t s);
 
 void launch_loss_l2(const float* image, const float* target, uint64_t n, float scale, float* adjoint,
                     float* loss_accum, cudaStream_t s);
 void launch_adam(float* param, const float* grad, float* m, float* v, uint64_t n, float lr, float beta1,
                  float beta2, float eps, float bc1, float bc2, int clamp_mode, const uint32_t* fixed_mask,
                  int fixed_mode, int stride, cudaStream_t s);
+
+// Ray-tet path (dtv_raytet.cu).
+void launch_walk_composite(const unsigned long long* b_offsets, const unsigned long long* b_records,
+                           const uint32_t* bf_global, const uint4* faces, const uint32_t* face_to_tet,
+                           const uint32_t* tet_faces, uint32_t num_tets, const int2* vfix, const VGeo* vgeo,
+                           const float4* colors, const CamDev& cam, const ShadeDev& sh, float4* image,
+                           float* tfinal, uint4* wstate, cudaStream_t s);
+void launch_walk_adjoint(const unsigned long long* b_offsets, const unsigned long long* b_records,
+                         const uint32_t* bf_global, const uint4* faces, const uint32_t* face_to_tet,
+                         const uint32_t* tet_faces, uint32_t num_tets, const int2* vfix, const VGeo* vgeo,
+                         const float4* colors, const CamDev& cam, const ShadeDev& sh, const float4* dimage,
+                         const float* tfinal, const uint4* wstate, uint32_t V, float4* grad_rows, float* grad_pos,
+                         float4* grad_col, cudaStream_t s);
 
 // Accessors used by the allocation-free entry point (dtv_noalloc.cu); they
 // expose what dtv_renderer_render derives from its arguments.

@@ -385,6 +385,10 @@ void launch_adjoint(const u64* offsets, const u64* records, const uint4* faces, 
     dim3 grid((cam.W + kTile - 1) / kTile, (cam.H + kTile - 1) / kTile);
     k_adjoint<<<grid, kTile * kTile, 0, s>>>(offsets, records, faces, vgeo, colors, cam.W, cam.H, cam, sh, dimage,
                                              tfinal, term, grad_rows);
+    launch_scatter_grads(grad_rows, V, grad_pos, grad_col, s);
+}
+
+void launch_scatter_grads(const float4* grad_rows, uint32_t V, float* grad_pos, float4* grad_col, cudaStream_t s) {
     if (V) k_scatter_grads<<<(V + 255) / 256, 256, 0, s>>>(grad_rows, V, grad_pos, grad_col);
 }
 

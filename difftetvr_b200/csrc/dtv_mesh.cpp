@@ -63,11 +63,13 @@ void build_faces(const uint32_t* cells, uint64_t T, uint64_t V, MeshHost& out) {
     out.tri.reserve(3 * (NF4 / 2 + 16));
     out.face_boundary.reserve(NF4 / 2 + 16);
     out.face_to_tet.reserve(2 * (NF4 / 2 + 16));
+    out.tet_faces.assign(NF4, 0u);
     for (uint64_t b = 0; b < V; ++b) {
         for (uint64_t i = start[b]; i < start[b + 1]; ++i) {
             const Rec& r = sorted[i];
             const bool same = (i > start[b]) && sorted[i - 1].v1 == r.v1 && sorted[i - 1].v2 == r.v2;
             const uint32_t tet = r.fid / 4;
+            out.tet_faces[r.fid] = uint32_t(out.face_boundary.size() - (same ? 1 : 0));
             if (!same) {
                 const int j = int(r.fid % 4);
                 for (int k = 0; k < 3; ++k) out.tri.push_back(cells[4 * uint64_t(tet) + kTetFaceTable[j][k]]);

@@ -254,6 +254,48 @@ __device__ __forceinline__ void frag_vertex_grads(const FragV& fr, float qx, flo
     }
 }
 
+// Adjoint of one sub-segment (colour c0 -> c1, density a, length tSeg) of
+// the 4-sub-segment integral.  T holds the transmittance after the segment and
+// is rebuilt in place to the one before it (T_in = T_out / A); gT is the
+// running transmittance adjoint.  Outputs: dL/dtSeg, dL/da and the colour
+// adjoints of both sub-segment ends.
+__device__ __forceinline__ void sub_segment_adjoint(float tSeg, float a, float4 c0, float4 c1, float gC0, float gC1,
+                                                    float gC2, float& T, float& gT, float& g_t, float& g_a,
+                                                    float& gc0x, float& gc0y, float& gc0z, float& gc1x, float& gc1y,
+                                                    float& gc1z) {
+    if (a > 0.f) {
+        const SegTerms st = seg_terms(tSeg, a);
+        const float cx = st.omA * c0.x + st.K * (c0.x - c1.x);
+        const float cy = st.omA * c0.y + st.K * (c0.y - c1.y);
+        const float cz = st.omA * c0.z + st.K * (c0.z - c1.z);
+        const float Tin = T / st.A;
+        const float gax = Tin * gC0, gay = Tin * gC1, gaz = Tin * gC2;
+        const float gA = Tin * gT;
+        gT = (gC0 * cx + gC1 * cy + gC2 * cz) + gT * st.A;
+        T = Tin;
+        const float aA = a * st.A;
+        g_t = gax * (aA * (c0.x + tSeg * (c1.x - c0.x))) + gay * (aA * (c0.y + tSeg * (c1.y - c0.y))) +
+              gaz * (aA * (c0.z + tSeg * (c1.z - c0.z))) - gA * aA;
+        const float dK = seg_dK_da(tSeg, a, st);
+        const float tA = tSeg * st.A;
+        g_a = gax * (tA * c0.x + dK * (c0.x - c1.x)) + gay * (tA * c0.y + dK * (c0.y - c1.y)) +
+              gaz * (tA * c0.z + dK * (c0.z - c1.z)) - gA * tA;
+        const float k0 = st.omA + st.K;
+        gc0x = k0 * gax; gc0y = k0 * gay; gc0z = k0 * gaz;
+        gc1x = -st.K * gax; gc1y = -st.K * gay; gc1z = -st.K * gaz;
+    } else {
+        // The forward drops the sub-segment for a <= 0; the gradient is the
+        // a -> 0+ limit (BackwardCommon.glsl:121-125) so a density clamped at
+        // zero can grow again.
+        const float gax = T * gC0, gay = T * gC1, gaz = T * gC2, gA = T * gT;
+        g_t = 0.f;
+        g_a = gax * (tSeg * c0.x + 0.5f * tSeg * tSeg * (c1.x - c0.x)) +
+              gay * (tSeg * c0.y + 0.5f * tSeg * tSeg * (c1.y - c0.y)) +
+              gaz * (tSeg * c0.z + 0.5f * tSeg * tSeg * (c1.z - c0.z)) - gA * tSeg;
+        gc0x = gc0y = gc0z = gc1x = gc1y = gc1z = 0.f;
+    }
+}
+
 __device__ __forceinline__ void adjoint_pixel(
     int px, int py, const u64* __restrict__ offsets, const u64* __restrict__ records, const uint4* __restrict__ faces,
     const VGeo* __restrict__ vgeo, const float4* __restrict__ colors, int W, const CamDev& cam, const ShadeDev& sh,
@@ -290,37 +332,8 @@ __device__ __forceinline__ void adjoint_pixel(
                 const float4 c1 = lerp4(ff.col, fb.col, fe);
                 const float a = (ff.col.w + (fb.col.w - ff.col.w) * fm) * atten;
                 float g_t, g_a, gc0x, gc0y, gc0z, gc1x, gc1y, gc1z;
-                if (a > 0.f) {
-                    const SegTerms st = seg_terms(tSeg, a);
-                    const float cx = st.omA * c0.x + st.K * (c0.x - c1.x);
-                    const float cy = st.omA * c0.y + st.K * (c0.y - c1.y);
-                    const float cz = st.omA * c0.z + st.K * (c0.z - c1.z);
-                    const float Tin = T / st.A;
-                    const float gax = Tin * gC0, gay = Tin * gC1, gaz = Tin * gC2;
-                    const float gA = Tin * gT;
-                    gT = (gC0 * cx + gC1 * cy + gC2 * cz) + gT * st.A;
-                    T = Tin;
-                    const float aA = a * st.A;
-                    g_t = gax * (aA * (c0.x + tSeg * (c1.x - c0.x))) + gay * (aA * (c0.y + tSeg * (c1.y - c0.y))) +
-                          gaz * (aA * (c0.z + tSeg * (c1.z - c0.z))) - gA * aA;
-                    const float dK = seg_dK_da(tSeg, a, st);
-                    const float tA = tSeg * st.A;
-                    g_a = gax * (tA * c0.x + dK * (c0.x - c1.x)) + gay * (tA * c0.y + dK * (c0.y - c1.y)) +
-                          gaz * (tA * c0.z + dK * (c0.z - c1.z)) - gA * tA;
-                    const float k0 = st.omA + st.K;
-                    gc0x = k0 * gax; gc0y = k0 * gay; gc0z = k0 * gaz;
-                    gc1x = -st.K * gax; gc1y = -st.K * gay; gc1z = -st.K * gaz;
-                } else {
-                    // The forward drops the sub-segment for a <= 0; the gradient
-                    // is the a -> 0+ limit (BackwardCommon.glsl:121-125) so a
-                    // density clamped at zero can grow again.
-                    const float gax = T * gC0, gay = T * gC1, gaz = T * gC2, gA = T * gT;
-                    g_t = 0.f;
-                    g_a = gax * (tSeg * c0.x + 0.5f * tSeg * tSeg * (c1.x - c0.x)) +
-                          gay * (tSeg * c0.y + 0.5f * tSeg * tSeg * (c1.y - c0.y)) +
-                          gaz * (tSeg * c0.z + 0.5f * tSeg * tSeg * (c1.z - c0.z)) - gA * tSeg;
-                    gc0x = gc0y = gc0z = gc1x = gc1y = gc1z = 0.f;
-                }
+                sub_segment_adjoint(tSeg, a, c0, c1, gC0, gC1, gC2, T, gT, g_t, g_a, gc0x, gc0y, gc0z, gc1x, gc1y,
+                                    gc1z);
                 g_tot += 0.25f * g_t;
                 gcol_f.x += (1.f - fbg) * gc0x + (1.f - fe) * gc1x;
                 gcol_f.y += (1.f - fbg) * gc0y + (1.f - fe) * gc1y;

@@ -1,0 +1,257 @@
+// Ray-tet path (the reference's intersection renderer) by traversal through
+// face adjacency.
+//
+// Reference: TetMeshRendererIntersection::render (TetMeshRendererIntersection.cpp:
+// 603-707) draws the camera-facing faces of every tet, sorted by depth, and
+// intersects each pixel ray with the whole tet (IntersectRasterization.glsl:
+// 139-273, intersectRayTet in RayIntersectionTests.glsl:77-106): one segment
+// per (pixel, tet), Euclidean length along the normalised ray, the 4-sub-segment
+// integral; its adjoint (AdjointIntersectRasterization.glsl:111-362) runs
+// front to back under pixel interlock.
+//
+// Here each pixel thread finds the tets its ray crosses by walking the mesh:
+// intervals start at the pixel's front-facing boundary fragments (a small
+// count / scan / fill / sort over the boundary faces only); from a tet entered
+// through face fe the ray leaves through the back face that covers the pixel
+// under the rasteriser's exact fixed-point rule, and continues into the tet on
+// the other side of that face until it leaves through a boundary face.  No
+// per-fragment storage exists beyond the boundary lists; the adjoint walks the
+// same tets backwards (previous tet = the one across the entry face), so the
+// backward pass needs no stored lists either.  Walks are bounded by the tet
+// count (a malformed mesh cannot loop forever).
+#include "dtv_internal.h"
+#include "dtv_path.cuh"
+
+namespace dtv {
+
+constexpr uint32_t kNoTet = 0xffffffffu;
+
+// Exact coverage of the pixel centre by face f (the rule of raster_face);
+// *front_stored: the face's stored winding faces the camera.
+__device__ __forceinline__ bool face_covers_px(const uint4* __restrict__ faces, const int2* __restrict__ vfix,
+                                               uint32_t f, int px, int py, bool* front_stored) {
+    const uint4 fc = faces[f];
+    const int2 q0 = vfix[fc.x], q1 = vfix[fc.y], q2 = vfix[fc.z];
+    if (q0.x == kInvalidFix || q1.x == kInvalidFix || q2.x == kInvalidFix) return false;
+    const long long X0 = q0.x, Y0 = q0.y, X1 = q1.x, Y1 = q1.y, X2 = q2.x, Y2 = q2.y;
+    const long long area2 = (X1 - X0) * (Y2 - Y0) - (Y1 - Y0) * (X2 - X0);
+    if (area2 == 0) return false;
+    *front_stored = area2 < 0;
+    long long ax1 = X1, ay1 = Y1, ax2 = X2, ay2 = Y2;
+    if (area2 < 0) {
+        ax1 = X2; ay1 = Y2;
+        ax2 = X1; ay2 = Y1;
+    }
+    const long long Xc = 256LL * px + 128, Yc = 256LL * py + 128;
+    const long long dx0 = ax2 - ax1, dy0 = ay2 - ay1;
+    const long long dx1 = X0 - ax2, dy1 = Y0 - ay2;
+    const long long dx2 = ax1 - X0, dy2 = ay1 - Y0;
+    return edge_inside(dx0 * (Yc - ay1) - dy0 * (Xc - ax1), dx0, dy0) &&
+           edge_inside(dx1 * (Yc - ay2) - dy1 * (Xc - ax2), dx1, dy1) &&
+           edge_inside(dx2 * (Yc - Y0) - dy2 * (Xc - X0), dx2, dy2);
+}
+
+// Face of tet t (not `skip`) covering the pixel that faces the camera
+// (want_front) or away from it with respect to t's outward normal.
+__device__ __forceinline__ uint32_t tet_face_at(const uint32_t* __restrict__ tet_faces,
+                                                const uint4* __restrict__ faces,
+                                                const uint32_t* __restrict__ f2t, const int2* __restrict__ vfix,
+                                                uint32_t t, uint32_t skip, bool want_front, int px, int py) {
+    const uint4 tf = reinterpret_cast<const uint4*>(tet_faces)[t];
+    const uint32_t fs[4] = {tf.x, tf.y, tf.z, tf.w};
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const uint32_t f = fs[j];
+        if (f == skip) continue;
+        bool front_stored;
+        if (!face_covers_px(faces, vfix, f, px, py, &front_stored)) continue;
+        const bool owner = f2t[2 * size_t(f)] == t;  // stored winding is outward for the face's first tet
+        if ((front_stored == owner) == want_front) return f;
+    }
+    return kNoTet;
+}
+
+__device__ __forceinline__ uint32_t other_tet(const uint32_t* __restrict__ f2t, uint32_t f, uint32_t t) {
+    const uint32_t a = f2t[2 * size_t(f)], b = f2t[2 * size_t(f) + 1];
+    return a == t ? b : a;
+}
+
+// Length of the pixel ray per unit of view depth (|d| with d.z_view = -1).
+__device__ __forceinline__ float ray_scale(const CamDev& cam, float qx, float qy) {
+    const float dx = (qx - cam.cx) / cam.f, dy = (qy - cam.cy) / cam.f;
+    return sqrtf(1.f + dx * dx + dy * dy);
+}
+
+__global__ void __launch_bounds__(kTile * kTile) k_walk_composite(
+    const u64* __restrict__ b_offsets, const u64* __restrict__ b_records, const uint32_t* __restrict__ bf_global,
+    const uint4* __restrict__ faces, const uint32_t* __restrict__ f2t, const uint32_t* __restrict__ tet_faces,
+    uint32_t num_tets, const int2* __restrict__ vfix, const VGeo* __restrict__ vgeo,
+    const float4* __restrict__ colors, CamDev cam, ShadeDev sh, float4* __restrict__ image,
+    float* __restrict__ tfinal, uint4* __restrict__ wstate) {
+    const int px = blockIdx.x * kTile + (threadIdx.x % kTile);
+    const int py = blockIdx.y * kTile + (threadIdx.x / kTile);
+    if (px >= cam.W || py >= cam.H) return;
+    const size_t p = size_t(py) * cam.W + px;
+    const u64 beg = b_offsets[p];
+    const uint32_t nb = uint32_t(b_offsets[p + 1] - beg);
+    const float qx = float(px) + 0.5f, qy = float(py) + 0.5f;
+    const float scale = ray_scale(cam, qx, qy);
+    float C0 = 0.f, C1 = 0.f, C2 = 0.f, T = 1.f;
+    uint32_t last_tet = kNoTet, last_entry = kNoTet, last_b = 0, nseg = 0;
+    bool stop = false;
+    for (uint32_t b = 0; b < nb && !stop; ++b) {
+        const uint32_t bits = uint32_t(b_records[beg + b]);
+        if (!(bits & 1u)) continue;  // intervals start at front-facing boundary faces
+        uint32_t fe = bf_global[bits >> 2];
+        uint32_t t = f2t[2 * size_t(fe)];
+        FragV f0 = load_frag(u64(fe) << 2, qx, qy, faces, vgeo, colors);
+        for (uint32_t step = 0; step <= num_tets; ++step) {
+            const uint32_t fx = tet_face_at(tet_faces, faces, f2t, vfix, t, fe, false, px, py);
+            if (fx == kNoTet) break;
+            if (sh.use_ert && T < sh.ert_thresh) {
+                stop = true;
+                break;
+            }
+            const FragV f1 = load_frag(u64(fx) << 2, qx, qy, faces, vgeo, colors);
+            const float tSeg = (f1.z - f0.z) * scale * 0.25f;
+#pragma unroll
+            for (int s = 0; s < kNumSubdivs; ++s) {
+                const float fb = 0.25f * s, fm = 0.25f * (s + 0.5f), fe4 = 0.25f * (s + 1);
+                const float4 c0 = lerp4(f0.col, f1.col, fb);
+                const float4 c1 = lerp4(f0.col, f1.col, fe4);
+                const float a = (f0.col.w + (f1.col.w - f0.col.w) * fm) * sh.atten;
+                if (!(a > 0.f)) continue;
+                const SegTerms st = seg_terms(tSeg, a);
+                C0 += T * (st.omA * c0.x + st.K * (c0.x - c1.x));
+                C1 += T * (st.omA * c0.y + st.K * (c0.y - c1.y));
+                C2 += T * (st.omA * c0.z + st.K * (c0.z - c1.z));
+                T *= st.A;
+            }
+            last_tet = t;
+            last_entry = fe;
+            last_b = b;
+            ++nseg;
+            if (faces[fx].w & 1u) break;  // left the mesh
+            const uint32_t tn = other_tet(f2t, fx, t);
+            if (tn == kNoTet) break;
+            t = tn;
+            fe = fx;
+            f0 = f1;
+        }
+    }
+    image[p] = make_float4(C0 + T * sh.clear[0], C1 + T * sh.clear[1], C2 + T * sh.clear[2],
+                           (1.f - T) + T * sh.clear[3]);
+    tfinal[p] = T;
+    wstate[p] = make_uint4(last_tet, last_entry, last_b, nseg);
+}
+
+__global__ void __launch_bounds__(kTile * kTile) k_walk_adjoint(
+    const u64* __restrict__ b_offsets, const u64* __restrict__ b_records, const uint32_t* __restrict__ bf_global,
+    const uint4* __restrict__ faces, const uint32_t* __restrict__ f2t, const uint32_t* __restrict__ tet_faces,
+    uint32_t num_tets, const int2* __restrict__ vfix, const VGeo* __restrict__ vgeo,
+    const float4* __restrict__ colors, CamDev cam, ShadeDev sh, const float4* __restrict__ dimage,
+    const float* __restrict__ tfinal, const uint4* __restrict__ wstate, float4* __restrict__ grad_rows) {
+    const int px = blockIdx.x * kTile + (threadIdx.x % kTile);
+    const int py = blockIdx.y * kTile + (threadIdx.x / kTile);
+    if (px >= cam.W || py >= cam.H) return;
+    const size_t p = size_t(py) * cam.W + px;
+    const uint4 ws = wstate[p];
+    if (ws.x == kNoTet) return;
+    const float4 g = dimage[p];
+    if (g.x == 0.f && g.y == 0.f && g.z == 0.f && g.w == 0.f) return;
+    const GradAcc acc{grad_rows};
+    const bool use_abs = sh.use_abs_grad != 0;
+    const u64 beg = b_offsets[p];
+    const float qx = float(px) + 0.5f, qy = float(py) + 0.5f;
+    const float scale = ray_scale(cam, qx, qy);
+    const float atten = sh.atten;
+    const float gC0 = g.x, gC1 = g.y, gC2 = g.z;
+    float gT = g.x * sh.clear[0] + g.y * sh.clear[1] + g.z * sh.clear[2] + g.w * (sh.clear[3] - 1.f);
+    float T = tfinal[p];
+    uint32_t t = ws.x, fe = ws.y;
+    int b = int(ws.z);
+    uint32_t fx = tet_face_at(tet_faces, faces, f2t, vfix, t, fe, false, px, py);
+    if (fx == kNoTet) return;
+    float gz_x = 0.f;
+    float4 gcol_x = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (uint32_t step = 0; step <= num_tets; ++step) {
+        const FragV f0 = load_frag(u64(fe) << 2, qx, qy, faces, vgeo, colors);
+        const FragV f1 = load_frag(u64(fx) << 2, qx, qy, faces, vgeo, colors);
+        const float tSeg = (f1.z - f0.z) * scale * 0.25f;
+        float g_tot = 0.f;
+        float4 gcol_e = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+        for (int s = kNumSubdivs - 1; s >= 0; --s) {
+            const float fbg = 0.25f * s, fm = 0.25f * (s + 0.5f), fen = 0.25f * (s + 1);
+            const float4 c0 = lerp4(f0.col, f1.col, fbg);
+            const float4 c1 = lerp4(f0.col, f1.col, fen);
+            const float a = (f0.col.w + (f1.col.w - f0.col.w) * fm) * atten;
+            float g_t, g_a, gc0x, gc0y, gc0z, gc1x, gc1y, gc1z;
+            sub_segment_adjoint(tSeg, a, c0, c1, gC0, gC1, gC2, T, gT, g_t, g_a, gc0x, gc0y, gc0z, gc1x, gc1y,
+                                gc1z);
+            g_tot += 0.25f * g_t;
+            gcol_e.x += (1.f - fbg) * gc0x + (1.f - fen) * gc1x;
+            gcol_e.y += (1.f - fbg) * gc0y + (1.f - fen) * gc1y;
+            gcol_e.z += (1.f - fbg) * gc0z + (1.f - fen) * gc1z;
+            gcol_x.x += fbg * gc0x + fen * gc1x;
+            gcol_x.y += fbg * gc0y + fen * gc1y;
+            gcol_x.z += fbg * gc0z + fen * gc1z;
+            gcol_e.w += (1.f - fm) * g_a * atten;
+            gcol_x.w += fm * g_a * atten;
+        }
+        float gz_e = -g_tot * scale;
+        gz_x += g_tot * scale;
+        frag_vertex_grads(f1, qx, qy, vgeo, colors, cam, gz_x, gcol_x, use_abs, acc);
+        if (faces[fe].w & 1u) {
+            frag_vertex_grads(f0, qx, qy, vgeo, colors, cam, gz_e, gcol_e, use_abs, acc);
+            // Previous interval: its exit is the last back-facing boundary fragment before b.
+            int bb = b - 1;
+            while (bb >= 0 && (uint32_t(b_records[beg + bb]) & 1u)) --bb;
+            if (bb < 0) return;
+            fx = bf_global[uint32_t(b_records[beg + bb]) >> 2];
+            t = f2t[2 * size_t(fx)];
+            fe = tet_face_at(tet_faces, faces, f2t, vfix, t, fx, true, px, py);
+            if (fe == kNoTet) return;
+            int be = bb - 1;
+            while (be >= 0 && !(uint32_t(b_records[beg + be]) & 1u)) --be;
+            b = be < 0 ? 0 : be;
+            gz_x = 0.f;
+            gcol_x = make_float4(0.f, 0.f, 0.f, 0.f);
+            continue;
+        }
+        const uint32_t tprev = other_tet(f2t, fe, t);
+        if (tprev == kNoTet) return;
+        const uint32_t feprev = tet_face_at(tet_faces, faces, f2t, vfix, tprev, fe, true, px, py);
+        if (feprev == kNoTet) return;
+        fx = fe;
+        gz_x = gz_e;
+        gcol_x = gcol_e;
+        t = tprev;
+        fe = feprev;
+    }
+}
+
+void launch_walk_composite(const u64* b_offsets, const u64* b_records, const uint32_t* bf_global,
+                           const uint4* faces, const uint32_t* face_to_tet, const uint32_t* tet_faces,
+                           uint32_t num_tets, const int2* vfix, const VGeo* vgeo, const float4* colors,
+                           const CamDev& cam, const ShadeDev& sh, float4* image, float* tfinal, uint4* wstate,
+                           cudaStream_t s) {
+    dim3 grid((cam.W + kTile - 1) / kTile, (cam.H + kTile - 1) / kTile);
+    k_walk_composite<<<grid, kTile * kTile, 0, s>>>(b_offsets, b_records, bf_global, faces, face_to_tet, tet_faces,
+                                                    num_tets, vfix, vgeo, colors, cam, sh, image, tfinal, wstate);
+}
+
+void launch_walk_adjoint(const u64* b_offsets, const u64* b_records, const uint32_t* bf_global, const uint4* faces,
+                         const uint32_t* face_to_tet, const uint32_t* tet_faces, uint32_t num_tets,
+                         const int2* vfix, const VGeo* vgeo, const float4* colors, const CamDev& cam,
+                         const ShadeDev& sh, const float4* dimage, const float* tfinal, const uint4* wstate,
+                         uint32_t V, float4* grad_rows, float* grad_pos, float4* grad_col, cudaStream_t s) {
+    cudaMemsetAsync(grad_rows, 0, sizeof(float4) * 2 * size_t(V), s);
+    dim3 grid((cam.W + kTile - 1) / kTile, (cam.H + kTile - 1) / kTile);
+    k_walk_adjoint<<<grid, kTile * kTile, 0, s>>>(b_offsets, b_records, bf_global, faces, face_to_tet, tet_faces,
+                                                  num_tets, vfix, vgeo, colors, cam, sh, dimage, tfinal, wstate,
+                                                  grad_rows);
+    launch_scatter_grads(grad_rows, V, grad_pos, grad_col, s);
+}
+
+}  // namespace dtv

@@ -27,7 +27,7 @@ class Renderer:
 
     def __init__(self, renderer_type: RendererType = RendererType.PPLL):
         renderer_type = RendererType(renderer_type)
-        if renderer_type != RendererType.PPLL:
+        if renderer_type == RendererType.PROJECTION:
             raise RuntimeError(f"RendererType.{renderer_type.name} is not provided by difftetvr_b200")
         self._type = renderer_type
         h = ctypes.c_void_p()
@@ -155,12 +155,11 @@ class Renderer:
         self._last_image = image
         return image
 
-    def render_adjoint(self, image_adjoint: torch.Tensor, use_abs_grad: bool = False) -> None:
+    def _check_adjoint(self, image_adjoint: torch.Tensor, name: str):
         mesh = self._tet_mesh
         if mesh is None or mesh.get_is_empty():
-            raise RuntimeError("Missing valid tet mesh in Renderer.render_adjoint.")
+            raise RuntimeError(f"Missing valid tet mesh in Renderer.{name}.")
         pos = mesh.get_vertex_positions()
-        col = mesh.get_vertex_colors()
         if not torch.is_tensor(image_adjoint) or image_adjoint.device != pos.device:
             raise RuntimeError(
                 "Error in render_adjoint: The tensors must be on the device used at initialization time.")
@@ -172,15 +171,41 @@ class Renderer:
             raise RuntimeError("Error in render_adjoint: The only data type currently supported is 32-bit float.")
         if tuple(image_adjoint.shape[:2]) != (self._height, self._width):
             raise RuntimeError("Error in render_adjoint: image size does not match the viewport.")
-        image_adjoint = image_adjoint.contiguous()
+        return mesh, image_adjoint.contiguous()
+
+    def _adjoint(self, mesh: TetMesh, image_adjoint: torch.Tensor, use_abs_grad: bool, grad_positions: torch.Tensor,
+                 grad_colors: torch.Tensor) -> None:
+        pos = mesh.get_vertex_positions()
+        col = mesh.get_vertex_colors()
+        stream = torch.cuda.current_stream(pos.device).cuda_stream
+        _lib.call("dtv_renderer_render_adjoint", self._handle, mesh.native.handle, pos.detach().data_ptr(),
+                  col.detach().data_ptr(), image_adjoint.data_ptr(), int(bool(use_abs_grad)),
+                  grad_positions.data_ptr(), grad_colors.data_ptr(), stream)
+
+    def render_adjoint(self, image_adjoint: torch.Tensor, use_abs_grad: bool = False) -> None:
+        """Adds the vertex position / colour gradients into the mesh tensors' .grad
+        (Module.cpp:922-959)."""
+        mesh, image_adjoint = self._check_adjoint(image_adjoint, "render_adjoint")
+        pos = mesh.get_vertex_positions()
+        col = mesh.get_vertex_colors()
         if pos.grad is None:
             pos.grad = torch.zeros_like(pos)
         if col.grad is None:
             col.grad = torch.zeros_like(col)
-        stream = torch.cuda.current_stream(pos.device).cuda_stream
-        _lib.call("dtv_renderer_render_adjoint", self._handle, mesh.native.handle, pos.detach().data_ptr(),
-                  col.detach().data_ptr(), image_adjoint.data_ptr(), int(bool(use_abs_grad)),
-                  pos.grad.data_ptr(), col.grad.data_ptr(), stream)
+        self._adjoint(mesh, image_adjoint, use_abs_grad, pos.grad, col.grad)
+
+    def render_adjoint_into(self, image_adjoint: torch.Tensor, grad_positions: torch.Tensor,
+                            grad_colors: torch.Tensor, use_abs_grad: bool = False) -> None:
+        """Adds the gradients into caller-owned contiguous float32 tensors
+        [V, 3] / [V, 4] (grad_colors 16-byte aligned) instead of .grad."""
+        mesh, image_adjoint = self._check_adjoint(image_adjoint, "render_adjoint_into")
+        V = mesh.get_num_vertices()
+        for t, c in ((grad_positions, 3), (grad_colors, 4)):
+            if (not torch.is_tensor(t) or t.dtype != torch.float32 or not t.is_contiguous()
+                    or tuple(t.shape) != (V, c) or t.device != image_adjoint.device):
+                raise RuntimeError(f"Error in render_adjoint_into: gradient tensors must be contiguous float32 "
+                                   f"[{V}, 3] / [{V}, 4] on the mesh's device.")
+        self._adjoint(mesh, image_adjoint, use_abs_grad, grad_positions, grad_colors)
 
     # -- fragment list export (Module.cpp:960-981) -------------------------
     def set_export_linked_list_data(self) -> None:

@@ -30,7 +30,7 @@ extern "C" {
 /* Renderer types, numbered as RendererType in src/Renderer/TetMeshRendererType.hpp:32-37. */
 #define DTV_RENDERER_PPLL 0
 #define DTV_RENDERER_PROJECTION 1   /* not provided; dtv_renderer_create returns DTV_ERR_ARG */
-#define DTV_RENDERER_INTERSECTION 2
+#define DTV_RENDERER_INTERSECTION 2 /* ray-tet: one segment per (pixel, tet), found by walking face adjacency */
 
 typedef struct dtv_mesh dtv_mesh;
 typedef struct dtv_renderer dtv_renderer;
@@ -130,12 +130,16 @@ int32_t dtv_renderer_get_num_fragments(const dtv_renderer* r, uint64_t* num_frag
  * get_start_offset_buffer (Module.cpp:960-981) with an offsets + records
  * layout: h_offsets u64[H*W+1], h_records u64[Nf] where
  * record = (fp32 view-depth bits << 32) | (faceIndex << 2) | (boundary << 1) | frontFacing.
- * Either pointer may be NULL; records_capacity is the element count of h_records. */
+ * Either pointer may be NULL; records_capacity is the element count of h_records.
+ * For an INTERSECTION renderer the lists hold the boundary faces only (the
+ * interval entries and exits of each pixel ray); faceIndex is the global face id. */
 int32_t dtv_renderer_copy_fragments(const dtv_renderer* r, uint64_t* h_offsets, uint64_t* h_records,
                                     uint64_t records_capacity, dtv_stream stream);
 
 /* Per-pixel state of the last render: final transmittance f32[H*W] and the
- * termination index u32[H*W] (terminationIndexImage, Forward.glsl:256-259). */
+ * termination index u32[H*W] (terminationIndexImage, Forward.glsl:256-259);
+ * for an INTERSECTION renderer the second array is the number of tet segments
+ * composited per pixel. */
 int32_t dtv_renderer_copy_pixel_state(const dtv_renderer* r, float* h_transmittance, uint32_t* h_termination,
                                       dtv_stream stream);
 
