@@ -42,6 +42,7 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-raytet", action="store_true")
     ap.add_argument("--batched-res", type=str, default="512,1024")
     ap.add_argument("--batched-steps", type=int, default=3)
     ap.add_argument("--no-serving", action="store_true")
@@ -126,7 +127,7 @@ def ncu_traffic_per_unit():
 
 
 # ---------------------------------------------------------------------------
-def build_scene(args, device):
+def build_scene(args, device, renderer_type=None):
     import numpy as np
     import torch
 
@@ -143,7 +144,7 @@ def build_scene(args, device):
         mesh = d.TetMesh()
         mesh.set_use_gradients(True)
         mesh.set_tet_mesh_data(cells, pos, col)
-        r = d.Renderer(d.RendererType.PPLL)
+        r = d.Renderer(d.RendererType.PPLL if renderer_type is None else renderer_type)
         r.set_tet_mesh(mesh)
         r.set_viewport_size(args.res, args.res)
         r.set_camera_fovy(S.FOVY_45)
@@ -303,6 +304,65 @@ def run_ours(args, rank, world):
         "clocks": clk,
     }
     return result, sc
+
+
+def run_raytet(args):
+    """Ray-tet traversal path (intersection renderer) on the plain workload:
+    same mesh, views, targets and step (render, loss, adjoint, Adam)."""
+    import torch
+
+    import difftetvr_b200 as d
+    from difftetvr_b200 import _lib
+    from difftetvr_b200.optim import CLAMP_NONNEGATIVE, Adam
+
+    device = torch.device("cuda", torch.cuda.current_device())
+    sc = build_scene(args, device, d.RendererType.INTERSECTION)
+    mesh, r, views, targets = sc["mesh"], sc["renderer"], sc["views"], sc["targets"]
+    pos, col = mesh.get_vertex_positions(), mesh.get_vertex_colors()
+    opt = Adam([{"params": [col], "lr": LR_COL, "clamp": CLAMP_NONNEGATIVE},
+                {"params": [pos], "lr": LR_POS}], betas=(0.9, 0.999), eps=1e-8)
+    n_img = targets[0].numel()
+    adj = torch.empty_like(targets[0])
+    loss_acc = torch.zeros(1, device=device)
+    stream = torch.cuda.current_stream(device)
+
+    def step(i):
+        pos.grad.zero_()
+        col.grad.zero_()
+        r.set_view_matrix(views[i % len(views)])
+        image = r.render()
+        _lib.call("dtv_loss_l2", image.data_ptr(), targets[i % len(views)].data_ptr(), n_img,
+                  1.0 / n_img, adj.data_ptr(), loss_acc.data_ptr(), stream.cuda_stream)
+        r.render_adjoint(adj)
+        opt.step()
+
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for i in range(args.steps):
+        step(args.warmup + i)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    ms = t0.elapsed_time(t1) / args.steps
+    # Stage breakdown on separate steps (stage events add host waits).
+    r.set_stage_timing(True)
+    stage_sum, segs = {k: 0.0 for k in r.STAGES}, 0
+    n_st = min(args.steps, 5)
+    for i in range(n_st):
+        step(i)
+        for k, v in r.get_stage_times().items():
+            stage_sum[k] += v
+        segs += int(r.get_pixel_state()[1].sum())
+    r.set_stage_timing(False)
+    out = {"iter_per_s": 1e3 / ms, "ms_per_step": ms, "segments_per_step": segs / n_st,
+           "boundary_fragments_per_step": r.get_num_fragments(),
+           "stage_ms": {k: round(v / n_st, 4) for k, v in stage_sum.items()},
+           "note": "segments = (pixel, tet) pairs composited; stages count/fill/sort run on boundary faces only"}
+    del sc
+    torch.cuda.empty_cache()
+    return out
 
 
 def run_batched(args, res: int, steps: int, warmup: int = 2):
@@ -568,6 +628,8 @@ def main():
     if world > 1:
         torch.distributed.barrier()
     result, sc = run_ours(args, rank, world)
+    if not args.no_raytet:
+        result["raytet"] = run_raytet(args)
     if not args.no_batched:
         import torch
         del sc["renderer"], sc["mesh"], sc["targets"]

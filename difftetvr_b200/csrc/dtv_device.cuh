@@ -2,7 +2,8 @@
 // volume-rendering path.  The discrete parts (projection to 1/256-pixel fixed
 // point, the edge-function coverage rule, the FP32 depth key) use explicitly
 // rounded FP32 intrinsics so they are bit-reproducible; the continuous parts
-// (barycentrics, colours, segment integrals, adjoints) use ordinary FP32.
+// (barycentrics, colours, segment integrals, adjoints) use ordinary FP32 with
+// the fast reciprocal (__fdividef) where a quotient feeds only them.
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -103,14 +104,14 @@ __device__ __forceinline__ void face_interp(const VGeo& a, const VGeo& b, const 
     const double E2 = d0x * d1y - d0y * d1x;
     const double A = E0 + E1 + E2;
     fi.A = float(A);
-    const float iA = 1.0f / fi.A;
+    const float iA = __fdividef(1.0f, fi.A);
     fi.lam[0] = float(E0) * iA;
     fi.lam[1] = float(E1) * iA;
     fi.lam[2] = float(E2) * iA;
     fi.dx[0] = float(d0x); fi.dx[1] = float(d1x); fi.dx[2] = float(d2x);
     fi.dy[0] = float(d0y); fi.dy[1] = float(d1y); fi.dy[2] = float(d2y);
     const float u0 = fi.lam[0] * a.iz, u1 = fi.lam[1] * b.iz, u2 = fi.lam[2] * c.iz;
-    fi.zb = 1.0f / (u0 + u1 + u2);
+    fi.zb = __fdividef(1.0f, u0 + u1 + u2);
     fi.bary[0] = u0 * fi.zb;
     fi.bary[1] = u1 * fi.zb;
     fi.bary[2] = u2 * fi.zb;

@@ -223,7 +223,7 @@ __device__ __forceinline__ void frag_vertex_grads(const FragV& fr, float qx, flo
         giz[j] = gu * fi.lam[j];
         sl += glam[j] * fi.lam[j];
     }
-    const float invA = 1.0f / fi.A;
+    const float invA = __fdividef(1.0f, fi.A);
     float gE[3];
 #pragma unroll
     for (int j = 0; j < 3; ++j) gE[j] = (glam[j] - sl) * invA;
@@ -264,11 +264,11 @@ __device__ __forceinline__ void sub_segment_adjoint(float tSeg, float a, float4 
                                                     float& gc0x, float& gc0y, float& gc0z, float& gc1x, float& gc1y,
                                                     float& gc1z) {
     if (a > 0.f) {
-        const SegTerms st = seg_terms(tSeg, a);
+        const SegTerms st = seg_terms_adj(tSeg, a);
         const float cx = st.omA * c0.x + st.K * (c0.x - c1.x);
         const float cy = st.omA * c0.y + st.K * (c0.y - c1.y);
         const float cz = st.omA * c0.z + st.K * (c0.z - c1.z);
-        const float Tin = T / st.A;
+        const float Tin = __fdividef(T, st.A);
         const float gax = Tin * gC0, gay = Tin * gC1, gaz = Tin * gC2;
         const float gA = Tin * gT;
         gT = (gC0 * cx + gC1 * cy + gC2 * cz) + gT * st.A;
@@ -276,7 +276,7 @@ __device__ __forceinline__ void sub_segment_adjoint(float tSeg, float a, float4 
         const float aA = a * st.A;
         g_t = gax * (aA * (c0.x + tSeg * (c1.x - c0.x))) + gay * (aA * (c0.y + tSeg * (c1.y - c0.y))) +
               gaz * (aA * (c0.z + tSeg * (c1.z - c0.z))) - gA * aA;
-        const float dK = seg_dK_da(tSeg, a, st);
+        const float dK = st.dK;
         const float tA = tSeg * st.A;
         g_a = gax * (tA * c0.x + dK * (c0.x - c1.x)) + gay * (tA * c0.y + dK * (c0.y - c1.y)) +
               gaz * (tA * c0.z + dK * (c0.z - c1.z)) - gA * tA;
