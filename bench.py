@@ -43,6 +43,13 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-raytet", action="store_true")
+    ap.add_argument("--no-scale", action="store_true")
+    ap.add_argument("--scale-n", type=int, default=128)
+    ap.add_argument("--scale-res", type=int, default=2048)
+    ap.add_argument("--scale-steps", type=int, default=3)
+    ap.add_argument("--scale-warmup", type=int, default=1)
+    ap.add_argument("--scale-cap-gb", type=float, default=40.0)
+    ap.add_argument("--scale-recompute-gb", type=float, default=4.0)
     ap.add_argument("--batched-res", type=str, default="512,1024")
     ap.add_argument("--batched-steps", type=int, default=3)
     ap.add_argument("--no-serving", action="store_true")
@@ -365,6 +372,84 @@ def run_raytet(args):
     return out
 
 
+def run_scale(args):
+    """Differentiation at scale: Kuhn n^3 at res^2, forward + autograd backward
+    (DifferentiableRenderer, L2 loss against a second-seed target) + Adam, with
+    the fragment lists stored whole under a 40 GB cap vs rebuilt per row band in
+    backward under a smaller budget."""
+    import torch
+
+    import difftetvr_b200 as d
+    from difftetvr_b200 import synthetic as S
+    from difftetvr_b200.optim import CLAMP_NONNEGATIVE, Adam, l2_loss
+
+    n, res = args.scale_n, args.scale_res
+    t_setup = time.perf_counter()
+    cells, pos = S.kuhn_mesh(n, seed=0)
+    col = S.gaussian_colors(pos, seed=0)
+    _, pos_t = S.kuhn_mesh(n, seed=1)
+    col_t = S.gaussian_colors(pos_t, seed=1)
+    view = S.sphere_camera(100)
+
+    def make(p, c):
+        m = d.TetMesh()
+        m.set_use_gradients(True)
+        m.set_tet_mesh_data(cells, p, c)
+        r = d.Renderer(d.RendererType.PPLL)
+        r.set_tet_mesh(m)
+        r.set_viewport_size(res, res)
+        r.set_camera_fovy(S.FOVY_45)
+        r.set_attenuation(1.0)
+        r.set_clear_color(d.vec4(0, 0, 0, 0))
+        r.set_view_matrix(view)
+        return m, r
+
+    m_t, r_t = make(pos_t, col_t)
+    with torch.no_grad():
+        target = r_t.render().clone()
+    del r_t, m_t
+    mesh, r = make(pos, col)
+    setup_s = time.perf_counter() - t_setup
+    p, c = mesh.get_vertex_positions(), mesh.get_vertex_colors()
+    opt = Adam([{"params": [c], "lr": LR_COL, "clamp": CLAMP_NONNEGATIVE}, {"params": [p], "lr": LR_POS}])
+    diff = d.DifferentiableRenderer(r)
+    stream = torch.cuda.current_stream()
+
+    def step():
+        opt.zero_grad(set_to_none=False)
+        img = diff()
+        loss = l2_loss(img, target)
+        loss.backward()
+        opt.step()
+        return img
+
+    out = {"workload": f"Kuhn {n}^3 ({6 * n ** 3} tets, {mesh.get_num_vertices()} verts), {res}x{res}, "
+                       f"fwd + autograd bwd + Adam", "setup_s": round(setup_s, 1), "modes": []}
+    for name, budget in (("stored", int(args.scale_cap_gb * 1e9)), ("recompute", int(args.scale_recompute_gb * 1e9))):
+        r.set_fragment_budget_bytes(budget)
+        for _ in range(args.scale_warmup):
+            img = step()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.scale_steps):
+            img = step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.scale_steps
+        nf = r.get_num_fragments()
+        bands = r.get_num_bands()
+        covered = int((img[..., 3] > 0).sum())
+        out["modes"].append({
+            "mode": name, "budget_bytes": budget, "bands": bands, "ms_per_step": ms, "iter_per_s": 1e3 / ms,
+            "fragments": nf, "record_bytes": 8 * nf,
+            "record_bytes_held": 8 * nf if bands == 0 else min(8 * nf, budget),
+            "mean_list_length_covered": nf / max(covered, 1), "fragments_per_s": nf / (ms / 1e3)})
+    del diff, r, mesh
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_batched(args, res: int, steps: int, warmup: int = 2):
     """Batching config: meshes Kuhn 64^3 / 24^3 / 40^3, 32 views per step on a
     Fibonacci sphere split 16 / 10 / 6, all at res x res; forward + adjoint +
@@ -630,6 +715,8 @@ def main():
     result, sc = run_ours(args, rank, world)
     if not args.no_raytet:
         result["raytet"] = run_raytet(args)
+    if not args.no_scale:
+        result["scale"] = run_scale(args)
     if not args.no_batched:
         import torch
         del sc["renderer"], sc["mesh"], sc["targets"]

@@ -19,6 +19,8 @@ DTV_ERR_BUDGET = 2
 DTV_ERR_CUDA = 3
 DTV_ERR_TIMEOUT = 4
 DTV_ERR_STATE = 5
+DTV_OVER_BUDGET_ERROR = 0
+DTV_OVER_BUDGET_RECOMPUTE = 1
 
 _ERR_NAMES = {
     DTV_ERR_ARG: "DTV_ERR_ARG",
@@ -52,7 +54,7 @@ class RenderParams(ctypes.Structure):
         ("early_ray_out_thresh", ctypes.c_float),
         ("clear_color", ctypes.c_float * 4),
         ("use_abs_grad", ctypes.c_int32),
-        ("reserved0", ctypes.c_int32),
+        ("over_budget", ctypes.c_int32),
         ("fragment_budget_bytes", ctypes.c_uint64),
     ]
 
@@ -112,6 +114,7 @@ SIGNATURES = {
     "dtv_renderer_render_adjoint": (ctypes.c_int32, [c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.c_int32, c_vp, c_vp,
                                                      c_vp]),
     "dtv_renderer_get_num_fragments": (ctypes.c_int32, [c_vp, c_u64p]),
+    "dtv_renderer_get_num_bands": (ctypes.c_int32, [c_vp, ctypes.POINTER(ctypes.c_int32)]),
     "dtv_renderer_copy_fragments": (ctypes.c_int32, [c_vp, c_vp, c_vp, ctypes.c_uint64, c_vp]),
     "dtv_renderer_copy_pixel_state": (ctypes.c_int32, [c_vp, c_vp, c_vp, c_vp]),
     "dtv_renderer_set_timing": (ctypes.c_int32, [c_vp, ctypes.c_int32]),

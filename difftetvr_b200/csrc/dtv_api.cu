@@ -2,11 +2,14 @@
 // include/difftetvr_b200.h).  Host orchestration: buffers, stage order, the
 // one host synchronisation per render (the exact fragment count from the scan
 // sizes the record buffer), error reporting.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <stdexcept>
 #include <string>
+#include <utility>
+#include <vector>
 #include "difftetvr_b200.h"
 #include "dtv_host.h"
 #include "dtv_internal.h"
@@ -78,6 +81,12 @@ struct dtv_renderer {
     DevBuf<uint32_t> long_list;
     DevBuf<uint32_t> flags;
     DevBuf<float4> grad_rows;     // [V][2] interleaved vertex gradient accumulator
+    // Row bands [row0, row1) of the last render when its lists exceeded the
+    // fragment budget (each band's lists are rebuilt by the adjoint); empty
+    // when the lists are stored whole.
+    std::vector<std::pair<int, int>> bands;
+    u64* h_rowoff = nullptr;      // pinned row-start offsets (H+1)
+    size_t h_rowoff_cap = 0;
     DevBuf<uint4> wstate;         // ray-tet path: (last tet, its entry face, boundary entry index, segments)
     u64* h_nf = nullptr;          // pinned
     uint32_t* h_flags = nullptr;  // pinned
@@ -110,6 +119,117 @@ void check_pending_flags(dtv_renderer* r) {
 
 void rec_event(dtv_renderer* r, int idx, cudaStream_t s) {
     if (r->timing) DTV_CK(cudaEventRecord(r->ev[idx], s));
+}
+
+// Splits the image into row bands whose fragment records each fit `cap`
+// (greedy, from the row-start offsets of the full scan).  Returns the largest
+// band's record count.
+uint64_t plan_bands(dtv_renderer* r, int W, int H, uint64_t cap, cudaStream_t s) {
+    if (r->h_rowoff_cap < size_t(H) + 1) {
+        if (r->h_rowoff) cudaFreeHost(r->h_rowoff);
+        r->h_rowoff = nullptr;
+        r->h_rowoff_cap = 0;
+        DTV_CK(cudaMallocHost(&r->h_rowoff, sizeof(u64) * (size_t(H) + 1)));
+        r->h_rowoff_cap = size_t(H) + 1;
+    }
+    // offsets[y * W] for y = 0..H: a strided copy of one u64 per row.
+    DTV_CK(cudaMemcpy2DAsync(r->h_rowoff, sizeof(u64), r->offsets.ptr, sizeof(u64) * size_t(W), sizeof(u64),
+                             size_t(H) + 1, cudaMemcpyDeviceToHost, s));
+    DTV_CK(cudaStreamSynchronize(s));
+    const u64* ro = r->h_rowoff;
+    uint64_t largest = 0;
+    int y0 = 0;
+    while (y0 < H) {
+        if (ro[y0 + 1] - ro[y0] > cap)
+            throw DtvError(DTV_ERR_BUDGET, "pixel row " + std::to_string(y0) + " alone needs " +
+                                               std::to_string(ro[y0 + 1] - ro[y0]) +
+                                               " fragments, over the budget of " + std::to_string(cap));
+        int y1 = y0 + 1;
+        while (y1 < H && ro[y1 + 1] - ro[y0] <= cap) ++y1;
+        r->bands.emplace_back(y0, y1);
+        largest = std::max<uint64_t>(largest, ro[y1] - ro[y0]);
+        y0 = y1;
+    }
+    return largest;
+}
+
+// Builds the sorted lists of rows [y0, y1) into the records buffer (band-local
+// offsets): scan of the band's counts, fill, per-pixel sort.  The band's
+// counts must hold the rasterised counts; the fill leaves them zero.
+void build_band_lists(dtv_renderer* r, const dtv_mesh* mesh, int W, int H, int y0, int y1, cudaStream_t s) {
+    const uint64_t p0 = uint64_t(y0) * W, pb = uint64_t(y1 - y0) * W;
+    dtv::launch_scan(r->counts.ptr + p0, pb, r->offsets.ptr + p0, r->scan_scratch.ptr, s);
+    check_launch("band scan");
+    dtv::launch_raster_fill(mesh->d_faces, uint32_t(mesh->host.num_faces), r->vproj.ptr, r->vfix.ptr, W, H,
+                            r->counts.ptr, r->offsets.ptr, r->records.ptr, s, y0, y1);
+    check_launch("band fill");
+    DTV_CK(cudaMemsetAsync(r->flags.ptr, 0, sizeof(uint32_t), s));  // long-list count; keep the error flag
+    dtv::launch_sort(r->offsets.ptr + p0, r->records.ptr, uint32_t(pb), r->long_list.ptr, r->flags.ptr, s);
+    check_launch("band sort");
+    dtv::launch_sort_long(r->offsets.ptr + p0, r->records.ptr, r->long_list.ptr, 0, r->flags.ptr, s);
+    check_launch("band sort long lists");
+}
+
+void record_flags(dtv_renderer* r, cudaStream_t s) {
+    DTV_CK(cudaMemcpyAsync(r->h_flags, r->flags.ptr, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    DTV_CK(cudaEventRecord(r->flags_event, s));
+    r->flags_pending = true;
+}
+
+// Forward in row bands (fragment lists over the budget): after the full count
+// and scan, each band's lists are built and composited in turn, so at most
+// `cap` records are held at once.  Counts of all rows come from the full count
+// pass; each band's fill consumes its rows' counts.
+void render_banded(dtv_renderer* r, const dtv_mesh* mesh, const float* d_colors, const dtv::CamDev& cam,
+                   const dtv::ShadeDev& sh, float* d_image, uint64_t cap, cudaStream_t s) {
+    const int W = cam.W, H = cam.H;
+    uint64_t largest = 0;
+    try {
+        largest = plan_bands(r, W, H, cap, s);
+        r->records.ensure(largest ? largest : 1, s, false, 1.0);
+    } catch (...) {
+        r->bands.clear();
+        cudaMemsetAsync(r->counts.ptr, 0, uint64_t(W) * H * sizeof(uint32_t), s);
+        throw;
+    }
+    rec_event(r, 3, s);
+    DTV_CK(cudaMemsetAsync(r->flags.ptr, 0, 2 * sizeof(uint32_t), s));
+    for (const auto& b : r->bands) {
+        build_band_lists(r, mesh, W, H, b.first, b.second, s);
+        dtv::launch_composite(r->offsets.ptr, r->records.ptr, mesh->d_faces, r->vgeo.ptr,
+                              reinterpret_cast<const float4*>(d_colors), W, H, sh,
+                              reinterpret_cast<float4*>(d_image), r->tfinal.ptr, r->term.ptr, s, b.first, b.second);
+        check_launch("band composite");
+    }
+    record_flags(r, s);
+    rec_event(r, 4, s);
+    rec_event(r, 5, s);
+    rec_event(r, 6, s);
+}
+
+// Adjoint of a banded render: per band, the lists are rebuilt (count, scan,
+// fill, sort of the band's rows, from the projection kept by the render) and
+// the band's adjoint accumulates into the shared gradient rows.
+void adjoint_banded(dtv_renderer* r, const dtv_mesh* mesh, const float* d_colors, const float* d_image_adjoint,
+                    const dtv::ShadeDev& sh, float* d_grad_positions, float* d_grad_colors, cudaStream_t s) {
+    const int W = r->cam.W, H = r->cam.H;
+    DTV_CK(cudaMemsetAsync(r->grad_rows.ptr, 0, sizeof(float4) * 2 * size_t(r->V ? r->V : 1), s));
+    DTV_CK(cudaMemsetAsync(r->flags.ptr, 0, 2 * sizeof(uint32_t), s));
+    for (const auto& b : r->bands) {
+        dtv::launch_raster_count(mesh->d_faces, uint32_t(mesh->host.num_faces), r->vproj.ptr, r->vfix.ptr, W, H,
+                                 r->counts.ptr, s, b.first, b.second);
+        check_launch("band count");
+        build_band_lists(r, mesh, W, H, b.first, b.second, s);
+        dtv::launch_adjoint_rows(r->offsets.ptr, r->records.ptr, mesh->d_faces, r->vgeo.ptr,
+                                 reinterpret_cast<const float4*>(d_colors), r->cam, sh,
+                                 reinterpret_cast<const float4*>(d_image_adjoint), r->tfinal.ptr, r->term.ptr,
+                                 b.first, b.second, r->grad_rows.ptr, s);
+        check_launch("band adjoint");
+    }
+    dtv::launch_scatter_grads(r->grad_rows.ptr, uint32_t(r->V), d_grad_positions,
+                              reinterpret_cast<float4*>(d_grad_colors), s);
+    check_launch("scatter gradients");
+    record_flags(r, s);
 }
 
 }  // namespace
@@ -280,6 +400,7 @@ int32_t dtv_renderer_destroy(dtv_renderer* r) {
     r->wstate.release();
     if (r->h_nf) cudaFreeHost(r->h_nf);
     if (r->h_flags) cudaFreeHost(r->h_flags);
+    if (r->h_rowoff) cudaFreeHost(r->h_rowoff);
     if (r->flags_event) cudaEventDestroy(r->flags_event);
     for (auto& e : r->ev)
         if (e) cudaEventDestroy(e);
@@ -338,12 +459,27 @@ int32_t dtv_renderer_render(dtv_renderer* r, const dtv_mesh* mesh, const float* 
         DTV_CK(cudaMemcpyAsync(r->h_nf, r->offsets.ptr + P, sizeof(u64), cudaMemcpyDeviceToHost, s));
         DTV_CK(cudaStreamSynchronize(s));
         const uint64_t nf = *r->h_nf;
-        if (params->fragment_budget_bytes && nf * sizeof(u64) > params->fragment_budget_bytes) {
-            // Leave counts zeroed for the next render.
-            DTV_CK(cudaMemsetAsync(r->counts.ptr, 0, P * sizeof(uint32_t), s));
-            throw DtvError(DTV_ERR_BUDGET, "render needs " + std::to_string(nf) + " fragments (" +
-                                               std::to_string(nf * sizeof(u64)) + " bytes), over the budget of " +
-                                               std::to_string(params->fragment_budget_bytes) + " bytes");
+        const uint64_t budget = params->fragment_budget_bytes;
+        r->bands.clear();
+        if (budget && nf * sizeof(u64) > budget) {
+            if (params->over_budget != DTV_OVER_BUDGET_RECOMPUTE || raytet) {
+                // Leave counts zeroed for the next render.
+                DTV_CK(cudaMemsetAsync(r->counts.ptr, 0, P * sizeof(uint32_t), s));
+                throw DtvError(DTV_ERR_BUDGET, "render needs " + std::to_string(nf) + " fragments (" +
+                                                   std::to_string(nf * sizeof(u64)) +
+                                                   " bytes), over the budget of " + std::to_string(budget) +
+                                                   " bytes");
+            }
+            render_banded(r, mesh, d_colors, cam, sh, d_image, budget / sizeof(u64), s);
+            r->adjoint_timed = false;
+            r->have_render = true;
+            r->mesh = mesh;
+            r->cam = cam;
+            r->sh = sh;
+            r->P = P;
+            r->V = V;
+            r->nf = nf;
+            return;
         }
         try {
             r->records.ensure(nf ? nf : 1, s, false, 1.25);
@@ -408,7 +544,9 @@ int32_t dtv_renderer_render_adjoint(dtv_renderer* r, const dtv_mesh* mesh, const
         sh.use_abs_grad = use_abs_grad ? 1 : 0;
         r->grad_rows.ensure(2 * (r->V ? r->V : 1), s);
         rec_event(r, 7, s);
-        if (r->type == DTV_RENDERER_INTERSECTION) {
+        if (!r->bands.empty()) {
+            adjoint_banded(r, mesh, d_colors, d_image_adjoint, sh, d_grad_positions, d_grad_colors, s);
+        } else if (r->type == DTV_RENDERER_INTERSECTION) {
             dtv::launch_walk_adjoint(r->offsets.ptr, r->records.ptr, mesh->d_bf_global, mesh->d_faces,
                                      mesh->d_face_to_tet, mesh->d_tet_faces, uint32_t(mesh->host.num_cells),
                                      r->vfix.ptr, r->vgeo.ptr, reinterpret_cast<const float4*>(d_colors), r->cam, sh,
@@ -436,11 +574,21 @@ int32_t dtv_renderer_get_num_fragments(const dtv_renderer* r, uint64_t* nf) {
     });
 }
 
+int32_t dtv_renderer_get_num_bands(const dtv_renderer* r, int32_t* num_bands) {
+    return guarded([&] {
+        require(r && num_bands, "null pointer");
+        *num_bands = r->have_render ? int32_t(r->bands.size()) : 0;
+    });
+}
+
 int32_t dtv_renderer_copy_fragments(const dtv_renderer* r, uint64_t* h_offsets, uint64_t* h_records,
                                     uint64_t cap, dtv_stream stream) {
     return guarded([&] {
         require(r != nullptr, "renderer is null");
         if (!r->have_render) throw DtvError(DTV_ERR_STATE, "no render to copy from");
+        if (!r->bands.empty())
+            throw DtvError(DTV_ERR_STATE, "the last render ran in " + std::to_string(r->bands.size()) +
+                                              " row bands under the fragment budget; its lists were not stored");
         cudaStream_t s = static_cast<cudaStream_t>(stream);
         if (h_offsets)
             DTV_CK(cudaMemcpyAsync(h_offsets, r->offsets.ptr, sizeof(u64) * (r->P + 1), cudaMemcpyDeviceToHost, s));

@@ -114,7 +114,7 @@ __global__ void __launch_bounds__(128) kb_raster(const BatchView* __restrict__ v
         const int v = view_of_item(g, first, nviews, [&](int i) { return views[i].face_base; });
         const BatchView& bv = views[v];
         raster_face<FILL>(uint32_t(g - bv.face_base), bv.faces, vproj + bv.vert_base, vfix + bv.vert_base,
-                          int(bv.W), int(bv.H), counts + bv.pix_base, offsets + bv.pix_base, records);
+                          int(bv.W), 0, int(bv.H), counts + bv.pix_base, offsets + bv.pix_base, records);
     }
 }
 

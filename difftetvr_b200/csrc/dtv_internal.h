@@ -27,11 +27,12 @@ void build_faces(const uint32_t* cells, uint64_t T, uint64_t V, MeshHost& out);
 // Launch wrappers (dtv_kernels.cu).  All run on `s`.
 void launch_project(const float* pos, uint32_t V, const CamDev& cam, float4* vproj, int2* vfix, VGeo* vgeo,
                     cudaStream_t s);
+// Pixel rows [row0, row1) only (row1 < 0: all rows).
 void launch_raster_count(const uint4* faces, uint32_t F, const float4* vproj, const int2* vfix, int W, int H,
-                         uint32_t* counts, cudaStream_t s);
+                         uint32_t* counts, cudaStream_t s, int row0 = 0, int row1 = -1);
 void launch_raster_fill(const uint4* faces, uint32_t F, const float4* vproj, const int2* vfix, int W, int H,
                         uint32_t* counts, const unsigned long long* offsets, unsigned long long* records,
-                        cudaStream_t s);
+                        cudaStream_t s, int row0 = 0, int row1 = -1);
 // Exclusive scan of counts[n] into offsets[n+1]; scratch must hold scan_scratch_elems(n) u64.
 size_t scan_scratch_elems(uint64_t n);
 void launch_scan(const uint32_t* counts, uint64_t n, unsigned long long* offsets, unsigned long long* scratch,
@@ -49,11 +50,16 @@ constexpr uint32_t kSortBlockCap = 16384;  // elements per block-sorted list (12
 
 void launch_composite(const unsigned long long* offsets, const unsigned long long* records, const uint4* faces,
                       const VGeo* vgeo, const float4* colors, int W, int H, const ShadeDev& sh, float4* image,
-                      float* tfinal, uint32_t* term, cudaStream_t s);
+                      float* tfinal, uint32_t* term, cudaStream_t s, int row0 = 0, int row1 = -1);
 void launch_adjoint(const unsigned long long* offsets, const unsigned long long* records, const uint4* faces,
                     const VGeo* vgeo, const float4* colors, const CamDev& cam, const ShadeDev& sh,
                     const float4* dimage, const float* tfinal, const uint32_t* term, uint32_t V,
                     float4* grad_rows, float* grad_pos, float4* grad_col, cudaStream_t s);
+// Adjoint of pixel rows [row0, row1) into grad_rows (no clearing, no scatter).
+void launch_adjoint_rows(const unsigned long long* offsets, const unsigned long long* records, const uint4* faces,
+                         const VGeo* vgeo, const float4* colors, const CamDev& cam, const ShadeDev& sh,
+                         const float4* dimage, const float* tfinal, const uint32_t* term, int row0, int row1,
+                         float4* grad_rows, cudaStream_t s);
 // Adds the interleaved [V][2] gradient rows into grad_pos [V,3] / grad_col [V,4].
 void launch_scatter_grads(const float4* grad_rows, uint32_t V, float* grad_pos, float4* grad_col, cudaStream_t s);
 

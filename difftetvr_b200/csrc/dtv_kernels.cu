@@ -37,22 +37,25 @@ void launch_project(const float* pos, uint32_t V, const CamDev& cam, float4* vpr
 template <bool FILL>
 __global__ void __launch_bounds__(128) k_raster(const uint4* __restrict__ faces, uint32_t F,
                                                 const float4* __restrict__ vproj, const int2* __restrict__ vfix,
-                                                int W, int H, uint32_t* __restrict__ counts,
+                                                int W, int row0, int row1, uint32_t* __restrict__ counts,
                                                 const u64* __restrict__ offsets, u64* __restrict__ records) {
     const uint32_t f = blockIdx.x * blockDim.x + threadIdx.x;
-    if (f < F) raster_face<FILL>(f, faces, vproj, vfix, W, H, counts, offsets, records);
+    if (f < F) raster_face<FILL>(f, faces, vproj, vfix, W, row0, row1, counts, offsets, records);
 }
 
 void launch_raster_count(const uint4* faces, uint32_t F, const float4* vproj, const int2* vfix, int W, int H,
-                         uint32_t* counts, cudaStream_t s) {
+                         uint32_t* counts, cudaStream_t s, int row0, int row1) {
     if (F == 0) return;
-    k_raster<false><<<(F + 127) / 128, 128, 0, s>>>(faces, F, vproj, vfix, W, H, counts, nullptr, nullptr);
+    if (row1 < 0) row1 = H;
+    k_raster<false><<<(F + 127) / 128, 128, 0, s>>>(faces, F, vproj, vfix, W, row0, row1, counts, nullptr,
+                                                    nullptr);
 }
 
 void launch_raster_fill(const uint4* faces, uint32_t F, const float4* vproj, const int2* vfix, int W, int H,
-                        uint32_t* counts, const u64* offsets, u64* records, cudaStream_t s) {
+                        uint32_t* counts, const u64* offsets, u64* records, cudaStream_t s, int row0, int row1) {
     if (F == 0) return;
-    k_raster<true><<<(F + 127) / 128, 128, 0, s>>>(faces, F, vproj, vfix, W, H, counts, offsets, records);
+    if (row1 < 0) row1 = H;
+    k_raster<true><<<(F + 127) / 128, 128, 0, s>>>(faces, F, vproj, vfix, W, row0, row1, counts, offsets, records);
 }
 
 // ---------------------------------------------------------------------------
@@ -333,31 +336,34 @@ void launch_sort_long(const u64* offsets, u64* records, const uint32_t* long_lis
 // (d) front-to-back compositing, one thread per pixel (composite_pixel).
 __global__ void __launch_bounds__(kTile * kTile) k_composite(
     const u64* __restrict__ offsets, const u64* __restrict__ records, const uint4* __restrict__ faces,
-    const VGeo* __restrict__ vgeo, const float4* __restrict__ colors, int W, int H, ShadeDev sh,
+    const VGeo* __restrict__ vgeo, const float4* __restrict__ colors, int W, int row0, int row1, ShadeDev sh,
     float4* __restrict__ image, float* __restrict__ tfinal, uint32_t* __restrict__ term) {
     const int px = blockIdx.x * kTile + (threadIdx.x % kTile);
-    const int py = blockIdx.y * kTile + (threadIdx.x / kTile);
-    if (px < W && py < H) composite_pixel(px, py, W, offsets, records, faces, vgeo, colors, sh, image, tfinal, term);
+    const int py = row0 + int(blockIdx.y) * kTile + int(threadIdx.x / kTile);
+    if (px < W && py < row1)
+        composite_pixel(px, py, W, offsets, records, faces, vgeo, colors, sh, image, tfinal, term);
 }
 
 void launch_composite(const u64* offsets, const u64* records, const uint4* faces, const VGeo* vgeo,
                       const float4* colors, int W, int H, const ShadeDev& sh, float4* image, float* tfinal,
-                      uint32_t* term, cudaStream_t s) {
-    dim3 grid((W + kTile - 1) / kTile, (H + kTile - 1) / kTile);
-    k_composite<<<grid, kTile * kTile, 0, s>>>(offsets, records, faces, vgeo, colors, W, H, sh, image, tfinal,
-                                               term);
+                      uint32_t* term, cudaStream_t s, int row0, int row1) {
+    if (row1 < 0) row1 = H;
+    if (row1 <= row0) return;
+    dim3 grid((W + kTile - 1) / kTile, (row1 - row0 + kTile - 1) / kTile);
+    k_composite<<<grid, kTile * kTile, 0, s>>>(offsets, records, faces, vgeo, colors, W, row0, row1, sh, image,
+                                               tfinal, term);
 }
 
 // ---------------------------------------------------------------------------
 // (f) adjoint (adjoint_pixel).
 __global__ void __launch_bounds__(kTile * kTile) k_adjoint(
     const u64* __restrict__ offsets, const u64* __restrict__ records, const uint4* __restrict__ faces,
-    const VGeo* __restrict__ vgeo, const float4* __restrict__ colors, int W, int H, CamDev cam, ShadeDev sh,
-    const float4* __restrict__ dimage, const float* __restrict__ tfinal, const uint32_t* __restrict__ term,
-    float4* __restrict__ grad_rows) {
+    const VGeo* __restrict__ vgeo, const float4* __restrict__ colors, int W, int row0, int row1, CamDev cam,
+    ShadeDev sh, const float4* __restrict__ dimage, const float* __restrict__ tfinal,
+    const uint32_t* __restrict__ term, float4* __restrict__ grad_rows) {
     const int px = blockIdx.x * kTile + (threadIdx.x % kTile);
-    const int py = blockIdx.y * kTile + (threadIdx.x / kTile);
-    if (px >= W || py >= H) return;
+    const int py = row0 + int(blockIdx.y) * kTile + int(threadIdx.x / kTile);
+    if (px >= W || py >= row1) return;
     adjoint_pixel(px, py, offsets, records, faces, vgeo, colors, W, cam, sh, dimage, tfinal, term,
                   GradAcc{grad_rows});
 }
@@ -382,10 +388,19 @@ void launch_adjoint(const u64* offsets, const u64* records, const uint4* faces, 
                     const float* tfinal, const uint32_t* term, uint32_t V, float4* grad_rows, float* grad_pos,
                     float4* grad_col, cudaStream_t s) {
     cudaMemsetAsync(grad_rows, 0, sizeof(float4) * 2 * size_t(V), s);
-    dim3 grid((cam.W + kTile - 1) / kTile, (cam.H + kTile - 1) / kTile);
-    k_adjoint<<<grid, kTile * kTile, 0, s>>>(offsets, records, faces, vgeo, colors, cam.W, cam.H, cam, sh, dimage,
-                                             tfinal, term, grad_rows);
+    launch_adjoint_rows(offsets, records, faces, vgeo, colors, cam, sh, dimage, tfinal, term, 0, cam.H, grad_rows,
+                        s);
     launch_scatter_grads(grad_rows, V, grad_pos, grad_col, s);
+}
+
+void launch_adjoint_rows(const u64* offsets, const u64* records, const uint4* faces, const VGeo* vgeo,
+                         const float4* colors, const CamDev& cam, const ShadeDev& sh, const float4* dimage,
+                         const float* tfinal, const uint32_t* term, int row0, int row1, float4* grad_rows,
+                         cudaStream_t s) {
+    if (row1 <= row0) return;
+    dim3 grid((cam.W + kTile - 1) / kTile, (row1 - row0 + kTile - 1) / kTile);
+    k_adjoint<<<grid, kTile * kTile, 0, s>>>(offsets, records, faces, vgeo, colors, cam.W, row0, row1, cam, sh,
+                                             dimage, tfinal, term, grad_rows);
 }
 
 void launch_scatter_grads(const float4* grad_rows, uint32_t V, float* grad_pos, float4* grad_col, cudaStream_t s) {

@@ -14,11 +14,12 @@ constexpr int kTile = 16;  // composite / adjoint pixel tile (16 x 16 threads)
 // the face's bounding box with incrementally updated int64 edge functions in
 // 1/256-pixel fixed point.  COUNT mode increments the per-pixel counter; FILL
 // mode writes the record at offsets[p] + (--counts[p]), leaving counts zeroed
-// for the next render.
+// for the next render.  Only pixel rows [row0, row1) are visited (row bands of
+// a render whose lists do not fit the fragment budget at once).
 template <bool FILL>
 __device__ __forceinline__ void raster_face(uint32_t f, const uint4* __restrict__ faces,
                                             const float4* __restrict__ vproj, const int2* __restrict__ vfix,
-                                            int W, int H, uint32_t* __restrict__ counts,
+                                            int W, int row0, int row1, uint32_t* __restrict__ counts,
                                             const u64* __restrict__ offsets, u64* __restrict__ records) {
     const uint4 fc = faces[f];
     const int2 q0 = vfix[fc.x], q1 = vfix[fc.y], q2 = vfix[fc.z];
@@ -37,8 +38,8 @@ __device__ __forceinline__ void raster_face(uint32_t f, const uint4* __restrict_
     const long long minY = min(Y0, min(Y1, Y2)), maxY = max(Y0, max(Y1, Y2));
     const int px0 = int(max(0LL, ceil_div256(minX - 128)));
     const int px1 = int(min((long long)W - 1, floor_div256(maxX - 128)));
-    const int py0 = int(max(0LL, ceil_div256(minY - 128)));
-    const int py1 = int(min((long long)H - 1, floor_div256(maxY - 128)));
+    const int py0 = int(max((long long)row0, ceil_div256(minY - 128)));
+    const int py1 = int(min((long long)row1 - 1, floor_div256(maxY - 128)));
     if (px0 > px1 || py0 > py1) return;
     // Edges e0: a1->a2, e1: a2->a0, e2: a0->a1.
     const long long dx0 = ax2 - ax1, dy0 = ay2 - ay1;

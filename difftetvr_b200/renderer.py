@@ -45,6 +45,7 @@ class Renderer:
         self._znear, self._zfar = 0.01, 100.0
         self._view = default_view_matrix()
         self._fragment_budget = 0
+        self._over_budget = _lib.DTV_OVER_BUDGET_RECOMPUTE
         self._coarse_to_fine_target = 0
         self._export_lists = False
         self._last_image: torch.Tensor | None = None
@@ -113,9 +114,23 @@ class Renderer:
             raise RuntimeError("Error in set_view_matrix: expected 16 values.")
         self._view = arr
 
-    def set_fragment_budget_bytes(self, budget: int) -> None:
-        """Bound on stored fragment records; renders beyond it raise DTV_ERR_BUDGET."""
+    def set_fragment_budget_bytes(self, budget: int, over_budget: str = "recompute") -> None:
+        """Bound on the fragment records held at once (0 = none).  Over it,
+        over_budget="recompute" renders in row bands that each fit and rebuilds
+        each band's lists in render_adjoint (the lists are not stored);
+        over_budget="error" raises RuntimeError (DTV_ERR_BUDGET)."""
+        if over_budget not in ("recompute", "error"):
+            raise ValueError("over_budget must be 'recompute' or 'error'")
         self._fragment_budget = int(budget)
+        self._over_budget = _lib.DTV_OVER_BUDGET_RECOMPUTE if over_budget == "recompute" else \
+            _lib.DTV_OVER_BUDGET_ERROR
+
+    def get_num_bands(self) -> int:
+        """0 if the last render stored its fragment lists whole, else the number
+        of row bands it ran in (each recomputed by render_adjoint)."""
+        n = ctypes.c_int32()
+        _lib.call("dtv_renderer_get_num_bands", self._handle, ctypes.byref(n))
+        return int(n.value)
 
     # -- render / adjoint (Module.cpp:912-959) ----------------------------
     def _camera(self) -> _lib.Camera:
@@ -139,6 +154,7 @@ class Renderer:
         p.clear_color[:] = self._clear
         p.use_abs_grad = int(use_abs_grad)
         p.fragment_budget_bytes = self._fragment_budget
+        p.over_budget = self._over_budget
         return p
 
     def render(self) -> torch.Tensor:

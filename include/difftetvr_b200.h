@@ -52,14 +52,23 @@ typedef struct dtv_camera {
 /* Per-render settings: Renderer.set_attenuation (Module.cpp:866),
  * set_use_early_ray_termination / set_early_ray_out_thresh (:868-870),
  * set_clear_color (:871-873); use_abs_grad is render_adjoint's flag (:922).
- * fragment_budget_bytes bounds the stored fragment records (0 = no bound). */
+ * fragment_budget_bytes bounds the fragment records held at once (0 = no
+ * bound).  When a render's records exceed it, over_budget selects what happens:
+ * DTV_OVER_BUDGET_ERROR fails the render with DTV_ERR_BUDGET;
+ * DTV_OVER_BUDGET_RECOMPUTE renders in row bands whose records each fit the
+ * budget (the lists are then not stored: dtv_renderer_render_adjoint rebuilds
+ * each band's lists before its adjoint, and dtv_renderer_copy_fragments fails
+ * with DTV_ERR_STATE).  A single pixel row over the budget is DTV_ERR_BUDGET
+ * in both modes. */
+#define DTV_OVER_BUDGET_ERROR 0
+#define DTV_OVER_BUDGET_RECOMPUTE 1
 typedef struct dtv_render_params {
     float attenuation;
     int32_t use_early_ray_termination;
     float early_ray_out_thresh;
     float clear_color[4];
     int32_t use_abs_grad;
-    int32_t reserved0;
+    int32_t over_budget;
     uint64_t fragment_budget_bytes;
 } dtv_render_params;
 
@@ -126,6 +135,12 @@ int32_t dtv_renderer_render_adjoint(dtv_renderer* r, const dtv_mesh* mesh, const
 /* Total fragments of the last render (exact, from the scan). */
 int32_t dtv_renderer_get_num_fragments(const dtv_renderer* r, uint64_t* num_fragments);
 
+/* Row bands of the last render: 0 when its fragment lists were stored whole,
+ * else the number of bands rendered (and recomputed by the adjoint) under
+ * fragment_budget_bytes with DTV_OVER_BUDGET_RECOMPUTE.  No counterpart in the
+ * reference, whose fragment buffer has a fixed size. */
+int32_t dtv_renderer_get_num_bands(const dtv_renderer* r, int32_t* num_bands);
+
 /* Sorted fragment lists of the last render: replaces get_fragment_buffer /
  * get_start_offset_buffer (Module.cpp:960-981) with an offsets + records
  * layout: h_offsets u64[H*W+1], h_records u64[Nf] where
@@ -145,7 +160,9 @@ int32_t dtv_renderer_copy_pixel_state(const dtv_renderer* r, float* h_transmitta
 
 /* Device time of each stage of the last render / adjoint, in ms:
  * [project, count, scan, fill, sort, composite, adjoint].  Stage timing is
- * recorded only after dtv_renderer_set_timing(r, 1). */
+ * recorded only after dtv_renderer_set_timing(r, 1).  A banded render reports
+ * its whole band loop (scan, fill, sort, composite per band) as fill; a banded
+ * adjoint includes the list rebuild. */
 int32_t dtv_renderer_set_timing(dtv_renderer* r, int32_t enable);
 int32_t dtv_renderer_stage_times(const dtv_renderer* r, float* h_ms, int32_t n);
 

@@ -200,7 +200,7 @@ def test_budget_error_is_reported():
     from difftetvr_b200._lib import DTV_ERR_BUDGET, DtvError
     sc = Scene(8, 128, seed=1)
     mesh, r = sc.make_renderer()
-    r.set_fragment_budget_bytes(1024)
+    r.set_fragment_budget_bytes(1024, over_budget="error")
     with pytest.raises(DtvError) as e:
         r.render()
     assert e.value.code == DTV_ERR_BUDGET
