@@ -12,6 +12,7 @@ from .types import (AABB3, ColorStorage, RendererType, SplitGradientType, TestCa
 from .tet_mesh import TetMesh, build_faces_host, build_hex_mesh, convert_hex_to_tet_indices  # noqa: F401
 from .renderer import Renderer  # noqa: F401
 from .pyutils import DifferentiableRenderer, DifferentiableRenderingFunction  # noqa: F401
+from .regularizer import TetRegularizer  # noqa: F401
 
 __version__ = "0.1.0"
 

@@ -115,6 +115,7 @@ SIGNATURES = {
                                                      c_vp]),
     "dtv_renderer_get_num_fragments": (ctypes.c_int32, [c_vp, c_u64p]),
     "dtv_renderer_get_num_bands": (ctypes.c_int32, [c_vp, ctypes.POINTER(ctypes.c_int32)]),
+    "dtv_tet_regularizer_grad": (ctypes.c_int32, [c_vp, c_vp, ctypes.c_float, ctypes.c_float, c_vp, c_vp, c_vp]),
     "dtv_renderer_copy_fragments": (ctypes.c_int32, [c_vp, c_vp, c_vp, ctypes.c_uint64, c_vp]),
     "dtv_renderer_copy_pixel_state": (ctypes.c_int32, [c_vp, c_vp, c_vp, c_vp]),
     "dtv_renderer_set_timing": (ctypes.c_int32, [c_vp, ctypes.c_int32]),

@@ -684,6 +684,8 @@ int32_t dtv_adam_step(float* d_param, const float* d_grad, float* d_m, float* d_
 // Helpers for the allocation-free entry point (dtv_noalloc.cu).
 namespace dtv {
 MeshView mesh_view(const dtv_mesh* m) { return MeshView{m->d_faces, m->host.num_faces, m->host.num_vertices}; }
+uint64_t mesh_num_cells(const dtv_mesh* m) { return m->host.num_cells; }
+const uint32_t* mesh_cells_device(const dtv_mesh* m) { return m->d_cells; }
 CamDev camera_constants(const dtv_camera& c) { return make_cam(c); }
 ShadeDev shade_constants(const dtv_render_params& p) { return make_shade(p); }
 }  // namespace dtv

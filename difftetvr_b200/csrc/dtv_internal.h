@@ -98,6 +98,8 @@ struct dtv_render_params;
 
 namespace dtv {
 MeshView mesh_view(const dtv_mesh* m);
+uint64_t mesh_num_cells(const dtv_mesh* m);
+const uint32_t* mesh_cells_device(const dtv_mesh* m);  // u32[4T], 16-byte aligned
 CamDev camera_constants(const dtv_camera& c);
 ShadeDev shade_constants(const dtv_render_params& p);
 }  // namespace dtv

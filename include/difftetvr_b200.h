@@ -166,6 +166,16 @@ int32_t dtv_renderer_copy_pixel_state(const dtv_renderer* r, float* h_transmitta
 int32_t dtv_renderer_set_timing(dtv_renderer* r, int32_t enable);
 int32_t dtv_renderer_stage_times(const dtv_renderer* r, float* h_ms, int32_t n);
 
+/* Tet-quality regularizer: replaces TetRegularizer.compute_grad (Module.cpp:663-695,
+ * 983-995; TetRegularizerPass.cpp:94; Data/Shaders/Optimizer/TetRegularizer.glsl:108-166).
+ * Per tet, the Parthasarathy quality q = 6 sqrt(2) V / l_rms^3 is penalised by
+ * the mirrored softplus (lambda / beta) log(1 + exp(-beta q)); its gradient is
+ * ADDED to d_grad_positions f32[3V].  d_loss (nullable, f32[1]) accumulates the
+ * penalty summed over tets (the reference does not compute the value).
+ * d_positions f32[3V] are the mesh's current vertex positions. */
+int32_t dtv_tet_regularizer_grad(const dtv_mesh* mesh, const float* d_positions, float lambda, float beta,
+                                 float* d_grad_positions, float* d_loss, dtv_stream stream);
+
 /* Allocation-free forward render.  No counterpart in the reference: it is for
  * callers that cannot allocate device memory while rendering (a host
  * framework that owns the device heap, or a serving loop that must not call

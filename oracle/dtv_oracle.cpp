@@ -1141,6 +1141,58 @@ void orc_segment_integral(double t, const double* c0, const double* c1, double a
     out4[3] = active ? 1.0 - A : 0.0;
 }
 
+// Tet-quality regularizer (Data/Shaders/Optimizer/TetRegularizer.glsl:108-166):
+// per tet, q = 6 sqrt(2) V / l_rms^3 with V = -det[p1-p0, p2-p0, p3-p0] / 6
+// (:91-93) and l_rms^2 = (sum of squared edge lengths) / 6 (:95-109); penalty
+// (lambda / beta) log(1 + exp(-beta q)) whose derivative -lambda / (1 + exp(beta q))
+// is :120; dq/dp written from the quotient rule on q = -c D / S^(3/2) with the
+// reference's denominator clamp max(S^(5/2), 1e-5) (:125-142).  Adds into
+// grad[3V]; returns the penalty summed over tets.
+double orc_tet_regularizer(const uint32_t* cells, int64_t T, const double* pos, double lambda, double beta,
+                           double* grad) {
+    const double c = 12.0 * std::sqrt(3.0);
+    double total = 0.0;
+    for (int64_t t = 0; t < T; ++t) {
+        double p[4][3];
+        for (int j = 0; j < 4; ++j)
+            for (int k = 0; k < 3; ++k) p[j][k] = pos[3 * size_t(cells[4 * t + j]) + k];
+        double e[4][3];  // e[j] = p[j] - p[0]
+        for (int j = 1; j < 4; ++j)
+            for (int k = 0; k < 3; ++k) e[j][k] = p[j][k] - p[0][k];
+        auto cross = [](const double* a, const double* b, double* o) {
+            o[0] = a[1] * b[2] - a[2] * b[1];
+            o[1] = a[2] * b[0] - a[0] * b[2];
+            o[2] = a[0] * b[1] - a[1] * b[0];
+        };
+        double dD[4][3];
+        cross(e[2], e[3], dD[1]);
+        cross(e[3], e[1], dD[2]);
+        cross(e[1], e[2], dD[3]);
+        for (int k = 0; k < 3; ++k) dD[0][k] = -(dD[1][k] + dD[2][k] + dD[3][k]);
+        const double D = dD[3][0] * e[3][0] + dD[3][1] * e[3][1] + dD[3][2] * e[3][2];
+        double S = 0.0;
+        for (int a = 0; a < 4; ++a)
+            for (int b = a + 1; b < 4; ++b)
+                for (int k = 0; k < 3; ++k) S += (p[a][k] - p[b][k]) * (p[a][k] - p[b][k]);
+        const double q = -c * D / std::pow(S, 1.5);
+        const double dLdq = -lambda / (1.0 + std::exp(beta * q));
+        const double den = std::max(std::pow(S, 2.5), 1e-5);
+        double sum[3] = {0, 0, 0};
+        for (int j = 0; j < 4; ++j)
+            for (int k = 0; k < 3; ++k) sum[k] += p[j][k];
+        for (int j = 0; j < 4; ++j) {
+            const size_t v = cells[4 * t + j];
+            for (int k = 0; k < 3; ++k) {
+                const double dS = 2.0 * (4.0 * p[j][k] - sum[k]);
+                grad[3 * v + k] += dLdq * (-c * S * dD[j][k] + 1.5 * c * D * dS) / den;
+            }
+        }
+        const double z = -beta * q;
+        total += (lambda / beta) * (std::max(z, 0.0) + std::log1p(std::exp(-std::fabs(z))));
+    }
+    return total;
+}
+
 int orc_num_threads(void) {
 #ifdef _OPENMP
     return omp_get_max_threads();

@@ -76,6 +76,8 @@ def load():
         lib.orc_segment_integral.restype = None
         lib.orc_segment_integral.argtypes = [ctypes.c_double, _vp, _vp, ctypes.c_double, _vp]
         lib.orc_num_threads.restype = ctypes.c_int
+        lib.orc_tet_regularizer.argtypes = [_vp, ctypes.c_int64, _vp, ctypes.c_double, ctypes.c_double, _vp]
+        lib.orc_tet_regularizer.restype = ctypes.c_double
         _lib = lib
     return _lib
 
@@ -228,6 +230,17 @@ def segment_integral(t, c0, c1, a):
     out = np.zeros(4, np.float64)
     lib.orc_segment_integral(float(t), _p(c0), _p(c1), float(a), _p(out))
     return out
+
+
+def tet_regularizer(cells, positions, reg_lambda: float, softplus_beta: float):
+    """FP64 tet-quality regularizer: (penalty summed over tets, gradient [V,3])."""
+    lib = load()
+    cells = np.ascontiguousarray(cells, np.uint32)
+    pos = np.ascontiguousarray(positions, np.float64)
+    grad = np.zeros_like(pos)
+    total = lib.orc_tet_regularizer(_p(cells), cells.shape[0], _p(pos), float(reg_lambda), float(softplus_beta),
+                                    _p(grad))
+    return float(total), grad
 
 
 def num_threads() -> int:
