@@ -171,6 +171,42 @@ class TetMesh:
         col = np.tile(np.array(tuple(const_color), dtype=np.float32), (pos.shape[0], 1))
         self.set_tet_mesh_data(cells, pos, col)
 
+    # -- files (Module.cpp:787-788) ------------------------------------------
+    def load_from_file(self, file_path: str) -> bool:
+        """TetMesh::loadFromFile (TetMesh.cpp:1084-1150): .bintet files; False
+        (with a warning) for an unsupported extension or an unreadable file."""
+        import warnings
+
+        from .mesh_io import SUPPORTED_EXTENSIONS, file_extension, read_bintet
+        ext = file_extension(file_path)
+        if ext not in SUPPORTED_EXTENSIONS:
+            warnings.warn(f"Error in TetMesh.load_from_file: Unsupported file extension '.{ext}'.")
+            return False
+        try:
+            cells, pos, vcol, ccol, _ = read_bintet(file_path)
+        except RuntimeError as e:
+            warnings.warn(f"Error in TetMesh.load_from_file: {e}")
+            return False
+        if vcol.shape[0] > 0:
+            self.set_tet_mesh_data(cells, pos, vcol)
+        if ccol is not None and ccol.shape[0] > 0:
+            self.set_tet_mesh_data_cell(cells, pos, ccol)
+        return True
+
+    def save_to_file(self, file_path: str) -> bool:
+        """TetMesh::saveToFile (TetMesh.cpp:1152-1173): .bintet (version 1 with
+        vertex colours, version 2 with cell colours)."""
+        from .mesh_io import SUPPORTED_EXTENSIONS, file_extension, write_bintet
+        ext = file_extension(file_path)
+        if ext not in SUPPORTED_EXTENSIONS:
+            raise RuntimeError(
+                f"Error in TetMeshData::createTetMeshWriterByExtension: Unsupported file extension '.{ext}'.")
+        pos = self._positions.detach().cpu().numpy()
+        vcol = None if self._colors is None else self._colors.detach().cpu().numpy()
+        ccol = None if self._cell_colors is None else self._cell_colors.detach().cpu().numpy()
+        write_bintet(file_path, self._cells, pos, vcol, ccol)
+        return True
+
     # -- accessors ---------------------------------------------------------
     def get_num_cells(self) -> int:
         return 0 if self._cells is None else int(self._cells.shape[0])

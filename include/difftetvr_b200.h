@@ -166,6 +166,23 @@ int32_t dtv_renderer_copy_pixel_state(const dtv_renderer* r, float* h_transmitta
 int32_t dtv_renderer_set_timing(dtv_renderer* r, int32_t enable);
 int32_t dtv_renderer_stage_times(const dtv_renderer* r, float* h_ms, int32_t n);
 
+/* .bintet mesh files: replaces BinTetLoader::loadFromFile / peekSizes and
+ * BinTetWriter::saveToFile (src/Tet/Loaders/BinTetLoader.cpp:37-138) behind
+ * TetMesh.load_from_file / save_to_file (Module.cpp:787-788).  Layout: u32
+ * version (1, or 2 with cell colours), then u32-count-prefixed arrays of cell
+ * indices (u32, count 4T), positions (3 f32 each), vertex colours (4 f32 each)
+ * and, in version 2, cell colours (4 f32 each).  Host memory only.  Invalid
+ * or truncated files fail with DTV_ERR_ARG.  dtv_bintet_read fills the arrays
+ * sized by dtv_bintet_peek (colour pointers may be NULL to skip). */
+int32_t dtv_bintet_peek(const char* path, uint32_t* version, uint64_t* num_cells, uint64_t* num_vertices,
+                        uint64_t* num_vertex_colors, uint64_t* num_cell_colors);
+int32_t dtv_bintet_read(const char* path, uint32_t* h_cells, float* h_positions, float* h_vertex_colors,
+                        float* h_cell_colors);
+/* Writes version 2 when num_cell_colors > 0, else version 1. */
+int32_t dtv_bintet_write(const char* path, const uint32_t* h_cells, uint64_t num_cells, const float* h_positions,
+                         uint64_t num_vertices, const float* h_vertex_colors, uint64_t num_vertex_colors,
+                         const float* h_cell_colors, uint64_t num_cell_colors);
+
 /* Tet-quality regularizer: replaces TetRegularizer.compute_grad (Module.cpp:663-695,
  * 983-995; TetRegularizerPass.cpp:94; Data/Shaders/Optimizer/TetRegularizer.glsl:108-166).
  * Per tet, the Parthasarathy quality q = 6 sqrt(2) V / l_rms^3 is penalised by
