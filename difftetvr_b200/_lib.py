@@ -113,6 +113,10 @@ SIGNATURES = {
                                              ctypes.POINTER(RenderParams), c_vp, c_vp]),
     "dtv_renderer_render_adjoint": (ctypes.c_int32, [c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.c_int32, c_vp, c_vp,
                                                      c_vp]),
+    "dtv_renderer_render_cells": (ctypes.c_int32, [c_vp, c_vp, c_vp, c_vp, ctypes.POINTER(Camera),
+                                                   ctypes.POINTER(RenderParams), c_vp, c_vp]),
+    "dtv_renderer_render_adjoint_cells": (ctypes.c_int32, [c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.c_int32, c_vp,
+                                                           c_vp, c_vp]),
     "dtv_renderer_get_num_fragments": (ctypes.c_int32, [c_vp, c_u64p]),
     "dtv_renderer_get_num_bands": (ctypes.c_int32, [c_vp, ctypes.POINTER(ctypes.c_int32)]),
     "dtv_bintet_peek": (ctypes.c_int32, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_uint32), c_u64p, c_u64p, c_u64p,

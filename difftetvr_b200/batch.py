@@ -56,6 +56,9 @@ class BatchRenderer:
             self._handle = None
 
     def set_meshes(self, meshes: list[TetMesh]) -> None:
+        from .types import ColorStorage
+        if any(m.get_color_storage() != ColorStorage.PER_VERTEX for m in meshes):
+            raise RuntimeError("BatchRenderer renders ColorStorage.PER_VERTEX meshes; use Renderer for PER_CELL.")
         self.meshes = list(meshes)
         n = len(self.meshes)
         arr_m = (ctypes.c_void_p * n)(*[m.native.handle.value for m in self.meshes])

@@ -85,6 +85,7 @@ struct dtv_renderer {
     // fragment budget (each band's lists are rebuilt by the adjoint); empty
     // when the lists are stored whole.
     std::vector<std::pair<int, int>> bands;
+    bool cells = false;           // last render used per-cell colours
     u64* h_rowoff = nullptr;      // pinned row-start offsets (H+1)
     size_t h_rowoff_cap = 0;
     DevBuf<uint4> wstate;         // ray-tet path: (last tet, its entry face, boundary entry index, segments)
@@ -176,6 +177,44 @@ void record_flags(dtv_renderer* r, cudaStream_t s) {
     r->flags_pending = true;
 }
 
+// Composite of rows [y0, y1) with the stored lists: per-vertex colours
+// (d_colors f32[4V]) or per-cell colours (f32[4T]).
+void composite_rows(dtv_renderer* r, const dtv_mesh* mesh, const float* d_colors, const dtv::CamDev& cam,
+                    const dtv::ShadeDev& sh, float* d_image, int y0, int y1, cudaStream_t s) {
+    if (r->cells)
+        dtv::launch_composite_cells(r->offsets.ptr, r->records.ptr, mesh->d_faces, mesh->d_face_to_tet, r->vgeo.ptr,
+                                    reinterpret_cast<const float4*>(d_colors), cam.W, cam.H, sh,
+                                    reinterpret_cast<float4*>(d_image), r->tfinal.ptr, r->term.ptr, s, y0, y1);
+    else
+        dtv::launch_composite(r->offsets.ptr, r->records.ptr, mesh->d_faces, r->vgeo.ptr,
+                              reinterpret_cast<const float4*>(d_colors), cam.W, cam.H, sh,
+                              reinterpret_cast<float4*>(d_image), r->tfinal.ptr, r->term.ptr, s, y0, y1);
+}
+
+// Adjoint of rows [y0, y1) into the gradient rows (per-cell: the cell colour
+// gradients go straight into d_grad_colors f32[4T]).
+void adjoint_rows(dtv_renderer* r, const dtv_mesh* mesh, const float* d_colors, const float* d_image_adjoint,
+                  const dtv::ShadeDev& sh, int y0, int y1, float* d_grad_colors, cudaStream_t s) {
+    if (r->cells)
+        dtv::launch_adjoint_cells_rows(r->offsets.ptr, r->records.ptr, mesh->d_faces, mesh->d_face_to_tet,
+                                       r->vgeo.ptr, reinterpret_cast<const float4*>(d_colors), r->cam, sh,
+                                       reinterpret_cast<const float4*>(d_image_adjoint), r->tfinal.ptr, r->term.ptr,
+                                       y0, y1, r->grad_rows.ptr, reinterpret_cast<float4*>(d_grad_colors), s);
+    else
+        dtv::launch_adjoint_rows(r->offsets.ptr, r->records.ptr, mesh->d_faces, r->vgeo.ptr,
+                                 reinterpret_cast<const float4*>(d_colors), r->cam, sh,
+                                 reinterpret_cast<const float4*>(d_image_adjoint), r->tfinal.ptr, r->term.ptr, y0, y1,
+                                 r->grad_rows.ptr, s);
+}
+
+void scatter_rows(dtv_renderer* r, float* d_grad_positions, float* d_grad_colors, cudaStream_t s) {
+    if (r->cells)
+        dtv::launch_scatter_positions(r->grad_rows.ptr, uint32_t(r->V), d_grad_positions, s);
+    else
+        dtv::launch_scatter_grads(r->grad_rows.ptr, uint32_t(r->V), d_grad_positions,
+                                  reinterpret_cast<float4*>(d_grad_colors), s);
+}
+
 // Forward in row bands (fragment lists over the budget): after the full count
 // and scan, each band's lists are built and composited in turn, so at most
 // `cap` records are held at once.  Counts of all rows come from the full count
@@ -196,9 +235,7 @@ void render_banded(dtv_renderer* r, const dtv_mesh* mesh, const float* d_colors,
     DTV_CK(cudaMemsetAsync(r->flags.ptr, 0, 2 * sizeof(uint32_t), s));
     for (const auto& b : r->bands) {
         build_band_lists(r, mesh, W, H, b.first, b.second, s);
-        dtv::launch_composite(r->offsets.ptr, r->records.ptr, mesh->d_faces, r->vgeo.ptr,
-                              reinterpret_cast<const float4*>(d_colors), W, H, sh,
-                              reinterpret_cast<float4*>(d_image), r->tfinal.ptr, r->term.ptr, s, b.first, b.second);
+        composite_rows(r, mesh, d_colors, cam, sh, d_image, b.first, b.second, s);
         check_launch("band composite");
     }
     record_flags(r, s);
@@ -220,14 +257,10 @@ void adjoint_banded(dtv_renderer* r, const dtv_mesh* mesh, const float* d_colors
                                  r->counts.ptr, s, b.first, b.second);
         check_launch("band count");
         build_band_lists(r, mesh, W, H, b.first, b.second, s);
-        dtv::launch_adjoint_rows(r->offsets.ptr, r->records.ptr, mesh->d_faces, r->vgeo.ptr,
-                                 reinterpret_cast<const float4*>(d_colors), r->cam, sh,
-                                 reinterpret_cast<const float4*>(d_image_adjoint), r->tfinal.ptr, r->term.ptr,
-                                 b.first, b.second, r->grad_rows.ptr, s);
+        adjoint_rows(r, mesh, d_colors, d_image_adjoint, sh, b.first, b.second, d_grad_colors, s);
         check_launch("band adjoint");
     }
-    dtv::launch_scatter_grads(r->grad_rows.ptr, uint32_t(r->V), d_grad_positions,
-                              reinterpret_cast<float4*>(d_grad_colors), s);
+    scatter_rows(r, d_grad_positions, d_grad_colors, s);
     check_launch("scatter gradients");
     record_flags(r, s);
 }
@@ -408,11 +441,19 @@ int32_t dtv_renderer_destroy(dtv_renderer* r) {
     return DTV_OK;
 }
 
-int32_t dtv_renderer_render(dtv_renderer* r, const dtv_mesh* mesh, const float* d_positions, const float* d_colors,
-                            const dtv_camera* camera, const dtv_render_params* params, float* d_image,
-                            dtv_stream stream) {
+}  // extern "C"
+
+namespace {
+
+// Forward render shared by dtv_renderer_render (per-vertex colours f32[4V])
+// and dtv_renderer_render_cells (per-cell colours f32[4T]).
+int32_t render_common(dtv_renderer* r, const dtv_mesh* mesh, const float* d_positions, const float* d_colors,
+                      const dtv_camera* camera, const dtv_render_params* params, float* d_image, dtv_stream stream,
+                      bool cells) {
     return guarded([&] {
         require(r && mesh && camera && params, "null handle or struct");
+        require(!cells || r->type == DTV_RENDERER_PPLL,
+                "per-cell colours are provided by the PPLL renderer only");
         require(d_positions && d_colors && d_image, "null device pointer");
         require((reinterpret_cast<uintptr_t>(d_colors) & 15u) == 0, "colors must be 16-byte aligned");
         require((reinterpret_cast<uintptr_t>(d_image) & 15u) == 0, "image must be 16-byte aligned");
@@ -423,6 +464,7 @@ int32_t dtv_renderer_render(dtv_renderer* r, const dtv_mesh* mesh, const float* 
         cudaStream_t s = static_cast<cudaStream_t>(stream);
         check_pending_flags(r);
         r->have_render = false;
+        r->cells = cells;
         const bool raytet = r->type == DTV_RENDERER_INTERSECTION;
         const uint64_t V = mesh->host.num_vertices;
         // The ray-tet path rasterises only the boundary faces (interval entries and exits).
@@ -508,9 +550,7 @@ int32_t dtv_renderer_render(dtv_renderer* r, const dtv_mesh* mesh, const float* 
                                        reinterpret_cast<float4*>(d_image), r->tfinal.ptr, r->wstate.ptr, s);
             check_launch("ray-tet walk");
         } else {
-            dtv::launch_composite(r->offsets.ptr, r->records.ptr, mesh->d_faces, r->vgeo.ptr,
-                                  reinterpret_cast<const float4*>(d_colors), W, H, sh,
-                                  reinterpret_cast<float4*>(d_image), r->tfinal.ptr, r->term.ptr, s);
+            composite_rows(r, mesh, d_colors, cam, sh, d_image, 0, H, s);
             check_launch("composite");
         }
         rec_event(r, 6, s);
@@ -525,9 +565,9 @@ int32_t dtv_renderer_render(dtv_renderer* r, const dtv_mesh* mesh, const float* 
     });
 }
 
-int32_t dtv_renderer_render_adjoint(dtv_renderer* r, const dtv_mesh* mesh, const float* d_positions,
-                                    const float* d_colors, const float* d_image_adjoint, int32_t use_abs_grad,
-                                    float* d_grad_positions, float* d_grad_colors, dtv_stream stream) {
+int32_t adjoint_common(dtv_renderer* r, const dtv_mesh* mesh, const float* d_positions, const float* d_colors,
+                       const float* d_image_adjoint, int32_t use_abs_grad, float* d_grad_positions,
+                       float* d_grad_colors, dtv_stream stream, bool cells) {
     return guarded([&] {
         require(r && mesh, "null handle");
         require(d_positions && d_colors && d_image_adjoint && d_grad_positions && d_grad_colors,
@@ -538,6 +578,9 @@ int32_t dtv_renderer_render_adjoint(dtv_renderer* r, const dtv_mesh* mesh, const
                 "image adjoint must be 16-byte aligned");
         if (!r->have_render) throw DtvError(DTV_ERR_STATE, "render_adjoint called before render");
         if (r->mesh != mesh) throw DtvError(DTV_ERR_STATE, "render_adjoint called with a different mesh");
+        if (r->cells != cells)
+            throw DtvError(DTV_ERR_STATE, cells ? "dtv_renderer_render_adjoint_cells after a per-vertex render"
+                                                : "dtv_renderer_render_adjoint after a per-cell render");
         cudaStream_t s = static_cast<cudaStream_t>(stream);
         check_pending_flags(r);
         dtv::ShadeDev sh = r->sh;
@@ -555,16 +598,46 @@ int32_t dtv_renderer_render_adjoint(dtv_renderer* r, const dtv_mesh* mesh, const
                                      reinterpret_cast<float4*>(d_grad_colors), s);
             check_launch("ray-tet adjoint walk");
         } else {
-            dtv::launch_adjoint(r->offsets.ptr, r->records.ptr, mesh->d_faces, r->vgeo.ptr,
-                                reinterpret_cast<const float4*>(d_colors), r->cam, sh,
-                                reinterpret_cast<const float4*>(d_image_adjoint), r->tfinal.ptr, r->term.ptr,
-                                uint32_t(r->V), r->grad_rows.ptr, d_grad_positions,
-                                reinterpret_cast<float4*>(d_grad_colors), s);
+            DTV_CK(cudaMemsetAsync(r->grad_rows.ptr, 0, sizeof(float4) * 2 * size_t(r->V ? r->V : 1), s));
+            adjoint_rows(r, mesh, d_colors, d_image_adjoint, sh, 0, r->cam.H, d_grad_colors, s);
             check_launch("adjoint");
+            scatter_rows(r, d_grad_positions, d_grad_colors, s);
+            check_launch("scatter gradients");
         }
         rec_event(r, 8, s);
         r->adjoint_timed = true;
     });
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t dtv_renderer_render(dtv_renderer* r, const dtv_mesh* mesh, const float* d_positions, const float* d_colors,
+                            const dtv_camera* camera, const dtv_render_params* params, float* d_image,
+                            dtv_stream stream) {
+    return render_common(r, mesh, d_positions, d_colors, camera, params, d_image, stream, false);
+}
+
+int32_t dtv_renderer_render_cells(dtv_renderer* r, const dtv_mesh* mesh, const float* d_positions,
+                                  const float* d_cell_colors, const dtv_camera* camera,
+                                  const dtv_render_params* params, float* d_image, dtv_stream stream) {
+    return render_common(r, mesh, d_positions, d_cell_colors, camera, params, d_image, stream, true);
+}
+
+int32_t dtv_renderer_render_adjoint(dtv_renderer* r, const dtv_mesh* mesh, const float* d_positions,
+                                    const float* d_colors, const float* d_image_adjoint, int32_t use_abs_grad,
+                                    float* d_grad_positions, float* d_grad_colors, dtv_stream stream) {
+    return adjoint_common(r, mesh, d_positions, d_colors, d_image_adjoint, use_abs_grad, d_grad_positions,
+                          d_grad_colors, stream, false);
+}
+
+int32_t dtv_renderer_render_adjoint_cells(dtv_renderer* r, const dtv_mesh* mesh, const float* d_positions,
+                                          const float* d_cell_colors, const float* d_image_adjoint,
+                                          int32_t use_abs_grad, float* d_grad_positions,
+                                          float* d_grad_cell_colors, dtv_stream stream) {
+    return adjoint_common(r, mesh, d_positions, d_cell_colors, d_image_adjoint, use_abs_grad, d_grad_positions,
+                          d_grad_cell_colors, stream, true);
 }
 
 int32_t dtv_renderer_get_num_fragments(const dtv_renderer* r, uint64_t* nf) {

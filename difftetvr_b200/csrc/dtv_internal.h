@@ -69,6 +69,19 @@ void launch_adam(float* param, const float* grad, float* m, float* v, uint64_t n
                  float beta2, float eps, float bc1, float bc2, int clamp_mode, const uint32_t* fixed_mask,
                  int fixed_mode, int stride, cudaStream_t s);
 
+// Per-cell colours (dtv_cells.cu): cell_colors f32[4T]; rows [row0, row1).
+void launch_composite_cells(const unsigned long long* offsets, const unsigned long long* records, const uint4* faces,
+                            const uint32_t* face_to_tet, const VGeo* vgeo, const float4* cell_colors, int W, int H,
+                            const ShadeDev& sh, float4* image, float* tfinal, uint32_t* term, cudaStream_t s,
+                            int row0, int row1);
+void launch_adjoint_cells_rows(const unsigned long long* offsets, const unsigned long long* records,
+                               const uint4* faces, const uint32_t* face_to_tet, const VGeo* vgeo,
+                               const float4* cell_colors, const CamDev& cam, const ShadeDev& sh, const float4* dimage,
+                               const float* tfinal, const uint32_t* term, int row0, int row1, float4* grad_rows,
+                               float4* grad_cells, cudaStream_t s);
+// Adds the position part of the [V][2] gradient rows into grad_pos [V,3].
+void launch_scatter_positions(const float4* grad_rows, uint32_t V, float* grad_pos, cudaStream_t s);
+
 // Ray-tet path (dtv_raytet.cu).
 void launch_walk_composite(const unsigned long long* b_offsets, const unsigned long long* b_records,
                            const uint32_t* bf_global, const uint4* faces, const uint32_t* face_to_tet,

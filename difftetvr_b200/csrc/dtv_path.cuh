@@ -297,6 +297,59 @@ __device__ __forceinline__ void sub_segment_adjoint(float tSeg, float a, float4 
     }
 }
 
+// Position gradients of one fragment from its depth adjoint alone (per-cell
+// colours: the fragment carries no colour, so only the depth path of
+// frag_vertex_grads remains).  One float4 atomic per vertex (position row).
+__device__ __forceinline__ void frag_position_grads(const uint4& fc, float qx, float qy,
+                                                    const VGeo* __restrict__ vgeo, const CamDev& cam, float gz,
+                                                    bool use_abs, float4* __restrict__ rows) {
+    const uint32_t vi[3] = {fc.x, fc.y, fc.z};
+    VGeo P[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) P[j] = vgeo[vi[j]];
+    FaceInterp fi;
+    face_interp(P[0], P[1], P[2], qx, qy, fi);
+    if (fi.clamped) return;  // the depth is clamped to a vertex depth: no dependence
+    const float gzz = gz * fi.zb * fi.zb;
+    float glam[3], giz[3], sl = 0.f;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        glam[j] = -gzz * P[j].iz;
+        giz[j] = -gzz * fi.lam[j];
+        sl += glam[j] * fi.lam[j];
+    }
+    const float invA = __fdividef(1.0f, fi.A);
+    float gE[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) gE[j] = (glam[j] - sl) * invA;
+    const float* dx = fi.dx;
+    const float* dy = fi.dy;
+    float gsx[3], gsy[3];
+    gsx[0] = -gE[1] * dy[2] + gE[2] * dy[1];
+    gsy[0] = gE[1] * dx[2] - gE[2] * dx[1];
+    gsx[1] = gE[0] * dy[2] - gE[2] * dy[0];
+    gsy[1] = -gE[0] * dx[2] + gE[2] * dx[0];
+    gsx[2] = -gE[0] * dy[1] + gE[1] * dy[0];
+    gsy[2] = gE[0] * dx[1] - gE[1] * dx[0];
+    const float* V = cam.V;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        const float iz = P[j].iz;
+        const float gxv = gsx[j] * cam.f * iz;
+        const float gyv = -gsy[j] * cam.f * iz;
+        const float gzv = (giz[j] + cam.f * (gsx[j] * P[j].xv - gsy[j] * P[j].yv)) * iz * iz;
+        float gp0 = V[0] * gxv + V[1] * gyv + V[2] * gzv;
+        float gp1 = V[4] * gxv + V[5] * gyv + V[6] * gzv;
+        float gp2 = V[8] * gxv + V[9] * gyv + V[10] * gzv;
+        if (use_abs) {
+            gp0 = fabsf(gp0);
+            gp1 = fabsf(gp1);
+            gp2 = fabsf(gp2);
+        }
+        atomicAdd(rows + 2 * size_t(vi[j]), make_float4(gp0, gp1, gp2, 0.f));
+    }
+}
+
 __device__ __forceinline__ void adjoint_pixel(
     int px, int py, const u64* __restrict__ offsets, const u64* __restrict__ records, const uint4* __restrict__ faces,
     const VGeo* __restrict__ vgeo, const float4* __restrict__ colors, int W, const CamDev& cam, const ShadeDev& sh,

@@ -10,6 +10,8 @@ from __future__ import annotations
 
 import torch
 
+from .types import ColorStorage
+
 
 class DifferentiableRenderingFunction(torch.autograd.Function):
     @staticmethod
@@ -50,7 +52,10 @@ class DifferentiableRenderer(torch.nn.Module):
     def forward(self):
         tet_mesh = self.renderer.get_tet_mesh()
         vertex_positions = tet_mesh.get_vertex_positions()
-        colors = tet_mesh.get_vertex_colors()
+        if tet_mesh.get_color_storage() == ColorStorage.PER_VERTEX:
+            colors = tet_mesh.get_vertex_colors()
+        else:
+            colors = tet_mesh.get_cell_colors()
         return DifferentiableRenderingFunction.apply(
             self.renderer, self.tet_regularizer, self.use_abs_grad, vertex_positions, colors)
 

@@ -12,7 +12,7 @@ import torch
 
 from . import _lib
 from .tet_mesh import TetMesh
-from .types import RendererType, vec4
+from .types import ColorStorage, RendererType, vec4
 
 
 def default_view_matrix() -> list[float]:
@@ -162,12 +162,14 @@ class Renderer:
         if mesh is None or mesh.get_is_empty():
             raise RuntimeError("Missing valid tet mesh in Renderer.render.")
         pos = mesh.get_vertex_positions().detach()
-        col = mesh.get_vertex_colors().detach()
+        cells = mesh.get_color_storage() == ColorStorage.PER_CELL
+        col = (mesh.get_cell_colors() if cells else mesh.get_vertex_colors()).detach()
         image = torch.empty((self._height, self._width, 4), dtype=torch.float32, device=pos.device)
         stream = torch.cuda.current_stream(pos.device).cuda_stream
         cam, prm = self._camera(), self._params()
-        _lib.call("dtv_renderer_render", self._handle, mesh.native.handle, pos.data_ptr(), col.data_ptr(),
-                  ctypes.byref(cam), ctypes.byref(prm), image.data_ptr(), stream)
+        _lib.call("dtv_renderer_render_cells" if cells else "dtv_renderer_render", self._handle,
+                  mesh.native.handle, pos.data_ptr(), col.data_ptr(), ctypes.byref(cam), ctypes.byref(prm),
+                  image.data_ptr(), stream)
         self._last_image = image
         return image
 
@@ -191,19 +193,22 @@ class Renderer:
 
     def _adjoint(self, mesh: TetMesh, image_adjoint: torch.Tensor, use_abs_grad: bool, grad_positions: torch.Tensor,
                  grad_colors: torch.Tensor) -> None:
+        """grad_colors: [V, 4] per-vertex or [T, 4] per-cell, by the mesh's colour storage."""
         pos = mesh.get_vertex_positions()
-        col = mesh.get_vertex_colors()
+        cells = mesh.get_color_storage() == ColorStorage.PER_CELL
+        col = mesh.get_cell_colors() if cells else mesh.get_vertex_colors()
         stream = torch.cuda.current_stream(pos.device).cuda_stream
-        _lib.call("dtv_renderer_render_adjoint", self._handle, mesh.native.handle, pos.detach().data_ptr(),
-                  col.detach().data_ptr(), image_adjoint.data_ptr(), int(bool(use_abs_grad)),
-                  grad_positions.data_ptr(), grad_colors.data_ptr(), stream)
+        _lib.call("dtv_renderer_render_adjoint_cells" if cells else "dtv_renderer_render_adjoint", self._handle,
+                  mesh.native.handle, pos.detach().data_ptr(), col.detach().data_ptr(), image_adjoint.data_ptr(),
+                  int(bool(use_abs_grad)), grad_positions.data_ptr(), grad_colors.data_ptr(), stream)
 
     def render_adjoint(self, image_adjoint: torch.Tensor, use_abs_grad: bool = False) -> None:
         """Adds the vertex position / colour gradients into the mesh tensors' .grad
         (Module.cpp:922-959)."""
         mesh, image_adjoint = self._check_adjoint(image_adjoint, "render_adjoint")
         pos = mesh.get_vertex_positions()
-        col = mesh.get_vertex_colors()
+        col = mesh.get_cell_colors() if mesh.get_color_storage() == ColorStorage.PER_CELL else \
+            mesh.get_vertex_colors()
         if pos.grad is None:
             pos.grad = torch.zeros_like(pos)
         if col.grad is None:
@@ -216,11 +221,12 @@ class Renderer:
         [V, 3] / [V, 4] (grad_colors 16-byte aligned) instead of .grad."""
         mesh, image_adjoint = self._check_adjoint(image_adjoint, "render_adjoint_into")
         V = mesh.get_num_vertices()
-        for t, c in ((grad_positions, 3), (grad_colors, 4)):
+        Nc = mesh.get_num_cells() if mesh.get_color_storage() == ColorStorage.PER_CELL else V
+        for t, rows, c in ((grad_positions, V, 3), (grad_colors, Nc, 4)):
             if (not torch.is_tensor(t) or t.dtype != torch.float32 or not t.is_contiguous()
-                    or tuple(t.shape) != (V, c) or t.device != image_adjoint.device):
+                    or tuple(t.shape) != (rows, c) or t.device != image_adjoint.device):
                 raise RuntimeError(f"Error in render_adjoint_into: gradient tensors must be contiguous float32 "
-                                   f"[{V}, 3] / [{V}, 4] on the mesh's device.")
+                                   f"[{V}, 3] / [{Nc}, 4] on the mesh's device.")
         self._adjoint(mesh, image_adjoint, use_abs_grad, grad_positions, grad_colors)
 
     # -- fragment list export (Module.cpp:960-981) -------------------------

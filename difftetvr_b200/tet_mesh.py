@@ -136,8 +136,28 @@ class TetMesh:
         self._vertex_boundary = torch.as_tensor(vb.astype(np.int32)).to(dev)
         self._attach_grads()
 
+    def set_tet_mesh_data_cell(self, cells, vertex_positions, cell_colors) -> None:
+        """TetMesh::setTetMeshDataCell: one RGBA per cell (ColorStorage.PER_CELL)."""
+        cells = np.ascontiguousarray(np.asarray(cells, dtype=np.uint32).reshape(-1, 4))
+        pos = torch.as_tensor(np.asarray(vertex_positions, dtype=np.float32).reshape(-1, 3))
+        ccol = torch.as_tensor(np.asarray(cell_colors, dtype=np.float32).reshape(-1, 4))
+        if ccol.shape[0] != cells.shape[0]:
+            raise RuntimeError("Error in TetMesh.set_tet_mesh_data_cell: #colors != #cells.")
+        if cells.size and int(cells.max()) >= pos.shape[0]:
+            raise RuntimeError("Error in TetMesh.set_tet_mesh_data_cell: cell index out of range.")
+        dev = _device()
+        self._cells = cells
+        self._color_storage = ColorStorage.PER_CELL
+        self._positions = pos.to(dev).contiguous()
+        self._colors = None
+        self._cell_colors = ccol.to(dev).contiguous()
+        self._native = NativeMesh(cells, pos.shape[0])
+        _, _, _, vb = self._native.copy_faces()
+        self._vertex_boundary = torch.as_tensor(vb.astype(np.int32)).to(dev)
+        self._attach_grads()
+
     def _attach_grads(self) -> None:
-        for t in (self._positions, self._colors):
+        for t in (self._positions, self._colors, self._cell_colors):
             if t is None:
                 continue
             t.requires_grad_(self._use_gradients)
@@ -165,11 +185,12 @@ class TetMesh:
     def set_hex_mesh_const(self, aabb: AABB3, xs: int, ys: int, zs: int, const_color: vec4,
                            color_storage: ColorStorage = ColorStorage.PER_VERTEX) -> None:
         """TetMesh::setHexMeshConst (TetMesh.cpp:1882-1936); xs, ys, zs are vertex counts."""
-        if color_storage != ColorStorage.PER_VERTEX:
-            raise RuntimeError("ColorStorage.PER_CELL is not provided by difftetvr_b200")
         cells, pos = build_hex_mesh(tuple(aabb.min), tuple(aabb.max), xs, ys, zs)
-        col = np.tile(np.array(tuple(const_color), dtype=np.float32), (pos.shape[0], 1))
-        self.set_tet_mesh_data(cells, pos, col)
+        c = np.array(tuple(const_color), dtype=np.float32)
+        if ColorStorage(color_storage) == ColorStorage.PER_CELL:
+            self.set_tet_mesh_data_cell(cells, pos, np.tile(c, (cells.shape[0], 1)))
+        else:
+            self.set_tet_mesh_data(cells, pos, np.tile(c, (pos.shape[0], 1)))
 
     # -- files (Module.cpp:787-788) ------------------------------------------
     def load_from_file(self, file_path: str) -> bool:
@@ -224,7 +245,8 @@ class TetMesh:
         return self._colors
 
     def get_cell_colors(self) -> torch.Tensor:
-        raise RuntimeError("ColorStorage.PER_CELL is not provided by difftetvr_b200")
+        """Per-cell RGBA [T, 4] (ColorStorage.PER_CELL meshes; None otherwise)."""
+        return self._cell_colors
 
     def get_cells(self) -> np.ndarray:
         return self._cells

@@ -132,6 +132,22 @@ int32_t dtv_renderer_render_adjoint(dtv_renderer* r, const dtv_mesh* mesh, const
                                     const float* d_colors, const float* d_image_adjoint, int32_t use_abs_grad,
                                     float* d_grad_positions, float* d_grad_colors, dtv_stream stream);
 
+/* Per-cell colours (ColorStorage::PER_CELL, Module.cpp:769-771): the same
+ * render / adjoint with one RGBA per tet, d_cell_colors f32[4T] (16-byte
+ * aligned).  Consecutive fragments bound a segment of the tet both faces
+ * belong to (tetIdUnion, LinkedListResolve.glsl:85-94) with that cell's
+ * constant colour and density (Forward.glsl:213-246, Backward.glsl:283-329);
+ * the termination index counts fragments.  The adjoint ADDS into
+ * d_grad_positions f32[3V] and d_grad_cell_colors f32[4T].  PPLL renderers
+ * only; an adjoint must use the same colour storage as the render. */
+int32_t dtv_renderer_render_cells(dtv_renderer* r, const dtv_mesh* mesh, const float* d_positions,
+                                  const float* d_cell_colors, const dtv_camera* camera,
+                                  const dtv_render_params* params, float* d_image, dtv_stream stream);
+int32_t dtv_renderer_render_adjoint_cells(dtv_renderer* r, const dtv_mesh* mesh, const float* d_positions,
+                                          const float* d_cell_colors, const float* d_image_adjoint,
+                                          int32_t use_abs_grad, float* d_grad_positions,
+                                          float* d_grad_cell_colors, dtv_stream stream);
+
 /* Total fragments of the last render (exact, from the scan). */
 int32_t dtv_renderer_get_num_fragments(const dtv_renderer* r, uint64_t* num_fragments);
 

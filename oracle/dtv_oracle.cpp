@@ -525,7 +525,8 @@ void frag_vertex_grads(const MeshR<R>& m, const CamConst& cam, uint32_t face, in
     for (int j = 0; j < 3; ++j) {
         b[j] = u[j] * zb;
         gb[j] = 0;
-        for (int k = 0; k < 4; ++k) gb[j] += gcol[k] * m.col[4 * vi[j] + k];
+        if (m.col)
+            for (int k = 0; k < 4; ++k) gb[j] += gcol[k] * m.col[4 * vi[j] + k];
         sb += gb[j] * b[j];
     }
     R glam[3], giz[3], sl = 0;
@@ -562,7 +563,8 @@ void frag_vertex_grads(const MeshR<R>& m, const CamConst& cam, uint32_t face, in
             for (int k = 0; k < 4; ++k) gc[k] = std::fabs(gc[k]);
         }
         for (int k = 0; k < 3; ++k) grad_pos[3 * vi[j] + k] += gp[k];
-        for (int k = 0; k < 4; ++k) grad_col[4 * vi[j] + k] += gc[k];
+        if (grad_col)
+            for (int k = 0; k < 4; ++k) grad_col[4 * vi[j] + k] += gc[k];
     }
 }
 
@@ -975,6 +977,176 @@ int raytet_impl(const uint32_t* tri, const uint32_t* fbits, const uint32_t* f2t,
     return 0;
 }
 
+// ---------------------------------------------------------------------------
+// Per-cell colours (ColorStorage::PER_CELL).  Forward.glsl:213-246: two
+// consecutive fragments bound a segment of the tet both faces belong to
+// (tetIdUnion, LinkedListResolve.glsl:85-94; no shared tet = empty space, no
+// segment); the segment has that cell's constant colour and density,
+// accumulateConst (ForwardCommon.glsl:37-40): A = exp(-a t), C = (1 - A) c,
+// with no sub-segments.  Early ray termination is checked before each
+// fragment and the termination index is the fragment index where the loop
+// stopped (:222-227, 256-259).  The adjoint (Backward.glsl:283-329 with
+// accumulateConstAdjoint, BackwardCommon.glsl:100-105) is the exact
+// derivative: cell colour gradients per segment, position gradients through
+// the two fragment depths.
+constexpr uint32_t kInvalidTet = 0xffffffffu;
+
+inline uint32_t tet_union(uint32_t a0, uint32_t a1, uint32_t b0, uint32_t b1) {
+    if ((a0 == b0 || a0 == b1) && a0 != kInvalidTet) return a0;
+    if ((a1 == b0 || a1 == b1) && a1 != kInvalidTet) return a1;
+    return kInvalidTet;
+}
+
+template <class R>
+R face_depth(const MeshR<R>& m, uint32_t face, int px, int py) {
+    const uint32_t i0 = m.tri[3 * face], i1 = m.tri[3 * face + 1], i2 = m.tri[3 * face + 2];
+    R lam[3], b[3], z;
+    face_bary(m.proj[i0], m.proj[i1], m.proj[i2], R(px) + R(0.5), R(py) + R(0.5), lam, b, z);
+    return z;
+}
+
+inline uint32_t rec_face(uint64_t rec) { return uint32_t(rec & 0xffffffffu) >> 2; }
+
+template <class R>
+void composite_pixel_cells(const MeshR<R>& m, const uint32_t* f2t, const R* ccol, const Params& prm,
+                           const uint64_t* recs, int64_t n, int px, int py, R out[4], R& Tfinal, uint32_t& term) {
+    const R atten = R(prm.attenuation);
+    R C[3] = {0, 0, 0};
+    R T = 1, zprev = 0;
+    uint32_t pa = kInvalidTet, pb = kInvalidTet;
+    int64_t i = 0;
+    for (; i < n; ++i) {
+        if (prm.use_ert && T < R(prm.ert_thresh)) break;
+        const uint32_t face = rec_face(recs[i]);
+        const R z = face_depth(m, face, px, py);
+        const uint32_t qa = f2t[2 * size_t(face)], qb = f2t[2 * size_t(face) + 1];
+        const uint32_t open = tet_union(qa, qb, pa, pb);
+        if (open != kInvalidTet) {
+            const R* c = ccol + 4 * size_t(open);
+            const R A = std::exp(-(c[3] * atten) * (z - zprev));
+            for (int k = 0; k < 3; ++k) C[k] += T * (R(1) - A) * c[k];
+            T *= A;
+        }
+        pa = qa;
+        pb = qb;
+        zprev = z;
+    }
+    term = uint32_t(i);
+    Tfinal = T;
+    for (int k = 0; k < 3; ++k) out[k] = C[k] + T * R(prm.clear_color[k]);
+    out[3] = (R(1) - T) + T * R(prm.clear_color[3]);
+}
+
+template <class R>
+void adjoint_pixel_cells(const MeshR<R>& m, const CamConst& cam, const uint32_t* f2t, const R* ccol,
+                         const Params& prm, const uint64_t* recs, int64_t n, int px, int py, R Tfinal, uint32_t term,
+                         const R g[4], R* grad_pos, R* grad_cell) {
+    const int64_t last = (prm.use_ert ? int64_t(term) : n) - 1;  // last fragment visited
+    if (last < 1) return;
+    const R atten = R(prm.attenuation);
+    const bool use_abs = prm.use_abs_grad != 0;
+    const R gC[3] = {g[0], g[1], g[2]};
+    R gT = g[0] * R(prm.clear_color[0]) + g[1] * R(prm.clear_color[1]) + g[2] * R(prm.clear_color[2]) +
+           g[3] * (R(prm.clear_color[3]) - R(1));
+    R T = Tfinal;
+    const R zero4[4] = {0, 0, 0, 0};
+    uint32_t fb = rec_face(recs[last]);
+    R zb = face_depth(m, fb, px, py), gz_b = 0;
+    for (int64_t i = last; i >= 1; --i) {
+        const uint32_t ff = rec_face(recs[i - 1]);
+        const R zf = face_depth(m, ff, px, py);
+        R gz_f = 0;
+        const uint32_t open = tet_union(f2t[2 * size_t(fb)], f2t[2 * size_t(fb) + 1], f2t[2 * size_t(ff)],
+                                        f2t[2 * size_t(ff) + 1]);
+        if (open != kInvalidTet) {
+            const R* c = ccol + 4 * size_t(open);
+            const R a = c[3] * atten, t = zb - zf;
+            const R A = std::exp(-a * t);
+            const R Tin = T / A;
+            R gcacc[3], dot_c = 0, dot_cacc = 0;
+            for (int k = 0; k < 3; ++k) {
+                gcacc[k] = Tin * gC[k];
+                dot_c += gcacc[k] * c[k];
+                dot_cacc += gC[k] * (R(1) - A) * c[k];
+            }
+            const R gA = Tin * gT - dot_c;  // dL/dA: through T_out and through C = (1 - A) c
+            gT = dot_cacc + gT * A;
+            T = Tin;
+            const R g_t = gA * (-a * A), g_a = gA * (-t * A);
+            R gc[4] = {gcacc[0] * (R(1) - A), gcacc[1] * (R(1) - A), gcacc[2] * (R(1) - A), g_a * atten};
+            if (use_abs)
+                for (int k = 0; k < 4; ++k) gc[k] = std::fabs(gc[k]);
+            for (int k = 0; k < 4; ++k) grad_cell[4 * size_t(open) + k] += gc[k];
+            gz_b += g_t;
+            gz_f -= g_t;
+        }
+        frag_vertex_grads(m, cam, fb, px, py, gz_b, zero4, use_abs, grad_pos, static_cast<R*>(nullptr));
+        fb = ff;
+        zb = zf;
+        gz_b = gz_f;
+    }
+    frag_vertex_grads(m, cam, fb, px, py, gz_b, zero4, use_abs, grad_pos, static_cast<R*>(nullptr));
+}
+
+template <class R>
+int cells_impl(const uint32_t* tri, const uint32_t* fbits, const uint32_t* f2t, int64_t F, const R* pos,
+               const R* ccol, int64_t V, int64_t T, const Camera* camp, const Params* prm, R* image, R* tfinal,
+               uint32_t* term, int64_t* nfrag, const R* image_adj, R* grad_pos, R* grad_cell,
+               const float* pos_coverage) {
+    CamConst cam = make_cam(*camp);
+    int r0, r1;
+    row_range(*prm, cam.H, r0, r1);
+    auto pf = pos_coverage ? project_all_f(pos_coverage, V, cam) : project_all_f(pos, V, cam);
+    FragLists fl = build_fragments(tri, fbits, F, pf, cam, r0, r1);
+    MeshR<R> m = make_mesh<R>(tri, pos, nullptr, V, cam);
+    const int W = cam.W;
+    int nthreads = 1;
+#ifdef _OPENMP
+    nthreads = omp_get_max_threads();
+#endif
+    std::vector<std::vector<R>> gp, gc;
+    if (image_adj) {
+        gp.assign(nthreads, std::vector<R>(3 * V, R(0)));
+        gc.assign(nthreads, std::vector<R>(4 * T, R(0)));
+    }
+#pragma omp parallel
+    {
+        int tid = 0;
+#ifdef _OPENMP
+        tid = omp_get_thread_num();
+#endif
+#pragma omp for schedule(dynamic, 4)
+        for (int py = r0; py < r1; ++py) {
+            for (int px = 0; px < W; ++px) {
+                const int64_t p = int64_t(py) * W + px;
+                const uint64_t* recs = fl.records.data() + fl.offsets[p];
+                const int64_t n = fl.offsets[p + 1] - fl.offsets[p];
+                R out[4], Tf;
+                uint32_t tm;
+                composite_pixel_cells(m, f2t, ccol, *prm, recs, n, px, py, out, Tf, tm);
+                if (image)
+                    for (int k = 0; k < 4; ++k) image[4 * p + k] = out[k];
+                if (tfinal) tfinal[p] = Tf;
+                if (term) term[p] = tm;
+                if (image_adj) {
+                    const R g[4] = {image_adj[4 * p], image_adj[4 * p + 1], image_adj[4 * p + 2],
+                                    image_adj[4 * p + 3]};
+                    adjoint_pixel_cells(m, cam, f2t, ccol, *prm, recs, n, px, py, Tf, tm, g, gp[tid].data(),
+                                        gc[tid].data());
+                }
+            }
+        }
+    }
+    if (image_adj) {
+        for (int t = 0; t < nthreads; ++t) {
+            for (int64_t i = 0; i < 3 * V; ++i) grad_pos[i] += gp[t][i];
+            for (int64_t i = 0; i < 4 * T; ++i) grad_cell[i] += gc[t][i];
+        }
+    }
+    if (nfrag) *nfrag = int64_t(fl.records.size());
+    return 0;
+}
+
 struct TempFace {
     uint32_t v[3];
     uint32_t face_id;
@@ -1139,6 +1311,17 @@ void orc_segment_integral(double t, const double* c0, const double* c1, double a
     bool active = seg_integral<double>(t, c0, c1, a, cacc, A);
     for (int k = 0; k < 3; ++k) out4[k] = cacc[k];
     out4[3] = active ? 1.0 - A : 0.0;
+}
+
+// Per-cell colours: forward (image, T_final, termination index, #fragments) and,
+// with image_adj, the adjoint added into grad_pos [3V] and grad_cell [4T].
+// pos_coverage (nullable): fragment lists from these positions (frozen lists).
+int orc_cells_f64(const uint32_t* tri, const uint32_t* fbits, const uint32_t* f2t, int64_t F, const double* pos,
+                  const double* ccol, int64_t V, int64_t T, const Camera* cam, const Params* prm, double* image,
+                  double* tfinal, uint32_t* term, int64_t* nfrag, const double* image_adj, double* grad_pos,
+                  double* grad_cell, const float* pos_coverage) {
+    return cells_impl<double>(tri, fbits, f2t, F, pos, ccol, V, T, cam, prm, image, tfinal, term, nfrag, image_adj,
+                              grad_pos, grad_cell, pos_coverage);
 }
 
 // Tet-quality regularizer (Data/Shaders/Optimizer/TetRegularizer.glsl:108-166):

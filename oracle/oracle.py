@@ -76,6 +76,10 @@ def load():
         lib.orc_segment_integral.restype = None
         lib.orc_segment_integral.argtypes = [ctypes.c_double, _vp, _vp, ctypes.c_double, _vp]
         lib.orc_num_threads.restype = ctypes.c_int
+        lib.orc_cells_f64.argtypes = [_vp, _vp, _vp, ctypes.c_int64, _vp, _vp, ctypes.c_int64, ctypes.c_int64,
+                                      ctypes.POINTER(Camera), ctypes.POINTER(Params), _vp, _vp, _vp, _vp, _vp, _vp,
+                                      _vp, _vp]
+        lib.orc_cells_f64.restype = ctypes.c_int
         lib.orc_tet_regularizer.argtypes = [_vp, ctypes.c_int64, _vp, ctypes.c_double, ctypes.c_double, _vp]
         lib.orc_tet_regularizer.restype = ctypes.c_double
         _lib = lib
@@ -230,6 +234,32 @@ def segment_integral(t, c0, c1, a):
     out = np.zeros(4, np.float64)
     lib.orc_segment_integral(float(t), _p(c0), _p(c1), float(a), _p(out))
     return out
+
+
+def render_cells(faces: Faces, positions, cell_colors, cam: Camera, prm: Params, image_adjoint=None,
+                 positions_coverage=None):
+    """Per-cell colours (ColorStorage.PER_CELL), FP64: (image [H,W,4], T_final, termination, #fragments) and,
+    with image_adjoint, also (grad_positions [V,3], grad_cell_colors [T,4])."""
+    lib = load()
+    pos = np.ascontiguousarray(positions, np.float64)
+    ccol = np.ascontiguousarray(cell_colors, np.float64)
+    V, T = pos.shape[0], ccol.shape[0]
+    P = cam.width * cam.height
+    img = np.zeros((P, 4))
+    tf = np.ones(P)
+    term = np.zeros(P, np.uint32)
+    nf = ctypes.c_int64()
+    gp = np.zeros((V, 3))
+    gc = np.zeros((T, 4))
+    gimg = None if image_adjoint is None else np.ascontiguousarray(image_adjoint, np.float64).reshape(-1, 4)
+    pc = None if positions_coverage is None else np.ascontiguousarray(positions_coverage, np.float32)
+    lib.orc_cells_f64(_p(faces.tri), _p(faces.face_boundary), _p(faces.face_to_tet), faces.num_faces, _p(pos),
+                      _p(ccol), V, T, ctypes.byref(cam), ctypes.byref(prm), _p(img), _p(tf), _p(term),
+                      ctypes.byref(nf), None if gimg is None else _p(gimg), _p(gp), _p(gc),
+                      None if pc is None else _p(pc))
+    H, W = cam.height, cam.width
+    out = (img.reshape(H, W, 4), tf.reshape(H, W), term.reshape(H, W), int(nf.value))
+    return out if gimg is None else out + (gp, gc)
 
 
 def tet_regularizer(cells, positions, reg_lambda: float, softplus_beta: float):

@@ -1,0 +1,128 @@
+"""Per-cell colours (ColorStorage.PER_CELL) on the CUDA path vs the FP64 oracle
+(B200): images within 1e-5, termination index, gradients of positions and
+cell colours within 1e-4 relative; banded recomputation; .bintet version 2;
+the autograd wrapper."""
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from difftetvr_b200 import synthetic as S
+from helpers import Scene, rel_err, two_block_scene
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def _cells_renderer(sc, ccol, atten=2.0, ert=False):
+    import difftetvr_b200 as d
+    m = d.TetMesh()
+    m.set_use_gradients(True)
+    m.set_tet_mesh_data_cell(sc.cells, sc.pos, ccol)
+    r = d.Renderer(d.RendererType.PPLL)
+    r.set_tet_mesh(m)
+    r.set_viewport_size(sc.res, sc.res)
+    r.set_camera_fovy(sc.fovy)
+    r.set_view_matrix(sc.view)
+    r.set_attenuation(atten)
+    r.set_use_early_ray_termination(ert)
+    r.set_early_ray_out_thresh(0.02 if ert else 1e-4)
+    r.set_clear_color(d.vec4(0, 0, 0, 0))
+    return m, r
+
+
+def _ccol(sc, seed):
+    return np.random.default_rng(seed).uniform(0.05, 2.0, size=(sc.cells.shape[0], 4)).astype(np.float32)
+
+
+@pytest.mark.parametrize("kind,n,res,ert", [("cube", 8, 128, False), ("cube", 16, 256, False),
+                                            ("cube", 12, 192, True), ("two_blocks", 4, 128, False)])
+def test_image_and_gradients_match_fp64_oracle(oracle, kind, n, res, ert):
+    sc = two_block_scene(n, res, seed=n) if kind == "two_blocks" else Scene(n, res, seed=n + 3)
+    ccol = _ccol(sc, n)
+    m, r = _cells_renderer(sc, ccol, ert=ert)
+    img = r.render().cpu().numpy().astype(np.float64)
+    _, term_g = r.get_pixel_state()
+    w = np.random.default_rng(7).normal(size=(res, res, 4)).astype(np.float32)
+    p, c = m.get_vertex_positions(), m.get_cell_colors()
+    p.grad.zero_()
+    c.grad.zero_()
+    r.render_adjoint(torch.from_numpy(w).cuda())
+    fa = oracle.Faces(sc.cells, sc.pos.shape[0])
+    prm = oracle.make_params(attenuation=2.0, use_ert=ert, ert_thresh=0.02)
+    img_o, _, term_o, nf_o, gp_o, gc_o = oracle.render_cells(fa, sc.pos, ccol, sc.oracle_camera(oracle), prm,
+                                                              image_adjoint=w.astype(np.float64))
+    assert r.get_num_fragments() == nf_o
+    same = term_g == term_o
+    assert same.mean() > 0.999
+    err = np.abs(img - img_o).max(-1)
+    assert err[same].max() < 1e-5, float(err[same].max())
+    assert rel_err(p.grad.cpu().numpy(), gp_o) < 1e-4, rel_err(p.grad.cpu().numpy(), gp_o)
+    assert rel_err(c.grad.cpu().numpy(), gc_o) < 1e-4, rel_err(c.grad.cpu().numpy(), gc_o)
+
+
+def test_banded_per_cell_equals_stored():
+    sc = Scene(12, 192, seed=4)
+    m, r = _cells_renderer(sc, _ccol(sc, 1))
+    w = torch.randn(192, 192, 4, device="cuda", generator=torch.Generator(device="cuda").manual_seed(0))
+    img_s = r.render().clone()
+    p, c = m.get_vertex_positions(), m.get_cell_colors()
+    p.grad.zero_()
+    c.grad.zero_()
+    r.render_adjoint(w)
+    gp_s, gc_s = p.grad.clone(), c.grad.clone()
+    r.set_fragment_budget_bytes(r.get_num_fragments() * 8 // 3)
+    img_b = r.render().clone()
+    p.grad.zero_()
+    c.grad.zero_()
+    r.render_adjoint(w)
+    assert r.get_num_bands() >= 3 and torch.equal(img_b, img_s)
+    assert rel_err(p.grad.cpu().numpy(), gp_s.cpu().numpy()) < 1e-5
+    assert rel_err(c.grad.cpu().numpy(), gc_s.cpu().numpy()) < 1e-5
+
+
+def test_bintet_v2_and_autograd(tmp_path):
+    import difftetvr_b200 as d
+    m = d.TetMesh()
+    m.set_use_gradients(True)
+    assert m.load_from_file(os.path.join(GOLDEN, "kuhn2_cells_v2.bintet"))
+    assert m.get_color_storage() == d.ColorStorage.PER_CELL and m.get_vertex_colors() is None
+    assert tuple(m.get_cell_colors().shape) == (m.get_num_cells(), 4)
+    out = str(tmp_path / "c.bintet")
+    assert m.save_to_file(out)
+    assert open(out, "rb").read() == open(os.path.join(GOLDEN, "kuhn2_cells_v2.bintet"), "rb").read()
+    r = d.Renderer(d.RendererType.PPLL)
+    r.set_tet_mesh(m)
+    r.set_viewport_size(64, 64)
+    r.set_view_matrix(S.look_at_view([1.2, 1.9, 2.4]))
+    r.set_attenuation(1.0)
+    img = d.DifferentiableRenderer(r)()
+    assert float(img[..., 3].max()) > 0.1
+    img.sum().backward()
+    assert float(m.get_cell_colors().grad.abs().sum()) > 0
+    assert float(m.get_vertex_positions().grad.abs().sum()) > 0
+    with pytest.raises(RuntimeError):
+        d.Renderer(d.RendererType.INTERSECTION).set_tet_mesh(m) or None
+        ri = d.Renderer(d.RendererType.INTERSECTION)
+        ri.set_tet_mesh(m)
+        ri.render()
+
+
+def test_hex_mesh_const_per_cell_matches_per_vertex():
+    """One constant colour: per-cell and per-vertex storage render the same
+    image up to FP32 rounding where every consecutive fragment pair shares a tet."""
+    import difftetvr_b200 as d
+    imgs = []
+    for storage in (d.ColorStorage.PER_VERTEX, d.ColorStorage.PER_CELL):
+        m = d.TetMesh()
+        m.set_hex_mesh_const(d.AABB3(d.vec3(-1, -1, -1), d.vec3(1, 1, 1)), 9, 9, 9, d.vec4(0.4, 0.6, 0.8, 0.9),
+                             storage)
+        r = d.Renderer(d.RendererType.PPLL)
+        r.set_tet_mesh(m)
+        r.set_viewport_size(96, 96)
+        r.set_view_matrix(S.sphere_camera(3))
+        r.set_attenuation(1.0)
+        imgs.append(r.render().cpu().numpy())
+    diff = np.abs(imgs[0] - imgs[1]).max(-1)
+    assert (diff < 1e-5).mean() > 0.99
