@@ -119,6 +119,11 @@ SIGNATURES = {
                                                            c_vp, c_vp]),
     "dtv_renderer_get_num_fragments": (ctypes.c_int32, [c_vp, c_u64p]),
     "dtv_renderer_get_num_bands": (ctypes.c_int32, [c_vp, ctypes.POINTER(ctypes.c_int32)]),
+    "dtv_mesh_subdivide_vertices": (ctypes.c_int32, [c_vp, ctypes.c_uint64, c_vp, ctypes.c_uint64, c_vp, c_vp, c_vp,
+                                                     ctypes.c_uint64, ctypes.c_float, ctypes.POINTER(c_vp)]),
+    "dtv_split_result_sizes": (ctypes.c_int32, [c_vp, c_u64p, c_u64p]),
+    "dtv_split_result_copy": (ctypes.c_int32, [c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "dtv_split_result_destroy": (ctypes.c_int32, [c_vp]),
     "dtv_bintet_peek": (ctypes.c_int32, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_uint32), c_u64p, c_u64p, c_u64p,
                                           c_u64p]),
     "dtv_bintet_read": (ctypes.c_int32, [ctypes.c_char_p, c_vp, c_vp, c_vp, c_vp]),

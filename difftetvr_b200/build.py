@@ -17,7 +17,7 @@ CSRC = os.path.join(PKG_DIR, "csrc")
 LIB_NAME = "libdifftetvr_b200.so"
 LIB_PATH = os.path.join(PKG_DIR, LIB_NAME)
 
-SOURCES = ["dtv_api.cu", "dtv_kernels.cu", "dtv_mesh.cpp", "dtv_noalloc.cu", "dtv_batch.cu", "dtv_raytet.cu", "dtv_regularizer.cu", "dtv_io.cpp", "dtv_cells.cu"]
+SOURCES = ["dtv_api.cu", "dtv_kernels.cu", "dtv_mesh.cpp", "dtv_noalloc.cu", "dtv_batch.cu", "dtv_raytet.cu", "dtv_regularizer.cu", "dtv_io.cpp", "dtv_cells.cu", "dtv_split.cpp"]
 HEADERS = ["dtv_types.h", "dtv_device.cuh", "dtv_segment.cuh", "dtv_internal.h", "dtv_host.h", "dtv_path.cuh"]
 
 NVCC_FLAGS = [

@@ -17,7 +17,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .types import AABB3, ColorStorage, TestCase, vec3, vec4
+from .types import AABB3, ColorStorage, SplitGradientType, TestCase, vec3, vec4
 
 # HEX_TO_TET_TABLE, src/Tet/TetMesh.cpp:104-117 (Kuhn split around diagonal 0-6).
 HEX_TO_TET_TABLE = np.array([[0, 4, 7, 6], [0, 4, 6, 5], [0, 3, 6, 7], [0, 3, 2, 6], [0, 1, 5, 6], [0, 1, 6, 2]],
@@ -191,6 +191,49 @@ class TetMesh:
             self.set_tet_mesh_data_cell(cells, pos, np.tile(c, (cells.shape[0], 1)))
         else:
             self.set_tet_mesh_data(cells, pos, np.tile(c, (pos.shape[0], 1)))
+
+    # -- coarse to fine (Module.cpp:820-832) ----------------------------------
+    def split_by_largest_gradient_magnitudes(self, volume_renderer, split_gradient_type: SplitGradientType,
+                                             splits_ratio: float) -> None:
+        """TetMesh::splitByLargestGradientMagnitudes (TetMesh.cpp:1786-1881):
+        the ceil(splits_ratio * V) vertices with the largest gradient magnitude
+        (|d position| for POSITION / ABS_POSITION and for per-cell meshes,
+        |d colour| otherwise) are subdivided in descending order, then the
+        renderer is given the refined mesh.  Gradients are read from .grad."""
+        V = self.get_num_vertices()
+        gtype = SplitGradientType(split_gradient_type)
+        use_pos = gtype in (SplitGradientType.POSITION, SplitGradientType.ABS_POSITION) or \
+            self._color_storage == ColorStorage.PER_CELL
+        g = (self._positions if use_pos else self._colors).grad
+        mag = np.zeros(V, np.float32) if g is None else g.detach().norm(dim=1).float().cpu().numpy()
+        num = min(int(np.ceil(float(splits_ratio) * V)), V)
+        # Descending (magnitude, index) pairs, as a reverse sort of the pairs.
+        order = np.lexsort((-np.arange(V), -mag.astype(np.float64)))[:num].astype(np.uint32)
+        cells = np.ascontiguousarray(self._cells)
+        pos = np.ascontiguousarray(self._positions.detach().cpu().numpy())
+        vcol = None if self._colors is None else np.ascontiguousarray(self._colors.detach().cpu().numpy())
+        ccol = None if self._cell_colors is None else np.ascontiguousarray(self._cell_colors.detach().cpu().numpy())
+        res = ctypes.c_void_p()
+        _lib.call("dtv_mesh_subdivide_vertices", cells.ctypes.data, cells.shape[0], pos.ctypes.data, V,
+                  None if vcol is None else vcol.ctypes.data, None if ccol is None else ccol.ctypes.data,
+                  order.ctypes.data, order.shape[0], ctypes.c_float(0.5), ctypes.byref(res))
+        try:
+            nt, nv = ctypes.c_uint64(), ctypes.c_uint64()
+            _lib.call("dtv_split_result_sizes", res, ctypes.byref(nt), ctypes.byref(nv))
+            c2 = np.empty((nt.value, 4), np.uint32)
+            p2 = np.empty((nv.value, 3), np.float32)
+            v2 = None if vcol is None else np.empty((nv.value, 4), np.float32)
+            cc2 = None if ccol is None else np.empty((nt.value, 4), np.float32)
+            _lib.call("dtv_split_result_copy", res, c2.ctypes.data, p2.ctypes.data,
+                      None if v2 is None else v2.ctypes.data, None if cc2 is None else cc2.ctypes.data)
+        finally:
+            _lib.load().dtv_split_result_destroy(res)
+        if cc2 is not None:
+            self.set_tet_mesh_data_cell(c2, p2, cc2)
+        else:
+            self.set_tet_mesh_data(c2, p2, v2)
+        if volume_renderer is not None:
+            volume_renderer.set_tet_mesh(self)
 
     # -- files (Module.cpp:787-788) ------------------------------------------
     def load_from_file(self, file_path: str) -> bool:

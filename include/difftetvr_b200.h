@@ -182,6 +182,26 @@ int32_t dtv_renderer_copy_pixel_state(const dtv_renderer* r, float* h_transmitta
 int32_t dtv_renderer_set_timing(dtv_renderer* r, int32_t enable);
 int32_t dtv_renderer_stage_times(const dtv_renderer* r, float* h_ms, int32_t n);
 
+/* Coarse-to-fine refinement: replaces TetMesh::subdivideVertices /
+ * subdivideAtVertex (src/Tet/TetMesh.cpp:1374-1600, 1757-1784) behind
+ * TetMesh.split_by_largest_gradient_magnitudes (Module.cpp:820-832).  For each
+ * vertex of h_split_vertices in order, every incident edge gets a new vertex
+ * at p_v + t (p_w - p_v) and every incident tet becomes the tet at v plus a
+ * prism cut into three tets (diagonals through the smallest vertex index of
+ * each quadrilateral: conforming); orientation and cell colour are inherited.
+ * Host memory; colour arrays nullable.  The result (cells u32[4T'], positions
+ * f32[3V'], vertex colours f32[4V'] / cell colours f32[4T'] when given) is
+ * read with dtv_split_result_sizes / _copy and freed with _destroy. */
+typedef struct dtv_split_result dtv_split_result;
+int32_t dtv_mesh_subdivide_vertices(const uint32_t* h_cells, uint64_t num_cells, const float* h_positions,
+                                    uint64_t num_vertices, const float* h_vertex_colors, const float* h_cell_colors,
+                                    const uint32_t* h_split_vertices, uint64_t num_split, float t,
+                                    dtv_split_result** out);
+int32_t dtv_split_result_sizes(const dtv_split_result* r, uint64_t* num_cells, uint64_t* num_vertices);
+int32_t dtv_split_result_copy(const dtv_split_result* r, uint32_t* h_cells, float* h_positions,
+                              float* h_vertex_colors, float* h_cell_colors);
+int32_t dtv_split_result_destroy(dtv_split_result* r);
+
 /* .bintet mesh files: replaces BinTetLoader::loadFromFile / peekSizes and
  * BinTetWriter::saveToFile (src/Tet/Loaders/BinTetLoader.cpp:37-138) behind
  * TetMesh.load_from_file / save_to_file (Module.cpp:787-788).  Layout: u32
