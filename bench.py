@@ -171,6 +171,22 @@ def build_scene(args, device, renderer_type=None):
             "renderer": r, "np": np}
 
 
+def max_over_ranks(ms: float, world: int, device=None) -> float:
+    """The slowest rank's device-timed duration (every rank calls this with its
+    own CUDA-event time; all ranks get the maximum)."""
+    if world <= 1:
+        return float(ms)
+    import torch
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world: int, steps: int, ms: float) -> float:
+    """Iterations/s of the whole job: every rank (replica) ran `steps` views."""
+    return world * steps / (ms / 1e3)
+
+
 def run_ours(args, rank, world):
     import torch
 
@@ -225,13 +241,9 @@ def run_ours(args, rank, world):
     t1.record(stream)
     barrier()
     clk = clocks.stop()
-    ms = t0.elapsed_time(t1)
+    ms = max_over_ranks(t0.elapsed_time(t1), world, device)
     r.set_stage_timing(False)
-    if world > 1:
-        tt = torch.tensor([ms], device=device)
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        ms = float(tt.item())
-    value = world * args.steps / (ms / 1e3)
+    value = whole_job_rate(world, args.steps, ms)
 
     # End-to-end through the public API, host buffers in the timed region.
     e2e = None
@@ -262,12 +274,8 @@ def run_ours(args, rank, world):
             e2e_step(i)
         e1.record(stream)
         barrier()
-        ems = e0.elapsed_time(e1)
-        if world > 1:
-            tt = torch.tensor([ems], device=device)
-            torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-            ems = float(tt.item())
-        e2e = {"value": world * args.steps / (ems / 1e3), "unit": "iter/s", "h2d_bytes_per_step": h2d,
+        ems = max_over_ranks(e0.elapsed_time(e1), world, device)
+        e2e = {"value": whole_job_rate(world, args.steps, ems), "unit": "iter/s", "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": 4, "ms_per_step": ems / args.steps,
                "api": "DifferentiableRenderer + optim.l2_loss + optim.Adam"}
 
