@@ -43,6 +43,8 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-raytet", action="store_true")
+    ap.add_argument("--profile", choices=["ppll", "intersection"], default=None,
+                    help="profiling case: Kuhn --n^3 at --res^2, one warm-up and one render + adjoint, no timing")
     ap.add_argument("--no-scale", action="store_true")
     ap.add_argument("--scale-n", type=int, default=128)
     ap.add_argument("--scale-res", type=int, default=2048)
@@ -598,8 +600,7 @@ def run_serving(args):
         r.set_camera_fovy(S.FOVY_45)
         r.set_attenuation(1.0)
         rends[k] = r
-    iso = []
-    for j, q in enumerate(make_requests(np.random.default_rng(7), 60)):
+    def solve_alone(q):
         r = rends[q.mesh]
         r.set_viewport_size(q.width, q.height)
         r.set_view_matrix(q.view_matrix)
@@ -609,13 +610,27 @@ def run_serving(args):
         if q.mode == "gradient":
             r.render_adjoint(((img - q.target) * (2.0 / img.numel())).contiguous())
         torch.cuda.synchronize()
-        if j >= 5:
-            iso.append((time.perf_counter() - t0) * 1e3)
-    iso = np.array(iso)
+        return (time.perf_counter() - t0) * 1e3
+
+    # Warm every (mesh, resolution, mode) once (first-use allocations), largest
+    # resolution first, then time a seeded sample of the request mix.
+    for k in names:
+        for res in sorted(res_choices, reverse=True):
+            for mode in ("gradient", "forward"):
+                solve_alone(Request(mesh=k, view_matrix=S.sphere_camera(1), width=res, height=res, mode=mode,
+                                    target=targets[res] if mode == "gradient" else None))
+    iso = np.array([solve_alone(q) for q in make_requests(np.random.default_rng(7), 80)])
     out = {"meshes": list(names), "resolutions": res_choices, "resolution_weights": res_w, "gradient_fraction": 0.3,
            "slots": be.slots, "isolated": {"p50_ms": float(np.percentile(iso, 50)),
                                             "p99_ms": float(np.percentile(iso, 99))}, "rates": []}
     budget = int(max(be.fragments_per_pixel(k) for k in names) * 1024 * 1024 * 4)
+    be.reserve(32, max(res_choices) ** 2, int(1.5 * budget))
+    # Warm-up pass (first batches of each slot), not reported.
+    eng = ServingEngine(be, budget_fragments=budget, max_batch=32)
+    eng.start()
+    for f in [eng.submit(q) for q in make_requests(np.random.default_rng(3), 24)]:
+        f.result(timeout=600)
+    eng.stop()
     for rate in [float(x) for x in args.serving_rates.split(",") if x]:
         rng = np.random.default_rng(int(rate))
         reqs = make_requests(rng, args.serving_requests)
@@ -699,8 +714,40 @@ def run_reference(args, rank, world):
     }
 
 
+def run_profile_case(args):
+    """A small fixed case for ncu: one warm-up and one render + adjoint of the
+    Kuhn n^3 mesh (seed 0) from sphere camera 100 at res x res."""
+    import torch
+
+    import difftetvr_b200 as d
+    from difftetvr_b200 import synthetic as S
+    cells, pos = S.kuhn_mesh(args.n, seed=0)
+    col = S.gaussian_colors(pos, seed=0)
+    mesh = d.TetMesh()
+    mesh.set_use_gradients(True)
+    mesh.set_tet_mesh_data(cells, pos, col)
+    rt = d.RendererType.INTERSECTION if args.profile == "intersection" else d.RendererType.PPLL
+    r = d.Renderer(rt)
+    r.set_tet_mesh(mesh)
+    r.set_viewport_size(args.res, args.res)
+    r.set_camera_fovy(S.FOVY_45)
+    r.set_attenuation(1.0)
+    r.set_clear_color(d.vec4(0, 0, 0, 0))
+    r.set_view_matrix(S.sphere_camera(100))
+    w = torch.randn(args.res, args.res, 4, device="cuda", generator=torch.Generator(device="cuda").manual_seed(0))
+    w *= 1e-3
+    for _ in range(2):
+        r.render()
+        r.render_adjoint(w)
+    torch.cuda.synchronize()
+    print(json.dumps({"profile": args.profile, "n": args.n, "res": args.res, "fragments": r.get_num_fragments()}))
+    return 0
+
+
 def main():
     args = parse_args()
+    if args.profile:
+        return run_profile_case(args)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if args.impl == "reference":

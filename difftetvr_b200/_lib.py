@@ -113,6 +113,8 @@ SIGNATURES = {
                                              ctypes.POINTER(RenderParams), c_vp, c_vp]),
     "dtv_renderer_render_adjoint": (ctypes.c_int32, [c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.c_int32, c_vp, c_vp,
                                                      c_vp]),
+    "dtv_batch_reserve": (ctypes.c_int32, [c_vp, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64,
+                                           ctypes.c_uint64, c_vp]),
     "dtv_renderer_render_cells": (ctypes.c_int32, [c_vp, c_vp, c_vp, c_vp, ctypes.POINTER(Camera),
                                                    ctypes.POINTER(RenderParams), c_vp, c_vp]),
     "dtv_renderer_render_adjoint_cells": (ctypes.c_int32, [c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.c_int32, c_vp,

@@ -66,6 +66,14 @@ class BatchRenderer:
         arr_c = (ctypes.c_void_p * n)(*[m.get_vertex_colors().data_ptr() for m in self.meshes])
         _lib.call("dtv_batch_set_meshes", self._handle, n, arr_m, arr_p, arr_c)
 
+    def reserve(self, max_views: int, max_vertices: int, max_pixels: int, max_fragments: int,
+                max_grad_vertices: int) -> None:
+        """Allocates scratch for batches up to these sizes now (dtv_batch_reserve),
+        so serving never allocates device memory between batches."""
+        import torch
+        _lib.call("dtv_batch_reserve", self._handle, int(max_views), int(max_vertices), int(max_pixels),
+                  int(max_fragments), int(max_grad_vertices), torch.cuda.current_stream().cuda_stream)
+
     def set_graph(self, enable: bool = True) -> None:
         _lib.call("dtv_batch_set_graph", self._handle, int(bool(enable)))
 

@@ -476,6 +476,41 @@ int32_t dtv_batch_create(dtv_batch** out) {
     });
 }
 
+int32_t dtv_batch_reserve(dtv_batch* b, uint64_t max_views, uint64_t max_vertices, uint64_t max_pixels,
+                          uint64_t max_fragments, uint64_t max_grad_vertices, dtv_stream stream) {
+    return guarded([&] {
+        require(b != nullptr, "batch is null");
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        const size_t nv = size_t(max_views ? max_views : 1);
+        ensure_pinned(reinterpret_cast<void**>(&b->h_views), b->h_views_cap, sizeof(BatchView) * nv);
+        ensure_pinned(reinterpret_cast<void**>(&b->h_slots), b->h_slots_cap, sizeof(BatchSlot) * nv);
+        b->d_views.ensure(nv, s);
+        b->d_slots.ensure(nv, s);
+        const u64 V = max_vertices ? max_vertices : 1, P = max_pixels ? max_pixels : 1;
+        b->vproj.ensure(V, s);
+        b->vfix.ensure(V, s);
+        b->vgeo.ensure(V, s);
+        b->counts.ensure(P, s, /*zero_new=*/true);
+        b->offsets.ensure(P + 1, s);
+        b->scan.ensure(dtv::scan_scratch_elems(P), s);
+        b->tfinal.ensure(P, s);
+        b->term.ensure(P, s);
+        b->long_list.ensure(P, s);
+        b->records.ensure(max_fragments ? max_fragments : 1, s);
+        b->grad_rows.ensure(2 * (max_grad_vertices ? max_grad_vertices : 1), s);
+        b->sort_flags.ensure(2, s);
+        b->ok.ensure(1, s);
+        b->total.ensure(1, s);
+        b->loss.ensure(1, s);
+        if (!b->h_ok) {
+            DTV_CK(cudaMallocHost(&b->h_ok, sizeof(uint32_t)));
+            DTV_CK(cudaMallocHost(&b->h_total, sizeof(u64)));
+            DTV_CK(cudaEventCreateWithFlags(&b->staging_free, cudaEventDisableTiming));
+        }
+        DTV_CK(cudaStreamSynchronize(s));
+    });
+}
+
 int32_t dtv_batch_destroy(dtv_batch* b) {
     if (!b) return DTV_OK;
     cudaDeviceSynchronize();

@@ -206,6 +206,15 @@ class GpuBackend:
                           for _ in range(self.slots)]
         self.fpp = {n: 64.0 for n in self.names}
 
+    def reserve(self, max_batch: int, max_pixels_per_request: int, budget_fragments: int) -> None:
+        """Sizes every slot's scratch for the largest admissible batch, so no
+        device allocation (which synchronises the whole device) happens while
+        serving."""
+        maxV = max(m.get_num_vertices() for m in self.meshes)
+        for br in self.renderers:
+            br.reserve(max_batch, max_batch * maxV, max_batch * max_pixels_per_request, budget_fragments,
+                       max_batch * maxV)
+
     def fragments_per_pixel(self, mesh: str) -> float:
         return self.fpp[mesh]
 

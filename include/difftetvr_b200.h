@@ -280,6 +280,13 @@ typedef struct dtv_batch_optim {
 
 int32_t dtv_batch_create(dtv_batch** out);
 int32_t dtv_batch_destroy(dtv_batch* batch);
+/* Sizes the batch's device scratch for up to max_views views, max_vertices
+ * projected vertices (sum over views of the view's mesh size), max_pixels
+ * pixels, max_fragments fragment records and max_grad_vertices gradient rows,
+ * so later batches within these bounds allocate nothing (device allocation
+ * synchronises the device, which a serving loop with several slots avoids). */
+int32_t dtv_batch_reserve(dtv_batch* batch, uint64_t max_views, uint64_t max_vertices, uint64_t max_pixels,
+                          uint64_t max_fragments, uint64_t max_grad_vertices, dtv_stream stream);
 /* Mesh table: topology handles plus device positions f32[V*3] and colours f32[V*4]
  * (updated in place by dtv_batch_train_step). */
 int32_t dtv_batch_set_meshes(dtv_batch* batch, int32_t num_meshes, const dtv_mesh* const* meshes,
