@@ -78,7 +78,7 @@ struct dtv_renderer {
     DevBuf<u64> scan_scratch;
     DevBuf<float> tfinal;
     DevBuf<uint32_t> term;
-    DevBuf<uint32_t> long_list;
+    DevBuf<uint32_t> long_list;     // sort scratch (length classes)
     DevBuf<uint32_t> flags;
     DevBuf<float4> grad_rows;     // [V][2] interleaved vertex gradient accumulator
     // Row bands [row0, row1) of the last render when its lists exceeded the
@@ -164,11 +164,8 @@ void build_band_lists(dtv_renderer* r, const dtv_mesh* mesh, int W, int H, int y
     dtv::launch_raster_fill(mesh->d_faces, uint32_t(mesh->host.num_faces), r->vproj.ptr, r->vfix.ptr, W, H,
                             r->counts.ptr, r->offsets.ptr, r->records.ptr, s, y0, y1);
     check_launch("band fill");
-    DTV_CK(cudaMemsetAsync(r->flags.ptr, 0, sizeof(uint32_t), s));  // long-list count; keep the error flag
     dtv::launch_sort(r->offsets.ptr + p0, r->records.ptr, uint32_t(pb), r->long_list.ptr, r->flags.ptr, s);
     check_launch("band sort");
-    dtv::launch_sort_long(r->offsets.ptr + p0, r->records.ptr, r->long_list.ptr, 0, r->flags.ptr, s);
-    check_launch("band sort long lists");
 }
 
 void record_flags(dtv_renderer* r, cudaStream_t s) {
@@ -486,7 +483,7 @@ int32_t render_common(dtv_renderer* r, const dtv_mesh* mesh, const float* d_posi
             r->wstate.ensure(P, s);
         else
             r->term.ensure(P, s);
-        r->long_list.ensure(P, s);
+        r->long_list.ensure(dtv::sort_scratch_elems(P), s);
         r->flags.ensure(2, s);
 
         rec_event(r, 0, s);
@@ -537,8 +534,6 @@ int32_t render_common(dtv_renderer* r, const dtv_mesh* mesh, const float* d_posi
         DTV_CK(cudaMemsetAsync(r->flags.ptr, 0, 2 * sizeof(uint32_t), s));
         dtv::launch_sort(r->offsets.ptr, r->records.ptr, uint32_t(P), r->long_list.ptr, r->flags.ptr, s);
         check_launch("sort");
-        dtv::launch_sort_long(r->offsets.ptr, r->records.ptr, r->long_list.ptr, 0, r->flags.ptr, s);
-        check_launch("sort long lists");
         DTV_CK(cudaMemcpyAsync(r->h_flags, r->flags.ptr, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
         DTV_CK(cudaEventRecord(r->flags_event, s));
         r->flags_pending = true;

@@ -421,7 +421,7 @@ void ensure_scratch(dtv_batch* b, cudaStream_t s) {
     b->scan.ensure(dtv::scan_scratch_elems(b->tot_pixels), s);
     b->tfinal.ensure(b->tot_pixels, s);
     b->term.ensure(b->tot_pixels, s);
-    b->long_list.ensure(b->tot_pixels, s);
+    b->long_list.ensure(dtv::sort_scratch_elems(b->tot_pixels), s);
     b->sort_flags.ensure(2, s);
     b->ok.ensure(1, s);
     b->total.ensure(1, s);
@@ -458,7 +458,6 @@ void enqueue_forward(dtv_batch* b, const dtv::ShadeDev& sh, bool guarded, cudaSt
         b->records.ptr, okp);
     DTV_CK(cudaMemsetAsync(b->sort_flags.ptr, 0, 2 * sizeof(uint32_t), s));
     launch_sort(b->offsets.ptr, b->records.ptr, uint32_t(b->tot_pixels), b->long_list.ptr, b->sort_flags.ptr, s, okp);
-    launch_sort_long(b->offsets.ptr, b->records.ptr, b->long_list.ptr, 0, b->sort_flags.ptr, s, okp);
     kb_composite<<<unsigned(b->tot_tiles), kTile * kTile, 0, s>>>(b->d_views.ptr, b->nviews, b->offsets.ptr,
                                                                   b->records.ptr, b->vgeo.ptr, sh, b->tfinal.ptr,
                                                                   b->term.ptr, okp);
@@ -495,7 +494,7 @@ int32_t dtv_batch_reserve(dtv_batch* b, uint64_t max_views, uint64_t max_vertice
         b->scan.ensure(dtv::scan_scratch_elems(P), s);
         b->tfinal.ensure(P, s);
         b->term.ensure(P, s);
-        b->long_list.ensure(P, s);
+        b->long_list.ensure(dtv::sort_scratch_elems(P), s);
         b->records.ensure(max_fragments ? max_fragments : 1, s);
         b->grad_rows.ensure(2 * (max_grad_vertices ? max_grad_vertices : 1), s);
         b->sort_flags.ensure(2, s);
@@ -634,7 +633,6 @@ int32_t dtv_batch_render(dtv_batch* b, int32_t num_views, const dtv_batch_view* 
         DTV_CK(cudaMemsetAsync(b->sort_flags.ptr, 0, 2 * sizeof(uint32_t), s));
         launch_sort(b->offsets.ptr, b->records.ptr, uint32_t(b->tot_pixels), b->long_list.ptr, b->sort_flags.ptr, s,
                     nullptr);
-        launch_sort_long(b->offsets.ptr, b->records.ptr, b->long_list.ptr, 0, b->sort_flags.ptr, s, nullptr);
         kb_composite<<<unsigned(b->tot_tiles), kTile * kTile, 0, s>>>(b->d_views.ptr, b->nviews, b->offsets.ptr,
                                                                       b->records.ptr, b->vgeo.ptr, b->sh,
                                                                       b->tfinal.ptr, b->term.ptr, nullptr);

@@ -37,14 +37,13 @@ void launch_raster_fill(const uint4* faces, uint32_t F, const float4* vproj, con
 size_t scan_scratch_elems(uint64_t n);
 void launch_scan(const uint32_t* counts, uint64_t n, unsigned long long* offsets, unsigned long long* scratch,
                  cudaStream_t s);
-// Per-pixel sort.  long_list holds up to P entries; flags[0] = number of long lists,
-// flags[1] = error (list longer than the block sort capacity).
-// With a non-null `ok`, the sorts do nothing when *ok == 0 (batched steps
-// whose records overflowed the buffer).
-void launch_sort(const unsigned long long* offsets, unsigned long long* records, uint32_t P, uint32_t* long_list,
+// Per-pixel sort of the lists of P pixels.  scratch holds sort_scratch_elems(P)
+// u32 (length-class counts and lists); flags[1] is set when a list is longer
+// than the block sort capacity.  With a non-null `ok`, the sort does nothing
+// when *ok == 0 (batched steps whose records overflowed the buffer).
+size_t sort_scratch_elems(uint64_t P);
+void launch_sort(const unsigned long long* offsets, unsigned long long* records, uint32_t P, uint32_t* scratch,
                  uint32_t* flags, cudaStream_t s, const uint32_t* ok = nullptr);
-void launch_sort_long(const unsigned long long* offsets, unsigned long long* records, const uint32_t* long_list,
-                      uint32_t num_long, uint32_t* flags, cudaStream_t s, const uint32_t* ok = nullptr);
 constexpr uint32_t kSortWarpCap = 1024;    // elements per warp list sorted in shared memory
 constexpr uint32_t kSortBlockCap = 16384;  // elements per block-sorted list (128 KiB shared memory)
 

@@ -5,6 +5,7 @@
 // count / prefix-scan / fill layout of 8-byte records in HBM:
 //   record = (fp32 view-depth bits << 32) | (face << 2) | (boundary << 1) | front
 // sorted per pixel by the 64-bit value (depth, then face index).
+#include <algorithm>
 #include "dtv_internal.h"
 #include "dtv_path.cuh"
 
@@ -248,88 +249,149 @@ __device__ __forceinline__ void bitonic_smem(u64* s, uint32_t N, uint32_t tid, u
 
 constexpr int kSortWarps = 8;
 
-__global__ void __launch_bounds__(kSortWarps * 32) k_sort_warp(const u64* __restrict__ offsets, u64* records,
-                                                                uint32_t P, uint32_t* __restrict__ long_list,
-                                                                uint32_t* __restrict__ flags,
-                                                                const uint32_t* __restrict__ ok) {
-    if (ok && *ok == 0u) return;
-    extern __shared__ u64 sm_sort[];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t p = blockIdx.x * kSortWarps + warp;
-    if (p >= P) return;
-    const u64 beg = offsets[p];
-    const uint32_t n = uint32_t(offsets[p + 1] - beg);
-    if (n <= 1) return;
-    u64* r = records + beg;
-    if (n <= 32) {
-        u64 v = lane < int(n) ? r[lane] : ~0ull;
-        v = bitonic32(v, lane);
-        if (lane < int(n)) r[lane] = v;
-        return;
-    }
-    if (n <= 64) { warp_sort_list<2>(r, n, lane); return; }
-    if (n <= 128) { warp_sort_list<4>(r, n, lane); return; }
-    if (n <= 256) { warp_sort_list<8>(r, n, lane); return; }
-    if (n <= 512) { warp_sort_list<16>(r, n, lane); return; }
-    if (n > kSortWarpCap) {
-        if (lane == 0) {
-            uint32_t idx = atomicAdd(&flags[0], 1u);
-            long_list[idx] = p;
-        }
-        return;
-    }
-    u64* s = sm_sort + size_t(warp) * kSortWarpCap;
-    uint32_t N = 64;
-    while (N < n) N <<= 1;
-    for (uint32_t i = lane; i < N; i += 32) s[i] = i < n ? r[i] : ~0ull;
-    __syncwarp();
-    bitonic_smem<false>(s, N, lane, 32);
-    for (uint32_t i = lane; i < n; i += 32) r[i] = s[i];
+// Length classes of the per-pixel lists.  A classification pass appends each
+// pixel with n >= 2 records to the list of its class (warp-aggregated
+// atomics); one kernel per class then sorts its lists, so each is compiled
+// with only the registers its class needs.  Classes 0..4: one warp per list,
+// 32 K records in registers (K = 1, 2, 4, 8, 16); class 5: one warp per list,
+// bitonic in shared memory (<= kSortWarpCap); class 6: one block per list
+// (<= kSortBlockCap).  Longer lists set flags[1].
+// Scratch layout (u32): [0, 16) class counts, then kSortClasses lists of P.
+constexpr int kSortClasses = 7;
+constexpr int kSortGridBlocks = 148 * 8;
+
+__device__ __forceinline__ int sort_class(uint32_t n) {
+    if (n <= 32) return 0;
+    if (n <= 64) return 1;
+    if (n <= 128) return 2;
+    if (n <= 256) return 3;
+    if (n <= 512) return 4;
+    if (n <= kSortWarpCap) return 5;
+    return 6;
 }
 
-__global__ void __launch_bounds__(1024) k_sort_long(const u64* __restrict__ offsets, u64* records,
-                                                    const uint32_t* __restrict__ long_list,
-                                                    uint32_t* __restrict__ flags, const uint32_t* __restrict__ ok) {
+__global__ void __launch_bounds__(256) k_sort_classify(const u64* __restrict__ offsets, uint32_t P,
+                                                       uint32_t* __restrict__ scratch, uint32_t* __restrict__ flags,
+                                                       const uint32_t* __restrict__ ok) {
     if (ok && *ok == 0u) return;
-    extern __shared__ u64 sm_sort[];
-    const uint32_t num_long = flags[0];
-    for (uint32_t li = blockIdx.x; li < num_long; li += gridDim.x) {
-        const uint32_t p = long_list[li];
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    int c = -1;
+    if (p < P) {
+        const uint32_t n = uint32_t(offsets[p + 1] - offsets[p]);
+        if (n > kSortBlockCap)
+            atomicExch(&flags[1], 1u);
+        else if (n > 1)
+            c = sort_class(n);
+    }
+    const unsigned act = __ballot_sync(kFull, c >= 0);
+    if (c < 0) return;
+    const unsigned peers = __match_any_sync(act, c);
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(peers) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(&scratch[c], uint32_t(__popc(peers)));
+    base = __shfl_sync(peers, base, leader);
+    const uint32_t rank = uint32_t(__popc(peers & ((1u << lane) - 1u)));
+    scratch[16 + size_t(c) * P + base + rank] = p;
+}
+
+// Classes 0..4: K records per lane in registers (K = 1: bitonic over shuffles).
+template <int K>
+__global__ void __launch_bounds__(kSortWarps * 32) k_sort_class_regs(const u64* __restrict__ offsets, u64* records,
+                                                                     const uint32_t* __restrict__ items,
+                                                                     const uint32_t* __restrict__ count,
+                                                                     const uint32_t* __restrict__ ok) {
+    if (ok && *ok == 0u) return;
+    const uint32_t num = *count;
+    const int lane = threadIdx.x & 31;
+    for (uint32_t i = blockIdx.x * kSortWarps + (threadIdx.x >> 5); i < num; i += gridDim.x * kSortWarps) {
+        const uint32_t p = items[i];
         const u64 beg = offsets[p];
         const uint32_t n = uint32_t(offsets[p + 1] - beg);
-        if (n > kSortBlockCap) {
-            if (threadIdx.x == 0) atomicExch(&flags[1], 1u);
-            continue;
+        u64* r = records + beg;
+        if (K == 1) {
+            u64 v = lane < int(n) ? r[lane] : ~0ull;
+            v = bitonic32(v, lane);
+            if (lane < int(n)) r[lane] = v;
+        } else {
+            warp_sort_list<K>(r, n, lane);
         }
+    }
+}
+
+// Class 5: one warp per list, bitonic in shared memory.
+__global__ void __launch_bounds__(kSortWarps * 32) k_sort_class_smem(const u64* __restrict__ offsets, u64* records,
+                                                                     const uint32_t* __restrict__ items,
+                                                                     const uint32_t* __restrict__ count,
+                                                                     const uint32_t* __restrict__ ok) {
+    if (ok && *ok == 0u) return;
+    extern __shared__ u64 sm_sort[];
+    const uint32_t num = *count;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    u64* s = sm_sort + size_t(warp) * kSortWarpCap;
+    for (uint32_t i = blockIdx.x * kSortWarps + warp; i < num; i += gridDim.x * kSortWarps) {
+        const uint32_t p = items[i];
+        const u64 beg = offsets[p];
+        const uint32_t n = uint32_t(offsets[p + 1] - beg);
         u64* r = records + beg;
         uint32_t N = 64;
         while (N < n) N <<= 1;
-        for (uint32_t i = threadIdx.x; i < N; i += blockDim.x) sm_sort[i] = i < n ? r[i] : ~0ull;
+        for (uint32_t j = lane; j < N; j += 32) s[j] = j < n ? r[j] : ~0ull;
+        __syncwarp();
+        bitonic_smem<false>(s, N, lane, 32);
+        for (uint32_t j = lane; j < n; j += 32) r[j] = s[j];
+        __syncwarp();
+    }
+}
+
+// Class 6: one block per list.
+__global__ void __launch_bounds__(1024) k_sort_class_block(const u64* __restrict__ offsets, u64* records,
+                                                           const uint32_t* __restrict__ items,
+                                                           const uint32_t* __restrict__ count,
+                                                           const uint32_t* __restrict__ ok) {
+    if (ok && *ok == 0u) return;
+    extern __shared__ u64 sm_sort[];
+    const uint32_t num = *count;
+    for (uint32_t i = blockIdx.x; i < num; i += gridDim.x) {
+        const uint32_t p = items[i];
+        const u64 beg = offsets[p];
+        const uint32_t n = uint32_t(offsets[p + 1] - beg);
+        u64* r = records + beg;
+        uint32_t N = 64;
+        while (N < n) N <<= 1;
+        for (uint32_t j = threadIdx.x; j < N; j += blockDim.x) sm_sort[j] = j < n ? r[j] : ~0ull;
         __syncthreads();
         bitonic_smem<true>(sm_sort, N, threadIdx.x, blockDim.x);
-        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) r[i] = sm_sort[i];
+        for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) r[j] = sm_sort[j];
         __syncthreads();
     }
 }
 
-void launch_sort(const u64* offsets, u64* records, uint32_t P, uint32_t* long_list, uint32_t* flags,
-                 cudaStream_t s, const uint32_t* ok) {
+size_t sort_scratch_elems(uint64_t P) { return 16 + size_t(kSortClasses) * size_t(P); }
+
+void launch_sort(const u64* offsets, u64* records, uint32_t P, uint32_t* scratch, uint32_t* flags, cudaStream_t s,
+                 const uint32_t* ok) {
     static bool attr_set = false;
-    const size_t smem = size_t(kSortWarps) * kSortWarpCap * sizeof(u64);
+    const size_t smem_warp = size_t(kSortWarps) * kSortWarpCap * sizeof(u64);
+    const size_t smem_block = size_t(kSortBlockCap) * sizeof(u64);
     if (!attr_set) {
-        cudaFuncSetAttribute(k_sort_warp, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-        cudaFuncSetAttribute(k_sort_long, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             int(kSortBlockCap * sizeof(u64)));
+        cudaFuncSetAttribute(k_sort_class_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_warp));
+        cudaFuncSetAttribute(k_sort_class_block, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_block));
         attr_set = true;
     }
     if (P == 0) return;
-    k_sort_warp<<<(P + kSortWarps - 1) / kSortWarps, kSortWarps * 32, smem, s>>>(offsets, records, P, long_list,
-                                                                                 flags, ok);
-}
-
-void launch_sort_long(const u64* offsets, u64* records, const uint32_t* long_list, uint32_t /*num_long*/,
-                      uint32_t* flags, cudaStream_t s, const uint32_t* ok) {
-    k_sort_long<<<296, 1024, kSortBlockCap * sizeof(u64), s>>>(offsets, records, long_list, flags, ok);
+    cudaMemsetAsync(scratch, 0, 16 * sizeof(uint32_t), s);
+    k_sort_classify<<<(P + 255) / 256, 256, 0, s>>>(offsets, P, scratch, flags, ok);
+    auto items = [&](int c) { return scratch + 16 + size_t(c) * P; };
+    const unsigned g = unsigned(std::min<uint64_t>(kSortGridBlocks, (uint64_t(P) + kSortWarps - 1) / kSortWarps));
+    k_sort_class_regs<1><<<g, kSortWarps * 32, 0, s>>>(offsets, records, items(0), scratch + 0, ok);
+    k_sort_class_regs<2><<<g, kSortWarps * 32, 0, s>>>(offsets, records, items(1), scratch + 1, ok);
+    k_sort_class_regs<4><<<g, kSortWarps * 32, 0, s>>>(offsets, records, items(2), scratch + 2, ok);
+    k_sort_class_regs<8><<<g, kSortWarps * 32, 0, s>>>(offsets, records, items(3), scratch + 3, ok);
+    k_sort_class_regs<16><<<g, kSortWarps * 32, 0, s>>>(offsets, records, items(4), scratch + 4, ok);
+    k_sort_class_smem<<<std::min(g, 296u), kSortWarps * 32, smem_warp, s>>>(offsets, records, items(5), scratch + 5,
+                                                                            ok);
+    k_sort_class_block<<<296, 1024, smem_block, s>>>(offsets, records, items(6), scratch + 6, ok);
 }
 
 // ---------------------------------------------------------------------------

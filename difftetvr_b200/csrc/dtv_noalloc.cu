@@ -14,7 +14,7 @@
 //   vertices  <= 65,536
 //   pixels    <= 65,536 (e.g. 256 x 256)
 //   fragments <= 4,194,304 (checked after the exact count of the scan)
-// The array is about 37 MiB and every GPU that loads this library holds it
+// The array is about 39 MiB and every GPU that loads this library holds it
 // until the process exits.
 //
 // Set-up: the first call on a device, with that device current, looks up the
@@ -51,7 +51,8 @@ constexpr size_t kOffScan = align256(kOffOffsets + sizeof(unsigned long long) * 
 constexpr size_t kOffTfinal = align256(kOffScan + sizeof(unsigned long long) * kNaScanElems);
 constexpr size_t kOffTerm = align256(kOffTfinal + sizeof(float) * kNaMaxPixels);
 constexpr size_t kOffLong = align256(kOffTerm + sizeof(uint32_t) * kNaMaxPixels);
-constexpr size_t kOffFlags = align256(kOffLong + sizeof(uint32_t) * kNaMaxPixels);
+constexpr size_t kNaSortElems = 16 + 7 * kNaMaxPixels;  // >= sort_scratch_elems(kNaMaxPixels)
+constexpr size_t kOffFlags = align256(kOffLong + sizeof(uint32_t) * kNaSortElems);
 constexpr size_t kOffRecords = align256(kOffFlags + 2 * sizeof(uint32_t));
 constexpr size_t kNaScratchBytes = align256(kOffRecords + sizeof(unsigned long long) * kNaMaxFragments);
 
@@ -151,7 +152,6 @@ extern "C" int32_t dtv_render_noalloc(const dtv_mesh* mesh, const float* d_posit
         dtv::launch_raster_fill(mv.faces, uint32_t(mv.num_faces), vproj, vfix, W, H, counts, offsets, records, s);
         NA_CK(cudaMemsetAsync(flags, 0, 2 * sizeof(uint32_t), s));
         dtv::launch_sort(offsets, records, uint32_t(P), long_list, flags, s);
-        dtv::launch_sort_long(offsets, records, long_list, 0, flags, s);
         dtv::launch_composite(offsets, records, mv.faces, vgeo, reinterpret_cast<const float4*>(d_colors), W, H, sh,
                               reinterpret_cast<float4*>(d_image), tfinal, term, s);
         NA_CK(cudaGetLastError());

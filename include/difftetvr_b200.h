@@ -234,7 +234,7 @@ int32_t dtv_tet_regularizer_grad(const dtv_mesh* mesh, const float* d_positions,
  * framework that owns the device heap, or a serving loop that must not call
  * cudaMalloc/cudaFree, which synchronise the device).  Same kernels and output
  * as dtv_renderer_render, with all scratch in one fixed file-scope device
- * array (about 37 MiB, held by every GPU that loads the library until exit).
+ * array (about 39 MiB, held by every GPU that loads the library until exit).
  * Limits: <= 65,536 vertices, <= 65,536 pixels, <= 4,194,304 fragments; larger
  * requests return DTV_ERR_ARG / DTV_ERR_BUDGET.  The first call on a device
  * looks up the array's address (make it before any stream capture).  Calls
