@@ -11,44 +11,35 @@ constexpr int kTile = 16;  // composite / adjoint pixel tile (16 x 16 threads)
 
 // ---------------------------------------------------------------------------
 // (a)+(b) face rasterisation.  One thread per face walks the pixel centres of
-// the face's bounding box with incrementally updated int64 edge functions in
+// the face's bounding box with incrementally updated integer edge functions in
 // 1/256-pixel fixed point.  COUNT mode increments the per-pixel counter; FILL
 // mode writes the record at offsets[p] + (--counts[p]), leaving counts zeroed
 // for the next render.  Only pixel rows [row0, row1) are visited (row bands of
 // a render whose lists do not fit the fragment budget at once).
-template <bool FILL>
-__device__ __forceinline__ void raster_face(uint32_t f, const uint4* __restrict__ faces,
-                                            const float4* __restrict__ vproj, const int2* __restrict__ vfix,
-                                            int W, int row0, int row1, uint32_t* __restrict__ counts,
-                                            const u64* __restrict__ offsets, u64* __restrict__ records) {
-    const uint4 fc = faces[f];
-    const int2 q0 = vfix[fc.x], q1 = vfix[fc.y], q2 = vfix[fc.z];
-    if (q0.x == kInvalidFix || q1.x == kInvalidFix || q2.x == kInvalidFix) return;
-    const long long X0 = q0.x, Y0 = q0.y, X1 = q1.x, Y1 = q1.y, X2 = q2.x, Y2 = q2.y;
-    const long long area2 = (X1 - X0) * (Y2 - Y0) - (Y1 - Y0) * (X2 - X0);
-    if (area2 == 0) return;
-    const uint32_t front = area2 < 0 ? 1u : 0u;
-    const uint32_t bits = (f << 2) | ((fc.w & 1u) << 1) | front;
-    long long ax0 = X0, ay0 = Y0, ax1 = X1, ay1 = Y1, ax2 = X2, ay2 = Y2;
-    if (area2 < 0) {
-        ax1 = X2; ay1 = Y2;
-        ax2 = X1; ay2 = Y1;
-    }
-    const long long minX = min(X0, min(X1, X2)), maxX = max(X0, max(X1, X2));
-    const long long minY = min(Y0, min(Y1, Y2)), maxY = max(Y0, max(Y1, Y2));
-    const int px0 = int(max(0LL, ceil_div256(minX - 128)));
-    const int px1 = int(min((long long)W - 1, floor_div256(maxX - 128)));
-    const int py0 = int(max((long long)row0, ceil_div256(minY - 128)));
-    const int py1 = int(min((long long)row1 - 1, floor_div256(maxY - 128)));
-    if (px0 > px1 || py0 > py1) return;
-    // Edges e0: a1->a2, e1: a2->a0, e2: a0->a1.
-    const long long dx0 = ax2 - ax1, dy0 = ay2 - ay1;
-    const long long dx1 = ax0 - ax2, dy1 = ay0 - ay2;
-    const long long dx2 = ax1 - ax0, dy2 = ay1 - ay0;
-    const long long Xs = 256LL * px0 + 128, Ys = 256LL * py0 + 128;
-    long long E0r = dx0 * (Ys - ay1) - dy0 * (Xs - ax1);
-    long long E1r = dx1 * (Ys - ay2) - dy1 * (Xs - ax2);
-    long long E2r = dx2 * (Ys - ay0) - dy2 * (Xs - ax0);
+//
+// Edge functions are translation invariant, so they are evaluated relative to
+// the bounding-box corner: for boxes under 64 px (2^14 fixed-point units) on
+// each side every product is below 2^29 and the exact values fit in 32-bit
+// integers (half the ALU work of the 64-bit form); larger faces use 64 bits.
+// Both give identical coverage.
+template <typename I>
+__device__ __forceinline__ bool edge_in(I E, I dx, I dy) {
+    return (E > 0) || (E == 0 && ((dy < 0) || (dy == 0 && dx > 0)));
+}
+
+template <bool FILL, typename I>
+__device__ __forceinline__ void raster_box(const uint4& fc, uint32_t bits, I ax0, I ay0, I ax1, I ay1, I ax2, I ay2,
+                                           I Xs, I Ys, int px0, int px1, int py0, int py1,
+                                           const float4* __restrict__ vproj, int W, uint32_t* __restrict__ counts,
+                                           const u64* __restrict__ offsets, u64* __restrict__ records) {
+    // Edges e0: a1->a2, e1: a2->a0, e2: a0->a1; (Xs, Ys) is the centre of
+    // pixel (px0, py0) in the same (possibly box-relative) coordinates.
+    const I dx0 = ax2 - ax1, dy0 = ay2 - ay1;
+    const I dx1 = ax0 - ax2, dy1 = ay0 - ay2;
+    const I dx2 = ax1 - ax0, dy2 = ay1 - ay0;
+    I E0r = dx0 * (Ys - ay1) - dy0 * (Xs - ax1);
+    I E1r = dx1 * (Ys - ay2) - dy1 * (Xs - ax2);
+    I E2r = dx2 * (Ys - ay0) - dy2 * (Xs - ax0);
     float4 va, vb, vc;
     if (FILL) {
         va = vproj[fc.x];
@@ -58,16 +49,16 @@ __device__ __forceinline__ void raster_face(uint32_t f, const uint4* __restrict_
     // Four pixels of a row per step: their coverage tests, depth keys, counter
     // atomics and offset loads are independent and issue back to back before
     // the record stores (the fill is bound by atomic round trips otherwise).
-    const long long sx0 = -dy0 * 256, sx1 = -dy1 * 256, sx2 = -dy2 * 256;
+    const I sx0 = -dy0 * I(256), sx1 = -dy1 * I(256), sx2 = -dy2 * I(256);
     for (int py = py0; py <= py1; ++py) {
-        long long E0 = E0r, E1 = E1r, E2 = E2r;
+        I E0 = E0r, E1 = E1r, E2 = E2r;
         const size_t row = size_t(py) * W;
         for (int px = px0; px <= px1; px += 4) {
             bool in[4];
 #pragma unroll
             for (int k = 0; k < 4; ++k)
-                in[k] = (px + k <= px1) && edge_inside(E0 + k * sx0, dx0, dy0) &&
-                        edge_inside(E1 + k * sx1, dx1, dy1) && edge_inside(E2 + k * sx2, dx2, dy2);
+                in[k] = (px + k <= px1) && edge_in<I>(E0 + I(k) * sx0, dx0, dy0) &&
+                        edge_in<I>(E1 + I(k) * sx1, dx1, dy1) && edge_in<I>(E2 + I(k) * sx2, dx2, dy2);
             if (FILL) {
                 uint32_t slot[4];
                 u64 off[4];
@@ -89,16 +80,51 @@ __device__ __forceinline__ void raster_face(uint32_t f, const uint4* __restrict_
                 for (int k = 0; k < 4; ++k)
                     if (in[k]) atomicAdd(&counts[row + px + k], 1u);
             }
-            E0 += 4 * sx0;
-            E1 += 4 * sx1;
-            E2 += 4 * sx2;
+            E0 += I(4) * sx0;
+            E1 += I(4) * sx1;
+            E2 += I(4) * sx2;
         }
-        E0r += dx0 * 256;
-        E1r += dx1 * 256;
-        E2r += dx2 * 256;
+        E0r += dx0 * I(256);
+        E1r += dx1 * I(256);
+        E2r += dx2 * I(256);
     }
 }
 
+template <bool FILL>
+__device__ __forceinline__ void raster_face(uint32_t f, const uint4* __restrict__ faces,
+                                            const float4* __restrict__ vproj, const int2* __restrict__ vfix,
+                                            int W, int row0, int row1, uint32_t* __restrict__ counts,
+                                            const u64* __restrict__ offsets, u64* __restrict__ records) {
+    const uint4 fc = faces[f];
+    const int2 q0 = vfix[fc.x], q1 = vfix[fc.y], q2 = vfix[fc.z];
+    if (q0.x == kInvalidFix || q1.x == kInvalidFix || q2.x == kInvalidFix) return;
+    const long long X0 = q0.x, Y0 = q0.y, X1 = q1.x, Y1 = q1.y, X2 = q2.x, Y2 = q2.y;
+    const long long area2 = (X1 - X0) * (Y2 - Y0) - (Y1 - Y0) * (X2 - X0);
+    if (area2 == 0) return;
+    const uint32_t front = area2 < 0 ? 1u : 0u;
+    const uint32_t bits = (f << 2) | ((fc.w & 1u) << 1) | front;
+    long long ax1 = X1, ay1 = Y1, ax2 = X2, ay2 = Y2;
+    if (area2 < 0) {
+        ax1 = X2; ay1 = Y2;
+        ax2 = X1; ay2 = Y1;
+    }
+    const long long minX = min(X0, min(X1, X2)), maxX = max(X0, max(X1, X2));
+    const long long minY = min(Y0, min(Y1, Y2)), maxY = max(Y0, max(Y1, Y2));
+    const int px0 = int(max(0LL, ceil_div256(minX - 128)));
+    const int px1 = int(min((long long)W - 1, floor_div256(maxX - 128)));
+    const int py0 = int(max((long long)row0, ceil_div256(minY - 128)));
+    const int py1 = int(min((long long)row1 - 1, floor_div256(maxY - 128)));
+    if (px0 > px1 || py0 > py1) return;
+    const long long Xs = 256LL * px0 + 128, Ys = 256LL * py0 + 128;
+    if (maxX - minX < (1LL << 14) && maxY - minY < (1LL << 14)) {
+        raster_box<FILL, int>(fc, bits, int(X0 - minX), int(Y0 - minY), int(ax1 - minX), int(ay1 - minY),
+                              int(ax2 - minX), int(ay2 - minY), int(Xs - minX), int(Ys - minY), px0, px1, py0, py1,
+                              vproj, W, counts, offsets, records);
+    } else {
+        raster_box<FILL, long long>(fc, bits, X0, Y0, ax1, ay1, ax2, ay2, Xs, Ys, px0, px1, py0, py1, vproj, W,
+                                    counts, offsets, records);
+    }
+}
 
 // ---------------------------------------------------------------------------
 // Fragment evaluation shared by composite and adjoint.
