@@ -228,6 +228,130 @@ __device__ __forceinline__ void warp_sort_list(u64* r, uint32_t n, int lane) {
     }
 }
 
+// Bitonic sort of 32 K keys of 32 bits in registers (layout as warp_sort_regs):
+// each compare-exchange is one min and one max, each exchange one shuffle.
+template <int K>
+__device__ __forceinline__ void warp_sort_regs32(uint32_t (&v)[K], int lane) {
+#pragma unroll
+    for (int k = 2; k <= 32 * K; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            if (j < K) {
+#pragma unroll
+                for (int r = 0; r < K; ++r) {
+                    const int l = r ^ j;
+                    if (l > r) {
+                        const bool up = ((lane * K + r) & k) == 0;
+                        const uint32_t a = v[r], b = v[l];
+                        const uint32_t mn = min(a, b), mx = max(a, b);
+                        v[r] = up ? mn : mx;
+                        v[l] = up ? mx : mn;
+                    }
+                }
+            } else {
+                const int lm = j / K;
+                const bool lower = (lane & lm) == 0;
+#pragma unroll
+                for (int r = 0; r < K; ++r) {
+                    const bool up = ((lane * K + r) & k) == 0;
+                    const uint32_t o = __shfl_xor_sync(kFull, v[r], lm);
+                    v[r] = (lower == up) ? min(v[r], o) : max(v[r], o);
+                }
+            }
+        }
+    }
+}
+
+// Sort of one list of n <= 32 K records (n <= 4096) through 32-bit surrogate
+// keys: (depth quantised to 20 bits over the list's depth range) << 12 | list
+// index.  Quantisation is monotone, so after sorting the keys and gathering
+// the records by index, only runs of equal quantised depth can be out of
+// order; odd-even transposition passes on the full 64-bit records restore
+// the exact (depth, face) order.  A list that is not in order after
+// kFixPasses passes (e.g. all depths equal) goes to the block sort.
+constexpr int kFixPasses = 16;
+
+template <int K>
+__device__ __forceinline__ bool fixup_pass(u64 (&v)[K], int lane, int parity) {
+    bool swapped = false;
+#pragma unroll
+    for (int q = parity; q + 1 < K; q += 2) {
+        if (v[q] > v[q + 1]) {
+            const u64 t = v[q];
+            v[q] = v[q + 1];
+            v[q + 1] = t;
+            swapped = true;
+        }
+    }
+    if (parity == 1) {
+        // Pair across the lane boundary: (lane, K-1) and (lane + 1, 0).
+        const u64 next0 = __shfl_down_sync(kFull, v[0], 1);
+        const u64 prevL = __shfl_up_sync(kFull, v[K - 1], 1);
+        const bool has_next = lane < 31, has_prev = lane > 0;
+        if (has_next && v[K - 1] > next0) {
+            v[K - 1] = next0;
+            swapped = true;
+        }
+        if (has_prev && prevL > v[0]) v[0] = prevL;
+    }
+    return swapped;
+}
+
+// Returns false when the list is not yet in order (the caller queues it for
+// the block sort, which runs later on the same stream).
+template <int K>
+__device__ __forceinline__ bool warp_sort_list_q(u64* r, uint32_t n, int lane) {
+    constexpr uint32_t kLevels = 1u << 20;
+    float dmin = 3.4e38f, dmax = 0.f;
+    uint32_t key[K];
+#pragma unroll
+    for (int q = 0; q < K; ++q) {
+        const uint32_t i = uint32_t(lane) * K + q;
+        if (i < n) {
+            const float d = __uint_as_float(uint32_t(r[i] >> 32));
+            dmin = fminf(dmin, d);
+            dmax = fmaxf(dmax, d);
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        dmin = fminf(dmin, __shfl_xor_sync(kFull, dmin, o));
+        dmax = fmaxf(dmax, __shfl_xor_sync(kFull, dmax, o));
+    }
+    const float scale = dmax > dmin ? float(kLevels - 1) / (dmax - dmin) : 0.f;
+#pragma unroll
+    for (int q = 0; q < K; ++q) {
+        const uint32_t i = uint32_t(lane) * K + q;
+        if (i < n) {
+            const float d = __uint_as_float(uint32_t(r[i] >> 32));
+            const uint32_t qd = min(uint32_t((d - dmin) * scale), kLevels - 1u);
+            key[q] = (qd << 12) | i;
+        } else {
+            key[q] = 0xffffffffu;
+        }
+    }
+    warp_sort_regs32<K>(key, lane);
+    u64 v[K];
+#pragma unroll
+    for (int q = 0; q < K; ++q) v[q] = key[q] != 0xffffffffu ? r[key[q] & 0xfffu] : ~0ull;
+    bool sorted = false;
+    for (int pass = 0; pass < kFixPasses; ++pass) {
+        const bool s0 = fixup_pass<K>(v, lane, 0);
+        const bool s1 = fixup_pass<K>(v, lane, 1);
+        if (!__any_sync(kFull, s0 || s1)) {
+            sorted = true;
+            break;
+        }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < K; ++q) {
+        const uint32_t i = uint32_t(lane) * K + q;
+        if (i < n) r[i] = v[q];
+    }
+    return sorted;
+}
+
 template <bool BLOCK>
 __device__ __forceinline__ void bitonic_smem(u64* s, uint32_t N, uint32_t tid, uint32_t nthr) {
     for (uint32_t k = 2; k <= N; k <<= 1) {
@@ -300,6 +424,8 @@ template <int K>
 __global__ void __launch_bounds__(kSortWarps * 32) k_sort_class_regs(const u64* __restrict__ offsets, u64* records,
                                                                      const uint32_t* __restrict__ items,
                                                                      const uint32_t* __restrict__ count,
+                                                                     uint32_t* __restrict__ redo_count,
+                                                                     uint32_t* __restrict__ redo_items,
                                                                      const uint32_t* __restrict__ ok) {
     if (ok && *ok == 0u) return;
     const uint32_t num = *count;
@@ -313,8 +439,8 @@ __global__ void __launch_bounds__(kSortWarps * 32) k_sort_class_regs(const u64* 
             u64 v = lane < int(n) ? r[lane] : ~0ull;
             v = bitonic32(v, lane);
             if (lane < int(n)) r[lane] = v;
-        } else {
-            warp_sort_list<K>(r, n, lane);
+        } else if (!warp_sort_list_q<K>(r, n, lane) && lane == 0) {
+            redo_items[atomicAdd(redo_count, 1u)] = p;
         }
     }
 }
@@ -384,11 +510,14 @@ void launch_sort(const u64* offsets, u64* records, uint32_t P, uint32_t* scratch
     k_sort_classify<<<(P + 255) / 256, 256, 0, s>>>(offsets, P, scratch, flags, ok);
     auto items = [&](int c) { return scratch + 16 + size_t(c) * P; };
     const unsigned g = unsigned(std::min<uint64_t>(kSortGridBlocks, (uint64_t(P) + kSortWarps - 1) / kSortWarps));
-    k_sort_class_regs<1><<<g, kSortWarps * 32, 0, s>>>(offsets, records, items(0), scratch + 0, ok);
-    k_sort_class_regs<2><<<g, kSortWarps * 32, 0, s>>>(offsets, records, items(1), scratch + 1, ok);
-    k_sort_class_regs<4><<<g, kSortWarps * 32, 0, s>>>(offsets, records, items(2), scratch + 2, ok);
-    k_sort_class_regs<8><<<g, kSortWarps * 32, 0, s>>>(offsets, records, items(3), scratch + 3, ok);
-    k_sort_class_regs<16><<<g, kSortWarps * 32, 0, s>>>(offsets, records, items(4), scratch + 4, ok);
+    // Lists the register sorts leave unsettled join the block-sort class (6).
+    uint32_t* redo_n = scratch + 6;
+    uint32_t* redo = items(6);
+    k_sort_class_regs<1><<<g, kSortWarps * 32, 0, s>>>(offsets, records, items(0), scratch + 0, redo_n, redo, ok);
+    k_sort_class_regs<2><<<g, kSortWarps * 32, 0, s>>>(offsets, records, items(1), scratch + 1, redo_n, redo, ok);
+    k_sort_class_regs<4><<<g, kSortWarps * 32, 0, s>>>(offsets, records, items(2), scratch + 2, redo_n, redo, ok);
+    k_sort_class_regs<8><<<g, kSortWarps * 32, 0, s>>>(offsets, records, items(3), scratch + 3, redo_n, redo, ok);
+    k_sort_class_regs<16><<<g, kSortWarps * 32, 0, s>>>(offsets, records, items(4), scratch + 4, redo_n, redo, ok);
     k_sort_class_smem<<<std::min(g, 296u), kSortWarps * 32, smem_warp, s>>>(offsets, records, items(5), scratch + 5,
                                                                             ok);
     k_sort_class_block<<<296, 1024, smem_block, s>>>(offsets, records, items(6), scratch + 6, ok);
