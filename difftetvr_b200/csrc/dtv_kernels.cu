@@ -421,7 +421,7 @@ __global__ void __launch_bounds__(256) k_sort_classify(const u64* __restrict__ o
 
 // Classes 0..4: K records per lane in registers (K = 1: bitonic over shuffles).
 template <int K>
-__global__ void __launch_bounds__(kSortWarps * 32) k_sort_class_regs(const u64* __restrict__ offsets, u64* records,
+__global__ void __launch_bounds__(kSortWarps * 32, K >= 16 ? 2 : 1) k_sort_class_regs(const u64* __restrict__ offsets, u64* records,
                                                                      const uint32_t* __restrict__ items,
                                                                      const uint32_t* __restrict__ count,
                                                                      uint32_t* __restrict__ redo_count,
