@@ -27,48 +27,67 @@ namespace dtv {
 constexpr uint32_t kNoTet = 0xffffffffu;
 
 // Exact coverage of the pixel centre by face f (the rule of raster_face);
-// *front_stored: the face's stored winding faces the camera.
+// *front_stored: the face's stored winding faces the camera.  The edge
+// functions are taken relative to the pixel centre: with every vertex within
+// 2^14 fixed-point units (64 px) of it they are exact in 32-bit integers,
+// otherwise in 64 bits; both give the raster's coverage.  No early exits, so
+// a warp's lanes stay together.
+template <typename I>
+__device__ __forceinline__ bool covers_rel(I r0x, I r0y, I r1x, I r1y, I r2x, I r2y, bool swap) {
+    // Vertices relative to the pixel centre; the orientation-normalised order
+    // is (0, 1, 2), or (0, 2, 1) when the stored winding is clockwise.
+    const I a1x = swap ? r2x : r1x, a1y = swap ? r2y : r1y;
+    const I a2x = swap ? r1x : r2x, a2y = swap ? r1y : r2y;
+    const I dx0 = a2x - a1x, dy0 = a2y - a1y;
+    const I dx1 = r0x - a2x, dy1 = r0y - a2y;
+    const I dx2 = a1x - r0x, dy2 = a1y - r0y;
+    // E = dx (Yc - ay) - dy (Xc - ax) with the pixel centre at the origin.
+    const I E0 = dy0 * a1x - dx0 * a1y;
+    const I E1 = dy1 * a2x - dx1 * a2y;
+    const I E2 = dy2 * r0x - dx2 * r0y;
+    return edge_in<I>(E0, dx0, dy0) & edge_in<I>(E1, dx1, dy1) & edge_in<I>(E2, dx2, dy2);
+}
+
 __device__ __forceinline__ bool face_covers_px(const uint4* __restrict__ faces, const int2* __restrict__ vfix,
                                                uint32_t f, int px, int py, bool* front_stored) {
     const uint4 fc = faces[f];
     const int2 q0 = vfix[fc.x], q1 = vfix[fc.y], q2 = vfix[fc.z];
-    if (q0.x == kInvalidFix || q1.x == kInvalidFix || q2.x == kInvalidFix) return false;
+    const bool valid = q0.x != kInvalidFix && q1.x != kInvalidFix && q2.x != kInvalidFix;
     const long long X0 = q0.x, Y0 = q0.y, X1 = q1.x, Y1 = q1.y, X2 = q2.x, Y2 = q2.y;
     const long long area2 = (X1 - X0) * (Y2 - Y0) - (Y1 - Y0) * (X2 - X0);
-    if (area2 == 0) return false;
     *front_stored = area2 < 0;
-    long long ax1 = X1, ay1 = Y1, ax2 = X2, ay2 = Y2;
-    if (area2 < 0) {
-        ax1 = X2; ay1 = Y2;
-        ax2 = X1; ay2 = Y1;
-    }
     const long long Xc = 256LL * px + 128, Yc = 256LL * py + 128;
-    const long long dx0 = ax2 - ax1, dy0 = ay2 - ay1;
-    const long long dx1 = X0 - ax2, dy1 = Y0 - ay2;
-    const long long dx2 = ax1 - X0, dy2 = ay1 - Y0;
-    return edge_inside(dx0 * (Yc - ay1) - dy0 * (Xc - ax1), dx0, dy0) &&
-           edge_inside(dx1 * (Yc - ay2) - dy1 * (Xc - ax2), dx1, dy1) &&
-           edge_inside(dx2 * (Yc - Y0) - dy2 * (Xc - X0), dx2, dy2);
+    const long long r0x = X0 - Xc, r0y = Y0 - Yc, r1x = X1 - Xc, r1y = Y1 - Yc, r2x = X2 - Xc, r2y = Y2 - Yc;
+    const long long m = max(max(max(llabs(r0x), llabs(r0y)), max(llabs(r1x), llabs(r1y))),
+                            max(llabs(r2x), llabs(r2y)));
+    bool in;
+    if (m < (1LL << 14))
+        in = covers_rel<int>(int(r0x), int(r0y), int(r1x), int(r1y), int(r2x), int(r2y), area2 < 0);
+    else
+        in = covers_rel<long long>(r0x, r0y, r1x, r1y, r2x, r2y, area2 < 0);
+    return valid && area2 != 0 && in;
 }
 
 // Face of tet t (not `skip`) covering the pixel that faces the camera
-// (want_front) or away from it with respect to t's outward normal.
+// (want_front) or away from it with respect to t's outward normal; the first
+// such face in the tet's face order.  All four faces are evaluated.
 __device__ __forceinline__ uint32_t tet_face_at(const uint32_t* __restrict__ tet_faces,
                                                 const uint4* __restrict__ faces,
                                                 const uint32_t* __restrict__ f2t, const int2* __restrict__ vfix,
                                                 uint32_t t, uint32_t skip, bool want_front, int px, int py) {
     const uint4 tf = reinterpret_cast<const uint4*>(tet_faces)[t];
     const uint32_t fs[4] = {tf.x, tf.y, tf.z, tf.w};
+    uint32_t found = kNoTet;
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
+    for (int j = 3; j >= 0; --j) {
         const uint32_t f = fs[j];
-        if (f == skip) continue;
         bool front_stored;
-        if (!face_covers_px(faces, vfix, f, px, py, &front_stored)) continue;
+        const bool cov = face_covers_px(faces, vfix, f, px, py, &front_stored);
         const bool owner = f2t[2 * size_t(f)] == t;  // stored winding is outward for the face's first tet
-        if ((front_stored == owner) == want_front) return f;
+        const bool match = f != skip && cov && ((front_stored == owner) == want_front);
+        found = match ? f : found;  // descending j: the smallest matching j wins
     }
-    return kNoTet;
+    return found;
 }
 
 __device__ __forceinline__ uint32_t other_tet(const uint32_t* __restrict__ f2t, uint32_t f, uint32_t t) {
@@ -82,7 +101,7 @@ __device__ __forceinline__ float ray_scale(const CamDev& cam, float qx, float qy
     return sqrtf(1.f + dx * dx + dy * dy);
 }
 
-__global__ void __launch_bounds__(kTile * kTile) k_walk_composite(
+__global__ void __launch_bounds__(kTile * kTile, 2) k_walk_composite(
     const u64* __restrict__ b_offsets, const u64* __restrict__ b_records, const uint32_t* __restrict__ bf_global,
     const uint4* __restrict__ faces, const uint32_t* __restrict__ f2t, const uint32_t* __restrict__ tet_faces,
     uint32_t num_tets, const int2* __restrict__ vfix, const VGeo* __restrict__ vgeo,
@@ -145,7 +164,7 @@ __global__ void __launch_bounds__(kTile * kTile) k_walk_composite(
     wstate[p] = make_uint4(last_tet, last_entry, last_b, nseg);
 }
 
-__global__ void __launch_bounds__(kTile * kTile) k_walk_adjoint(
+__global__ void __launch_bounds__(kTile * kTile, 2) k_walk_adjoint(
     const u64* __restrict__ b_offsets, const u64* __restrict__ b_records, const uint32_t* __restrict__ bf_global,
     const uint4* __restrict__ faces, const uint32_t* __restrict__ f2t, const uint32_t* __restrict__ tet_faces,
     uint32_t num_tets, const int2* __restrict__ vfix, const VGeo* __restrict__ vgeo,
