@@ -47,6 +47,15 @@ class Camera(ctypes.Structure):
     ]
 
 
+class Tuning(ctypes.Structure):
+    _fields_ = [
+        ("composite_tile", ctypes.c_int32),
+        ("adjoint_tile", ctypes.c_int32),
+        ("sort_surrogate_classes", ctypes.c_uint32),
+        ("reserved", ctypes.c_int32),
+    ]
+
+
 class RenderParams(ctypes.Structure):
     _fields_ = [
         ("attenuation", ctypes.c_float),
@@ -120,6 +129,10 @@ SIGNATURES = {
     "dtv_renderer_render_adjoint_cells": (ctypes.c_int32, [c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.c_int32, c_vp,
                                                            c_vp, c_vp]),
     "dtv_renderer_get_num_fragments": (ctypes.c_int32, [c_vp, c_u64p]),
+    "dtv_renderer_set_tuning": (ctypes.c_int32, [c_vp, ctypes.POINTER(Tuning)]),
+    "dtv_renderer_get_tuning": (ctypes.c_int32, [c_vp, ctypes.POINTER(Tuning)]),
+    "dtv_batch_set_tuning": (ctypes.c_int32, [c_vp, ctypes.POINTER(Tuning)]),
+    "dtv_batch_get_tuning": (ctypes.c_int32, [c_vp, ctypes.POINTER(Tuning)]),
     "dtv_renderer_get_num_bands": (ctypes.c_int32, [c_vp, ctypes.POINTER(ctypes.c_int32)]),
     "dtv_mesh_subdivide_vertices": (ctypes.c_int32, [c_vp, ctypes.c_uint64, c_vp, ctypes.c_uint64, c_vp, c_vp, c_vp,
                                                      ctypes.c_uint64, ctypes.c_float, ctypes.POINTER(c_vp)]),

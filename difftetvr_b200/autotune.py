@@ -1,0 +1,114 @@
+"""Autotuner: picks the kernel configuration of a renderer (pixel tile of the
+composite and adjoint blocks, sort method per list-length class) or of a batch
+renderer (sort method per class) by timing the candidates on the caller's own
+workload with CUDA events.  Every configuration gives identical results, so
+the search only changes speed.  Coordinate search: each knob in turn, the
+others held at their best value so far.  Results are cached per workload key
+(resolution, mesh size, renderer type, colour storage)."""
+from __future__ import annotations
+
+import torch
+
+TILES = (0, 1, 2)               # 16x16, 32x8, 8x32 pixels per 256-thread block
+SORT_CLASSES = (1, 2, 3, 4)     # lists of up to 64, 128, 256, 512 records
+
+_cache: dict = {}
+
+
+def _time_ms(fn, trials: int) -> float:
+    fn()  # warm-up (first-use allocations)
+    best = float("inf")
+    for _ in range(trials):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    return best
+
+
+def _key(renderer) -> tuple:
+    mesh = renderer.get_tet_mesh()
+    w, h = renderer.get_viewport_size()
+    return ("renderer", int(renderer.get_renderer_type()), w, h, mesh.get_num_cells(), mesh.get_num_faces(),
+            int(mesh.get_color_storage()))
+
+
+def autotune_renderer(renderer, trials: int = 3, force: bool = False) -> dict:
+    """Times render (+ adjoint when the mesh uses gradients) for each candidate
+    and leaves the fastest configuration set on the renderer.  Returns
+    {"tuning": ..., "ms": ..., "timings": [...]}."""
+    key = _key(renderer)
+    if not force and key in _cache:
+        renderer.set_tuning(**_cache[key]["tuning"])
+        return _cache[key]
+    mesh = renderer.get_tet_mesh()
+    pos = mesh.get_vertex_positions()
+    w, h = renderer.get_viewport_size()
+    adj = torch.full((h, w, 4), 1e-3, device=pos.device)
+    cells = mesh.get_cell_colors() if mesh.get_cell_colors() is not None else mesh.get_vertex_colors()
+    gp = torch.zeros_like(pos.detach())
+    gc = torch.zeros_like(cells.detach())
+    with_adjoint = pos.requires_grad
+
+    def step():
+        renderer.render()
+        if with_adjoint:
+            renderer.render_adjoint_into(adj, gp, gc)
+
+    timings = []
+
+    def measure(**cfg):
+        renderer.set_tuning(**cfg)
+        ms = _time_ms(step, trials)
+        timings.append({**renderer.get_tuning(), "ms": ms})
+        return ms
+
+    best = renderer.get_tuning()
+    best_ms = measure(**best)
+    for knob, values in (("composite_tile", TILES), ("adjoint_tile", TILES if with_adjoint else (best["adjoint_tile"],))):
+        for v in values:
+            if v == best[knob]:
+                continue
+            cand = dict(best, **{knob: v})
+            ms = measure(**cand)
+            if ms < best_ms:
+                best, best_ms = cand, ms
+    for c in SORT_CLASSES:
+        cand = dict(best, sort_surrogate_classes=best["sort_surrogate_classes"] ^ (1 << c))
+        ms = measure(**cand)
+        if ms < best_ms:
+            best, best_ms = cand, ms
+    renderer.set_tuning(**best)
+    out = {"tuning": best, "ms": best_ms, "timings": timings}
+    _cache[key] = out
+    return out
+
+
+def autotune_batch(batch_renderer, views, trials: int = 2, force: bool = False) -> dict:
+    """Times BatchRenderer.render(views) for each sort method per list-length
+    class and leaves the fastest set.  Returns {"tuning": ..., "ms": ...}."""
+    key = ("batch", tuple((v.mesh, v.width, v.height) for v in views))
+    if not force and key in _cache:
+        batch_renderer.set_tuning(**_cache[key]["tuning"])
+        return _cache[key]
+    timings = []
+
+    def measure(mask):
+        batch_renderer.set_tuning(sort_surrogate_classes=mask)
+        ms = _time_ms(lambda: batch_renderer.render(views), trials)
+        timings.append({"sort_surrogate_classes": mask, "ms": ms})
+        return ms
+
+    best = batch_renderer.get_tuning()["sort_surrogate_classes"]
+    best_ms = measure(best)
+    for c in SORT_CLASSES:
+        cand = best ^ (1 << c)
+        ms = measure(cand)
+        if ms < best_ms:
+            best, best_ms = cand, ms
+    batch_renderer.set_tuning(sort_surrogate_classes=best)
+    out = {"tuning": {"sort_surrogate_classes": best}, "ms": best_ms, "timings": timings}
+    _cache[key] = out
+    return out

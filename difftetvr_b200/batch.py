@@ -74,6 +74,17 @@ class BatchRenderer:
         _lib.call("dtv_batch_reserve", self._handle, int(max_views), int(max_vertices), int(max_pixels),
                   int(max_fragments), int(max_grad_vertices), torch.cuda.current_stream().cuda_stream)
 
+    def get_tuning(self) -> dict:
+        t = _lib.Tuning()
+        _lib.call("dtv_batch_get_tuning", self._handle, ctypes.byref(t))
+        return {"sort_surrogate_classes": t.sort_surrogate_classes}
+
+    def set_tuning(self, sort_surrogate_classes: int) -> None:
+        """Sort method per list-length class (bit c, c = 1..4): 32-bit
+        surrogate keys or the 64-bit network; identical results."""
+        t = _lib.Tuning(0, 0, int(sort_surrogate_classes), 0)
+        _lib.call("dtv_batch_set_tuning", self._handle, ctypes.byref(t))
+
     def set_graph(self, enable: bool = True) -> None:
         _lib.call("dtv_batch_set_graph", self._handle, int(bool(enable)))
 

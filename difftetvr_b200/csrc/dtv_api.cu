@@ -86,6 +86,7 @@ struct dtv_renderer {
     // when the lists are stored whole.
     std::vector<std::pair<int, int>> bands;
     bool cells = false;           // last render used per-cell colours
+    dtv_tuning tuning{0, 0, dtv::kSortSurrogateDefault, 0};
     u64* h_rowoff = nullptr;      // pinned row-start offsets (H+1)
     size_t h_rowoff_cap = 0;
     DevBuf<uint4> wstate;         // ray-tet path: (last tet, its entry face, boundary entry index, segments)
@@ -164,7 +165,8 @@ void build_band_lists(dtv_renderer* r, const dtv_mesh* mesh, int W, int H, int y
     dtv::launch_raster_fill(mesh->d_faces, uint32_t(mesh->host.num_faces), r->vproj.ptr, r->vfix.ptr, W, H,
                             r->counts.ptr, r->offsets.ptr, r->records.ptr, s, y0, y1);
     check_launch("band fill");
-    dtv::launch_sort(r->offsets.ptr + p0, r->records.ptr, uint32_t(pb), r->long_list.ptr, r->flags.ptr, s);
+    dtv::launch_sort(r->offsets.ptr + p0, r->records.ptr, uint32_t(pb), r->long_list.ptr, r->flags.ptr, s, nullptr,
+                     r->tuning.sort_surrogate_classes);
     check_launch("band sort");
 }
 
@@ -185,7 +187,8 @@ void composite_rows(dtv_renderer* r, const dtv_mesh* mesh, const float* d_colors
     else
         dtv::launch_composite(r->offsets.ptr, r->records.ptr, mesh->d_faces, r->vgeo.ptr,
                               reinterpret_cast<const float4*>(d_colors), cam.W, cam.H, sh,
-                              reinterpret_cast<float4*>(d_image), r->tfinal.ptr, r->term.ptr, s, y0, y1);
+                              reinterpret_cast<float4*>(d_image), r->tfinal.ptr, r->term.ptr, s, y0, y1,
+                              r->tuning.composite_tile);
 }
 
 // Adjoint of rows [y0, y1) into the gradient rows (per-cell: the cell colour
@@ -201,7 +204,7 @@ void adjoint_rows(dtv_renderer* r, const dtv_mesh* mesh, const float* d_colors, 
         dtv::launch_adjoint_rows(r->offsets.ptr, r->records.ptr, mesh->d_faces, r->vgeo.ptr,
                                  reinterpret_cast<const float4*>(d_colors), r->cam, sh,
                                  reinterpret_cast<const float4*>(d_image_adjoint), r->tfinal.ptr, r->term.ptr, y0, y1,
-                                 r->grad_rows.ptr, s);
+                                 r->grad_rows.ptr, s, r->tuning.adjoint_tile);
 }
 
 void scatter_rows(dtv_renderer* r, float* d_grad_positions, float* d_grad_colors, cudaStream_t s) {
@@ -532,7 +535,8 @@ int32_t render_common(dtv_renderer* r, const dtv_mesh* mesh, const float* d_posi
         check_launch("raster fill");
         rec_event(r, 4, s);
         DTV_CK(cudaMemsetAsync(r->flags.ptr, 0, 2 * sizeof(uint32_t), s));
-        dtv::launch_sort(r->offsets.ptr, r->records.ptr, uint32_t(P), r->long_list.ptr, r->flags.ptr, s);
+        dtv::launch_sort(r->offsets.ptr, r->records.ptr, uint32_t(P), r->long_list.ptr, r->flags.ptr, s, nullptr,
+                         r->tuning.sort_surrogate_classes);
         check_launch("sort");
         DTV_CK(cudaMemcpyAsync(r->h_flags, r->flags.ptr, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
         DTV_CK(cudaEventRecord(r->flags_event, s));
@@ -639,6 +643,23 @@ int32_t dtv_renderer_get_num_fragments(const dtv_renderer* r, uint64_t* nf) {
     return guarded([&] {
         require(r && nf, "null pointer");
         *nf = r->have_render ? r->nf : 0;
+    });
+}
+
+int32_t dtv_renderer_set_tuning(dtv_renderer* r, const dtv_tuning* t) {
+    return guarded([&] {
+        require(r && t, "null pointer");
+        require(t->composite_tile >= 0 && t->composite_tile <= 2 && t->adjoint_tile >= 0 && t->adjoint_tile <= 2,
+                "tile index must be 0, 1 or 2");
+        require((t->sort_surrogate_classes & ~0x1eu) == 0, "sort_surrogate_classes uses bits 1..4 only");
+        r->tuning = *t;
+    });
+}
+
+int32_t dtv_renderer_get_tuning(const dtv_renderer* r, dtv_tuning* t) {
+    return guarded([&] {
+        require(r && t, "null pointer");
+        *t = r->tuning;
     });
 }
 

@@ -42,14 +42,20 @@ void launch_scan(const uint32_t* counts, uint64_t n, unsigned long long* offsets
 // than the block sort capacity.  With a non-null `ok`, the sort does nothing
 // when *ok == 0 (batched steps whose records overflowed the buffer).
 size_t sort_scratch_elems(uint64_t P);
+// surrogate_classes: bit c set = list-length class c (1..4: up to 64, 128,
+// 256, 512 records) is sorted through 32-bit surrogate keys, else through the
+// 64-bit network (same result either way).
+constexpr uint32_t kSortSurrogateDefault = 0x1eu;
 void launch_sort(const unsigned long long* offsets, unsigned long long* records, uint32_t P, uint32_t* scratch,
-                 uint32_t* flags, cudaStream_t s, const uint32_t* ok = nullptr);
+                 uint32_t* flags, cudaStream_t s, const uint32_t* ok = nullptr,
+                 uint32_t surrogate_classes = kSortSurrogateDefault);
 constexpr uint32_t kSortWarpCap = 1024;    // elements per warp list sorted in shared memory
 constexpr uint32_t kSortBlockCap = 16384;  // elements per block-sorted list (128 KiB shared memory)
 
+// tile: pixel tile of the 256-thread blocks (0: 16 x 16, 1: 32 x 8, 2: 8 x 32).
 void launch_composite(const unsigned long long* offsets, const unsigned long long* records, const uint4* faces,
                       const VGeo* vgeo, const float4* colors, int W, int H, const ShadeDev& sh, float4* image,
-                      float* tfinal, uint32_t* term, cudaStream_t s, int row0 = 0, int row1 = -1);
+                      float* tfinal, uint32_t* term, cudaStream_t s, int row0 = 0, int row1 = -1, int tile = 0);
 void launch_adjoint(const unsigned long long* offsets, const unsigned long long* records, const uint4* faces,
                     const VGeo* vgeo, const float4* colors, const CamDev& cam, const ShadeDev& sh,
                     const float4* dimage, const float* tfinal, const uint32_t* term, uint32_t V,
@@ -58,7 +64,7 @@ void launch_adjoint(const unsigned long long* offsets, const unsigned long long*
 void launch_adjoint_rows(const unsigned long long* offsets, const unsigned long long* records, const uint4* faces,
                          const VGeo* vgeo, const float4* colors, const CamDev& cam, const ShadeDev& sh,
                          const float4* dimage, const float* tfinal, const uint32_t* term, int row0, int row1,
-                         float4* grad_rows, cudaStream_t s);
+                         float4* grad_rows, cudaStream_t s, int tile = 0);
 // Adds the interleaved [V][2] gradient rows into grad_pos [V,3] / grad_col [V,4].
 void launch_scatter_grads(const float4* grad_rows, uint32_t V, float* grad_pos, float4* grad_col, cudaStream_t s);
 

@@ -420,7 +420,7 @@ __global__ void __launch_bounds__(256) k_sort_classify(const u64* __restrict__ o
 }
 
 // Classes 0..4: K records per lane in registers (K = 1: bitonic over shuffles).
-template <int K>
+template <int K, bool Q>
 __global__ void __launch_bounds__(kSortWarps * 32, K >= 16 ? 2 : 1) k_sort_class_regs(const u64* __restrict__ offsets, u64* records,
                                                                      const uint32_t* __restrict__ items,
                                                                      const uint32_t* __restrict__ count,
@@ -439,6 +439,8 @@ __global__ void __launch_bounds__(kSortWarps * 32, K >= 16 ? 2 : 1) k_sort_class
             u64 v = lane < int(n) ? r[lane] : ~0ull;
             v = bitonic32(v, lane);
             if (lane < int(n)) r[lane] = v;
+        } else if (!Q) {
+            warp_sort_list<K>(r, n, lane);
         } else if (!warp_sort_list_q<K>(r, n, lane) && lane == 0) {
             redo_items[atomicAdd(redo_count, 1u)] = p;
         }
@@ -495,8 +497,17 @@ __global__ void __launch_bounds__(1024) k_sort_class_block(const u64* __restrict
 
 size_t sort_scratch_elems(uint64_t P) { return 16 + size_t(kSortClasses) * size_t(P); }
 
+template <int K>
+void sort_class(bool q, unsigned g, const u64* offsets, u64* records, const uint32_t* items, const uint32_t* count,
+                uint32_t* redo_n, uint32_t* redo, const uint32_t* ok, cudaStream_t s) {
+    if (q)
+        k_sort_class_regs<K, true><<<g, kSortWarps * 32, 0, s>>>(offsets, records, items, count, redo_n, redo, ok);
+    else
+        k_sort_class_regs<K, false><<<g, kSortWarps * 32, 0, s>>>(offsets, records, items, count, redo_n, redo, ok);
+}
+
 void launch_sort(const u64* offsets, u64* records, uint32_t P, uint32_t* scratch, uint32_t* flags, cudaStream_t s,
-                 const uint32_t* ok) {
+                 const uint32_t* ok, uint32_t surrogate_classes) {
     static bool attr_set = false;
     const size_t smem_warp = size_t(kSortWarps) * kSortWarpCap * sizeof(u64);
     const size_t smem_block = size_t(kSortBlockCap) * sizeof(u64);
@@ -513,11 +524,13 @@ void launch_sort(const u64* offsets, u64* records, uint32_t P, uint32_t* scratch
     // Lists the register sorts leave unsettled join the block-sort class (6).
     uint32_t* redo_n = scratch + 6;
     uint32_t* redo = items(6);
-    k_sort_class_regs<1><<<g, kSortWarps * 32, 0, s>>>(offsets, records, items(0), scratch + 0, redo_n, redo, ok);
-    k_sort_class_regs<2><<<g, kSortWarps * 32, 0, s>>>(offsets, records, items(1), scratch + 1, redo_n, redo, ok);
-    k_sort_class_regs<4><<<g, kSortWarps * 32, 0, s>>>(offsets, records, items(2), scratch + 2, redo_n, redo, ok);
-    k_sort_class_regs<8><<<g, kSortWarps * 32, 0, s>>>(offsets, records, items(3), scratch + 3, redo_n, redo, ok);
-    k_sort_class_regs<16><<<g, kSortWarps * 32, 0, s>>>(offsets, records, items(4), scratch + 4, redo_n, redo, ok);
+    auto q = [&](int c) { return ((surrogate_classes >> c) & 1u) != 0; };
+    k_sort_class_regs<1, false><<<g, kSortWarps * 32, 0, s>>>(offsets, records, items(0), scratch + 0, redo_n, redo,
+                                                              ok);
+    sort_class<2>(q(1), g, offsets, records, items(1), scratch + 1, redo_n, redo, ok, s);
+    sort_class<4>(q(2), g, offsets, records, items(2), scratch + 2, redo_n, redo, ok, s);
+    sort_class<8>(q(3), g, offsets, records, items(3), scratch + 3, redo_n, redo, ok, s);
+    sort_class<16>(q(4), g, offsets, records, items(4), scratch + 4, redo_n, redo, ok, s);
     k_sort_class_smem<<<std::min(g, 296u), kSortWarps * 32, smem_warp, s>>>(offsets, records, items(5), scratch + 5,
                                                                             ok);
     k_sort_class_block<<<296, 1024, smem_block, s>>>(offsets, records, items(6), scratch + 6, ok);
@@ -525,35 +538,54 @@ void launch_sort(const u64* offsets, u64* records, uint32_t P, uint32_t* scratch
 
 // ---------------------------------------------------------------------------
 // (d) front-to-back compositing, one thread per pixel (composite_pixel).
-__global__ void __launch_bounds__(kTile * kTile) k_composite(
+// Pixel tiles of 256 threads: TX x (256 / TX) pixels (tile index 0: 16 x 16,
+// 1: 32 x 8, 2: 8 x 32; chosen by the renderer's tuning).
+template <int TX>
+__global__ void __launch_bounds__(256) k_composite(
     const u64* __restrict__ offsets, const u64* __restrict__ records, const uint4* __restrict__ faces,
     const VGeo* __restrict__ vgeo, const float4* __restrict__ colors, int W, int row0, int row1, ShadeDev sh,
     float4* __restrict__ image, float* __restrict__ tfinal, uint32_t* __restrict__ term) {
-    const int px = blockIdx.x * kTile + (threadIdx.x % kTile);
-    const int py = row0 + int(blockIdx.y) * kTile + int(threadIdx.x / kTile);
+    constexpr int TY = 256 / TX;
+    const int px = blockIdx.x * TX + (threadIdx.x % TX);
+    const int py = row0 + int(blockIdx.y) * TY + int(threadIdx.x / TX);
     if (px < W && py < row1)
         composite_pixel(px, py, W, offsets, records, faces, vgeo, colors, sh, image, tfinal, term);
 }
 
+template <int TX>
+void composite_tiles(const u64* offsets, const u64* records, const uint4* faces, const VGeo* vgeo,
+                     const float4* colors, int W, int row0, int row1, const ShadeDev& sh, float4* image,
+                     float* tfinal, uint32_t* term, cudaStream_t s) {
+    constexpr int TY = 256 / TX;
+    dim3 grid((W + TX - 1) / TX, (row1 - row0 + TY - 1) / TY);
+    k_composite<TX><<<grid, 256, 0, s>>>(offsets, records, faces, vgeo, colors, W, row0, row1, sh, image, tfinal,
+                                         term);
+}
+
 void launch_composite(const u64* offsets, const u64* records, const uint4* faces, const VGeo* vgeo,
                       const float4* colors, int W, int H, const ShadeDev& sh, float4* image, float* tfinal,
-                      uint32_t* term, cudaStream_t s, int row0, int row1) {
+                      uint32_t* term, cudaStream_t s, int row0, int row1, int tile) {
     if (row1 < 0) row1 = H;
     if (row1 <= row0) return;
-    dim3 grid((W + kTile - 1) / kTile, (row1 - row0 + kTile - 1) / kTile);
-    k_composite<<<grid, kTile * kTile, 0, s>>>(offsets, records, faces, vgeo, colors, W, row0, row1, sh, image,
-                                               tfinal, term);
+    if (tile == 1)
+        composite_tiles<32>(offsets, records, faces, vgeo, colors, W, row0, row1, sh, image, tfinal, term, s);
+    else if (tile == 2)
+        composite_tiles<8>(offsets, records, faces, vgeo, colors, W, row0, row1, sh, image, tfinal, term, s);
+    else
+        composite_tiles<16>(offsets, records, faces, vgeo, colors, W, row0, row1, sh, image, tfinal, term, s);
 }
 
 // ---------------------------------------------------------------------------
 // (f) adjoint (adjoint_pixel).
-__global__ void __launch_bounds__(kTile * kTile) k_adjoint(
+template <int TX>
+__global__ void __launch_bounds__(256) k_adjoint(
     const u64* __restrict__ offsets, const u64* __restrict__ records, const uint4* __restrict__ faces,
     const VGeo* __restrict__ vgeo, const float4* __restrict__ colors, int W, int row0, int row1, CamDev cam,
     ShadeDev sh, const float4* __restrict__ dimage, const float* __restrict__ tfinal,
     const uint32_t* __restrict__ term, float4* __restrict__ grad_rows) {
-    const int px = blockIdx.x * kTile + (threadIdx.x % kTile);
-    const int py = row0 + int(blockIdx.y) * kTile + int(threadIdx.x / kTile);
+    constexpr int TY = 256 / TX;
+    const int px = blockIdx.x * TX + (threadIdx.x % TX);
+    const int py = row0 + int(blockIdx.y) * TY + int(threadIdx.x / TX);
     if (px >= W || py >= row1) return;
     adjoint_pixel(px, py, offsets, records, faces, vgeo, colors, W, cam, sh, dimage, tfinal, term,
                   GradAcc{grad_rows});
@@ -584,14 +616,30 @@ void launch_adjoint(const u64* offsets, const u64* records, const uint4* faces, 
     launch_scatter_grads(grad_rows, V, grad_pos, grad_col, s);
 }
 
+template <int TX>
+void adjoint_tiles(const u64* offsets, const u64* records, const uint4* faces, const VGeo* vgeo,
+                   const float4* colors, const CamDev& cam, const ShadeDev& sh, const float4* dimage,
+                   const float* tfinal, const uint32_t* term, int row0, int row1, float4* grad_rows, cudaStream_t s) {
+    constexpr int TY = 256 / TX;
+    dim3 grid((cam.W + TX - 1) / TX, (row1 - row0 + TY - 1) / TY);
+    k_adjoint<TX><<<grid, 256, 0, s>>>(offsets, records, faces, vgeo, colors, cam.W, row0, row1, cam, sh, dimage,
+                                       tfinal, term, grad_rows);
+}
+
 void launch_adjoint_rows(const u64* offsets, const u64* records, const uint4* faces, const VGeo* vgeo,
                          const float4* colors, const CamDev& cam, const ShadeDev& sh, const float4* dimage,
                          const float* tfinal, const uint32_t* term, int row0, int row1, float4* grad_rows,
-                         cudaStream_t s) {
+                         cudaStream_t s, int tile) {
     if (row1 <= row0) return;
-    dim3 grid((cam.W + kTile - 1) / kTile, (row1 - row0 + kTile - 1) / kTile);
-    k_adjoint<<<grid, kTile * kTile, 0, s>>>(offsets, records, faces, vgeo, colors, cam.W, row0, row1, cam, sh,
-                                             dimage, tfinal, term, grad_rows);
+    if (tile == 1)
+        adjoint_tiles<32>(offsets, records, faces, vgeo, colors, cam, sh, dimage, tfinal, term, row0, row1, grad_rows,
+                          s);
+    else if (tile == 2)
+        adjoint_tiles<8>(offsets, records, faces, vgeo, colors, cam, sh, dimage, tfinal, term, row0, row1, grad_rows,
+                         s);
+    else
+        adjoint_tiles<16>(offsets, records, faces, vgeo, colors, cam, sh, dimage, tfinal, term, row0, row1, grad_rows,
+                          s);
 }
 
 void launch_scatter_grads(const float4* grad_rows, uint32_t V, float* grad_pos, float4* grad_col, cudaStream_t s) {

@@ -125,6 +125,26 @@ class Renderer:
         self._over_budget = _lib.DTV_OVER_BUDGET_RECOMPUTE if over_budget == "recompute" else \
             _lib.DTV_OVER_BUDGET_ERROR
 
+    # -- kernel configuration (difftetvr_b200.autotune chooses it) -----------
+    def get_tuning(self) -> dict:
+        t = _lib.Tuning()
+        _lib.call("dtv_renderer_get_tuning", self._handle, ctypes.byref(t))
+        return {"composite_tile": t.composite_tile, "adjoint_tile": t.adjoint_tile,
+                "sort_surrogate_classes": t.sort_surrogate_classes}
+
+    def set_tuning(self, composite_tile: int | None = None, adjoint_tile: int | None = None,
+                   sort_surrogate_classes: int | None = None) -> None:
+        """Pixel tile of the composite / adjoint blocks (0: 16x16, 1: 32x8,
+        2: 8x32) and the sort method per list-length class (bit c of
+        sort_surrogate_classes, c = 1..4).  Results are identical for every
+        setting."""
+        cur = self.get_tuning()
+        t = _lib.Tuning(cur["composite_tile"] if composite_tile is None else int(composite_tile),
+                        cur["adjoint_tile"] if adjoint_tile is None else int(adjoint_tile),
+                        cur["sort_surrogate_classes"] if sort_surrogate_classes is None else int(sort_surrogate_classes),
+                        0)
+        _lib.call("dtv_renderer_set_tuning", self._handle, ctypes.byref(t))
+
     def get_num_bands(self) -> int:
         """0 if the last render stored its fragment lists whole, else the number
         of row bands it ran in (each recomputed by render_adjoint)."""

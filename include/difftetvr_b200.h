@@ -148,6 +148,22 @@ int32_t dtv_renderer_render_adjoint_cells(dtv_renderer* r, const dtv_mesh* mesh,
                                           int32_t use_abs_grad, float* d_grad_positions,
                                           float* d_grad_cell_colors, dtv_stream stream);
 
+/* Kernel configuration of a renderer (or batch): the pixel tile of the
+ * composite and adjoint blocks (0: 16 x 16, 1: 32 x 8, 2: 8 x 32 pixels) and,
+ * per list-length class c (bit c; 1..4 = lists of up to 64, 128, 256, 512
+ * records), whether the per-pixel sort goes through 32-bit surrogate keys or
+ * the 64-bit network.  Every setting gives the same lists, images and
+ * gradients; they differ in speed only.  An autotuner (difftetvr_b200.autotune)
+ * times them on the caller's workload.  Batches use only sort_surrogate_classes. */
+typedef struct dtv_tuning {
+    int32_t composite_tile;
+    int32_t adjoint_tile;
+    uint32_t sort_surrogate_classes;
+    int32_t reserved;
+} dtv_tuning;
+int32_t dtv_renderer_set_tuning(dtv_renderer* r, const dtv_tuning* tuning);
+int32_t dtv_renderer_get_tuning(const dtv_renderer* r, dtv_tuning* tuning);
+
 /* Total fragments of the last render (exact, from the scan). */
 int32_t dtv_renderer_get_num_fragments(const dtv_renderer* r, uint64_t* num_fragments);
 
@@ -285,6 +301,8 @@ int32_t dtv_batch_destroy(dtv_batch* batch);
  * pixels, max_fragments fragment records and max_grad_vertices gradient rows,
  * so later batches within these bounds allocate nothing (device allocation
  * synchronises the device, which a serving loop with several slots avoids). */
+int32_t dtv_batch_set_tuning(dtv_batch* batch, const dtv_tuning* tuning);
+int32_t dtv_batch_get_tuning(const dtv_batch* batch, dtv_tuning* tuning);
 int32_t dtv_batch_reserve(dtv_batch* batch, uint64_t max_views, uint64_t max_vertices, uint64_t max_pixels,
                           uint64_t max_fragments, uint64_t max_grad_vertices, dtv_stream stream);
 /* Mesh table: topology handles plus device positions f32[V*3] and colours f32[V*4]
