@@ -15,6 +15,24 @@ from .tet_mesh import TetMesh
 from .types import ColorStorage, RendererType, vec4
 
 
+def linked_list_view(offsets: np.ndarray, records: np.ndarray, width: int, height: int):
+    """(nodes u32[N, 3] = (bits, depth bits, next), heads i32[H, W]) from the
+    offsets [P+1] / sorted records [N] layout; next and empty heads are -1."""
+    off = np.asarray(offsets, np.int64)
+    rec = np.asarray(records, np.uint64)
+    n = rec.shape[0]
+    nodes = np.empty((n, 3), np.uint32)
+    nodes[:, 0] = (rec & np.uint64(0xFFFFFFFF)).astype(np.uint32)
+    nodes[:, 1] = (rec >> np.uint64(32)).astype(np.uint32)
+    nxt = np.arange(1, n + 1, dtype=np.int64)
+    ends = off[1:][np.diff(off) > 0] - 1  # last node of every non-empty list
+    nxt[ends] = -1
+    nodes[:, 2] = nxt.astype(np.int64).astype(np.uint32)
+    counts = np.diff(off)
+    heads = np.where(counts > 0, off[:-1], -1).astype(np.int32).reshape(height, width)
+    return nodes, heads
+
+
 def default_view_matrix() -> list[float]:
     """Camera at (0, 0, 0.8) with identity orientation (Module.cpp:458-463), column-major."""
     m = np.eye(4, dtype=np.float64)
@@ -278,6 +296,18 @@ class Renderer:
         """Per-pixel list offsets as int64 [H*W+1] (pixel p owns records [o[p], o[p+1]))."""
         off, _ = self.get_fragment_lists()
         return torch.from_numpy(off.view(np.int64).copy())
+
+    def get_linked_list_buffers(self) -> tuple[torch.Tensor, torch.Tensor]:
+        """The fragment lists in the layout of the reference's PPLL export
+        (get_fragment_buffer [N, 3] float32 / get_start_offset_buffer [H, W]
+        int32, TetMeshRendererPPLL.cpp:816-860): node i = (bits, depth, next)
+        with the uint fields stored as float32 bit patterns, bits = face << 2 |
+        boundary << 1 | front, next = index of the next node or -1 (0xFFFFFFFF),
+        head = -1 for empty pixels.  Here the lists are in front-to-back order
+        and the depth is view depth (the reference stores NDC depth)."""
+        off, rec = self.get_fragment_lists()
+        nodes, heads = linked_list_view(off, rec, self._width, self._height)
+        return torch.from_numpy(nodes.view(np.float32)), torch.from_numpy(heads)
 
     def get_pixel_state(self) -> tuple[np.ndarray, np.ndarray]:
         """(final transmittance f32[H,W], termination index u32[H,W]) of the last render."""

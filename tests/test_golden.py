@@ -113,3 +113,24 @@ def test_bintet_round_trip_and_errors(tmp_path):
         assert e.value.code == DTV_ERR_ARG, what
     with pytest.raises(DtvError):
         read_bintet(str(tmp_path / "missing.bintet"))
+
+
+def test_linked_list_view_of_the_fixture_lists():
+    """The reference-layout view (PPLL nodes + heads) of the 8^3 fixture lists:
+    following next from each head visits exactly the pixel's sorted records."""
+    from difftetvr_b200.renderer import linked_list_view
+    g = load("oracle_8_128.npz")
+    off, rec = g["offsets"], g["records"]
+    nodes, heads = linked_list_view(off, rec, 128, 128)
+    assert nodes.shape == (rec.shape[0], 3) and heads.shape == (128, 128)
+    flat = heads.reshape(-1)
+    for p in np.flatnonzero(np.diff(off) > 0)[::97]:
+        i, walked = int(flat[p]), []
+        while i != -1:
+            walked.append((int(nodes[i, 1]) << 32) | int(nodes[i, 0]))
+            nx = int(nodes[i, 2])
+            i = -1 if nx == 0xFFFFFFFF else nx
+        assert walked == [int(x) for x in rec[off[p]:off[p + 1]]]
+    assert np.all(flat[np.diff(off) == 0] == -1)
+    depth = nodes[:, 1].view(np.float32)
+    assert np.all(depth > 0)
