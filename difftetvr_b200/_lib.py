@@ -156,6 +156,9 @@ SIGNATURES = {
     "dtv_batch_set_meshes": (ctypes.c_int32, [c_vp, ctypes.c_int32, c_vp, c_vp, c_vp]),
     "dtv_batch_render": (ctypes.c_int32, [c_vp, ctypes.c_int32, ctypes.POINTER(BatchView), ctypes.POINTER(RenderParams),
                                           c_vp]),
+    "dtv_batch_render_async": (ctypes.c_int32, [c_vp, ctypes.c_int32, ctypes.POINTER(BatchView),
+                                                ctypes.POINTER(RenderParams), c_vp]),
+    "dtv_batch_render_status": (ctypes.c_int32, [c_vp, ctypes.POINTER(ctypes.c_int32), c_u64p]),
     "dtv_batch_render_adjoint": (ctypes.c_int32, [c_vp, ctypes.c_int32, ctypes.POINTER(BatchView), ctypes.c_int32,
                                                   ctypes.POINTER(BatchGradSlot), ctypes.c_int32, c_vp]),
     "dtv_batch_train_step": (ctypes.c_int32, [c_vp, ctypes.c_int32, ctypes.POINTER(BatchView),

@@ -131,6 +131,24 @@ class BatchRenderer:
         self._last_views = views
         return [v.image for v in views]
 
+    def render_async(self, views: list[View]) -> list[torch.Tensor]:
+        """render() without a host synchronisation, bounded by the reserved
+        record capacity (reserve()); check render_status() once the stream has
+        passed it and call render() again if it did not fit."""
+        device = self.meshes[0].get_vertex_positions().device
+        arr = self._views(views, device)
+        prm = self._params()
+        _lib.call("dtv_batch_render_async", self._handle, len(views), arr, ctypes.byref(prm),
+                  torch.cuda.current_stream(device).cuda_stream)
+        self._last_views = views
+        return [v.image for v in views]
+
+    def render_status(self) -> tuple[bool, int]:
+        """(fit, fragments) of the last render_async (its stream must be past it)."""
+        fits, nf = ctypes.c_int32(), ctypes.c_uint64()
+        _lib.call("dtv_batch_render_status", self._handle, ctypes.byref(fits), ctypes.byref(nf))
+        return bool(fits.value), int(nf.value)
+
     def render_adjoint(self, slots: list[tuple[int, torch.Tensor, torch.Tensor]], use_abs_grad: bool = False):
         """slots: (mesh index, grad_positions [V,3], grad_colors [V,4]) per gradient slot;
         views of the last render() name their slot in View.grad_slot."""

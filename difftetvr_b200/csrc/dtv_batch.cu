@@ -351,6 +351,7 @@ struct dtv_batch {
     u64 capacity = 0;
     uint64_t steps_rerun = 0;
     uint32_t sort_surrogate_classes = dtv::kSortSurrogateDefault;
+    bool async_render = false;  // last render enqueued without a host sync (capacity-guarded)
 };
 
 namespace {
@@ -662,6 +663,38 @@ int32_t dtv_batch_render(dtv_batch* b, int32_t num_views, const dtv_batch_view* 
         check_launch("batch render");
         b->last_fragments = nf;
         b->have_render = true;
+        b->async_render = false;
+    });
+}
+
+int32_t dtv_batch_render_async(dtv_batch* b, int32_t num_views, const dtv_batch_view* views,
+                               const dtv_render_params* params, dtv_stream stream) {
+    return guarded([&] {
+        require(b && views && params, "null argument");
+        if (b->records.cap == 0)
+            throw DtvError(DTV_ERR_STATE, "dtv_batch_render_async needs record capacity (dtv_batch_reserve)");
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        b->have_render = false;
+        build_views(b, num_views, views, /*train=*/false, false);
+        ensure_scratch(b, s);
+        b->sh = dtv::shade_constants(*params);
+        upload_views(b, s);
+        b->capacity = b->records.cap;
+        enqueue_forward(b, b->sh, /*guarded=*/true, s);
+        DTV_CK(cudaMemcpyAsync(b->h_ok, b->ok.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        DTV_CK(cudaMemcpyAsync(b->h_total, b->total.ptr, sizeof(u64), cudaMemcpyDeviceToHost, s));
+        b->have_render = true;
+        b->async_render = true;
+    });
+}
+
+int32_t dtv_batch_render_status(const dtv_batch* b, int32_t* fits, uint64_t* num_fragments) {
+    return guarded([&] {
+        require(b && fits && num_fragments, "null pointer");
+        if (!b->have_render || !b->async_render)
+            throw DtvError(DTV_ERR_STATE, "no dtv_batch_render_async to report on");
+        *fits = *b->h_ok != 0u ? 1 : 0;
+        *num_fragments = *b->h_total;
     });
 }
 
@@ -720,7 +753,8 @@ int32_t dtv_batch_render_adjoint(dtv_batch* b, int32_t num_views, const dtv_batc
         using namespace dtv;
         kb_adjoint<<<unsigned(b->tot_tiles), kTile * kTile, 0, s>>>(b->d_views.ptr, b->nviews, b->offsets.ptr,
                                                                     b->records.ptr, b->vgeo.ptr, sh, b->tfinal.ptr,
-                                                                    b->term.ptr, b->grad_rows.ptr, nullptr);
+                                                                    b->term.ptr, b->grad_rows.ptr,
+                                                                    b->async_render ? b->ok.ptr : nullptr);
         if (rows)
             kb_scatter<<<grid_for(rows, 256, 148 * 16), 256, 0, s>>>(b->d_slots.ptr, num_slots, rows,
                                                                      b->grad_rows.ptr);

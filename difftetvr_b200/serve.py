@@ -206,6 +206,25 @@ class GpuBackend:
                           for _ in range(self.slots)]
         self.fpp = {n: 64.0 for n in self.names}
 
+    def _rerun(self, handle):
+        torch = self.torch
+        br, stream = self.renderers[handle["slot"]], self.streams[handle["slot"]]
+        with torch.cuda.stream(stream):
+            br.render(handle["views"])
+            # Same slot order as launch(): views name their slot in grad_slot.
+            slots = [(handle["views"][i].mesh, gp, gc) for i, gp, gc in handle["grads"]]
+            for _, gp, gc in slots:
+                gp.zero_()
+                gc.zero_()
+            for i, (r, v) in enumerate(zip(handle["reqs"], handle["views"])):
+                if r.mode == "gradient":
+                    n = float(v.width * v.height * 4)
+                    v.image_adjoint = (v.image - r.target) * (2.0 / n)
+            if slots:
+                br.render_adjoint(slots)
+        stream.synchronize()
+        return handle
+
     def reserve(self, max_batch: int, max_pixels_per_request: int, budget_fragments: int) -> None:
         """Sizes every slot's scratch for the largest admissible batch, so no
         device allocation (which synchronises the whole device) happens while
@@ -214,6 +233,7 @@ class GpuBackend:
         for br in self.renderers:
             br.reserve(max_batch, max_batch * maxV, max_batch * max_pixels_per_request, budget_fragments,
                        max_batch * maxV)
+        self._reserved = True
 
     def fragments_per_pixel(self, mesh: str) -> float:
         return self.fpp[mesh]
@@ -237,8 +257,11 @@ class GpuBackend:
         views = [View(mesh=self.index[r.mesh], view_matrix=r.view_matrix, width=r.width, height=r.height,
                       fovy=r.fovy) for r in reqs]
         grads = []
+        reserved = getattr(self, "_reserved", False)
         with torch.cuda.stream(stream):
-            br.render(views)
+            # With reserved scratch the batch is enqueued without a host
+            # synchronisation; finish() checks that it fit.
+            (br.render_async if reserved else br.render)(views)
             slots = []
             for i, (r, v) in enumerate(zip(reqs, views)):
                 if r.mode == "gradient":
@@ -254,9 +277,9 @@ class GpuBackend:
                 br.render_adjoint([(m, gp, gc) for (m, gp, gc) in slots])
             ev = torch.cuda.Event()
             ev.record(stream)
-        fr = br.info()["fragments"]
         px = sum(r.pixels for r in reqs)
-        return {"event": ev, "views": views, "reqs": reqs, "grads": grads, "fragments": fr, "pixels": px}
+        return {"event": ev, "views": views, "reqs": reqs, "grads": grads, "pixels": px, "slot": slot,
+                "async": reserved}
 
     def done(self, handle) -> bool:
         return handle["event"].query()
@@ -264,6 +287,16 @@ class GpuBackend:
     def finish(self, handle) -> list[Result]:
         handle["event"].synchronize()
         reqs, views = handle["reqs"], handle["views"]
+        br = self.renderers[handle["slot"]]
+        if handle["async"]:
+            fits, nf = br.render_status()
+            if not fits:
+                # Over the reserved capacity: run the batch again with exact sizing.
+                handle = self._rerun(handle)
+                nf = br.info()["fragments"]
+            handle["fragments"] = nf
+        else:
+            handle["fragments"] = br.info()["fragments"]
         # Per-mesh fragments-per-pixel estimate from the exact batch count.
         by_mesh = {}
         for r in reqs:

@@ -301,6 +301,16 @@ int32_t dtv_batch_destroy(dtv_batch* batch);
  * pixels, max_fragments fragment records and max_grad_vertices gradient rows,
  * so later batches within these bounds allocate nothing (device allocation
  * synchronises the device, which a serving loop with several slots avoids). */
+/* Forward render of a batch without a host synchronisation (for serving
+ * loops): the record capacity already allocated (dtv_batch_reserve) bounds the
+ * batch, and the kernels after the count and scan do nothing when the records
+ * would not fit.  Once the stream has passed this render, dtv_batch_render_status
+ * reports whether it fit and the fragment count; a batch that did not fit must
+ * be rendered again with dtv_batch_render.  A dtv_batch_render_adjoint after
+ * it is skipped on the device likewise. */
+int32_t dtv_batch_render_async(dtv_batch* batch, int32_t num_views, const dtv_batch_view* views,
+                               const dtv_render_params* params, dtv_stream stream);
+int32_t dtv_batch_render_status(const dtv_batch* batch, int32_t* fits, uint64_t* num_fragments);
 int32_t dtv_batch_set_tuning(dtv_batch* batch, const dtv_tuning* tuning);
 int32_t dtv_batch_get_tuning(const dtv_batch* batch, dtv_tuning* tuning);
 int32_t dtv_batch_reserve(dtv_batch* batch, uint64_t max_views, uint64_t max_vertices, uint64_t max_pixels,

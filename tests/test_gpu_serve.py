@@ -68,3 +68,32 @@ def test_mixed_stream_results_equal_isolated_results():
             assert rel_err(res.grad_colors.cpu().numpy(), gc.cpu().numpy()) < 1e-5
     st = eng.latency_stats()
     assert st["requests"] == len(reqs) and st["p99_ms"] > 0
+
+
+@pytest.mark.parametrize("reserve_fragments", [4_000_000, 20_000])
+def test_reserved_async_serving_equals_isolated(reserve_fragments):
+    """With reserved slot scratch the engine enqueues batches without a host
+    synchronisation; a batch over the reserved record capacity (the small
+    reservation) is detected when it completes and run again exactly."""
+    meshes = {"a": make_mesh(8, 1), "b": make_mesh(6, 2)}
+    be = GpuBackend(meshes, slots=2)
+    be.calibrate(S.sphere_camera(0), res=64)
+    be.reserve(4, 96 * 96, reserve_fragments)
+    eng = ServingEngine(be, budget_fragments=4_000_000, max_batch=4)
+    g = torch.Generator(device="cuda").manual_seed(2)
+    reqs = []
+    for i in range(10):
+        mode = "gradient" if i % 2 == 0 else "forward"
+        tgt = torch.rand(96, 96, 4, device="cuda", generator=g) if mode == "gradient" else None
+        reqs.append(Request(mesh="ab"[i % 2], view_matrix=S.sphere_camera(200 + i), width=96, height=96,
+                            mode=mode, target=tgt, fovy=math.radians(45.0)))
+    torch.cuda.synchronize()
+    eng.start()
+    results = [f.result(timeout=120) for f in [eng.submit(r) for r in reqs]]
+    eng.stop()
+    for r, res in zip(reqs, results):
+        img, gp, gc = alone(meshes[r.mesh], r)
+        assert float((res.image - img).abs().max()) <= 1e-6
+        if r.mode == "gradient":
+            assert rel_err(res.grad_positions.cpu().numpy(), gp.cpu().numpy()) < 1e-5
+            assert rel_err(res.grad_colors.cpu().numpy(), gc.cpu().numpy()) < 1e-5
