@@ -41,6 +41,8 @@ class Request:
     t_arrival: float = 0.0
     t_start: float = 0.0
     t_finish: float = 0.0
+    batch_id: int = -1
+    batch_size: int = 0
     future: Future = field(default_factory=Future, repr=False)
 
     @property
@@ -150,6 +152,8 @@ class ServingEngine:
             t = time.perf_counter()
             for r in batch:
                 r.t_start = t
+                r.batch_id = self.batches
+                r.batch_size = len(batch)
             self.busy[slot] = (self.backend.launch(slot, batch), batch)
             self.batches += 1
             progressed = True
@@ -177,15 +181,28 @@ class ServingEngine:
             self.thread.join(timeout=timeout)
 
     # -- statistics ------------------------------------------------------------
-    def latency_stats(self) -> dict:
-        lat = np.array([(r.t_finish - r.t_arrival) * 1e3 for r in self.completed]) if self.completed else np.zeros(0)
-        if lat.size == 0:
+    def latency_stats(self, slowest: int = 3) -> dict:
+        """Latency percentiles (arrival to result), split into queueing
+        (arrival to batch launch) and service (launch to result), plus the
+        `slowest` requests with their batch."""
+        done = self.completed
+        if not done:
             return {"requests": 0}
-        span = max(r.t_finish for r in self.completed) - min(r.t_arrival for r in self.completed)
+        lat = np.array([(r.t_finish - r.t_arrival) * 1e3 for r in done])
+        wait = np.array([(r.t_start - r.t_arrival) * 1e3 for r in done])
+        svc = lat - wait
+        span = max(r.t_finish for r in done) - min(r.t_arrival for r in done)
+        worst = np.argsort(lat)[::-1][:slowest]
         return {"requests": int(lat.size), "p50_ms": float(np.percentile(lat, 50)),
                 "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(lat.mean()),
+                "queue_p50_ms": float(np.percentile(wait, 50)), "queue_p99_ms": float(np.percentile(wait, 99)),
+                "service_p50_ms": float(np.percentile(svc, 50)), "service_p99_ms": float(np.percentile(svc, 99)),
                 "throughput_rps": float(lat.size / span) if span > 0 else float("nan"),
-                "batches": self.batches, "rejected": self.rejected}
+                "batches": self.batches, "rejected": self.rejected,
+                "slowest": [{"ms": round(float(lat[i]), 3), "queue_ms": round(float(wait[i]), 3),
+                             "batch": done[i].batch_id, "batch_size": done[i].batch_size,
+                             "mesh": done[i].mesh, "pixels": done[i].pixels, "mode": done[i].mode}
+                            for i in worst]}
 
 
 class GpuBackend:
@@ -305,11 +322,16 @@ class GpuBackend:
             (m, px), = by_mesh.items()
             self.observe(m, px, handle["fragments"])
         g = {i: (gp, gc) for i, gp, gc in handle["grads"]}
+        # Losses of the gradient requests on the slot's stream, read back at once.
+        grad_idx = [i for i, r in enumerate(reqs) if r.mode == "gradient"]
+        losses = {}
+        if grad_idx:
+            torch = self.torch
+            with torch.cuda.stream(self.streams[handle["slot"]]):
+                vals = torch.stack([((views[i].image - reqs[i].target) ** 2).mean() for i in grad_idx])
+                losses = dict(zip(grad_idx, vals.tolist()))
         out = []
         for i, (r, v) in enumerate(zip(reqs, views)):
             gp, gc = g.get(i, (None, None))
-            loss = None
-            if r.mode == "gradient":
-                loss = float(((v.image - r.target) ** 2).mean())
-            out.append(Result(r.id, v.image, gp, gc, loss))
+            out.append(Result(r.id, v.image, gp, gc, losses.get(i)))
         return out
