@@ -15,6 +15,7 @@ rank runs an independent replica (the path has no data-path collective).
 from __future__ import annotations
 
 import argparse
+import collections
 import json
 import os
 import subprocess
@@ -638,15 +639,19 @@ def run_serving(args):
         eng = ServingEngine(be, budget_fragments=budget, max_batch=32)
         eng.start()
         t = time.perf_counter()
-        futs = []
+        # The client takes each result as it completes (so result tensors are
+        # released as a real client would, back to the slots' memory pools).
+        futs = collections.deque()
         for q, g in zip(reqs, gaps):
+            while futs and futs[0].done():
+                futs.popleft().result()
             t += g
             dt = t - time.perf_counter()
             if dt > 0:
                 time.sleep(dt)  # sleeping (not spinning) keeps the GIL free for the engine thread
             futs.append(eng.submit(q))
-        for f in futs:
-            f.result(timeout=600)
+        while futs:
+            futs.popleft().result(timeout=600)
         eng.stop()
         st = eng.latency_stats()
         st["rate_rps"] = rate

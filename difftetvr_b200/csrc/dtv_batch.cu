@@ -102,20 +102,27 @@ __global__ void __launch_bounds__(256) kb_project(const BatchView* __restrict__ 
     }
 }
 
-template <bool FILL>
+template <bool FILL, bool WIDE>
 __global__ void __launch_bounds__(128) kb_raster(const BatchView* __restrict__ views, int nviews, u64 total,
                                                  const float4* __restrict__ vproj, const int2* __restrict__ vfix,
                                                  uint32_t* __restrict__ counts, const u64* __restrict__ offsets,
                                                  u64* __restrict__ records, const uint32_t* __restrict__ ok) {
     if (FILL && !batch_ok(ok)) return;
+    __shared__ RasterJob jobs[4][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const u64 first = u64(blockIdx.x) * blockDim.x;
     const u64 g = first + threadIdx.x;
+    bool live = false;
+    RasterJob J;
     if (g < total) {
         const int v = view_of_item(g, first, nviews, [&](int i) { return views[i].face_base; });
         const BatchView& bv = views[v];
-        raster_face<FILL>(uint32_t(g - bv.face_base), bv.faces, vproj + bv.vert_base, vfix + bv.vert_base,
-                          int(bv.W), 0, int(bv.H), counts + bv.pix_base, offsets + bv.pix_base, records);
+        live = raster_setup(uint32_t(g - bv.face_base), bv.faces, vfix + bv.vert_base, uint32_t(bv.vert_base),
+                            int(bv.W), 0, int(bv.H), bv.pix_base, J) &&
+               (J.wide != 0) == WIDE;
     }
+    if (live) jobs[w][lane] = J;
+    raster_warp<FILL, WIDE>(jobs[w], __ballot_sync(0xffffffffu, live), lane, vproj, counts, offsets, records);
 }
 
 // ok = (records fit the buffer); *total_out = number of records.
@@ -406,6 +413,7 @@ void build_views(dtv_batch* b, int nviews, const dtv_batch_view* views, bool tra
         b->h_views[i] = bv;
     }
     (void)internal_dimage;
+    require(vb < (u64(1) << 32), "a batch holds fewer than 2^32 vertices in total");
     b->nviews = nviews;
     b->tot_verts = vb;
     b->tot_faces = fb;
@@ -441,6 +449,20 @@ void upload_views(dtv_batch* b, cudaStream_t s) {
     DTV_CK(cudaEventRecord(b->staging_free, s));
 }
 
+// Count (FILL false) or fill pass over every view's faces: the 32-bit faces,
+// then the 64-bit ones (kb_raster).
+template <bool FILL>
+void launch_kb_raster(dtv_batch* b, const uint32_t* okp, cudaStream_t s) {
+    using namespace dtv;
+    const unsigned blocks = grid_for(b->tot_faces, 128, 0x7fffffffu);
+    kb_raster<FILL, false><<<blocks, 128, 0, s>>>(b->d_views.ptr, b->nviews, b->tot_faces, b->vproj.ptr,
+                                                  b->vfix.ptr, b->counts.ptr, FILL ? b->offsets.ptr : nullptr,
+                                                  FILL ? b->records.ptr : nullptr, okp);
+    kb_raster<FILL, true><<<blocks, 128, 0, s>>>(b->d_views.ptr, b->nviews, b->tot_faces, b->vproj.ptr,
+                                                 b->vfix.ptr, b->counts.ptr, FILL ? b->offsets.ptr : nullptr,
+                                                 FILL ? b->records.ptr : nullptr, okp);
+}
+
 // Enqueues project, count, scan, [capacity guard], fill, sort, composite.
 // With `guarded`, kernels after the scan run only if the records fit.
 void enqueue_forward(dtv_batch* b, const dtv::ShadeDev& sh, bool guarded, cudaStream_t s) {
@@ -448,16 +470,13 @@ void enqueue_forward(dtv_batch* b, const dtv::ShadeDev& sh, bool guarded, cudaSt
     const uint32_t* okp = guarded ? b->ok.ptr : nullptr;
     kb_project<<<grid_for(b->tot_verts, 256, 0x7fffffffu), 256, 0, s>>>(b->d_views.ptr, b->nviews, b->tot_verts,
                                                                         b->vproj.ptr, b->vfix.ptr, b->vgeo.ptr);
-    kb_raster<false><<<grid_for(b->tot_faces, 128, 0x7fffffffu), 128, 0, s>>>(
-        b->d_views.ptr, b->nviews, b->tot_faces, b->vproj.ptr, b->vfix.ptr, b->counts.ptr, nullptr, nullptr, nullptr);
+    launch_kb_raster<false>(b, nullptr, s);
     launch_scan(b->counts.ptr, b->tot_pixels, b->offsets.ptr, b->scan.ptr, s);
     if (guarded) {
         kb_check_capacity<<<1, 1, 0, s>>>(b->offsets.ptr + b->tot_pixels, b->capacity, b->ok.ptr, b->total.ptr);
         kb_clear_counts<<<grid_for(b->tot_pixels, 256, 148 * 16), 256, 0, s>>>(b->counts.ptr, b->tot_pixels, okp);
     }
-    kb_raster<true><<<grid_for(b->tot_faces, 128, 0x7fffffffu), 128, 0, s>>>(
-        b->d_views.ptr, b->nviews, b->tot_faces, b->vproj.ptr, b->vfix.ptr, b->counts.ptr, b->offsets.ptr,
-        b->records.ptr, okp);
+    launch_kb_raster<true>(b, okp, s);
     DTV_CK(cudaMemsetAsync(b->sort_flags.ptr, 0, 2 * sizeof(uint32_t), s));
     launch_sort(b->offsets.ptr, b->records.ptr, uint32_t(b->tot_pixels), b->long_list.ptr, b->sort_flags.ptr, s, okp,
                 b->sort_surrogate_classes);
@@ -633,9 +652,7 @@ int32_t dtv_batch_render(dtv_batch* b, int32_t num_views, const dtv_batch_view* 
         kb_project<<<grid_for(b->tot_verts, 256, 0x7fffffffu), 256, 0, s>>>(b->d_views.ptr, b->nviews,
                                                                             b->tot_verts, b->vproj.ptr, b->vfix.ptr,
                                                                             b->vgeo.ptr);
-        kb_raster<false><<<grid_for(b->tot_faces, 128, 0x7fffffffu), 128, 0, s>>>(
-            b->d_views.ptr, b->nviews, b->tot_faces, b->vproj.ptr, b->vfix.ptr, b->counts.ptr, nullptr, nullptr,
-            nullptr);
+        launch_kb_raster<false>(b, nullptr, s);
         launch_scan(b->counts.ptr, b->tot_pixels, b->offsets.ptr, b->scan.ptr, s);
         check_launch("batch count");
         DTV_CK(cudaMemcpyAsync(b->h_total, b->offsets.ptr + b->tot_pixels, sizeof(u64), cudaMemcpyDeviceToHost, s));
@@ -651,9 +668,7 @@ int32_t dtv_batch_render(dtv_batch* b, int32_t num_views, const dtv_batch_view* 
             cudaMemsetAsync(b->counts.ptr, 0, sizeof(uint32_t) * b->tot_pixels, s);
             throw;
         }
-        kb_raster<true><<<grid_for(b->tot_faces, 128, 0x7fffffffu), 128, 0, s>>>(
-            b->d_views.ptr, b->nviews, b->tot_faces, b->vproj.ptr, b->vfix.ptr, b->counts.ptr, b->offsets.ptr,
-            b->records.ptr, nullptr);
+        launch_kb_raster<true>(b, nullptr, s);
         DTV_CK(cudaMemsetAsync(b->sort_flags.ptr, 0, 2 * sizeof(uint32_t), s));
         launch_sort(b->offsets.ptr, b->records.ptr, uint32_t(b->tot_pixels), b->long_list.ptr, b->sort_flags.ptr, s,
                     nullptr, b->sort_surrogate_classes);

@@ -34,29 +34,46 @@ void launch_project(const float* pos, uint32_t V, const CamDev& cam, float4* vpr
     k_project<<<(V + 255) / 256, 256, 0, s>>>(pos, V, cam, vproj, vfix, vgeo);
 }
 
-// (a)+(b) face rasterisation: one thread per face (raster_face, dtv_path.cuh).
-template <bool FILL>
-__global__ void __launch_bounds__(128) k_raster(const uint4* __restrict__ faces, uint32_t F,
-                                                const float4* __restrict__ vproj, const int2* __restrict__ vfix,
-                                                int W, int row0, int row1, uint32_t* __restrict__ counts,
-                                                const u64* __restrict__ offsets, u64* __restrict__ records) {
+// (a)+(b) face rasterisation: 32 faces per warp, the warp's lanes spread over
+// each face's pixels in turn (raster_warp, dtv_path.cuh).
+constexpr int kRasterWarps = 4;
+
+template <bool FILL, bool WIDE>
+__global__ void __launch_bounds__(32 * kRasterWarps) k_raster(const uint4* __restrict__ faces, uint32_t F,
+                                                              const float4* __restrict__ vproj,
+                                                              const int2* __restrict__ vfix, int W, int row0, int row1,
+                                                              uint32_t* __restrict__ counts,
+                                                              const u64* __restrict__ offsets,
+                                                              u64* __restrict__ records) {
+    __shared__ RasterJob jobs[kRasterWarps][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t f = blockIdx.x * blockDim.x + threadIdx.x;
-    if (f < F) raster_face<FILL>(f, faces, vproj, vfix, W, row0, row1, counts, offsets, records);
+    RasterJob J;
+    const bool live = f < F && raster_setup(f, faces, vfix, 0u, W, row0, row1, 0ull, J) && (J.wide != 0) == WIDE;
+    if (live) jobs[w][lane] = J;
+    raster_warp<FILL, WIDE>(jobs[w], __ballot_sync(kFull, live), lane, vproj, counts, offsets, records);
 }
 
 void launch_raster_count(const uint4* faces, uint32_t F, const float4* vproj, const int2* vfix, int W, int H,
                          uint32_t* counts, cudaStream_t s, int row0, int row1) {
     if (F == 0) return;
     if (row1 < 0) row1 = H;
-    k_raster<false><<<(F + 127) / 128, 128, 0, s>>>(faces, F, vproj, vfix, W, row0, row1, counts, nullptr,
-                                                    nullptr);
+    const unsigned blocks = (F + 32 * kRasterWarps - 1) / (32 * kRasterWarps);
+    k_raster<false, false><<<blocks, 32 * kRasterWarps, 0, s>>>(faces, F, vproj, vfix, W, row0, row1, counts, nullptr,
+                                                                nullptr);
+    k_raster<false, true><<<blocks, 32 * kRasterWarps, 0, s>>>(faces, F, vproj, vfix, W, row0, row1, counts, nullptr,
+                                                               nullptr);
 }
 
 void launch_raster_fill(const uint4* faces, uint32_t F, const float4* vproj, const int2* vfix, int W, int H,
                         uint32_t* counts, const u64* offsets, u64* records, cudaStream_t s, int row0, int row1) {
     if (F == 0) return;
     if (row1 < 0) row1 = H;
-    k_raster<true><<<(F + 127) / 128, 128, 0, s>>>(faces, F, vproj, vfix, W, row0, row1, counts, offsets, records);
+    const unsigned blocks = (F + 32 * kRasterWarps - 1) / (32 * kRasterWarps);
+    k_raster<true, false><<<blocks, 32 * kRasterWarps, 0, s>>>(faces, F, vproj, vfix, W, row0, row1, counts, offsets,
+                                                               records);
+    k_raster<true, true><<<blocks, 32 * kRasterWarps, 0, s>>>(faces, F, vproj, vfix, W, row0, row1, counts, offsets,
+                                                              records);
 }
 
 // ---------------------------------------------------------------------------

@@ -1,6 +1,7 @@
 // Per-face and per-pixel bodies of the hot path, shared by the single-view
 // kernels (dtv_kernels.cu) and the batched multi-view kernels (dtv_batch.cu).
 #pragma once
+#include <type_traits>
 #include "dtv_device.cuh"
 #include "dtv_segment.cuh"
 
@@ -10,119 +11,185 @@ using u64 = unsigned long long;
 constexpr int kTile = 16;  // composite / adjoint pixel tile (16 x 16 threads)
 
 // ---------------------------------------------------------------------------
-// (a)+(b) face rasterisation.  One thread per face walks the pixel centres of
-// the face's bounding box with incrementally updated integer edge functions in
-// 1/256-pixel fixed point.  COUNT mode increments the per-pixel counter; FILL
+// (a)+(b) face rasterisation, warp-cooperative.  Each lane of a warp sets up
+// one face (projected fixed-point vertices, orientation, clipped bounding box)
+// into shared memory; the warp then takes the faces one at a time and spreads
+// the pixels of the face's bounding box over its 32 lanes (pixel k of the box,
+// row-major, goes to lane k mod 32), so lanes stay busy whatever the sizes of
+// the faces a warp holds.  COUNT mode increments the per-pixel counter; FILL
 // mode writes the record at offsets[p] + (--counts[p]), leaving counts zeroed
 // for the next render.  Only pixel rows [row0, row1) are visited (row bands of
 // a render whose lists do not fit the fragment budget at once).
 //
-// Edge functions are translation invariant, so they are evaluated relative to
-// the bounding-box corner: for boxes under 64 px (2^14 fixed-point units) on
-// each side every product is below 2^29 and the exact values fit in 32-bit
-// integers (half the ALU work of the 64-bit form); larger faces use 64 bits.
-// Both give identical coverage.
+// Coverage: edge functions in 1/256-pixel fixed point, evaluated relative to
+// the centre of the box's first pixel (edge functions are translation
+// invariant, so the values are the exact ones).  For boxes under 64 px
+// (2^14 units) on each side every term is below 2^29 and 32-bit integers are
+// exact; larger faces use 64 bits.  Both give identical coverage.
 template <typename I>
 __device__ __forceinline__ bool edge_in(I E, I dx, I dy) {
     return (E > 0) || (E == 0 && ((dy < 0) || (dy == 0 && dx > 0)));
 }
 
-template <bool FILL, typename I>
-__device__ __forceinline__ void raster_box(const uint4& fc, uint32_t bits, I ax0, I ay0, I ax1, I ay1, I ax2, I ay2,
-                                           I Xs, I Ys, int px0, int px1, int py0, int py1,
-                                           const float4* __restrict__ vproj, int W, uint32_t* __restrict__ counts,
-                                           const u64* __restrict__ offsets, u64* __restrict__ records) {
-    // Edges e0: a1->a2, e1: a2->a0, e2: a0->a1; (Xs, Ys) is the centre of
-    // pixel (px0, py0) in the same (possibly box-relative) coordinates.
-    const I dx0 = ax2 - ax1, dy0 = ay2 - ay1;
-    const I dx1 = ax0 - ax2, dy1 = ay0 - ay2;
-    const I dx2 = ax1 - ax0, dy2 = ay1 - ay0;
-    I E0r = dx0 * (Ys - ay1) - dy0 * (Xs - ax1);
-    I E1r = dx1 * (Ys - ay2) - dy1 * (Xs - ax2);
-    I E2r = dx2 * (Ys - ay0) - dy2 * (Xs - ax0);
-    float4 va, vb, vc;
-    if (FILL) {
-        va = vproj[fc.x];
-        vb = vproj[fc.y];
-        vc = vproj[fc.z];
-    }
-    // Four pixels of a row per step: their coverage tests, depth keys, counter
-    // atomics and offset loads are independent and issue back to back before
-    // the record stores (the fill is bound by atomic round trips otherwise).
-    const I sx0 = -dy0 * I(256), sx1 = -dy1 * I(256), sx2 = -dy2 * I(256);
-    for (int py = py0; py <= py1; ++py) {
-        I E0 = E0r, E1 = E1r, E2 = E2r;
-        const size_t row = size_t(py) * W;
-        for (int px = px0; px <= px1; px += 4) {
-            bool in[4];
-#pragma unroll
-            for (int k = 0; k < 4; ++k)
-                in[k] = (px + k <= px1) && edge_in<I>(E0 + I(k) * sx0, dx0, dy0) &&
-                        edge_in<I>(E1 + I(k) * sx1, dx1, dy1) && edge_in<I>(E2 + I(k) * sx2, dx2, dy2);
-            if (FILL) {
-                uint32_t slot[4];
-                u64 off[4];
-                float z[4];
-#pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    if (in[k]) {
-                        const size_t p = row + px + k;
-                        off[k] = offsets[p];
-                        slot[k] = atomicSub(&counts[p], 1u);
-                        z[k] = depth_key(va, vb, vc, float(px + k) + 0.5f, float(py) + 0.5f);
-                    }
-                }
-#pragma unroll
-                for (int k = 0; k < 4; ++k)
-                    if (in[k]) records[off[k] + slot[k] - 1u] = (u64(__float_as_uint(z[k])) << 32) | bits;
-            } else {
-#pragma unroll
-                for (int k = 0; k < 4; ++k)
-                    if (in[k]) atomicAdd(&counts[row + px + k], 1u);
-            }
-            E0 += I(4) * sx0;
-            E1 += I(4) * sx1;
-            E2 += I(4) * sx2;
-        }
-        E0r += dx0 * I(256);
-        E1r += dx1 * I(256);
-        E2r += dx2 * I(256);
-    }
-}
+struct __align__(16) RasterJob {
+    int ax0, ay0, ax1, ay1, ax2, ay2;  // vertices, relative to the first pixel centre; E > 0 inside
+    int px0, py0, bw, bh;              // first pixel and size of the clipped bounding box
+    uint32_t bits;                     // record low word: face << 2 | boundary << 1 | front
+    uint32_t v0, v1, v2;               // vertex rows of vproj (depth key)
+    int W;                             // image width (pixel rows of counts / offsets)
+    int wide;                          // edge functions need 64 bits
+    u64 pix_base;                      // first pixel of the image in counts / offsets
+};
 
-template <bool FILL>
-__device__ __forceinline__ void raster_face(uint32_t f, const uint4* __restrict__ faces,
-                                            const float4* __restrict__ vproj, const int2* __restrict__ vfix,
-                                            int W, int row0, int row1, uint32_t* __restrict__ counts,
-                                            const u64* __restrict__ offsets, u64* __restrict__ records) {
+// Setup of face f (vertex indices local to vfix; vproj rows = vert_base + index).
+__device__ __forceinline__ bool raster_setup(uint32_t f, const uint4* __restrict__ faces,
+                                             const int2* __restrict__ vfix, uint32_t vert_base, int W, int row0,
+                                             int row1, u64 pix_base, RasterJob& J) {
     const uint4 fc = faces[f];
     const int2 q0 = vfix[fc.x], q1 = vfix[fc.y], q2 = vfix[fc.z];
-    if (q0.x == kInvalidFix || q1.x == kInvalidFix || q2.x == kInvalidFix) return;
+    if (q0.x == kInvalidFix || q1.x == kInvalidFix || q2.x == kInvalidFix) return false;
     const long long X0 = q0.x, Y0 = q0.y, X1 = q1.x, Y1 = q1.y, X2 = q2.x, Y2 = q2.y;
     const long long area2 = (X1 - X0) * (Y2 - Y0) - (Y1 - Y0) * (X2 - X0);
-    if (area2 == 0) return;
-    const uint32_t front = area2 < 0 ? 1u : 0u;
-    const uint32_t bits = (f << 2) | ((fc.w & 1u) << 1) | front;
-    long long ax1 = X1, ay1 = Y1, ax2 = X2, ay2 = Y2;
-    if (area2 < 0) {
-        ax1 = X2; ay1 = Y2;
-        ax2 = X1; ay2 = Y1;
-    }
+    if (area2 == 0) return false;
     const long long minX = min(X0, min(X1, X2)), maxX = max(X0, max(X1, X2));
     const long long minY = min(Y0, min(Y1, Y2)), maxY = max(Y0, max(Y1, Y2));
     const int px0 = int(max(0LL, ceil_div256(minX - 128)));
     const int px1 = int(min((long long)W - 1, floor_div256(maxX - 128)));
     const int py0 = int(max((long long)row0, ceil_div256(minY - 128)));
     const int py1 = int(min((long long)row1 - 1, floor_div256(maxY - 128)));
-    if (px0 > px1 || py0 > py1) return;
+    if (px0 > px1 || py0 > py1) return false;
     const long long Xs = 256LL * px0 + 128, Ys = 256LL * py0 + 128;
-    if (maxX - minX < (1LL << 14) && maxY - minY < (1LL << 14)) {
-        raster_box<FILL, int>(fc, bits, int(X0 - minX), int(Y0 - minY), int(ax1 - minX), int(ay1 - minY),
-                              int(ax2 - minX), int(ay2 - minY), int(Xs - minX), int(Ys - minY), px0, px1, py0, py1,
-                              vproj, W, counts, offsets, records);
+    // Counter-clockwise order (E > 0 inside): swap vertices 1 and 2 of a front face.
+    const bool front = area2 < 0;
+    J.ax0 = int(X0 - Xs);
+    J.ay0 = int(Y0 - Ys);
+    J.ax1 = int((front ? X2 : X1) - Xs);
+    J.ay1 = int((front ? Y2 : Y1) - Ys);
+    J.ax2 = int((front ? X1 : X2) - Xs);
+    J.ay2 = int((front ? Y1 : Y2) - Ys);
+    J.px0 = px0;
+    J.py0 = py0;
+    J.bw = px1 - px0 + 1;
+    J.bh = py1 - py0 + 1;
+    J.bits = (f << 2) | ((fc.w & 1u) << 1) | (front ? 1u : 0u);
+    J.v0 = vert_base + fc.x;
+    J.v1 = vert_base + fc.y;
+    J.v2 = vert_base + fc.z;
+    J.W = W;
+    J.wide = (maxX - minX < (1LL << 14) && maxY - minY < (1LL << 14)) ? 0 : 1;
+    J.pix_base = pix_base;
+    return true;
+}
+
+// Pixel (c, r) of job J's box: coverage test and count / record write.  U
+// pixels per lane per step so the fill's offset loads, counter atomics and
+// depth keys of both issue before the stores.
+template <bool FILL, typename I, int U>
+__device__ __forceinline__ void raster_pixels(const RasterJob& J, const int (&c)[U], const int (&r)[U],
+                                              const bool (&valid)[U], I B0, I B1, I B2, I dx0, I dy0, I dx1, I dy1,
+                                              I dx2, I dy2, const float4& va, const float4& vb, const float4& vc,
+                                              uint32_t* __restrict__ counts, const u64* __restrict__ offsets,
+                                              u64* __restrict__ records) {
+    bool in[U];
+    u64 p[U];
+#pragma unroll
+    for (int k = 0; k < U; ++k) {
+        const I X = I(c[k]) * I(256), Y = I(r[k]) * I(256);
+        in[k] = valid[k] && edge_in<I>(B0 + dx0 * Y - dy0 * X, dx0, dy0) &&
+                edge_in<I>(B1 + dx1 * Y - dy1 * X, dx1, dy1) && edge_in<I>(B2 + dx2 * Y - dy2 * X, dx2, dy2);
+        p[k] = J.pix_base + u64(J.py0 + r[k]) * u64(J.W) + u64(J.px0 + c[k]);
+    }
+    if (FILL) {
+        uint32_t slot[U];
+        u64 off[U];
+        float z[U];
+#pragma unroll
+        for (int k = 0; k < U; ++k) {
+            if (in[k]) {
+                off[k] = offsets[p[k]];
+                slot[k] = atomicSub(&counts[p[k]], 1u);
+                z[k] = depth_key(va, vb, vc, float(J.px0 + c[k]) + 0.5f, float(J.py0 + r[k]) + 0.5f);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < U; ++k)
+            if (in[k]) records[off[k] + slot[k] - 1u] = (u64(__float_as_uint(z[k])) << 32) | J.bits;
     } else {
-        raster_box<FILL, long long>(fc, bits, X0, Y0, ax1, ay1, ax2, ay2, Xs, Ys, px0, px1, py0, py1, vproj, W,
-                                    counts, offsets, records);
+#pragma unroll
+        for (int k = 0; k < U; ++k)
+            if (in[k]) atomicAdd(&counts[p[k]], 1u);
+    }
+}
+
+// Box pixel k -> (column, row).  For boxes of at most 2^21 pixels the row is
+// floor((k + 1/2) * rn(1/bw)) in FP32: k + 1/2 is exact, the product is within
+// 2^-23 relative of (k + 1/2) / bw, i.e. within rows * 2^-23 < 1/(4 bw) of it,
+// while (k + 1/2) / bw is at least 1/(2 bw) away from every integer.
+template <bool FILL, typename I>
+__device__ __forceinline__ void raster_job(const RasterJob& J, int lane, const float4* __restrict__ vproj,
+                                           uint32_t* __restrict__ counts, const u64* __restrict__ offsets,
+                                           u64* __restrict__ records) {
+    constexpr int U = sizeof(I) == 4 ? 2 : 1;  // one pixel per step on the rare 64-bit path
+    const I dx0 = I(J.ax2) - I(J.ax1), dy0 = I(J.ay2) - I(J.ay1);
+    const I dx1 = I(J.ax0) - I(J.ax2), dy1 = I(J.ay0) - I(J.ay2);
+    const I dx2 = I(J.ax1) - I(J.ax0), dy2 = I(J.ay1) - I(J.ay0);
+    // Edge functions at the first pixel centre (the origin).
+    const I B0 = dy0 * I(J.ax1) - dx0 * I(J.ay1);
+    const I B1 = dy1 * I(J.ax2) - dx1 * I(J.ay2);
+    const I B2 = dy2 * I(J.ax0) - dx2 * I(J.ay0);
+    float4 va = make_float4(0.f, 0.f, 0.f, 0.f), vb = va, vc = va;
+    if (FILL) {
+        va = vproj[J.v0];
+        vb = vproj[J.v1];
+        vc = vproj[J.v2];
+    }
+    const int area = J.bw * J.bh;
+    if (area <= (1 << 21)) {
+        const float inv = __frcp_rn(float(J.bw));
+        for (int base = 0; base < area; base += 32 * U) {
+            int c[U], r[U];
+            bool valid[U];
+#pragma unroll
+            for (int k = 0; k < U; ++k) {
+                const int idx = base + 32 * k + lane;
+                valid[k] = idx < area;
+                r[k] = __float2int_rz(__fmul_rn(__fadd_rn(float(idx), 0.5f), inv));
+                c[k] = idx - r[k] * J.bw;
+            }
+            raster_pixels<FILL, I, U>(J, c, r, valid, B0, B1, B2, dx0, dy0, dx1, dy1, dx2, dy2, va, vb, vc, counts,
+                                      offsets, records);
+        }
+    } else {
+        for (int row = 0; row < J.bh; ++row)
+            for (int col = 0; col < J.bw; col += 32 * U) {
+                int c[U], r[U];
+                bool valid[U];
+#pragma unroll
+                for (int k = 0; k < U; ++k) {
+                    c[k] = col + 32 * k + lane;
+                    r[k] = row;
+                    valid[k] = c[k] < J.bw;
+                }
+                raster_pixels<FILL, I, U>(J, c, r, valid, B0, B1, B2, dx0, dy0, dx1, dy1, dx2, dy2, va, vb, vc,
+                                          counts, offsets, records);
+            }
+    }
+}
+
+// The warp's jobs (one per lane that has one, `live` the ballot), one at a time.
+// The 32-bit and 64-bit faces go to separate launches (WIDE), so that the
+// common 32-bit kernel keeps the register count of its own path.
+template <bool FILL, bool WIDE>
+__device__ __forceinline__ void raster_warp(const RasterJob* jobs, uint32_t live, int lane,
+                                            const float4* __restrict__ vproj, uint32_t* __restrict__ counts,
+                                            const u64* __restrict__ offsets, u64* __restrict__ records) {
+    __syncwarp();
+    while (live) {
+        const int k = __ffs(live) - 1;
+        live &= live - 1;
+        const RasterJob J = jobs[k];
+        raster_job<FILL, typename std::conditional<WIDE, long long, int>::type>(J, lane, vproj, counts, offsets,
+                                                                                records);
     }
 }
 
@@ -136,13 +203,13 @@ struct FragV {
     uint32_t v0, v1, v2;
 };
 
-__device__ __forceinline__ FragV load_frag(u64 rec, float qx, float qy, const uint4* __restrict__ faces,
-                                           const VGeo* __restrict__ vgeo, const float4* __restrict__ colors) {
+// Fragment values from the record's low word (face << 2 | bits) and the
+// face's vertex indices.
+__device__ __forceinline__ FragV load_frag_face(uint32_t lo, const uint4& fc, float qx, float qy,
+                                                const VGeo* __restrict__ vgeo, const float4* __restrict__ colors) {
     FragV fr;
-    const uint32_t lo = uint32_t(rec);
     fr.face = lo >> 2;
     fr.bits = lo & 3u;
-    const uint4 fc = faces[fr.face];
     fr.v0 = fc.x;
     fr.v1 = fc.y;
     fr.v2 = fc.z;
@@ -155,6 +222,17 @@ __device__ __forceinline__ FragV load_frag(u64 rec, float qx, float qy, const ui
                          bary[0] * c0.z + bary[1] * c1.z + bary[2] * c2.z,
                          bary[0] * c0.w + bary[1] * c1.w + bary[2] * c2.w);
     return fr;
+}
+
+__device__ __forceinline__ FragV load_frag(u64 rec, float qx, float qy, const uint4* __restrict__ faces,
+                                           const VGeo* __restrict__ vgeo, const float4* __restrict__ colors) {
+    const uint32_t lo = uint32_t(rec);
+    return load_frag_face(lo, faces[lo >> 2], qx, qy, vgeo, colors);
+}
+
+// Low word of record i of a list (the face and its two flag bits).
+__device__ __forceinline__ uint32_t record_lo(const u64* __restrict__ records, u64 i) {
+    return reinterpret_cast<const uint32_t*>(records)[2 * i];
 }
 
 // ---------------------------------------------------------------------------
@@ -395,11 +473,22 @@ __device__ __forceinline__ void adjoint_pixel(
     if (last < 1) return;
     const float atten = sh.atten;
     const bool use_abs = sh.use_abs_grad != 0;
+    // The dependent loads record -> face -> vertex rows are software-pipelined:
+    // while fragment i's segment is processed, the face of fragment i-2 and the
+    // record of fragment i-3 are already in flight.
     FragV fb = load_frag(records[beg + last], qx, qy, faces, vgeo, colors);
+    uint32_t lo_f = record_lo(records, beg + last - 1);
+    uint4 fc_f = faces[lo_f >> 2];
+    uint32_t lo_n = last >= 2 ? record_lo(records, beg + last - 2) : 0u;
     float gz_b = 0.f;
     float4 gcol_b = make_float4(0.f, 0.f, 0.f, 0.f);
     for (int i = last; i >= 1; --i) {
-        const FragV ff = load_frag(records[beg + i - 1], qx, qy, faces, vgeo, colors);
+        const FragV ff = load_frag_face(lo_f, fc_f, qx, qy, vgeo, colors);
+        if (i >= 2) {
+            fc_f = faces[lo_n >> 2];
+            lo_f = lo_n;
+            if (i >= 3) lo_n = record_lo(records, beg + i - 3);
+        }
         float gz_f = 0.f;
         float4 gcol_f = make_float4(0.f, 0.f, 0.f, 0.f);
         if (!skip_pair(ff.bits, fb.bits)) {

@@ -43,6 +43,7 @@ class Request:
     t_finish: float = 0.0
     batch_id: int = -1
     batch_size: int = 0
+    info: dict = field(default_factory=dict)   # backend's per-batch figures (enqueue / device time, rerun)
     future: Future = field(default_factory=Future, repr=False)
 
     @property
@@ -201,7 +202,8 @@ class ServingEngine:
                 "batches": self.batches, "rejected": self.rejected,
                 "slowest": [{"ms": round(float(lat[i]), 3), "queue_ms": round(float(wait[i]), 3),
                              "batch": done[i].batch_id, "batch_size": done[i].batch_size,
-                             "mesh": done[i].mesh, "pixels": done[i].pixels, "mode": done[i].mode}
+                             "mesh": done[i].mesh, "pixels": done[i].pixels, "mode": done[i].mode,
+                             **done[i].info}
                             for i in worst]}
 
 
@@ -242,14 +244,31 @@ class GpuBackend:
         stream.synchronize()
         return handle
 
-    def reserve(self, max_batch: int, max_pixels_per_request: int, budget_fragments: int) -> None:
+    def reserve(self, max_batch: int, max_pixels_per_request: int, budget_fragments: int,
+                result_batches: int = 4) -> None:
         """Sizes every slot's scratch for the largest admissible batch, so no
-        device allocation (which synchronises the whole device) happens while
-        serving."""
+        device allocation (an implicit synchronisation of the whole device,
+        which would wait for the other slots' batches) happens while serving.
+        The library's scratch is reserved directly; the per-request tensors
+        (images, image adjoints, gradients) come from PyTorch's caching
+        allocator, whose pool of each slot stream is grown here to hold
+        `result_batches` full batches of them at once."""
+        torch = self.torch
         maxV = max(m.get_num_vertices() for m in self.meshes)
         for br in self.renderers:
             br.reserve(max_batch, max_batch * maxV, max_batch * max_pixels_per_request, budget_fragments,
                        max_batch * maxV)
+        per_batch = max_batch * (2 * 16 * max_pixels_per_request + 28 * maxV)
+        dev = self.meshes[0].get_vertex_positions().device
+        for st in self.streams:
+            with torch.cuda.stream(st):
+                block = torch.empty(result_batches * per_batch, dtype=torch.uint8, device=dev)
+                # Tensors under 1 MiB (small meshes' gradients, losses) come
+                # from the allocator's separate pool of 2 MiB segments.
+                small = [torch.empty(1 << 19, dtype=torch.uint8, device=dev)
+                         for _ in range(4 * result_batches * max_batch)]
+                del block, small
+        torch.cuda.synchronize()
         self._reserved = True
 
     def fragments_per_pixel(self, mesh: str) -> float:
@@ -275,10 +294,14 @@ class GpuBackend:
                       fovy=r.fovy) for r in reqs]
         grads = []
         reserved = getattr(self, "_reserved", False)
+        t0, c0 = time.perf_counter(), time.thread_time()
         with torch.cuda.stream(stream):
+            ev0 = torch.cuda.Event(enable_timing=True)
+            ev0.record(stream)
             # With reserved scratch the batch is enqueued without a host
             # synchronisation; finish() checks that it fit.
             (br.render_async if reserved else br.render)(views)
+            t1 = time.perf_counter()
             slots = []
             for i, (r, v) in enumerate(zip(reqs, views)):
                 if r.mode == "gradient":
@@ -290,30 +313,45 @@ class GpuBackend:
                     gc = torch.zeros_like(m.get_vertex_colors(), memory_format=torch.contiguous_format)
                     slots.append((v.mesh, gp.detach(), gc.detach()))
                     grads.append((i, gp, gc))
+            t2 = time.perf_counter()
             if slots:
                 br.render_adjoint([(m, gp, gc) for (m, gp, gc) in slots])
-            ev = torch.cuda.Event()
+            ev = torch.cuda.Event(enable_timing=True)
             ev.record(stream)
+        t3 = time.perf_counter()
         px = sum(r.pixels for r in reqs)
-        return {"event": ev, "views": views, "reqs": reqs, "grads": grads, "pixels": px, "slot": slot,
-                "async": reserved}
+        # Host time of the enqueue: forward, adjoint inputs, adjoint; and the
+        # engine thread's CPU time over it (wall >> CPU: the thread was blocked).
+        parts = [round((b - a) * 1e3, 3) for a, b in ((t0, t1), (t1, t2), (t2, t3))]
+        return {"event": ev, "start_event": ev0, "enqueue_ms": (t3 - t0) * 1e3, "enqueue_parts_ms": parts,
+                "enqueue_cpu_ms": round((time.thread_time() - c0) * 1e3, 3), "views": views,
+                "reqs": reqs, "grads": grads, "pixels": px, "slot": slot, "async": reserved}
 
     def done(self, handle) -> bool:
         return handle["event"].query()
 
     def finish(self, handle) -> list[Result]:
+        tf = time.perf_counter()
         handle["event"].synchronize()
         reqs, views = handle["reqs"], handle["views"]
         br = self.renderers[handle["slot"]]
+        info = {"enqueue_ms": round(handle["enqueue_ms"], 3), "enqueue_parts_ms": handle["enqueue_parts_ms"],
+                "enqueue_cpu_ms": handle["enqueue_cpu_ms"],
+                "device_ms": round(handle["start_event"].elapsed_time(handle["event"]), 3), "rerun": False}
         if handle["async"]:
             fits, nf = br.render_status()
             if not fits:
                 # Over the reserved capacity: run the batch again with exact sizing.
+                t0 = time.perf_counter()
                 handle = self._rerun(handle)
                 nf = br.info()["fragments"]
+                info.update(rerun=True, rerun_ms=round((time.perf_counter() - t0) * 1e3, 3))
             handle["fragments"] = nf
         else:
             handle["fragments"] = br.info()["fragments"]
+        info["fragments"] = int(handle["fragments"])
+        for r in reqs:
+            r.info = info
         # Per-mesh fragments-per-pixel estimate from the exact batch count.
         by_mesh = {}
         for r in reqs:
@@ -334,4 +372,5 @@ class GpuBackend:
         for i, (r, v) in enumerate(zip(reqs, views)):
             gp, gc = g.get(i, (None, None))
             out.append(Result(r.id, v.image, gp, gc, losses.get(i)))
+        info["finish_ms"] = round((time.perf_counter() - tf) * 1e3, 3)
         return out

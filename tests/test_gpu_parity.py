@@ -25,7 +25,9 @@ def _oracle_all(O, sc, w=None, ert=None):
     return out
 
 
-@pytest.mark.parametrize("n,res", [(8, 128), (16, 512), (32, 256)])
+# (2, 512): every face's box is over 64 px (64-bit edge functions);
+# (1, 3072): boxes of more than 2^21 pixels (row-by-row walk).
+@pytest.mark.parametrize("n,res", [(8, 128), (16, 512), (32, 256), (2, 512), (1, 3072)])
 def test_fragment_lists_bit_exact(oracle, n, res):
     sc = Scene(n, res, seed=n)
     mesh, r = sc.make_renderer()
