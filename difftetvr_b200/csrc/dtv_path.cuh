@@ -81,23 +81,39 @@ __device__ __forceinline__ bool raster_setup(uint32_t f, const uint4* __restrict
     return true;
 }
 
-// Pixel (c, r) of job J's box: coverage test and count / record write.  U
-// pixels per lane per step so the fill's offset loads, counter atomics and
-// depth keys of both issue before the stores.
+// Edge function of one edge over the box, with the coverage tie rule folded
+// in: for integer E, "E > 0, or E == 0 and the edge is a top-left edge
+// (dy < 0, or dy == 0 and dx > 0)" is "E + t - 1 >= 0" with t = 1 for a
+// top-left edge, 0 otherwise.  T(c, r) = base + sx c + sy r is that shifted
+// value at pixel (c, r) of the box, so a pixel is covered iff the three
+// values are all non-negative, i.e. iff the sign bit of their OR is clear.
+template <typename I>
+struct EdgeT {
+    I base, sx, sy;
+    __device__ __forceinline__ void set(I ax, I ay, I bx, I by) {  // edge a -> b
+        const I dx = bx - ax, dy = by - ay;
+        const I t = ((dy < 0) || (dy == 0 && dx > 0)) ? I(1) : I(0);
+        base = dy * ax - dx * ay + t - I(1);  // E at the origin: dx (0 - ay) - dy (0 - ax)
+        sx = -dy * I(256);
+        sy = dx * I(256);
+    }
+    __device__ __forceinline__ I at(int c, int r) const { return base + sx * I(c) + sy * I(r); }
+};
+
+// U pixels of job J's box per lane per step: coverage tests, then (FILL) the
+// offset loads, counter atomics and depth keys of all U before the stores.
 template <bool FILL, typename I, int U>
 __device__ __forceinline__ void raster_pixels(const RasterJob& J, const int (&c)[U], const int (&r)[U],
-                                              const bool (&valid)[U], I B0, I B1, I B2, I dx0, I dy0, I dx1, I dy1,
-                                              I dx2, I dy2, const float4& va, const float4& vb, const float4& vc,
-                                              uint32_t* __restrict__ counts, const u64* __restrict__ offsets,
-                                              u64* __restrict__ records) {
+                                              const bool (&valid)[U], const EdgeT<I>& e0, const EdgeT<I>& e1,
+                                              const EdgeT<I>& e2, u64 pbase, const float4& va, const float4& vb,
+                                              const float4& vc, uint32_t* __restrict__ counts,
+                                              const u64* __restrict__ offsets, u64* __restrict__ records) {
     bool in[U];
     u64 p[U];
 #pragma unroll
     for (int k = 0; k < U; ++k) {
-        const I X = I(c[k]) * I(256), Y = I(r[k]) * I(256);
-        in[k] = valid[k] && edge_in<I>(B0 + dx0 * Y - dy0 * X, dx0, dy0) &&
-                edge_in<I>(B1 + dx1 * Y - dy1 * X, dx1, dy1) && edge_in<I>(B2 + dx2 * Y - dy2 * X, dx2, dy2);
-        p[k] = J.pix_base + u64(J.py0 + r[k]) * u64(J.W) + u64(J.px0 + c[k]);
+        in[k] = valid[k] && (e0.at(c[k], r[k]) | e1.at(c[k], r[k]) | e2.at(c[k], r[k])) >= I(0);
+        p[k] = pbase + uint32_t(r[k] * J.W + c[k]);
     }
     if (FILL) {
         uint32_t slot[U];
@@ -121,58 +137,128 @@ __device__ __forceinline__ void raster_pixels(const RasterJob& J, const int (&c)
     }
 }
 
-// Box pixel k -> (column, row).  For boxes of at most 2^21 pixels the row is
-// floor((k + 1/2) * rn(1/bw)) in FP32: k + 1/2 is exact, the product is within
-// 2^-23 relative of (k + 1/2) / bw, i.e. within rows * 2^-23 < 1/(4 bw) of it,
-// while (k + 1/2) / bw is at least 1/(2 bw) away from every integer.
+// Conservative column range of row r for one edge: T(c, r) >= 0 is
+// c >= -q / sx (sx > 0) or c <= -q / sx (sx < 0), q = base + sy r; sx = 0
+// makes the row all-in or all-out.  The bound is taken in FP32 (relative
+// error a few 2^-24, below 0.01 px for every bound inside the box) and the
+// caller widens the range by one pixel on each side, so it holds every
+// covered pixel; each pixel of the range is then tested exactly.
+template <typename I>
+__device__ __forceinline__ void span_edge(const EdgeT<I>& e, float inv_sx, int r, float& lo, float& hi,
+                                          bool& empty) {
+    const I q = e.base + e.sy * I(r);
+    if (e.sx == I(0)) {
+        empty |= q < I(0);
+    } else {
+        const float b = -float(q) * inv_sx;
+        if (e.sx > I(0))
+            lo = fmaxf(lo, b);
+        else
+            hi = fminf(hi, b);
+    }
+}
+
+// Count pass over a face whose box is under 64 px a side: box pixel k goes
+// to lane k mod 32, two pixels per lane per step.  Row of pixel k:
+// floor((k + 1/2) * rn(1/bw)) in FP32 -- k + 1/2 is exact (k < 2^12), the
+// product is within 2^-23 relative of (k + 1/2) / bw, i.e. within
+// rows * 2^-23 < 1/(4 bw) of it, while (k + 1/2) / bw is at least 1/(2 bw)
+// away from every integer.
+__device__ __forceinline__ void count_job_box(const RasterJob& J, int lane, uint32_t* __restrict__ counts) {
+    constexpr int U = 2;
+    EdgeT<int> e0, e1, e2;
+    e0.set(J.ax1, J.ay1, J.ax2, J.ay2);
+    e1.set(J.ax2, J.ay2, J.ax0, J.ay0);
+    e2.set(J.ax0, J.ay0, J.ax1, J.ay1);
+    const u64 pbase = J.pix_base + u64(J.py0) * u64(J.W) + u64(J.px0);
+    const float4 none = make_float4(0.f, 0.f, 0.f, 0.f);
+    const int area = J.bw * J.bh;
+    const float inv = __frcp_rn(float(J.bw));
+    for (int base = 0; base < area; base += 32 * U) {
+        int c[U], r[U];
+        bool valid[U];
+#pragma unroll
+        for (int k = 0; k < U; ++k) {
+            const int idx = base + 32 * k + lane;
+            valid[k] = idx < area;
+            r[k] = __float2int_rz(__fmul_rn(__fadd_rn(float(idx), 0.5f), inv));
+            c[k] = idx - r[k] * J.bw;
+        }
+        raster_pixels<false, int, U>(J, c, r, valid, e0, e1, e2, pbase, none, none, none, counts, nullptr,
+                                     nullptr);
+    }
+}
+
+// One face: the warp takes the box rows 32 at a time (lane = row), finds each
+// row's candidate span, and spreads the concatenated spans over its lanes
+// (slot s -> row by a binary search of the spans' exclusive prefix sums).
+// Fewer slots than the whole box (about the covered pixels plus two per row)
+// for more work per face: used by the fill, whose covered pixels dominate,
+// and for 64-bit faces; the count of 32-bit faces walks the box.
 template <bool FILL, typename I>
 __device__ __forceinline__ void raster_job(const RasterJob& J, int lane, const float4* __restrict__ vproj,
                                            uint32_t* __restrict__ counts, const u64* __restrict__ offsets,
                                            u64* __restrict__ records) {
+    if (!FILL && sizeof(I) == 4) {
+        count_job_box(J, lane, counts);
+        return;
+    }
     constexpr int U = sizeof(I) == 4 ? 2 : 1;  // one pixel per step on the rare 64-bit path
-    const I dx0 = I(J.ax2) - I(J.ax1), dy0 = I(J.ay2) - I(J.ay1);
-    const I dx1 = I(J.ax0) - I(J.ax2), dy1 = I(J.ay0) - I(J.ay2);
-    const I dx2 = I(J.ax1) - I(J.ax0), dy2 = I(J.ay1) - I(J.ay0);
-    // Edge functions at the first pixel centre (the origin).
-    const I B0 = dy0 * I(J.ax1) - dx0 * I(J.ay1);
-    const I B1 = dy1 * I(J.ax2) - dx1 * I(J.ay2);
-    const I B2 = dy2 * I(J.ax0) - dx2 * I(J.ay0);
+    // Counter-clockwise edges e0: 1 -> 2, e1: 2 -> 0, e2: 0 -> 1.
+    EdgeT<I> e0, e1, e2;
+    e0.set(I(J.ax1), I(J.ay1), I(J.ax2), I(J.ay2));
+    e1.set(I(J.ax2), I(J.ay2), I(J.ax0), I(J.ay0));
+    e2.set(I(J.ax0), I(J.ay0), I(J.ax1), I(J.ay1));
+    const float i0 = e0.sx != I(0) ? __frcp_rn(float(e0.sx)) : 0.f;
+    const float i1 = e1.sx != I(0) ? __frcp_rn(float(e1.sx)) : 0.f;
+    const float i2 = e2.sx != I(0) ? __frcp_rn(float(e2.sx)) : 0.f;
+    const u64 pbase = J.pix_base + u64(J.py0) * u64(J.W) + u64(J.px0);
     float4 va = make_float4(0.f, 0.f, 0.f, 0.f), vb = va, vc = va;
     if (FILL) {
         va = vproj[J.v0];
         vb = vproj[J.v1];
         vc = vproj[J.v2];
     }
-    const int area = J.bw * J.bh;
-    if (area <= (1 << 21)) {
-        const float inv = __frcp_rn(float(J.bw));
-        for (int base = 0; base < area; base += 32 * U) {
-            int c[U], r[U];
+    const float wmax = float(J.bw - 1);
+    for (int r0 = 0; r0 < J.bh; r0 += 32) {
+        const int r = r0 + lane;
+        int xl = 0, len = 0;
+        if (r < J.bh) {
+            float lo = 0.f, hi = wmax;
+            bool empty = false;
+            span_edge(e0, i0, r, lo, hi, empty);
+            span_edge(e1, i1, r, lo, hi, empty);
+            span_edge(e2, i2, r, lo, hi, empty);
+            if (!empty) {
+                xl = max(0, int(fminf(lo, wmax + 1.f)) - 1);               // lo >= 0: int() is floor
+                const int xr = min(J.bw - 1, int(floorf(fmaxf(hi, -1.f))) + 1);
+                len = max(0, xr - xl + 1);
+            }
+        }
+        int incl = len;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        const int excl = incl - len;
+        const int total = __shfl_sync(0xffffffffu, incl, 31);
+        for (int s0 = 0; s0 < total; s0 += 32 * U) {
+            int c[U], rr[U];
             bool valid[U];
 #pragma unroll
             for (int k = 0; k < U; ++k) {
-                const int idx = base + 32 * k + lane;
-                valid[k] = idx < area;
-                r[k] = __float2int_rz(__fmul_rn(__fadd_rn(float(idx), 0.5f), inv));
-                c[k] = idx - r[k] * J.bw;
-            }
-            raster_pixels<FILL, I, U>(J, c, r, valid, B0, B1, B2, dx0, dy0, dx1, dy1, dx2, dy2, va, vb, vc, counts,
-                                      offsets, records);
-        }
-    } else {
-        for (int row = 0; row < J.bh; ++row)
-            for (int col = 0; col < J.bw; col += 32 * U) {
-                int c[U], r[U];
-                bool valid[U];
+                const int sl = s0 + 32 * k + lane;
+                int i = 0;  // last row whose span starts at or before slot sl
 #pragma unroll
-                for (int k = 0; k < U; ++k) {
-                    c[k] = col + 32 * k + lane;
-                    r[k] = row;
-                    valid[k] = c[k] < J.bw;
-                }
-                raster_pixels<FILL, I, U>(J, c, r, valid, B0, B1, B2, dx0, dy0, dx1, dy1, dx2, dy2, va, vb, vc,
-                                          counts, offsets, records);
+                for (int step = 16; step >= 1; step >>= 1)
+                    if (__shfl_sync(0xffffffffu, excl, i + step) <= sl) i += step;
+                valid[k] = sl < total;
+                rr[k] = r0 + i;
+                c[k] = __shfl_sync(0xffffffffu, xl, i) + (sl - __shfl_sync(0xffffffffu, excl, i));
             }
+            raster_pixels<FILL, I, U>(J, c, rr, valid, e0, e1, e2, pbase, va, vb, vc, counts, offsets, records);
+        }
     }
 }
 

@@ -1,8 +1,8 @@
-"""Box pixel index -> (row, column) map of the warp-cooperative rasteriser:
-row = trunc(rn(rn(k + 1/2) * rn(1/bw))) in FP32 equals floor(k / bw) for every
-box of at most 2^21 pixels (the kernel walks larger boxes row by row).  FP32
-arithmetic here is IEEE round-to-nearest, as the kernel's __fadd_rn,
-__fmul_rn and __frcp_rn."""
+"""Box pixel index -> (row, column) map of the warp-cooperative count pass:
+row = trunc(rn(rn(k + 1/2) * rn(1/bw))) in FP32 equals floor(k / bw).  The
+kernel uses it for boxes under 64 px a side (k < 2^12); it holds for every box
+of at most 2^21 pixels, checked here.  FP32 arithmetic here is IEEE
+round-to-nearest, as the kernel's __fadd_rn, __fmul_rn and __frcp_rn."""
 import numpy as np
 
 MAX_AREA = 1 << 21
