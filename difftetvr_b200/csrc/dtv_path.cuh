@@ -322,6 +322,29 @@ __device__ __forceinline__ uint32_t record_lo(const u64* __restrict__ records, u
 }
 
 // ---------------------------------------------------------------------------
+// One segment of a pixel's ray between a front fragment (colour cf) and a back
+// fragment (colour cb): the 4-sub-segment integral (ForwardCommon.glsl:42-49
+// per sub-segment, colour and density linear along the segment), front to
+// back.  Per sub-segment starting at fraction s, c0 = cf + s (cb - cf) and
+// c1 - c0 = (cb - cf) / 4, so C += T ((1 - A) c0 - (K / 4) (cb - cf)).
+__device__ __forceinline__ void segment_composite(float tSeg, const float4& cf, const float4& cb, float atten,
+                                                  float& C0, float& C1, float& C2, float& T) {
+    const float d0 = cb.x - cf.x, d1 = cb.y - cf.y, d2 = cb.z - cf.z, dw = cb.w - cf.w;
+#pragma unroll
+    for (int s = 0; s < kNumSubdivs; ++s) {
+        const float fs = 0.25f * s, fm = 0.25f * (s + 0.5f);
+        const float a = (cf.w + dw * fm) * atten;
+        if (!(a > 0.f)) continue;  // a <= 0 contributes nothing
+        const SegTerms st = seg_terms(tSeg, a);
+        const float w = T * st.omA, k = T * (0.25f * st.K);
+        C0 += w * (cf.x + d0 * fs) - k * d0;
+        C1 += w * (cf.y + d1 * fs) - k * d1;
+        C2 += w * (cf.z + d2 * fs) - k * d2;
+        T *= st.A;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // (d) front-to-back compositing, one thread per pixel (16x16 pixel tiles).
 // Forward.glsl:159-211 with early ray termination (:169-173) and the
 // termination index (:256-259); final transmittance is kept for the adjoint.
@@ -342,20 +365,7 @@ __device__ __forceinline__ void composite_pixel(
             f0 = f1;
             f1 = load_frag(records[beg + i], qx, qy, faces, vgeo, colors);
             if (skip_pair(f0.bits, f1.bits)) continue;
-            const float tSeg = (f1.z - f0.z) * 0.25f;
-#pragma unroll
-            for (int s = 0; s < kNumSubdivs; ++s) {
-                const float fb = 0.25f * s, fm = 0.25f * (s + 0.5f), fe = 0.25f * (s + 1);
-                const float4 c0 = lerp4(f0.col, f1.col, fb);
-                const float4 c1 = lerp4(f0.col, f1.col, fe);
-                const float a = (f0.col.w + (f1.col.w - f0.col.w) * fm) * sh.atten;
-                if (!(a > 0.f)) continue;  // a <= 0 contributes nothing
-                const SegTerms st = seg_terms(tSeg, a);
-                C0 += T * (st.omA * c0.x + st.K * (c0.x - c1.x));
-                C1 += T * (st.omA * c0.y + st.K * (c0.y - c1.y));
-                C2 += T * (st.omA * c0.z + st.K * (c0.z - c1.z));
-                T *= st.A;
-            }
+            segment_composite((f1.z - f0.z) * 0.25f, f0.col, f1.col, sh.atten, C0, C1, C2, T);
         }
     }
     image[p] = make_float4(C0 + T * sh.clear[0], C1 + T * sh.clear[1], C2 + T * sh.clear[2],
@@ -445,45 +455,52 @@ __device__ __forceinline__ void frag_vertex_grads(const FragV& fr, float qx, flo
     }
 }
 
-// Adjoint of one sub-segment (colour c0 -> c1, density a, length tSeg) of
-// the 4-sub-segment integral.  T holds the transmittance after the segment and
-// is rebuilt in place to the one before it (T_in = T_out / A); gT is the
-// running transmittance adjoint.  Outputs: dL/dtSeg, dL/da and the colour
-// adjoints of both sub-segment ends.
-__device__ __forceinline__ void sub_segment_adjoint(float tSeg, float a, float4 c0, float4 c1, float gC0, float gC1,
-                                                    float gC2, float& T, float& gT, float& g_t, float& g_a,
-                                                    float& gc0x, float& gc0y, float& gc0z, float& gc1x, float& gc1y,
-                                                    float& gc1z) {
-    if (a > 0.f) {
-        const SegTerms st = seg_terms_adj(tSeg, a);
-        const float cx = st.omA * c0.x + st.K * (c0.x - c1.x);
-        const float cy = st.omA * c0.y + st.K * (c0.y - c1.y);
-        const float cz = st.omA * c0.z + st.K * (c0.z - c1.z);
-        const float Tin = __fdividef(T, st.A);
-        const float gax = Tin * gC0, gay = Tin * gC1, gaz = Tin * gC2;
-        const float gA = Tin * gT;
-        gT = (gC0 * cx + gC1 * cy + gC2 * cz) + gT * st.A;
-        T = Tin;
-        const float aA = a * st.A;
-        g_t = gax * (aA * (c0.x + tSeg * (c1.x - c0.x))) + gay * (aA * (c0.y + tSeg * (c1.y - c0.y))) +
-              gaz * (aA * (c0.z + tSeg * (c1.z - c0.z))) - gA * aA;
-        const float dK = st.dK;
-        const float tA = tSeg * st.A;
-        g_a = gax * (tA * c0.x + dK * (c0.x - c1.x)) + gay * (tA * c0.y + dK * (c0.y - c1.y)) +
-              gaz * (tA * c0.z + dK * (c0.z - c1.z)) - gA * tA;
-        const float k0 = st.omA + st.K;
-        gc0x = k0 * gax; gc0y = k0 * gay; gc0z = k0 * gaz;
-        gc1x = -st.K * gax; gc1y = -st.K * gay; gc1z = -st.K * gaz;
-    } else {
-        // The forward drops the sub-segment for a <= 0; the gradient is the
-        // a -> 0+ limit (BackwardCommon.glsl:121-125) so a density clamped at
-        // zero can grow again.
-        const float gax = T * gC0, gay = T * gC1, gaz = T * gC2, gA = T * gT;
-        g_t = 0.f;
-        g_a = gax * (tSeg * c0.x + 0.5f * tSeg * tSeg * (c1.x - c0.x)) +
-              gay * (tSeg * c0.y + 0.5f * tSeg * tSeg * (c1.y - c0.y)) +
-              gaz * (tSeg * c0.z + 0.5f * tSeg * tSeg * (c1.z - c0.z)) - gA * tSeg;
-        gc0x = gc0y = gc0z = gc1x = gc1y = gc1z = 0.f;
+// Adjoint of one segment of a pixel's ray between a front fragment (colour
+// cf) and a back fragment (colour cb), the 4-sub-segment integral taken back
+// to front.  T holds the transmittance after the segment and is rebuilt in
+// place to the one before it (T_in = T_out / A); gT is the running
+// transmittance adjoint.
+//
+// The pixel's colour adjoint gC = dL/dC.rgb enters every colour term through
+// dot products, so the sub-segment math runs on scalars: P0 = gC . c0 and
+// D = gC . (c1 - c0) for sub-segment colours c0 -> c1 (P0 and D are linear in
+// pf = gC . cf.rgb and pb = gC . cb.rgb), and the colour adjoint of each
+// fragment is gC times a scalar weight.  With A = exp(-a t), 1 - A and
+// K = (t + 1/a) A - 1/a (dtv_segment.cuh), C = (1 - A) c0 - K (c1 - c0):
+//   gT_in  = (1 - A) P0 - K D + gT A
+//   dL/dt  = a T_out (P0 + t D - gT)        dL/da = T_in (t A (P0 - gT) - dK/da D)
+//   colour weights: front += T_in ((1 - s) (1 - A) + K/4), back += T_in (s (1 - A) - K/4)
+// for a sub-segment starting at fraction s of the segment.  A sub-segment with
+// a <= 0 is dropped by the forward; its gradient is the a -> 0+ limit
+// (BackwardCommon.glsl:121-125) so a density clamped at zero can grow again.
+// Outputs (added): g_tot = dL/d(segment length), the colour weights wf / wb and
+// the alpha adjoints af / ab of the front / back fragment.
+__device__ __forceinline__ void segment_adjoint(float tSeg, const float4& cf, const float4& cb, float pf, float pb,
+                                                float atten, float& T, float& gT, float& g_tot, float& wf,
+                                                float& wb, float& af, float& ab) {
+    const float dp = pb - pf, D = 0.25f * dp, dw = cb.w - cf.w;
+#pragma unroll
+    for (int s = kNumSubdivs - 1; s >= 0; --s) {
+        const float fs = 0.25f * s, fm = 0.25f * (s + 0.5f);
+        const float P0 = pf + fs * dp;
+        const float a = (cf.w + dw * fm) * atten;
+        float g_a;
+        if (a > 0.f) {
+            const SegTerms st = seg_terms_adj(tSeg, a);
+            const float Tin = __fdividef(T, st.A);
+            const float gTo = gT;
+            gT = st.omA * P0 - st.K * D + gTo * st.A;
+            g_tot += 0.25f * (a * T) * (P0 + tSeg * D - gTo);
+            g_a = Tin * (tSeg * st.A * (P0 - gTo) - st.dK * D);
+            T = Tin;
+            const float qK = 0.25f * st.K, tw = Tin * st.omA;
+            wf += (1.f - fs) * tw + Tin * qK;
+            wb += fs * tw - Tin * qK;
+        } else {
+            g_a = T * (tSeg * (P0 - gT) + 0.5f * tSeg * tSeg * D);
+        }
+        af += (1.f - fm) * g_a * atten;
+        ab += fm * g_a * atten;
     }
 }
 
@@ -566,8 +583,10 @@ __device__ __forceinline__ void adjoint_pixel(
     uint32_t lo_f = record_lo(records, beg + last - 1);
     uint4 fc_f = faces[lo_f >> 2];
     uint32_t lo_n = last >= 2 ? record_lo(records, beg + last - 2) : 0u;
-    float gz_b = 0.f;
-    float4 gcol_b = make_float4(0.f, 0.f, 0.f, 0.f);
+    // Per fragment: depth adjoint, colour weight (colour adjoint = gC x weight)
+    // and alpha adjoint, of the back fragment (b) and the front one (f).
+    float pb = gC0 * fb.col.x + gC1 * fb.col.y + gC2 * fb.col.z;
+    float gz_b = 0.f, wb = 0.f, ab = 0.f;
     for (int i = last; i >= 1; --i) {
         const FragV ff = load_frag_face(lo_f, fc_f, qx, qy, vgeo, colors);
         if (i >= 2) {
@@ -575,39 +594,24 @@ __device__ __forceinline__ void adjoint_pixel(
             lo_f = lo_n;
             if (i >= 3) lo_n = record_lo(records, beg + i - 3);
         }
-        float gz_f = 0.f;
-        float4 gcol_f = make_float4(0.f, 0.f, 0.f, 0.f);
+        const float pf = gC0 * ff.col.x + gC1 * ff.col.y + gC2 * ff.col.z;
+        float gz_f = 0.f, wf = 0.f, af = 0.f;
         if (!skip_pair(ff.bits, fb.bits)) {
-            const float tSeg = (fb.z - ff.z) * 0.25f;
             float g_tot = 0.f;
-#pragma unroll
-            for (int s = kNumSubdivs - 1; s >= 0; --s) {
-                const float fbg = 0.25f * s, fm = 0.25f * (s + 0.5f), fe = 0.25f * (s + 1);
-                const float4 c0 = lerp4(ff.col, fb.col, fbg);
-                const float4 c1 = lerp4(ff.col, fb.col, fe);
-                const float a = (ff.col.w + (fb.col.w - ff.col.w) * fm) * atten;
-                float g_t, g_a, gc0x, gc0y, gc0z, gc1x, gc1y, gc1z;
-                sub_segment_adjoint(tSeg, a, c0, c1, gC0, gC1, gC2, T, gT, g_t, g_a, gc0x, gc0y, gc0z, gc1x, gc1y,
-                                    gc1z);
-                g_tot += 0.25f * g_t;
-                gcol_f.x += (1.f - fbg) * gc0x + (1.f - fe) * gc1x;
-                gcol_f.y += (1.f - fbg) * gc0y + (1.f - fe) * gc1y;
-                gcol_f.z += (1.f - fbg) * gc0z + (1.f - fe) * gc1z;
-                gcol_b.x += fbg * gc0x + fe * gc1x;
-                gcol_b.y += fbg * gc0y + fe * gc1y;
-                gcol_b.z += fbg * gc0z + fe * gc1z;
-                gcol_f.w += (1.f - fm) * g_a * atten;
-                gcol_b.w += fm * g_a * atten;
-            }
+            segment_adjoint((fb.z - ff.z) * 0.25f, ff.col, fb.col, pf, pb, atten, T, gT, g_tot, wf, wb, af, ab);
             gz_f -= g_tot;
             gz_b += g_tot;
         }
-        frag_vertex_grads(fb, qx, qy, vgeo, colors, cam, gz_b, gcol_b, use_abs, acc);
+        frag_vertex_grads(fb, qx, qy, vgeo, colors, cam, gz_b, make_float4(gC0 * wb, gC1 * wb, gC2 * wb, ab),
+                          use_abs, acc);
         fb = ff;
+        pb = pf;
         gz_b = gz_f;
-        gcol_b = gcol_f;
+        wb = wf;
+        ab = af;
     }
-    frag_vertex_grads(fb, qx, qy, vgeo, colors, cam, gz_b, gcol_b, use_abs, acc);
+    frag_vertex_grads(fb, qx, qy, vgeo, colors, cam, gz_b, make_float4(gC0 * wb, gC1 * wb, gC2 * wb, ab), use_abs,
+                      acc);
 }
 
 

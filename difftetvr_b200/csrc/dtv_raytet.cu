@@ -132,20 +132,7 @@ __global__ void __launch_bounds__(kTile * kTile, 2) k_walk_composite(
                 break;
             }
             const FragV f1 = load_frag(u64(fx) << 2, qx, qy, faces, vgeo, colors);
-            const float tSeg = (f1.z - f0.z) * scale * 0.25f;
-#pragma unroll
-            for (int s = 0; s < kNumSubdivs; ++s) {
-                const float fb = 0.25f * s, fm = 0.25f * (s + 0.5f), fe4 = 0.25f * (s + 1);
-                const float4 c0 = lerp4(f0.col, f1.col, fb);
-                const float4 c1 = lerp4(f0.col, f1.col, fe4);
-                const float a = (f0.col.w + (f1.col.w - f0.col.w) * fm) * sh.atten;
-                if (!(a > 0.f)) continue;
-                const SegTerms st = seg_terms(tSeg, a);
-                C0 += T * (st.omA * c0.x + st.K * (c0.x - c1.x));
-                C1 += T * (st.omA * c0.y + st.K * (c0.y - c1.y));
-                C2 += T * (st.omA * c0.z + st.K * (c0.z - c1.z));
-                T *= st.A;
-            }
+            segment_composite((f1.z - f0.z) * scale * 0.25f, f0.col, f1.col, sh.atten, C0, C1, C2, T);
             last_tet = t;
             last_entry = fe;
             last_b = b;
@@ -191,38 +178,24 @@ __global__ void __launch_bounds__(kTile * kTile, 2) k_walk_adjoint(
     int b = int(ws.z);
     uint32_t fx = tet_face_at(tet_faces, faces, f2t, vfix, t, fe, false, px, py);
     if (fx == kNoTet) return;
-    float gz_x = 0.f;
-    float4 gcol_x = make_float4(0.f, 0.f, 0.f, 0.f);
+    // Per fragment: depth adjoint, colour weight (colour adjoint = gC x weight)
+    // and alpha adjoint of the exit (x) and entry (e) fragments of the tet.
+    float gz_x = 0.f, wx = 0.f, ax = 0.f;
     for (uint32_t step = 0; step <= num_tets; ++step) {
         const FragV f0 = load_frag(u64(fe) << 2, qx, qy, faces, vgeo, colors);
         const FragV f1 = load_frag(u64(fx) << 2, qx, qy, faces, vgeo, colors);
         const float tSeg = (f1.z - f0.z) * scale * 0.25f;
-        float g_tot = 0.f;
-        float4 gcol_e = make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll
-        for (int s = kNumSubdivs - 1; s >= 0; --s) {
-            const float fbg = 0.25f * s, fm = 0.25f * (s + 0.5f), fen = 0.25f * (s + 1);
-            const float4 c0 = lerp4(f0.col, f1.col, fbg);
-            const float4 c1 = lerp4(f0.col, f1.col, fen);
-            const float a = (f0.col.w + (f1.col.w - f0.col.w) * fm) * atten;
-            float g_t, g_a, gc0x, gc0y, gc0z, gc1x, gc1y, gc1z;
-            sub_segment_adjoint(tSeg, a, c0, c1, gC0, gC1, gC2, T, gT, g_t, g_a, gc0x, gc0y, gc0z, gc1x, gc1y,
-                                gc1z);
-            g_tot += 0.25f * g_t;
-            gcol_e.x += (1.f - fbg) * gc0x + (1.f - fen) * gc1x;
-            gcol_e.y += (1.f - fbg) * gc0y + (1.f - fen) * gc1y;
-            gcol_e.z += (1.f - fbg) * gc0z + (1.f - fen) * gc1z;
-            gcol_x.x += fbg * gc0x + fen * gc1x;
-            gcol_x.y += fbg * gc0y + fen * gc1y;
-            gcol_x.z += fbg * gc0z + fen * gc1z;
-            gcol_e.w += (1.f - fm) * g_a * atten;
-            gcol_x.w += fm * g_a * atten;
-        }
+        const float p0 = gC0 * f0.col.x + gC1 * f0.col.y + gC2 * f0.col.z;
+        const float p1 = gC0 * f1.col.x + gC1 * f1.col.y + gC2 * f1.col.z;
+        float g_tot = 0.f, we = 0.f, ae = 0.f;
+        segment_adjoint(tSeg, f0.col, f1.col, p0, p1, atten, T, gT, g_tot, we, wx, ae, ax);
         float gz_e = -g_tot * scale;
         gz_x += g_tot * scale;
-        frag_vertex_grads(f1, qx, qy, vgeo, colors, cam, gz_x, gcol_x, use_abs, acc);
+        frag_vertex_grads(f1, qx, qy, vgeo, colors, cam, gz_x, make_float4(gC0 * wx, gC1 * wx, gC2 * wx, ax), use_abs,
+                          acc);
         if (faces[fe].w & 1u) {
-            frag_vertex_grads(f0, qx, qy, vgeo, colors, cam, gz_e, gcol_e, use_abs, acc);
+            frag_vertex_grads(f0, qx, qy, vgeo, colors, cam, gz_e, make_float4(gC0 * we, gC1 * we, gC2 * we, ae),
+                              use_abs, acc);
             // Previous interval: its exit is the last back-facing boundary fragment before b.
             int bb = b - 1;
             while (bb >= 0 && (uint32_t(b_records[beg + bb]) & 1u)) --bb;
@@ -235,7 +208,8 @@ __global__ void __launch_bounds__(kTile * kTile, 2) k_walk_adjoint(
             while (be >= 0 && !(uint32_t(b_records[beg + be]) & 1u)) --be;
             b = be < 0 ? 0 : be;
             gz_x = 0.f;
-            gcol_x = make_float4(0.f, 0.f, 0.f, 0.f);
+            wx = 0.f;
+            ax = 0.f;
             continue;
         }
         const uint32_t tprev = other_tet(f2t, fe, t);
@@ -244,7 +218,8 @@ __global__ void __launch_bounds__(kTile * kTile, 2) k_walk_adjoint(
         if (feprev == kNoTet) return;
         fx = fe;
         gz_x = gz_e;
-        gcol_x = gcol_e;
+        wx = we;
+        ax = ae;
         t = tprev;
         fe = feprev;
     }
