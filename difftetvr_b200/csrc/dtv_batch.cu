@@ -202,14 +202,15 @@ __global__ void __launch_bounds__(kTile * kTile) kb_adjoint(const BatchView* __r
                                                             const uint32_t* __restrict__ term,
                                                             float4* __restrict__ grad_rows,
                                                             const uint32_t* __restrict__ ok) {
+    __shared__ float4 vcache[6 * kTile * kTile];
     if (!batch_ok(ok)) return;
     int v, px, py;
     if (!tile_pixel(views, nviews, v, px, py)) return;
     const BatchView& bv = views[v];
     if (bv.grad_slot < 0 || bv.dimage == nullptr) return;
+    VertCache acc{grad_rows + 2 * bv.grad_base, vcache + threadIdx.x, kTile * kTile};
     adjoint_pixel(px, py, offsets + bv.pix_base, records, bv.faces, vgeo + bv.vert_base, bv.colors, int(bv.W),
-                  bv.cam, sh, bv.dimage, tfinal + bv.pix_base, term + bv.pix_base,
-                  GradAcc{grad_rows + 2 * bv.grad_base});
+                  bv.cam, sh, bv.dimage, tfinal + bv.pix_base, term + bv.pix_base, acc);
 }
 
 // Adds each slot's accumulated rows into its gradient buffers.

@@ -386,16 +386,86 @@ __device__ __forceinline__ void composite_pixel(
 struct GradAcc {
     float4* rows;   // [V][2]
 
-    __device__ __forceinline__ void add(uint32_t v, float gp0, float gp1, float gp2, float4 gc) const {
-        atomicAdd(rows + 2 * size_t(v), make_float4(gp0, gp1, gp2, 0.f));
+    __device__ __forceinline__ void add(uint32_t v, float4 gp, float4 gc) const {
+        atomicAdd(rows + 2 * size_t(v), gp);
         atomicAdd(rows + 2 * size_t(v) + 1, gc);
+    }
+    __device__ __forceinline__ void add_face(const uint32_t (&v)[3], const float4 (&gp)[3], const float4 (&gc)[3]) {
+#pragma unroll
+        for (int j = 0; j < 3; ++j) add(v[j], gp[j], gc[j]);
+    }
+    __device__ __forceinline__ void flush() {}
+};
+
+// Vertex-row accumulator with a per-thread cache of the three vertices of the
+// last face it was given.  Consecutive fragments of a pixel's list bound one
+// tet, so their faces share an edge: each new face usually brings one new
+// vertex and retires one, and only the retired vertex's row goes to global
+// memory (two float4 atomics instead of six per fragment; the gradient
+// atomics bound the adjoint otherwise).  The cached rows live in shared
+// memory (slot s, part c of this thread at sm[(2 s + c) * stride]); flush()
+// writes the remaining ones at the end of the pixel.  (A block-wide
+// shared-memory table behind it, summing the tile's pixels before the global
+// atomics, measured slower: neighbouring pixels contend for the same entries.)
+struct VertCache {
+    static constexpr uint32_t kNone = 0xffffffffu;
+    float4* rows;   // [V][2] global rows
+    float4* sm;     // this thread's slot 0, part 0
+    int stride;     // threads of the block
+    uint32_t id0 = kNone, id1 = kNone, id2 = kNone;
+
+    __device__ __forceinline__ float4* slot(int s) const { return sm + 2 * s * stride; }
+    __device__ __forceinline__ void spill(int s, uint32_t v) const {
+        if (v == kNone) return;
+        const float4* q = slot(s);
+        atomicAdd(rows + 2 * size_t(v), q[0]);
+        atomicAdd(rows + 2 * size_t(v) + 1, q[stride]);
+    }
+    __device__ __forceinline__ void add_face(const uint32_t (&v)[3], const float4 (&gp)[3], const float4 (&gc)[3]) {
+        int m[3];  // cache slot holding each vertex of the face, -1 if none
+#pragma unroll
+        for (int k = 0; k < 3; ++k) m[k] = v[k] == id0 ? 0 : (v[k] == id1 ? 1 : (v[k] == id2 ? 2 : -1));
+        bool u0 = m[0] == 0 || m[1] == 0 || m[2] == 0;
+        bool u1 = m[0] == 1 || m[1] == 1 || m[2] == 1;
+        bool u2 = m[0] == 2 || m[1] == 2 || m[2] == 2;
+        // Retire the cached vertices the face does not have.
+        if (!u0) { spill(0, id0); id0 = kNone; }
+        if (!u1) { spill(1, id1); id1 = kNone; }
+        if (!u2) { spill(2, id2); id2 = kNone; }
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            if (m[k] >= 0) {
+                float4* q = slot(m[k]);
+                const float4 a = q[0], b = q[stride];
+                q[0] = make_float4(a.x + gp[k].x, a.y + gp[k].y, a.z + gp[k].z, 0.f);
+                q[stride] = make_float4(b.x + gc[k].x, b.y + gc[k].y, b.z + gc[k].z, b.w + gc[k].w);
+            } else {
+                const int s = !u0 ? 0 : (!u1 ? 1 : 2);
+                u0 |= s == 0;
+                u1 |= s == 1;
+                u2 |= s == 2;
+                if (s == 0) id0 = v[k];
+                else if (s == 1) id1 = v[k];
+                else id2 = v[k];
+                float4* q = slot(s);
+                q[0] = gp[k];
+                q[stride] = gc[k];
+            }
+        }
+    }
+    __device__ __forceinline__ void flush() {
+        spill(0, id0);
+        spill(1, id1);
+        spill(2, id2);
+        id0 = id1 = id2 = kNone;
     }
 };
 
+template <class Acc>
 __device__ __forceinline__ void frag_vertex_grads(const FragV& fr, float qx, float qy,
                                                   const VGeo* __restrict__ vgeo,
                                                   const float4* __restrict__ colors, const CamDev& cam,
-                                                  float gz, float4 gcol, bool use_abs, const GradAcc& acc) {
+                                                  float gz, float4 gcol, bool use_abs, Acc& acc) {
     const uint32_t vi[3] = {fr.v0, fr.v1, fr.v2};
     VGeo P[3];
     float4 Cv[3];
@@ -436,6 +506,7 @@ __device__ __forceinline__ void frag_vertex_grads(const FragV& fr, float qx, flo
     gsx[2] = -gE[0] * dy[1] + gE[1] * dy[0];
     gsy[2] = gE[0] * dx[1] - gE[1] * dx[0];
     const float* V = cam.V;
+    float4 gpv[3], gcv[3];
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
         const float iz = P[j].iz;
@@ -451,8 +522,10 @@ __device__ __forceinline__ void frag_vertex_grads(const FragV& fr, float qx, flo
             gp0 = fabsf(gp0); gp1 = fabsf(gp1); gp2 = fabsf(gp2);
             gc = make_float4(fabsf(gc.x), fabsf(gc.y), fabsf(gc.z), fabsf(gc.w));
         }
-        acc.add(vi[j], gp0, gp1, gp2, gc);
+        gpv[j] = make_float4(gp0, gp1, gp2, 0.f);
+        gcv[j] = gc;
     }
+    acc.add_face(vi, gpv, gcv);
 }
 
 // Adjoint of one segment of a pixel's ray between a front fragment (colour
@@ -557,11 +630,12 @@ __device__ __forceinline__ void frag_position_grads(const uint4& fc, float qx, f
     }
 }
 
+template <class Acc>
 __device__ __forceinline__ void adjoint_pixel(
     int px, int py, const u64* __restrict__ offsets, const u64* __restrict__ records, const uint4* __restrict__ faces,
     const VGeo* __restrict__ vgeo, const float4* __restrict__ colors, int W, const CamDev& cam, const ShadeDev& sh,
     const float4* __restrict__ dimage, const float* __restrict__ tfinal, const uint32_t* __restrict__ term,
-    const GradAcc& acc) {
+    Acc& acc) {
     const size_t p = size_t(py) * W + px;
     const u64 beg = offsets[p];
     const uint32_t n = uint32_t(offsets[p + 1] - beg);
@@ -612,6 +686,7 @@ __device__ __forceinline__ void adjoint_pixel(
     }
     frag_vertex_grads(fb, qx, qy, vgeo, colors, cam, gz_b, make_float4(gC0 * wb, gC1 * wb, gC2 * wb, ab), use_abs,
                       acc);
+    acc.flush();
 }
 
 

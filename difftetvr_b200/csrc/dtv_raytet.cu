@@ -165,7 +165,6 @@ __global__ void __launch_bounds__(kTile * kTile, 2) k_walk_adjoint(
     if (ws.x == kNoTet) return;
     const float4 g = dimage[p];
     if (g.x == 0.f && g.y == 0.f && g.z == 0.f && g.w == 0.f) return;
-    const GradAcc acc{grad_rows};
     const bool use_abs = sh.use_abs_grad != 0;
     const u64 beg = b_offsets[p];
     const float qx = float(px) + 0.5f, qy = float(py) + 0.5f;
@@ -178,6 +177,9 @@ __global__ void __launch_bounds__(kTile * kTile, 2) k_walk_adjoint(
     int b = int(ws.z);
     uint32_t fx = tet_face_at(tet_faces, faces, f2t, vfix, t, fe, false, px, py);
     if (fx == kNoTet) return;
+    // Vertex rows straight to global memory: the shared-memory vertex cache of
+    // the list path measured slower here (register spills in the walk).
+    GradAcc acc{grad_rows};
     // Per fragment: depth adjoint, colour weight (colour adjoint = gC x weight)
     // and alpha adjoint of the exit (x) and entry (e) fragments of the tet.
     float gz_x = 0.f, wx = 0.f, ax = 0.f;
@@ -199,11 +201,11 @@ __global__ void __launch_bounds__(kTile * kTile, 2) k_walk_adjoint(
             // Previous interval: its exit is the last back-facing boundary fragment before b.
             int bb = b - 1;
             while (bb >= 0 && (uint32_t(b_records[beg + bb]) & 1u)) --bb;
-            if (bb < 0) return;
+            if (bb < 0) break;
             fx = bf_global[uint32_t(b_records[beg + bb]) >> 2];
             t = f2t[2 * size_t(fx)];
             fe = tet_face_at(tet_faces, faces, f2t, vfix, t, fx, true, px, py);
-            if (fe == kNoTet) return;
+            if (fe == kNoTet) break;
             int be = bb - 1;
             while (be >= 0 && !(uint32_t(b_records[beg + be]) & 1u)) --be;
             b = be < 0 ? 0 : be;
@@ -213,9 +215,9 @@ __global__ void __launch_bounds__(kTile * kTile, 2) k_walk_adjoint(
             continue;
         }
         const uint32_t tprev = other_tet(f2t, fe, t);
-        if (tprev == kNoTet) return;
+        if (tprev == kNoTet) break;
         const uint32_t feprev = tet_face_at(tet_faces, faces, f2t, vfix, tprev, fe, true, px, py);
-        if (feprev == kNoTet) return;
+        if (feprev == kNoTet) break;
         fx = fe;
         gz_x = gz_e;
         wx = we;
@@ -223,6 +225,7 @@ __global__ void __launch_bounds__(kTile * kTile, 2) k_walk_adjoint(
         t = tprev;
         fe = feprev;
     }
+    acc.flush();
 }
 
 void launch_walk_composite(const u64* b_offsets, const u64* b_records, const uint32_t* bf_global,
