@@ -194,7 +194,7 @@ __global__ void __launch_bounds__(256) kb_loss(const BatchView* __restrict__ vie
     }
 }
 
-__global__ void __launch_bounds__(kTile * kTile) kb_adjoint(const BatchView* __restrict__ views, int nviews,
+__global__ void __launch_bounds__(kTile * kTile, 2) kb_adjoint(const BatchView* __restrict__ views, int nviews,
                                                             const u64* __restrict__ offsets,
                                                             const u64* __restrict__ records,
                                                             const VGeo* __restrict__ vgeo, ShadeDev sh,
@@ -202,13 +202,14 @@ __global__ void __launch_bounds__(kTile * kTile) kb_adjoint(const BatchView* __r
                                                             const uint32_t* __restrict__ term,
                                                             float4* __restrict__ grad_rows,
                                                             const uint32_t* __restrict__ ok) {
-    __shared__ float4 vcache[6 * kTile * kTile];
+    __shared__ float4 vcache4[3 * kTile * kTile];
+    __shared__ float vcache1[3 * kTile * kTile];
     if (!batch_ok(ok)) return;
     int v, px, py;
     if (!tile_pixel(views, nviews, v, px, py)) return;
     const BatchView& bv = views[v];
     if (bv.grad_slot < 0 || bv.dimage == nullptr) return;
-    VertCache acc{grad_rows + 2 * bv.grad_base, vcache + threadIdx.x, kTile * kTile};
+    VertCache acc{grad_rows + 2 * bv.grad_base, vcache4 + threadIdx.x, vcache1 + threadIdx.x, kTile * kTile};
     adjoint_pixel(px, py, offsets + bv.pix_base, records, bv.faces, vgeo + bv.vert_base, bv.colors, int(bv.W),
                   bv.cam, sh, bv.dimage, tfinal + bv.pix_base, term + bv.pix_base, acc);
 }

@@ -600,12 +600,13 @@ __global__ void __launch_bounds__(256) k_adjoint(
     const VGeo* __restrict__ vgeo, const float4* __restrict__ colors, int W, int row0, int row1, CamDev cam,
     ShadeDev sh, const float4* __restrict__ dimage, const float* __restrict__ tfinal,
     const uint32_t* __restrict__ term, float4* __restrict__ grad_rows) {
-    __shared__ float4 vcache[6 * 256];
+    __shared__ float4 vcache4[3 * 256];
+    __shared__ float vcache1[3 * 256];
     constexpr int TY = 256 / TX;
     const int px = blockIdx.x * TX + (threadIdx.x % TX);
     const int py = row0 + int(blockIdx.y) * TY + int(threadIdx.x / TX);
     if (px >= W || py >= row1) return;
-    VertCache acc{grad_rows, vcache + threadIdx.x, 256};
+    VertCache acc{grad_rows, vcache4 + threadIdx.x, vcache1 + threadIdx.x, 256};
     adjoint_pixel(px, py, offsets, records, faces, vgeo, colors, W, cam, sh, dimage, tfinal, term, acc);
 }
 

@@ -383,16 +383,22 @@ __device__ __forceinline__ void composite_pixel(
 // colour rgba) share one 32-byte row of an interleaved buffer and are added
 // with two float4 vector atomics, so each vertex update touches one L2 sector
 // (scalar atomics into the [V,3] / [V,4] layout touch about three).
+// Vertex gradient sinks.  A fragment's colour adjoint is the pixel's colour
+// adjoint gC times a scalar (segment_adjoint), so a vertex's contribution from
+// one pixel is its position gradient xyz, a weight s1 (colour rgb = gC s1)
+// and the alpha gradient s2; set_pixel() gives the sink gC (|gC| for absolute
+// gradients, whose s1 is then the absolute weight).
 struct GradAcc {
-    float4* rows;   // [V][2]
+    float4* rows;   // [V][2]: position xyz, pad; colour rgba
+    float g0 = 0.f, g1 = 0.f, g2 = 0.f;
 
-    __device__ __forceinline__ void add(uint32_t v, float4 gp, float4 gc) const {
-        atomicAdd(rows + 2 * size_t(v), gp);
-        atomicAdd(rows + 2 * size_t(v) + 1, gc);
-    }
-    __device__ __forceinline__ void add_face(const uint32_t (&v)[3], const float4 (&gp)[3], const float4 (&gc)[3]) {
+    __device__ __forceinline__ void set_pixel(float a0, float a1, float a2) { g0 = a0; g1 = a1; g2 = a2; }
+    __device__ __forceinline__ void add_face(const uint32_t (&v)[3], const float4 (&gp)[3], const float (&s2)[3]) {
 #pragma unroll
-        for (int j = 0; j < 3; ++j) add(v[j], gp[j], gc[j]);
+        for (int j = 0; j < 3; ++j) {
+            atomicAdd(rows + 2 * size_t(v[j]), make_float4(gp[j].x, gp[j].y, gp[j].z, 0.f));
+            atomicAdd(rows + 2 * size_t(v[j]) + 1, make_float4(g0 * gp[j].w, g1 * gp[j].w, g2 * gp[j].w, s2[j]));
+        }
     }
     __device__ __forceinline__ void flush() {}
 };
@@ -402,26 +408,30 @@ struct GradAcc {
 // tet, so their faces share an edge: each new face usually brings one new
 // vertex and retires one, and only the retired vertex's row goes to global
 // memory (two float4 atomics instead of six per fragment; the gradient
-// atomics bound the adjoint otherwise).  The cached rows live in shared
-// memory (slot s, part c of this thread at sm[(2 s + c) * stride]); flush()
-// writes the remaining ones at the end of the pixel.  (A block-wide
-// shared-memory table behind it, summing the tile's pixels before the global
-// atomics, measured slower: neighbouring pixels contend for the same entries.)
+// atomics bound the adjoint otherwise).  The cached values (position xyz and
+// colour weight in a float4, alpha in a float) live in shared memory: slot s
+// of thread t at c4[t + s * stride], c1[t + s * stride]; flush() writes the
+// remaining ones at the end of the pixel.  (A block-wide shared-memory table
+// behind it, summing the tile's pixels with shared-memory atomics, and a
+// warp-wide merge of equal retired vertices both measured slower.)
 struct VertCache {
     static constexpr uint32_t kNone = 0xffffffffu;
     float4* rows;   // [V][2] global rows
-    float4* sm;     // this thread's slot 0, part 0
+    float4* c4;     // this thread's slot 0: position xyz, colour weight
+    float* c1;      // this thread's slot 0: alpha
     int stride;     // threads of the block
+    float g0 = 0.f, g1 = 0.f, g2 = 0.f;
     uint32_t id0 = kNone, id1 = kNone, id2 = kNone;
 
-    __device__ __forceinline__ float4* slot(int s) const { return sm + 2 * s * stride; }
+    __device__ __forceinline__ void set_pixel(float a0, float a1, float a2) { g0 = a0; g1 = a1; g2 = a2; }
     __device__ __forceinline__ void spill(int s, uint32_t v) const {
         if (v == kNone) return;
-        const float4* q = slot(s);
-        atomicAdd(rows + 2 * size_t(v), q[0]);
-        atomicAdd(rows + 2 * size_t(v) + 1, q[stride]);
+        const float4 q = c4[s * stride];
+        const float a = c1[s * stride];
+        atomicAdd(rows + 2 * size_t(v), make_float4(q.x, q.y, q.z, 0.f));
+        atomicAdd(rows + 2 * size_t(v) + 1, make_float4(g0 * q.w, g1 * q.w, g2 * q.w, a));
     }
-    __device__ __forceinline__ void add_face(const uint32_t (&v)[3], const float4 (&gp)[3], const float4 (&gc)[3]) {
+    __device__ __forceinline__ void add_face(const uint32_t (&v)[3], const float4 (&gp)[3], const float (&s2)[3]) {
         int m[3];  // cache slot holding each vertex of the face, -1 if none
 #pragma unroll
         for (int k = 0; k < 3; ++k) m[k] = v[k] == id0 ? 0 : (v[k] == id1 ? 1 : (v[k] == id2 ? 2 : -1));
@@ -435,10 +445,10 @@ struct VertCache {
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
             if (m[k] >= 0) {
-                float4* q = slot(m[k]);
-                const float4 a = q[0], b = q[stride];
-                q[0] = make_float4(a.x + gp[k].x, a.y + gp[k].y, a.z + gp[k].z, 0.f);
-                q[stride] = make_float4(b.x + gc[k].x, b.y + gc[k].y, b.z + gc[k].z, b.w + gc[k].w);
+                const int o = m[k] * stride;
+                const float4 q = c4[o];
+                c4[o] = make_float4(q.x + gp[k].x, q.y + gp[k].y, q.z + gp[k].z, q.w + gp[k].w);
+                c1[o] += s2[k];
             } else {
                 const int s = !u0 ? 0 : (!u1 ? 1 : 2);
                 u0 |= s == 0;
@@ -447,9 +457,8 @@ struct VertCache {
                 if (s == 0) id0 = v[k];
                 else if (s == 1) id1 = v[k];
                 else id2 = v[k];
-                float4* q = slot(s);
-                q[0] = gp[k];
-                q[stride] = gc[k];
+                c4[s * stride] = gp[k];
+                c1[s * stride] = s2[k];
             }
         }
     }
@@ -461,11 +470,16 @@ struct VertCache {
     }
 };
 
+// Vertex gradients of one fragment from its depth adjoint gz, its colour
+// adjoint gC w (gC = (g0, g1, g2), the pixel's) and its alpha adjoint ga,
+// through the perspective-correct barycentrics and the projection.
 template <class Acc>
 __device__ __forceinline__ void frag_vertex_grads(const FragV& fr, float qx, float qy,
                                                   const VGeo* __restrict__ vgeo,
                                                   const float4* __restrict__ colors, const CamDev& cam,
-                                                  float gz, float4 gcol, bool use_abs, Acc& acc) {
+                                                  float gz, float g0, float g1, float g2, float w, float ga,
+                                                  bool use_abs, Acc& acc) {
+    const float4 gcol = make_float4(g0 * w, g1 * w, g2 * w, ga);
     const uint32_t vi[3] = {fr.v0, fr.v1, fr.v2};
     VGeo P[3];
     float4 Cv[3];
@@ -506,7 +520,8 @@ __device__ __forceinline__ void frag_vertex_grads(const FragV& fr, float qx, flo
     gsx[2] = -gE[0] * dy[1] + gE[1] * dy[0];
     gsy[2] = gE[0] * dx[1] - gE[1] * dx[0];
     const float* V = cam.V;
-    float4 gpv[3], gcv[3];
+    float4 gpv[3];
+    float gav[3];
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
         const float iz = P[j].iz;
@@ -517,15 +532,16 @@ __device__ __forceinline__ void frag_vertex_grads(const FragV& fr, float qx, flo
         float gp0 = V[0] * gxv + V[1] * gyv + V[2] * gzv;
         float gp1 = V[4] * gxv + V[5] * gyv + V[6] * gzv;
         float gp2 = V[8] * gxv + V[9] * gyv + V[10] * gzv;
-        float4 gc = f4scale(gcol, fi.bary[j]);
+        float s1 = w * fi.bary[j], s2 = ga * fi.bary[j];
         if (use_abs) {
             gp0 = fabsf(gp0); gp1 = fabsf(gp1); gp2 = fabsf(gp2);
-            gc = make_float4(fabsf(gc.x), fabsf(gc.y), fabsf(gc.z), fabsf(gc.w));
+            s1 = fabsf(s1);
+            s2 = fabsf(s2);
         }
-        gpv[j] = make_float4(gp0, gp1, gp2, 0.f);
-        gcv[j] = gc;
+        gpv[j] = make_float4(gp0, gp1, gp2, s1);
+        gav[j] = s2;
     }
-    acc.add_face(vi, gpv, gcv);
+    acc.add_face(vi, gpv, gav);
 }
 
 // Adjoint of one segment of a pixel's ray between a front fragment (colour
@@ -650,6 +666,10 @@ __device__ __forceinline__ void adjoint_pixel(
     if (last < 1) return;
     const float atten = sh.atten;
     const bool use_abs = sh.use_abs_grad != 0;
+    if (use_abs)
+        acc.set_pixel(fabsf(gC0), fabsf(gC1), fabsf(gC2));
+    else
+        acc.set_pixel(gC0, gC1, gC2);
     // The dependent loads record -> face -> vertex rows are software-pipelined:
     // while fragment i's segment is processed, the face of fragment i-2 and the
     // record of fragment i-3 are already in flight.
@@ -676,16 +696,14 @@ __device__ __forceinline__ void adjoint_pixel(
             gz_f -= g_tot;
             gz_b += g_tot;
         }
-        frag_vertex_grads(fb, qx, qy, vgeo, colors, cam, gz_b, make_float4(gC0 * wb, gC1 * wb, gC2 * wb, ab),
-                          use_abs, acc);
+        frag_vertex_grads(fb, qx, qy, vgeo, colors, cam, gz_b, gC0, gC1, gC2, wb, ab, use_abs, acc);
         fb = ff;
         pb = pf;
         gz_b = gz_f;
         wb = wf;
         ab = af;
     }
-    frag_vertex_grads(fb, qx, qy, vgeo, colors, cam, gz_b, make_float4(gC0 * wb, gC1 * wb, gC2 * wb, ab), use_abs,
-                      acc);
+    frag_vertex_grads(fb, qx, qy, vgeo, colors, cam, gz_b, gC0, gC1, gC2, wb, ab, use_abs, acc);
     acc.flush();
 }
 

@@ -180,6 +180,10 @@ __global__ void __launch_bounds__(kTile * kTile, 2) k_walk_adjoint(
     // Vertex rows straight to global memory: the shared-memory vertex cache of
     // the list path measured slower here (register spills in the walk).
     GradAcc acc{grad_rows};
+    if (use_abs)
+        acc.set_pixel(fabsf(gC0), fabsf(gC1), fabsf(gC2));
+    else
+        acc.set_pixel(gC0, gC1, gC2);
     // Per fragment: depth adjoint, colour weight (colour adjoint = gC x weight)
     // and alpha adjoint of the exit (x) and entry (e) fragments of the tet.
     float gz_x = 0.f, wx = 0.f, ax = 0.f;
@@ -193,11 +197,9 @@ __global__ void __launch_bounds__(kTile * kTile, 2) k_walk_adjoint(
         segment_adjoint(tSeg, f0.col, f1.col, p0, p1, atten, T, gT, g_tot, we, wx, ae, ax);
         float gz_e = -g_tot * scale;
         gz_x += g_tot * scale;
-        frag_vertex_grads(f1, qx, qy, vgeo, colors, cam, gz_x, make_float4(gC0 * wx, gC1 * wx, gC2 * wx, ax), use_abs,
-                          acc);
+        frag_vertex_grads(f1, qx, qy, vgeo, colors, cam, gz_x, gC0, gC1, gC2, wx, ax, use_abs, acc);
         if (faces[fe].w & 1u) {
-            frag_vertex_grads(f0, qx, qy, vgeo, colors, cam, gz_e, make_float4(gC0 * we, gC1 * we, gC2 * we, ae),
-                              use_abs, acc);
+            frag_vertex_grads(f0, qx, qy, vgeo, colors, cam, gz_e, gC0, gC1, gC2, we, ae, use_abs, acc);
             // Previous interval: its exit is the last back-facing boundary fragment before b.
             int bb = b - 1;
             while (bb >= 0 && (uint32_t(b_records[beg + bb]) & 1u)) --bb;
