@@ -52,7 +52,7 @@ class Tuning(ctypes.Structure):
         ("composite_tile", ctypes.c_int32),
         ("adjoint_tile", ctypes.c_int32),
         ("sort_surrogate_classes", ctypes.c_uint32),
-        ("reserved", ctypes.c_int32),
+        ("sort_bucket_classes", ctypes.c_uint32),
     ]
 
 

@@ -11,6 +11,26 @@ import torch
 
 TILES = (0, 1, 2)               # 16x16, 32x8, 8x32 pixels per 256-thread block
 SORT_CLASSES = (1, 2, 3, 4)     # lists of up to 64, 128, 256, 512 records
+SORT_METHODS = ("bucket", "surrogate", "network")
+
+
+def sort_method(tuning: dict, c: int) -> str:
+    """Sort method of list-length class c under `tuning` (bucket bits win)."""
+    if (tuning["sort_bucket_classes"] >> c) & 1:
+        return "bucket"
+    return "surrogate" if (tuning["sort_surrogate_classes"] >> c) & 1 else "network"
+
+
+def with_sort_method(tuning: dict, c: int, method: str) -> dict:
+    """`tuning` with class c switched to `method`."""
+    bit = 1 << c
+    b = tuning["sort_bucket_classes"] & ~bit
+    q = tuning["sort_surrogate_classes"] & ~bit
+    if method == "bucket":
+        b |= bit
+    elif method == "surrogate":
+        q |= bit
+    return dict(tuning, sort_bucket_classes=b, sort_surrogate_classes=q)
 
 _cache: dict = {}
 
@@ -76,10 +96,13 @@ def autotune_renderer(renderer, trials: int = 3, force: bool = False) -> dict:
             if ms < best_ms:
                 best, best_ms = cand, ms
     for c in SORT_CLASSES:
-        cand = dict(best, sort_surrogate_classes=best["sort_surrogate_classes"] ^ (1 << c))
-        ms = measure(**cand)
-        if ms < best_ms:
-            best, best_ms = cand, ms
+        for method in SORT_METHODS:
+            if method == sort_method(best, c):
+                continue
+            cand = with_sort_method(best, c, method)
+            ms = measure(**cand)
+            if ms < best_ms:
+                best, best_ms = cand, ms
     renderer.set_tuning(**best)
     out = {"tuning": best, "ms": best_ms, "timings": timings}
     _cache[key] = out
@@ -88,27 +111,31 @@ def autotune_renderer(renderer, trials: int = 3, force: bool = False) -> dict:
 
 def autotune_batch(batch_renderer, views, trials: int = 2, force: bool = False) -> dict:
     """Times BatchRenderer.render(views) for each sort method per list-length
-    class and leaves the fastest set.  Returns {"tuning": ..., "ms": ...}."""
+    class (depth buckets, surrogate keys, 64-bit network) and leaves the
+    fastest set.  Returns {"tuning": ..., "ms": ...}."""
     key = ("batch", tuple((v.mesh, v.width, v.height) for v in views))
     if not force and key in _cache:
         batch_renderer.set_tuning(**_cache[key]["tuning"])
         return _cache[key]
     timings = []
 
-    def measure(mask):
-        batch_renderer.set_tuning(sort_surrogate_classes=mask)
+    def measure(cfg):
+        batch_renderer.set_tuning(**cfg)
         ms = _time_ms(lambda: batch_renderer.render(views), trials)
-        timings.append({"sort_surrogate_classes": mask, "ms": ms})
+        timings.append({**cfg, "ms": ms})
         return ms
 
-    best = batch_renderer.get_tuning()["sort_surrogate_classes"]
+    best = batch_renderer.get_tuning()
     best_ms = measure(best)
     for c in SORT_CLASSES:
-        cand = best ^ (1 << c)
-        ms = measure(cand)
-        if ms < best_ms:
-            best, best_ms = cand, ms
-    batch_renderer.set_tuning(sort_surrogate_classes=best)
-    out = {"tuning": {"sort_surrogate_classes": best}, "ms": best_ms, "timings": timings}
+        for method in SORT_METHODS:
+            if method == sort_method(best, c):
+                continue
+            cand = with_sort_method(best, c, method)
+            ms = measure(cand)
+            if ms < best_ms:
+                best, best_ms = cand, ms
+    batch_renderer.set_tuning(**best)
+    out = {"tuning": best, "ms": best_ms, "timings": timings}
     _cache[key] = out
     return out

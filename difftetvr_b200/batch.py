@@ -77,12 +77,16 @@ class BatchRenderer:
     def get_tuning(self) -> dict:
         t = _lib.Tuning()
         _lib.call("dtv_batch_get_tuning", self._handle, ctypes.byref(t))
-        return {"sort_surrogate_classes": t.sort_surrogate_classes}
+        return {"sort_surrogate_classes": t.sort_surrogate_classes, "sort_bucket_classes": t.sort_bucket_classes}
 
-    def set_tuning(self, sort_surrogate_classes: int) -> None:
-        """Sort method per list-length class (bit c, c = 1..4): 32-bit
-        surrogate keys or the 64-bit network; identical results."""
-        t = _lib.Tuning(0, 0, int(sort_surrogate_classes), 0)
+    def set_tuning(self, sort_surrogate_classes: int | None = None, sort_bucket_classes: int | None = None) -> None:
+        """Sort method per list-length class c = 1..4: depth buckets (bit c
+        of sort_bucket_classes), else 32-bit surrogate keys (bit c of
+        sort_surrogate_classes), else the 64-bit network; identical results."""
+        cur = self.get_tuning()
+        t = _lib.Tuning(0, 0, cur["sort_surrogate_classes"] if sort_surrogate_classes is None
+                        else int(sort_surrogate_classes),
+                        cur["sort_bucket_classes"] if sort_bucket_classes is None else int(sort_bucket_classes))
         _lib.call("dtv_batch_set_tuning", self._handle, ctypes.byref(t))
 
     def set_graph(self, enable: bool = True) -> None:

@@ -86,7 +86,7 @@ struct dtv_renderer {
     // when the lists are stored whole.
     std::vector<std::pair<int, int>> bands;
     bool cells = false;           // last render used per-cell colours
-    dtv_tuning tuning{0, 0, dtv::kSortSurrogateDefault, 0};
+    dtv_tuning tuning{0, 0, dtv::kSortSurrogateDefault, dtv::kSortBucketDefault};
     u64* h_rowoff = nullptr;      // pinned row-start offsets (H+1)
     size_t h_rowoff_cap = 0;
     DevBuf<uint4> wstate;         // ray-tet path: (last tet, its entry face, boundary entry index, segments)
@@ -166,7 +166,7 @@ void build_band_lists(dtv_renderer* r, const dtv_mesh* mesh, int W, int H, int y
                             r->counts.ptr, r->offsets.ptr, r->records.ptr, s, y0, y1);
     check_launch("band fill");
     dtv::launch_sort(r->offsets.ptr + p0, r->records.ptr, uint32_t(pb), r->long_list.ptr, r->flags.ptr, s, nullptr,
-                     r->tuning.sort_surrogate_classes);
+                     r->tuning.sort_surrogate_classes, r->tuning.sort_bucket_classes);
     check_launch("band sort");
 }
 
@@ -536,7 +536,7 @@ int32_t render_common(dtv_renderer* r, const dtv_mesh* mesh, const float* d_posi
         rec_event(r, 4, s);
         DTV_CK(cudaMemsetAsync(r->flags.ptr, 0, 2 * sizeof(uint32_t), s));
         dtv::launch_sort(r->offsets.ptr, r->records.ptr, uint32_t(P), r->long_list.ptr, r->flags.ptr, s, nullptr,
-                         r->tuning.sort_surrogate_classes);
+                         r->tuning.sort_surrogate_classes, r->tuning.sort_bucket_classes);
         check_launch("sort");
         DTV_CK(cudaMemcpyAsync(r->h_flags, r->flags.ptr, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
         DTV_CK(cudaEventRecord(r->flags_event, s));
@@ -651,7 +651,8 @@ int32_t dtv_renderer_set_tuning(dtv_renderer* r, const dtv_tuning* t) {
         require(r && t, "null pointer");
         require(t->composite_tile >= 0 && t->composite_tile <= 2 && t->adjoint_tile >= 0 && t->adjoint_tile <= 2,
                 "tile index must be 0, 1 or 2");
-        require((t->sort_surrogate_classes & ~0x1eu) == 0, "sort_surrogate_classes uses bits 1..4 only");
+        require((t->sort_surrogate_classes & ~0x1eu) == 0 && (t->sort_bucket_classes & ~0x1eu) == 0,
+                "sort class masks use bits 1..4 only");
         r->tuning = *t;
     });
 }

@@ -360,6 +360,7 @@ struct dtv_batch {
     u64 capacity = 0;
     uint64_t steps_rerun = 0;
     uint32_t sort_surrogate_classes = dtv::kSortSurrogateDefault;
+    uint32_t sort_bucket_classes = dtv::kSortBucketDefault;
     bool async_render = false;  // last render enqueued without a host sync (capacity-guarded)
 };
 
@@ -481,7 +482,7 @@ void enqueue_forward(dtv_batch* b, const dtv::ShadeDev& sh, bool guarded, cudaSt
     launch_kb_raster<true>(b, okp, s);
     DTV_CK(cudaMemsetAsync(b->sort_flags.ptr, 0, 2 * sizeof(uint32_t), s));
     launch_sort(b->offsets.ptr, b->records.ptr, uint32_t(b->tot_pixels), b->long_list.ptr, b->sort_flags.ptr, s, okp,
-                b->sort_surrogate_classes);
+                b->sort_surrogate_classes, b->sort_bucket_classes);
     kb_composite<<<unsigned(b->tot_tiles), kTile * kTile, 0, s>>>(b->d_views.ptr, b->nviews, b->offsets.ptr,
                                                                   b->records.ptr, b->vgeo.ptr, sh, b->tfinal.ptr,
                                                                   b->term.ptr, okp);
@@ -502,21 +503,24 @@ int32_t dtv_batch_create(dtv_batch** out) {
 int32_t dtv_batch_set_tuning(dtv_batch* b, const dtv_tuning* t) {
     return guarded([&] {
         require(b && t, "null pointer");
-        require((t->sort_surrogate_classes & ~0x1eu) == 0, "sort_surrogate_classes uses bits 1..4 only");
-        if (b->sort_surrogate_classes != t->sort_surrogate_classes && b->exec) {
+        require((t->sort_surrogate_classes & ~0x1eu) == 0 && (t->sort_bucket_classes & ~0x1eu) == 0,
+                "sort class masks use bits 1..4 only");
+        if ((b->sort_surrogate_classes != t->sort_surrogate_classes ||
+             b->sort_bucket_classes != t->sort_bucket_classes) && b->exec) {
             // The captured step holds the old sort launches.
             cudaGraphExecDestroy(b->exec);
             b->exec = nullptr;
             b->graph_sig.clear();
         }
         b->sort_surrogate_classes = t->sort_surrogate_classes;
+        b->sort_bucket_classes = t->sort_bucket_classes;
     });
 }
 
 int32_t dtv_batch_get_tuning(const dtv_batch* b, dtv_tuning* t) {
     return guarded([&] {
         require(b && t, "null pointer");
-        *t = dtv_tuning{0, 0, b->sort_surrogate_classes, 0};
+        *t = dtv_tuning{0, 0, b->sort_surrogate_classes, b->sort_bucket_classes};
     });
 }
 
@@ -673,7 +677,7 @@ int32_t dtv_batch_render(dtv_batch* b, int32_t num_views, const dtv_batch_view* 
         launch_kb_raster<true>(b, nullptr, s);
         DTV_CK(cudaMemsetAsync(b->sort_flags.ptr, 0, 2 * sizeof(uint32_t), s));
         launch_sort(b->offsets.ptr, b->records.ptr, uint32_t(b->tot_pixels), b->long_list.ptr, b->sort_flags.ptr, s,
-                    nullptr, b->sort_surrogate_classes);
+                    nullptr, b->sort_surrogate_classes, b->sort_bucket_classes);
         kb_composite<<<unsigned(b->tot_tiles), kTile * kTile, 0, s>>>(b->d_views.ptr, b->nviews, b->offsets.ptr,
                                                                       b->records.ptr, b->vgeo.ptr, b->sh,
                                                                       b->tfinal.ptr, b->term.ptr, nullptr);

@@ -464,6 +464,119 @@ __global__ void __launch_bounds__(kSortWarps * 32, K >= 16 ? 2 : 1) k_sort_class
     }
 }
 
+// Classes 2..4 by distribution: one warp per list of n <= 32 K records.
+// Each record goes to bucket floor((depth - min) * n / (max - min)) of n
+// buckets (monotone in the depth), buckets are counted (shared-memory
+// atomics), scanned and scattered in shared memory, so only records of one
+// bucket can be out of order; the odd-even passes of the surrogate-key sort
+// then restore the exact (depth, face) order, and a list that needs more than
+// kFixPasses passes goes to the block sort.  About 30 instructions per record
+// against the bitonic network's log2(N) (log2(N) + 1) / 2 stages.  Shared
+// arrays are skewed (one pad element per 16 records, per 32 counters) so
+// the lane-strided accesses hit distinct banks.
+__device__ __forceinline__ uint32_t skew16(uint32_t i) { return i + (i >> 4); }
+__device__ __forceinline__ uint32_t skew32(uint32_t i) { return i + (i >> 5); }
+
+template <int K>
+__host__ __device__ constexpr int bucket_warps() { return K >= 16 ? 4 : 8; }
+
+template <int K>
+__global__ void __launch_bounds__(bucket_warps<K>() * 32) k_sort_class_bucket(
+    const u64* __restrict__ offsets, u64* records, const uint32_t* __restrict__ items,
+    const uint32_t* __restrict__ count, uint32_t* __restrict__ redo_count, uint32_t* __restrict__ redo_items,
+    const uint32_t* __restrict__ ok) {
+    constexpr int N = 32 * K, W = bucket_warps<K>();
+    __shared__ u64 sbuf[W][N + N / 16];
+    __shared__ uint32_t scnt[W][N + N / 32];
+    if (ok && *ok == 0u) return;
+    const uint32_t num = *count;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    u64* buf = sbuf[w];
+    uint32_t* cnt = scnt[w];
+    for (uint32_t it = blockIdx.x * W + w; it < num; it += gridDim.x * W) {
+        const uint32_t p = items[it];
+        const u64 beg = offsets[p];
+        const uint32_t n = uint32_t(offsets[p + 1] - beg);
+        u64* r = records + beg;
+        u64 v[K];
+        float dmin = 3.4e38f, dmax = 0.f;
+#pragma unroll
+        for (int q = 0; q < K; ++q) {
+            const uint32_t i = uint32_t(q * 32 + lane);
+            v[q] = i < n ? r[i] : ~0ull;
+            cnt[skew32(uint32_t(lane * K + q))] = 0u;
+            if (i < n) {
+                const float d = __uint_as_float(uint32_t(v[q] >> 32));
+                dmin = fminf(dmin, d);
+                dmax = fmaxf(dmax, d);
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            dmin = fminf(dmin, __shfl_xor_sync(kFull, dmin, o));
+            dmax = fmaxf(dmax, __shfl_xor_sync(kFull, dmax, o));
+        }
+        const float scale = dmax > dmin ? float(n) / (dmax - dmin) : 0.f;
+        __syncwarp();
+        uint32_t b[K], rk[K];
+#pragma unroll
+        for (int q = 0; q < K; ++q) {
+            if (uint32_t(q * 32 + lane) < n) {
+                const float d = __uint_as_float(uint32_t(v[q] >> 32));
+                b[q] = min(uint32_t((d - dmin) * scale), n - 1u);
+                rk[q] = atomicAdd(&cnt[skew32(b[q])], 1u);
+            }
+        }
+        __syncwarp();
+        // Exclusive scan of the counts: lane owns buckets [K lane, K lane + K).
+        uint32_t c[K], tot = 0;
+#pragma unroll
+        for (int q = 0; q < K; ++q) {
+            c[q] = tot;
+            tot += cnt[skew32(uint32_t(lane * K + q))];
+        }
+        uint32_t incl = tot;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(kFull, incl, o);
+            if (lane >= o) incl += t;
+        }
+        const uint32_t base = incl - tot;
+#pragma unroll
+        for (int q = 0; q < K; ++q) cnt[skew32(uint32_t(lane * K + q))] = base + c[q];
+        __syncwarp();
+#pragma unroll
+        for (int q = 0; q < K; ++q)
+            if (uint32_t(q * 32 + lane) < n) buf[skew16(cnt[skew32(b[q])] + rk[q])] = v[q];
+        __syncwarp();
+#pragma unroll
+        for (int q = 0; q < K; ++q) {
+            const uint32_t i = uint32_t(lane * K + q);
+            v[q] = i < n ? buf[skew16(i)] : ~0ull;
+        }
+        bool sorted = false;
+        for (int pass = 0; pass < kFixPasses; ++pass) {
+            const bool s0 = fixup_pass<K>(v, lane, 0);
+            const bool s1 = fixup_pass<K>(v, lane, 1);
+            if (!__any_sync(kFull, s0 || s1)) {
+                sorted = true;
+                break;
+            }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int q = 0; q < K; ++q) buf[skew16(uint32_t(lane * K + q))] = v[q];
+        __syncwarp();
+#pragma unroll
+        for (int q = 0; q < K; ++q) {
+            const uint32_t i = uint32_t(q * 32 + lane);
+            if (i < n) r[i] = buf[skew16(i)];
+        }
+        if (!sorted && lane == 0) redo_items[atomicAdd(redo_count, 1u)] = p;
+        __syncwarp();
+    }
+}
+
 // Class 5: one warp per list, bitonic in shared memory.
 __global__ void __launch_bounds__(kSortWarps * 32) k_sort_class_smem(const u64* __restrict__ offsets, u64* records,
                                                                      const uint32_t* __restrict__ items,
@@ -515,16 +628,18 @@ __global__ void __launch_bounds__(1024) k_sort_class_block(const u64* __restrict
 size_t sort_scratch_elems(uint64_t P) { return 16 + size_t(kSortClasses) * size_t(P); }
 
 template <int K>
-void sort_class(bool q, unsigned g, const u64* offsets, u64* records, const uint32_t* items, const uint32_t* count,
-                uint32_t* redo_n, uint32_t* redo, const uint32_t* ok, cudaStream_t s) {
-    if (q)
+void sort_class(int method, unsigned g, const u64* offsets, u64* records, const uint32_t* items,
+                const uint32_t* count, uint32_t* redo_n, uint32_t* redo, const uint32_t* ok, cudaStream_t s) {
+    if (method == 2)
+        k_sort_class_bucket<K><<<g, bucket_warps<K>() * 32, 0, s>>>(offsets, records, items, count, redo_n, redo, ok);
+    else if (method == 1)
         k_sort_class_regs<K, true><<<g, kSortWarps * 32, 0, s>>>(offsets, records, items, count, redo_n, redo, ok);
     else
         k_sort_class_regs<K, false><<<g, kSortWarps * 32, 0, s>>>(offsets, records, items, count, redo_n, redo, ok);
 }
 
 void launch_sort(const u64* offsets, u64* records, uint32_t P, uint32_t* scratch, uint32_t* flags, cudaStream_t s,
-                 const uint32_t* ok, uint32_t surrogate_classes) {
+                 const uint32_t* ok, uint32_t surrogate_classes, uint32_t bucket_classes) {
     static bool attr_set = false;
     const size_t smem_warp = size_t(kSortWarps) * kSortWarpCap * sizeof(u64);
     const size_t smem_block = size_t(kSortBlockCap) * sizeof(u64);
@@ -541,7 +656,10 @@ void launch_sort(const u64* offsets, u64* records, uint32_t P, uint32_t* scratch
     // Lists the register sorts leave unsettled join the block-sort class (6).
     uint32_t* redo_n = scratch + 6;
     uint32_t* redo = items(6);
-    auto q = [&](int c) { return ((surrogate_classes >> c) & 1u) != 0; };
+    // Per class: 2 = distribution sort, 1 = surrogate keys, 0 = 64-bit bitonic.
+    auto q = [&](int c) {
+        return ((bucket_classes >> c) & 1u) ? 2 : (((surrogate_classes >> c) & 1u) ? 1 : 0);
+    };
     k_sort_class_regs<1, false><<<g, kSortWarps * 32, 0, s>>>(offsets, records, items(0), scratch + 0, redo_n, redo,
                                                               ok);
     sort_class<2>(q(1), g, offsets, records, items(1), scratch + 1, redo_n, redo, ok, s);

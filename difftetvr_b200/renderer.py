@@ -148,19 +148,20 @@ class Renderer:
         t = _lib.Tuning()
         _lib.call("dtv_renderer_get_tuning", self._handle, ctypes.byref(t))
         return {"composite_tile": t.composite_tile, "adjoint_tile": t.adjoint_tile,
-                "sort_surrogate_classes": t.sort_surrogate_classes}
+                "sort_surrogate_classes": t.sort_surrogate_classes, "sort_bucket_classes": t.sort_bucket_classes}
 
     def set_tuning(self, composite_tile: int | None = None, adjoint_tile: int | None = None,
-                   sort_surrogate_classes: int | None = None) -> None:
+                   sort_surrogate_classes: int | None = None, sort_bucket_classes: int | None = None) -> None:
         """Pixel tile of the composite / adjoint blocks (0: 16x16, 1: 32x8,
-        2: 8x32) and the sort method per list-length class (bit c of
-        sort_surrogate_classes, c = 1..4).  Results are identical for every
-        setting."""
+        2: 8x32) and the sort method per list-length class c = 1..4: depth
+        buckets (bit c of sort_bucket_classes), else 32-bit surrogate keys (bit
+        c of sort_surrogate_classes), else the 64-bit network.  Results are
+        identical for every setting."""
         cur = self.get_tuning()
-        t = _lib.Tuning(cur["composite_tile"] if composite_tile is None else int(composite_tile),
-                        cur["adjoint_tile"] if adjoint_tile is None else int(adjoint_tile),
-                        cur["sort_surrogate_classes"] if sort_surrogate_classes is None else int(sort_surrogate_classes),
-                        0)
+        pick = lambda v, k: cur[k] if v is None else int(v)
+        t = _lib.Tuning(pick(composite_tile, "composite_tile"), pick(adjoint_tile, "adjoint_tile"),
+                        pick(sort_surrogate_classes, "sort_surrogate_classes"),
+                        pick(sort_bucket_classes, "sort_bucket_classes"))
         _lib.call("dtv_renderer_set_tuning", self._handle, ctypes.byref(t))
 
     def get_num_bands(self) -> int:

@@ -151,15 +151,17 @@ int32_t dtv_renderer_render_adjoint_cells(dtv_renderer* r, const dtv_mesh* mesh,
 /* Kernel configuration of a renderer (or batch): the pixel tile of the
  * composite and adjoint blocks (0: 16 x 16, 1: 32 x 8, 2: 8 x 32 pixels) and,
  * per list-length class c (bit c; 1..4 = lists of up to 64, 128, 256, 512
- * records), whether the per-pixel sort goes through 32-bit surrogate keys or
- * the 64-bit network.  Every setting gives the same lists, images and
+ * records), the per-pixel sort method: distribution into depth buckets plus
+ * exact fix-up (bit c of sort_bucket_classes), else 32-bit surrogate keys
+ * through a bitonic network (bit c of sort_surrogate_classes), else the
+ * 64-bit bitonic network.  Every setting gives the same lists, images and
  * gradients; they differ in speed only.  An autotuner (difftetvr_b200.autotune)
- * times them on the caller's workload.  Batches use only sort_surrogate_classes. */
+ * times them on the caller's workload.  Batches use only the sort fields. */
 typedef struct dtv_tuning {
     int32_t composite_tile;
     int32_t adjoint_tile;
     uint32_t sort_surrogate_classes;
-    int32_t reserved;
+    uint32_t sort_bucket_classes;
 } dtv_tuning;
 int32_t dtv_renderer_set_tuning(dtv_renderer* r, const dtv_tuning* tuning);
 int32_t dtv_renderer_get_tuning(const dtv_renderer* r, dtv_tuning* tuning);

@@ -10,9 +10,12 @@ from helpers import Scene, rel_err
 
 pytestmark = pytest.mark.gpu
 
-CONFIGS = [dict(composite_tile=1, adjoint_tile=2, sort_surrogate_classes=0x00),
-           dict(composite_tile=2, adjoint_tile=1, sort_surrogate_classes=0x0a),
-           dict(composite_tile=0, adjoint_tile=0, sort_surrogate_classes=0x1e)]
+CONFIGS = [dict(composite_tile=1, adjoint_tile=2, sort_surrogate_classes=0x00, sort_bucket_classes=0x00),
+           dict(composite_tile=2, adjoint_tile=1, sort_surrogate_classes=0x0a, sort_bucket_classes=0x00),
+           dict(composite_tile=0, adjoint_tile=0, sort_surrogate_classes=0x1e, sort_bucket_classes=0x00),
+           dict(composite_tile=1, adjoint_tile=0, sort_surrogate_classes=0x00, sort_bucket_classes=0x1e),
+           dict(composite_tile=0, adjoint_tile=1, sort_surrogate_classes=0x06, sort_bucket_classes=0x12)]
+DEFAULT = dict(composite_tile=0, adjoint_tile=0, sort_surrogate_classes=0x1e, sort_bucket_classes=0x1c)
 
 
 def _run(mesh, r, w):
@@ -30,7 +33,7 @@ def test_every_configuration_gives_the_same_results():
     mesh, r = sc.make_renderer()
     w = torch.randn(200, 200, 4, device="cuda", generator=torch.Generator(device="cuda").manual_seed(1))
     ref = _run(mesh, r, w)
-    assert r.get_tuning() == dict(composite_tile=0, adjoint_tile=0, sort_surrogate_classes=0x1e)
+    assert r.get_tuning() == DEFAULT
     for cfg in CONFIGS:
         r.set_tuning(**cfg)
         assert r.get_tuning() == cfg
@@ -42,6 +45,8 @@ def test_every_configuration_gives_the_same_results():
         r.set_tuning(composite_tile=3)
     with pytest.raises(RuntimeError):
         r.set_tuning(sort_surrogate_classes=0x1)
+    with pytest.raises(RuntimeError):
+        r.set_tuning(sort_bucket_classes=0x20)
 
 
 def test_autotuner_sets_and_caches_a_configuration():
@@ -51,8 +56,8 @@ def test_autotuner_sets_and_caches_a_configuration():
     out = autotune.autotune_renderer(r, trials=2, force=True)
     t = out["tuning"]
     assert t["composite_tile"] in (0, 1, 2) and t["adjoint_tile"] in (0, 1, 2)
-    assert (t["sort_surrogate_classes"] & ~0x1e) == 0
-    assert r.get_tuning() == t and len(out["timings"]) >= 9 and out["ms"] > 0
+    assert (t["sort_surrogate_classes"] & ~0x1e) == 0 and (t["sort_bucket_classes"] & ~0x1e) == 0
+    assert r.get_tuning() == t and len(out["timings"]) >= 13 and out["ms"] > 0
     r.set_tuning(composite_tile=(t["composite_tile"] + 1) % 3)
     again = autotune.autotune_renderer(r)  # cached: restores the chosen configuration
     assert again is out and r.get_tuning() == t
@@ -73,10 +78,10 @@ def test_batch_sort_configuration_and_autotune():
     br = BatchRenderer(meshes, attenuation=1.0)
     views = [View(mesh=i % 2, view_matrix=S.sphere_camera(50 + i), width=96, height=80) for i in range(4)]
     ref = [im.clone() for im in br.render(views)]
-    for mask in (0x00, 0x14):
-        br.set_tuning(sort_surrogate_classes=mask)
-        assert br.get_tuning()["sort_surrogate_classes"] == mask
+    for q, b in ((0x00, 0x00), (0x14, 0x00), (0x00, 0x1e)):
+        br.set_tuning(sort_surrogate_classes=q, sort_bucket_classes=b)
+        assert br.get_tuning() == dict(sort_surrogate_classes=q, sort_bucket_classes=b)
         for a, b in zip(br.render(views), ref):
             assert torch.equal(a, b)
     out = autotune.autotune_batch(br, views, trials=1, force=True)
-    assert br.get_tuning() == out["tuning"] and len(out["timings"]) == 5
+    assert br.get_tuning() == out["tuning"] and len(out["timings"]) == 9
