@@ -10,8 +10,9 @@
 //   K     = (t + 1/a) A - 1/a = -t x psi(x),   psi(x) = (phi1(x) - e^-x) / x
 //   dK/da = t^2 chi(x),       chi(x) = (1 - e^-x (1 + x + x^2)) / x^2
 // For x < 0.5 phi1, psi and chi come from their Taylor series (derived from
-// the exponential series; coefficients below), which avoids the cancellation
-// of the direct form (~1e-3 relative error in FP32 at a t ~ 1e-4).
+// the exponential series; coefficients below; degree 5 below x = 1/8, degree
+// 8-9 above), which avoids the cancellation of the direct form (~1e-3
+// relative error in FP32 at a t ~ 1e-4).
 // exp and the divisions use the fast hardware approximations (__expf,
 // __fdividef: a few ulp), well inside the path's 1e-5 image / 1e-4 gradient
 // tolerances; the discrete depth key never goes through this file.
@@ -71,13 +72,51 @@ __device__ __forceinline__ float series_chi(float x) {
     return p;
 }
 
+// The same series to degree 5, for x < 1/8: the first omitted term at x = 1/8
+// is x^6/7! = 7.6e-10 for phi1, 7 x^6/8! = 6.6e-10 for psi and
+// 49 x^6/8! = 4.6e-9 for chi, at most about 1e-8 of the value (under one
+// FP32 ulp).  At the path's densities and segment lengths nearly every
+// sub-segment has x < 1/8.
+__device__ __forceinline__ float series_phi1_short(float x) {
+    float p = -1.38888889e-3f;
+    p = fmaf(p, x, 8.33333333e-3f);
+    p = fmaf(p, x, -4.16666667e-2f);
+    p = fmaf(p, x, 0.166666667f);
+    p = fmaf(p, x, -0.5f);
+    p = fmaf(p, x, 1.0f);
+    return p;
+}
+
+__device__ __forceinline__ float series_psi_short(float x) {
+    float p = -1.19047619e-3f;
+    p = fmaf(p, x, 6.94444444e-3f);
+    p = fmaf(p, x, -3.33333333e-2f);
+    p = fmaf(p, x, 0.125f);
+    p = fmaf(p, x, -0.333333333f);
+    p = fmaf(p, x, 0.5f);
+    return p;
+}
+
+__device__ __forceinline__ float series_chi_short(float x) {
+    float p = 7.14285714e-3f;
+    p = fmaf(p, x, -3.47222222e-2f);
+    p = fmaf(p, x, 0.133333333f);
+    p = fmaf(p, x, -0.375f);
+    p = fmaf(p, x, 0.666666667f);
+    p = fmaf(p, x, -0.5f);
+    return p;
+}
+
 // Forward terms; caller guarantees a > 0.  (The reference drops a < 1e-6; the
 // continuous value kept here differs from that by at most a t.)
 __device__ __forceinline__ SegTerms seg_terms(float t, float a) {
     SegTerms s;
     const float x = a * t;
     s.A = __expf(-x);
-    if (x < 0.5f) {
+    if (x < 0.125f) {
+        s.omA = x * series_phi1_short(x);
+        s.K = -t * x * series_psi_short(x);
+    } else if (x < 0.5f) {
         s.omA = x * series_phi1(x);
         s.K = -t * x * series_psi(x);
     } else {
@@ -95,7 +134,11 @@ __device__ __forceinline__ SegTerms seg_terms_adj(float t, float a) {
     const float x = a * t;
     s.A = __expf(-x);
     float chi;
-    if (x < 0.5f) {
+    if (x < 0.125f) {
+        s.omA = x * series_phi1_short(x);
+        s.K = -t * x * series_psi_short(x);
+        chi = series_chi_short(x);
+    } else if (x < 0.5f) {
         s.omA = x * series_phi1(x);
         s.K = -t * x * series_psi(x);
         chi = series_chi(x);
