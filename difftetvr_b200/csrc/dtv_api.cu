@@ -207,12 +207,16 @@ void adjoint_rows(dtv_renderer* r, const dtv_mesh* mesh, const float* d_colors, 
                                  r->grad_rows.ptr, s, r->tuning.adjoint_tile);
 }
 
-void scatter_rows(dtv_renderer* r, float* d_grad_positions, float* d_grad_colors, cudaStream_t s) {
+// The list adjoint (launch_adjoint_rows) leaves screen-space position rows
+// unless absolute gradients were asked for.
+void scatter_rows(dtv_renderer* r, const dtv::ShadeDev& sh, float* d_grad_positions, float* d_grad_colors,
+                  cudaStream_t s) {
     if (r->cells)
         dtv::launch_scatter_positions(r->grad_rows.ptr, uint32_t(r->V), d_grad_positions, s);
     else
         dtv::launch_scatter_grads(r->grad_rows.ptr, uint32_t(r->V), d_grad_positions,
-                                  reinterpret_cast<float4*>(d_grad_colors), s);
+                                  reinterpret_cast<float4*>(d_grad_colors), s,
+                                  sh.use_abs_grad ? nullptr : r->vgeo.ptr, &r->cam);
 }
 
 // Forward in row bands (fragment lists over the budget): after the full count
@@ -260,7 +264,7 @@ void adjoint_banded(dtv_renderer* r, const dtv_mesh* mesh, const float* d_colors
         adjoint_rows(r, mesh, d_colors, d_image_adjoint, sh, b.first, b.second, d_grad_colors, s);
         check_launch("band adjoint");
     }
-    scatter_rows(r, d_grad_positions, d_grad_colors, s);
+    scatter_rows(r, sh, d_grad_positions, d_grad_colors, s);
     check_launch("scatter gradients");
     record_flags(r, s);
 }
@@ -600,7 +604,7 @@ int32_t adjoint_common(dtv_renderer* r, const dtv_mesh* mesh, const float* d_pos
             DTV_CK(cudaMemsetAsync(r->grad_rows.ptr, 0, sizeof(float4) * 2 * size_t(r->V ? r->V : 1), s));
             adjoint_rows(r, mesh, d_colors, d_image_adjoint, sh, 0, r->cam.H, d_grad_colors, s);
             check_launch("adjoint");
-            scatter_rows(r, d_grad_positions, d_grad_colors, s);
+            scatter_rows(r, sh, d_grad_positions, d_grad_colors, s);
             check_launch("scatter gradients");
         }
         rec_event(r, 8, s);

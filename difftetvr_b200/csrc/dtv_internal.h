@@ -67,7 +67,10 @@ void launch_adjoint_rows(const unsigned long long* offsets, const unsigned long 
                          const float4* dimage, const float* tfinal, const uint32_t* term, int row0, int row1,
                          float4* grad_rows, cudaStream_t s, int tile = 0);
 // Adds the interleaved [V][2] gradient rows into grad_pos [V,3] / grad_col [V,4].
-void launch_scatter_grads(const float4* grad_rows, uint32_t V, float* grad_pos, float4* grad_col, cudaStream_t s);
+// screen_vgeo / cam: rows hold screen-space position adjoints of that camera
+// (the list adjoint without absolute gradients); nullptr: world-space rows.
+void launch_scatter_grads(const float4* grad_rows, uint32_t V, float* grad_pos, float4* grad_col, cudaStream_t s,
+                          const VGeo* screen_vgeo = nullptr, const CamDev* cam = nullptr);
 
 void launch_loss_l2(const float* image, const float* target, uint64_t n, float scale, float* adjoint,
                     float* loss_accum, cudaStream_t s);

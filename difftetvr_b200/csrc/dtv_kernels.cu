@@ -712,7 +712,7 @@ void launch_composite(const u64* offsets, const u64* records, const uint4* faces
 
 // ---------------------------------------------------------------------------
 // (f) adjoint (adjoint_pixel).
-template <int TX>
+template <int TX, bool SCREEN>
 __global__ void __launch_bounds__(256) k_adjoint(
     const u64* __restrict__ offsets, const u64* __restrict__ records, const uint4* __restrict__ faces,
     const VGeo* __restrict__ vgeo, const float4* __restrict__ colors, int W, int row0, int row1, CamDev cam,
@@ -725,16 +725,25 @@ __global__ void __launch_bounds__(256) k_adjoint(
     const int py = row0 + int(blockIdx.y) * TY + int(threadIdx.x / TX);
     if (px >= W || py >= row1) return;
     VertCache acc{grad_rows, vcache4 + threadIdx.x, vcache1 + threadIdx.x, 256};
-    adjoint_pixel(px, py, offsets, records, faces, vgeo, colors, W, cam, sh, dimage, tfinal, term, acc);
+    adjoint_pixel<VertCache, SCREEN>(px, py, offsets, records, faces, vgeo, colors, W, cam, sh, dimage, tfinal, term,
+                                     acc);
 }
 
-// Adds the interleaved rows into the caller's gradient buffers.
+// Adds the interleaved rows into the caller's gradient buffers (SCREEN: the
+// position rows hold screen-space adjoints, converted here per vertex).
+template <bool SCREEN>
 __global__ void __launch_bounds__(256) k_scatter_grads(const float4* __restrict__ rows, uint32_t V,
                                                        float* __restrict__ grad_pos,
-                                                       float4* __restrict__ grad_col) {
+                                                       float4* __restrict__ grad_col,
+                                                       const VGeo* __restrict__ vgeo, CamDev cam) {
     const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= V) return;
-    const float4 a = rows[2 * size_t(v)], b = rows[2 * size_t(v) + 1];
+    float4 a = rows[2 * size_t(v)];
+    const float4 b = rows[2 * size_t(v) + 1];
+    if (SCREEN) {
+        const float3 w = screen_to_world(a, vgeo[v], cam);
+        a = make_float4(w.x, w.y, w.z, 0.f);
+    }
     float* gp = grad_pos + 3 * size_t(v);
     gp[0] += a.x;
     gp[1] += a.y;
@@ -750,7 +759,7 @@ void launch_adjoint(const u64* offsets, const u64* records, const uint4* faces, 
     cudaMemsetAsync(grad_rows, 0, sizeof(float4) * 2 * size_t(V), s);
     launch_adjoint_rows(offsets, records, faces, vgeo, colors, cam, sh, dimage, tfinal, term, 0, cam.H, grad_rows,
                         s);
-    launch_scatter_grads(grad_rows, V, grad_pos, grad_col, s);
+    launch_scatter_grads(grad_rows, V, grad_pos, grad_col, s, sh.use_abs_grad ? nullptr : vgeo, &cam);
 }
 
 template <int TX>
@@ -759,8 +768,14 @@ void adjoint_tiles(const u64* offsets, const u64* records, const uint4* faces, c
                    const float* tfinal, const uint32_t* term, int row0, int row1, float4* grad_rows, cudaStream_t s) {
     constexpr int TY = 256 / TX;
     dim3 grid((cam.W + TX - 1) / TX, (row1 - row0 + TY - 1) / TY);
-    k_adjoint<TX><<<grid, 256, 0, s>>>(offsets, records, faces, vgeo, colors, cam.W, row0, row1, cam, sh, dimage,
-                                       tfinal, term, grad_rows);
+    // Rows in screen space unless absolute gradients are asked for (see
+    // frag_vertex_grads); launch_scatter_grads converts with the same rule.
+    if (sh.use_abs_grad)
+        k_adjoint<TX, false><<<grid, 256, 0, s>>>(offsets, records, faces, vgeo, colors, cam.W, row0, row1, cam, sh,
+                                                  dimage, tfinal, term, grad_rows);
+    else
+        k_adjoint<TX, true><<<grid, 256, 0, s>>>(offsets, records, faces, vgeo, colors, cam.W, row0, row1, cam, sh,
+                                                 dimage, tfinal, term, grad_rows);
 }
 
 void launch_adjoint_rows(const u64* offsets, const u64* records, const uint4* faces, const VGeo* vgeo,
@@ -779,8 +794,13 @@ void launch_adjoint_rows(const u64* offsets, const u64* records, const uint4* fa
                           s);
 }
 
-void launch_scatter_grads(const float4* grad_rows, uint32_t V, float* grad_pos, float4* grad_col, cudaStream_t s) {
-    if (V) k_scatter_grads<<<(V + 255) / 256, 256, 0, s>>>(grad_rows, V, grad_pos, grad_col);
+void launch_scatter_grads(const float4* grad_rows, uint32_t V, float* grad_pos, float4* grad_col, cudaStream_t s,
+                          const VGeo* screen_vgeo, const CamDev* cam) {
+    if (!V) return;
+    if (screen_vgeo)
+        k_scatter_grads<true><<<(V + 255) / 256, 256, 0, s>>>(grad_rows, V, grad_pos, grad_col, screen_vgeo, *cam);
+    else
+        k_scatter_grads<false><<<(V + 255) / 256, 256, 0, s>>>(grad_rows, V, grad_pos, grad_col, nullptr, CamDev{});
 }
 
 // ---------------------------------------------------------------------------

@@ -472,8 +472,13 @@ struct VertCache {
 
 // Vertex gradients of one fragment from its depth adjoint gz, its colour
 // adjoint gC w (gC = (g0, g1, g2), the pixel's) and its alpha adjoint ga,
-// through the perspective-correct barycentrics and the projection.
-template <class Acc>
+// through the perspective-correct barycentrics and the projection.  With
+// SCREEN the position part stops at the vertex's screen-space adjoints
+// (d/dsx, d/dsy, d/d(1/ze)): the projection is linear in them with
+// coefficients of the vertex alone, so it is applied once per vertex when the
+// rows are scattered (screen_to_world) -- valid for one camera per row buffer
+// and without absolute-value gradients.
+template <class Acc, bool SCREEN = false>
 __device__ __forceinline__ void frag_vertex_grads(const FragV& fr, float qx, float qy,
                                                   const VGeo* __restrict__ vgeo,
                                                   const float4* __restrict__ colors, const CamDev& cam,
@@ -522,6 +527,15 @@ __device__ __forceinline__ void frag_vertex_grads(const FragV& fr, float qx, flo
     const float* V = cam.V;
     float4 gpv[3];
     float gav[3];
+    if (SCREEN) {
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            gpv[j] = make_float4(gsx[j], gsy[j], giz[j], w * fi.bary[j]);
+            gav[j] = ga * fi.bary[j];
+        }
+        acc.add_face(vi, gpv, gav);
+        return;
+    }
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
         const float iz = P[j].iz;
@@ -646,7 +660,19 @@ __device__ __forceinline__ void frag_position_grads(const uint4& fc, float qx, f
     }
 }
 
-template <class Acc>
+// World-space position gradient of a vertex from its summed screen-space
+// adjoints a = (d/dsx, d/dsy, d/d(1/ze)) (frag_vertex_grads with SCREEN).
+__device__ __forceinline__ float3 screen_to_world(const float4& a, const VGeo& P, const CamDev& cam) {
+    const float iz = P.iz;
+    const float gxv = a.x * cam.f * iz;
+    const float gyv = -a.y * cam.f * iz;
+    const float gzv = (a.z + cam.f * (a.x * P.xv - a.y * P.yv)) * iz * iz;
+    const float* V = cam.V;
+    return make_float3(V[0] * gxv + V[1] * gyv + V[2] * gzv, V[4] * gxv + V[5] * gyv + V[6] * gzv,
+                       V[8] * gxv + V[9] * gyv + V[10] * gzv);
+}
+
+template <class Acc, bool SCREEN = false>
 __device__ __forceinline__ void adjoint_pixel(
     int px, int py, const u64* __restrict__ offsets, const u64* __restrict__ records, const uint4* __restrict__ faces,
     const VGeo* __restrict__ vgeo, const float4* __restrict__ colors, int W, const CamDev& cam, const ShadeDev& sh,
@@ -696,14 +722,14 @@ __device__ __forceinline__ void adjoint_pixel(
             gz_f -= g_tot;
             gz_b += g_tot;
         }
-        frag_vertex_grads(fb, qx, qy, vgeo, colors, cam, gz_b, gC0, gC1, gC2, wb, ab, use_abs, acc);
+        frag_vertex_grads<Acc, SCREEN>(fb, qx, qy, vgeo, colors, cam, gz_b, gC0, gC1, gC2, wb, ab, use_abs, acc);
         fb = ff;
         pb = pf;
         gz_b = gz_f;
         wb = wf;
         ab = af;
     }
-    frag_vertex_grads(fb, qx, qy, vgeo, colors, cam, gz_b, gC0, gC1, gC2, wb, ab, use_abs, acc);
+    frag_vertex_grads<Acc, SCREEN>(fb, qx, qy, vgeo, colors, cam, gz_b, gC0, gC1, gC2, wb, ab, use_abs, acc);
     acc.flush();
 }
 
