@@ -151,6 +151,7 @@ __global__ void __launch_bounds__(kTile * kTile, 2) k_walk_composite(
     wstate[p] = make_uint4(last_tet, last_entry, last_b, nseg);
 }
 
+template <bool SCREEN>
 __global__ void __launch_bounds__(kTile * kTile, 2) k_walk_adjoint(
     const u64* __restrict__ b_offsets, const u64* __restrict__ b_records, const uint32_t* __restrict__ bf_global,
     const uint4* __restrict__ faces, const uint32_t* __restrict__ f2t, const uint32_t* __restrict__ tet_faces,
@@ -197,9 +198,10 @@ __global__ void __launch_bounds__(kTile * kTile, 2) k_walk_adjoint(
         segment_adjoint(tSeg, f0.col, f1.col, p0, p1, atten, T, gT, g_tot, we, wx, ae, ax);
         float gz_e = -g_tot * scale;
         gz_x += g_tot * scale;
-        frag_vertex_grads(f1, qx, qy, vgeo, colors, cam, gz_x, gC0, gC1, gC2, wx, ax, use_abs, acc);
+        frag_vertex_grads<GradAcc, SCREEN>(f1, qx, qy, vgeo, colors, cam, gz_x, gC0, gC1, gC2, wx, ax, use_abs, acc);
         if (faces[fe].w & 1u) {
-            frag_vertex_grads(f0, qx, qy, vgeo, colors, cam, gz_e, gC0, gC1, gC2, we, ae, use_abs, acc);
+            frag_vertex_grads<GradAcc, SCREEN>(f0, qx, qy, vgeo, colors, cam, gz_e, gC0, gC1, gC2, we, ae, use_abs,
+                                               acc);
             // Previous interval: its exit is the last back-facing boundary fragment before b.
             int bb = b - 1;
             while (bb >= 0 && (uint32_t(b_records[beg + bb]) & 1u)) --bb;
@@ -247,10 +249,17 @@ void launch_walk_adjoint(const u64* b_offsets, const u64* b_records, const uint3
                          uint32_t V, float4* grad_rows, float* grad_pos, float4* grad_col, cudaStream_t s) {
     cudaMemsetAsync(grad_rows, 0, sizeof(float4) * 2 * size_t(V), s);
     dim3 grid((cam.W + kTile - 1) / kTile, (cam.H + kTile - 1) / kTile);
-    k_walk_adjoint<<<grid, kTile * kTile, 0, s>>>(b_offsets, b_records, bf_global, faces, face_to_tet, tet_faces,
-                                                  num_tets, vfix, vgeo, colors, cam, sh, dimage, tfinal, wstate,
-                                                  grad_rows);
-    launch_scatter_grads(grad_rows, V, grad_pos, grad_col, s);
+    // Screen-space position rows unless absolute gradients are asked for
+    // (frag_vertex_grads); the scatter converts them per vertex.
+    if (sh.use_abs_grad)
+        k_walk_adjoint<false><<<grid, kTile * kTile, 0, s>>>(b_offsets, b_records, bf_global, faces, face_to_tet,
+                                                             tet_faces, num_tets, vfix, vgeo, colors, cam, sh, dimage,
+                                                             tfinal, wstate, grad_rows);
+    else
+        k_walk_adjoint<true><<<grid, kTile * kTile, 0, s>>>(b_offsets, b_records, bf_global, faces, face_to_tet,
+                                                            tet_faces, num_tets, vfix, vgeo, colors, cam, sh, dimage,
+                                                            tfinal, wstate, grad_rows);
+    launch_scatter_grads(grad_rows, V, grad_pos, grad_col, s, sh.use_abs_grad ? nullptr : vgeo, &cam);
 }
 
 }  // namespace dtv
