@@ -527,33 +527,32 @@ __device__ __forceinline__ void frag_vertex_grads(const FragV& fr, float qx, flo
     const float* V = cam.V;
     float4 gpv[3];
     float gav[3];
-    if (SCREEN) {
+    if constexpr (SCREEN) {
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
             gpv[j] = make_float4(gsx[j], gsy[j], giz[j], w * fi.bary[j]);
             gav[j] = ga * fi.bary[j];
         }
-        acc.add_face(vi, gpv, gav);
-        return;
-    }
+    } else {
 #pragma unroll
-    for (int j = 0; j < 3; ++j) {
-        const float iz = P[j].iz;
-        const float gxv = gsx[j] * cam.f * iz;
-        const float gyv = -gsy[j] * cam.f * iz;
-        const float giz_t = giz[j] + cam.f * (gsx[j] * P[j].xv - gsy[j] * P[j].yv);
-        const float gzv = giz_t * iz * iz;
-        float gp0 = V[0] * gxv + V[1] * gyv + V[2] * gzv;
-        float gp1 = V[4] * gxv + V[5] * gyv + V[6] * gzv;
-        float gp2 = V[8] * gxv + V[9] * gyv + V[10] * gzv;
-        float s1 = w * fi.bary[j], s2 = ga * fi.bary[j];
-        if (use_abs) {
-            gp0 = fabsf(gp0); gp1 = fabsf(gp1); gp2 = fabsf(gp2);
-            s1 = fabsf(s1);
-            s2 = fabsf(s2);
+        for (int j = 0; j < 3; ++j) {
+            const float iz = P[j].iz;
+            const float gxv = gsx[j] * cam.f * iz;
+            const float gyv = -gsy[j] * cam.f * iz;
+            const float giz_t = giz[j] + cam.f * (gsx[j] * P[j].xv - gsy[j] * P[j].yv);
+            const float gzv = giz_t * iz * iz;
+            float gp0 = V[0] * gxv + V[1] * gyv + V[2] * gzv;
+            float gp1 = V[4] * gxv + V[5] * gyv + V[6] * gzv;
+            float gp2 = V[8] * gxv + V[9] * gyv + V[10] * gzv;
+            float s1 = w * fi.bary[j], s2 = ga * fi.bary[j];
+            if (use_abs) {
+                gp0 = fabsf(gp0); gp1 = fabsf(gp1); gp2 = fabsf(gp2);
+                s1 = fabsf(s1);
+                s2 = fabsf(s2);
+            }
+            gpv[j] = make_float4(gp0, gp1, gp2, s1);
+            gav[j] = s2;
         }
-        gpv[j] = make_float4(gp0, gp1, gp2, s1);
-        gav[j] = s2;
     }
     acc.add_face(vi, gpv, gav);
 }
