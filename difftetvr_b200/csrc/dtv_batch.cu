@@ -125,6 +125,14 @@ __global__ void __launch_bounds__(128) kb_raster(const BatchView* __restrict__ v
     raster_warp<FILL, WIDE>(jobs[w], __ballot_sync(0xffffffffu, live), lane, vproj, counts, offsets, records);
 }
 
+// Per-row prefix of the count pass's difference arrays, one view per grid row.
+__global__ void __launch_bounds__(256) kb_row_prefix(const BatchView* __restrict__ views,
+                                                     uint32_t* __restrict__ counts) {
+    const BatchView& bv = views[blockIdx.y];
+    const uint32_t row = blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (row < bv.H) row_prefix_warp(counts + bv.pix_base + size_t(row) * bv.W, int(bv.W), threadIdx.x & 31);
+}
+
 // ok = (records fit the buffer); *total_out = number of records.
 __global__ void kb_check_capacity(const u64* __restrict__ offsets_end, u64 capacity, uint32_t* __restrict__ ok,
                                   u64* __restrict__ total_out) {
@@ -350,6 +358,7 @@ struct dtv_batch {
     // shapes of the last render (for the adjoint)
     int nviews = 0;
     u64 tot_verts = 0, tot_faces = 0, tot_pixels = 0, tot_tiles = 0, tot_rows = 0;
+    uint32_t max_height = 0;  // tallest view (grid of the count's row prefix)
     dtv::ShadeDev sh{};
     bool have_render = false;
     u64 last_fragments = 0;
@@ -422,6 +431,9 @@ void build_views(dtv_batch* b, int nviews, const dtv_batch_view* views, bool tra
     b->tot_faces = fb;
     b->tot_pixels = pb;
     b->tot_tiles = tb;
+    uint32_t mh = 0;
+    for (int i = 0; i < nviews; ++i) mh = std::max(mh, b->h_views[i].H);
+    b->max_height = mh;
 }
 
 void ensure_scratch(dtv_batch* b, cudaStream_t s) {
@@ -453,7 +465,8 @@ void upload_views(dtv_batch* b, cudaStream_t s) {
 }
 
 // Count (FILL false) or fill pass over every view's faces: the 32-bit faces,
-// then the 64-bit ones (kb_raster).
+// then the 64-bit ones (kb_raster); the count's difference arrays are then
+// summed along each view's rows (kb_row_prefix).
 template <bool FILL>
 void launch_kb_raster(dtv_batch* b, const uint32_t* okp, cudaStream_t s) {
     using namespace dtv;
@@ -464,6 +477,10 @@ void launch_kb_raster(dtv_batch* b, const uint32_t* okp, cudaStream_t s) {
     kb_raster<FILL, true><<<blocks, 128, 0, s>>>(b->d_views.ptr, b->nviews, b->tot_faces, b->vproj.ptr,
                                                  b->vfix.ptr, b->counts.ptr, FILL ? b->offsets.ptr : nullptr,
                                                  FILL ? b->records.ptr : nullptr, okp);
+    if (!FILL) {
+        dim3 grid(unsigned(b->max_height + 7) / 8, unsigned(b->nviews));
+        kb_row_prefix<<<grid, 256, 0, s>>>(b->d_views.ptr, b->counts.ptr);
+    }
 }
 
 // Enqueues project, count, scan, [capacity guard], fill, sort, composite.
@@ -806,6 +823,7 @@ void enqueue_train_body(dtv_batch* b, const dtv::AdamConst& ac, int nslots, cuda
 
 std::vector<u64> train_signature(const dtv_batch* b, const dtv::AdamConst& ac, int nslots) {
     std::vector<u64> sig = {u64(b->nviews), b->tot_verts, b->tot_faces, b->tot_pixels, b->tot_tiles, b->tot_rows,
+                            u64(b->max_height),
                             b->capacity, u64(nslots), u64(uintptr_t(b->records.ptr)),
                             u64(uintptr_t(b->dimage_internal.ptr)), u64(uintptr_t(b->grad_rows.ptr))};
     const uint32_t* shw = reinterpret_cast<const uint32_t*>(&b->sh);

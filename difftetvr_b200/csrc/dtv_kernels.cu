@@ -54,15 +54,23 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster(const uint4* __res
     raster_warp<FILL, WIDE>(jobs[w], __ballot_sync(kFull, live), lane, vproj, counts, offsets, records);
 }
 
+// Difference array of the count pass -> per-pixel counts, rows [row0, row1).
+__global__ void __launch_bounds__(256) k_row_prefix(uint32_t* __restrict__ counts, int W, int row0, int row1) {
+    const int row = row0 + int(blockIdx.x) * 8 + int(threadIdx.x >> 5);
+    if (row < row1) row_prefix_warp(counts + size_t(row) * W, W, threadIdx.x & 31);
+}
+
 void launch_raster_count(const uint4* faces, uint32_t F, const float4* vproj, const int2* vfix, int W, int H,
                          uint32_t* counts, cudaStream_t s, int row0, int row1) {
     if (F == 0) return;
     if (row1 < 0) row1 = H;
+    if (row1 <= row0) return;
     const unsigned blocks = (F + 32 * kRasterWarps - 1) / (32 * kRasterWarps);
     k_raster<false, false><<<blocks, 32 * kRasterWarps, 0, s>>>(faces, F, vproj, vfix, W, row0, row1, counts, nullptr,
                                                                 nullptr);
     k_raster<false, true><<<blocks, 32 * kRasterWarps, 0, s>>>(faces, F, vproj, vfix, W, row0, row1, counts, nullptr,
                                                                nullptr);
+    k_row_prefix<<<unsigned(row1 - row0 + 7) / 8, 256, 0, s>>>(counts, W, row0, row1);
 }
 
 void launch_raster_fill(const uint4* faces, uint32_t F, const float4* vproj, const int2* vfix, int W, int H,

@@ -13,13 +13,15 @@ constexpr int kTile = 16;  // composite / adjoint pixel tile (16 x 16 threads)
 // ---------------------------------------------------------------------------
 // (a)+(b) face rasterisation, warp-cooperative.  Each lane of a warp sets up
 // one face (projected fixed-point vertices, orientation, clipped bounding box)
-// into shared memory; the warp then takes the faces one at a time and spreads
-// the pixels of the face's bounding box over its 32 lanes (pixel k of the box,
-// row-major, goes to lane k mod 32), so lanes stay busy whatever the sizes of
-// the faces a warp holds.  COUNT mode increments the per-pixel counter; FILL
-// mode writes the record at offsets[p] + (--counts[p]), leaving counts zeroed
-// for the next render.  Only pixel rows [row0, row1) are visited (row bands of
-// a render whose lists do not fit the fragment budget at once).
+// into shared memory; the warp then takes the faces one at a time.  Each box
+// row of a face meets it in one interval of pixel centres, found exactly per
+// row (row_span).  COUNT mode adds +1 / -1 at the ends of each row's interval
+// to a per-row difference array in `counts`, which row_prefix_counts turns
+// into per-pixel counts; FILL mode spreads the covered pixels of the face over
+// the warp's lanes and writes each record at offsets[p] + (--counts[p]),
+// leaving counts zeroed for the next render.  Only pixel rows [row0, row1) are
+// visited (row bands of a render whose lists do not fit the fragment budget at
+// once).
 //
 // Coverage: edge functions in 1/256-pixel fixed point, evaluated relative to
 // the centre of the box's first pixel (edge functions are translation
@@ -100,164 +102,182 @@ struct EdgeT {
     __device__ __forceinline__ I at(int c, int r) const { return base + sx * I(c) + sy * I(r); }
 };
 
-// U pixels of job J's box per lane per step: coverage tests, then (FILL) the
-// offset loads, counter atomics and depth keys of all U before the stores.
-template <bool FILL, typename I, int U>
-__device__ __forceinline__ void raster_pixels(const RasterJob& J, const int (&c)[U], const int (&r)[U],
-                                              const bool (&valid)[U], const EdgeT<I>& e0, const EdgeT<I>& e1,
-                                              const EdgeT<I>& e2, u64 pbase, const float4& va, const float4& vb,
-                                              const float4& vc, uint32_t* __restrict__ counts,
-                                              const u64* __restrict__ offsets, u64* __restrict__ records) {
-    bool in[U];
-    u64 p[U];
-#pragma unroll
-    for (int k = 0; k < U; ++k) {
-        in[k] = valid[k] && (e0.at(c[k], r[k]) | e1.at(c[k], r[k]) | e2.at(c[k], r[k])) >= I(0);
-        p[k] = pbase + uint32_t(r[k] * J.W + c[k]);
-    }
-    if (FILL) {
-        uint32_t slot[U];
-        u64 off[U];
-        float z[U];
-#pragma unroll
-        for (int k = 0; k < U; ++k) {
-            if (in[k]) {
-                off[k] = offsets[p[k]];
-                slot[k] = atomicSub(&counts[p[k]], 1u);
-                z[k] = depth_key(va, vb, vc, float(J.px0 + c[k]) + 0.5f, float(J.py0 + r[k]) + 0.5f);
-            }
-        }
-#pragma unroll
-        for (int k = 0; k < U; ++k)
-            if (in[k]) records[off[k] + slot[k] - 1u] = (u64(__float_as_uint(z[k])) << 32) | J.bits;
-    } else {
-#pragma unroll
-        for (int k = 0; k < U; ++k)
-            if (in[k]) atomicAdd(&counts[p[k]], 1u);
-    }
-}
-
-// Conservative column range of row r for one edge: T(c, r) >= 0 is
-// c >= -q / sx (sx > 0) or c <= -q / sx (sx < 0), q = base + sy r; sx = 0
-// makes the row all-in or all-out.  The bound is taken in FP32 (relative
-// error a few 2^-24, below 0.01 px for every bound inside the box) and the
-// caller widens the range by one pixel on each side, so it holds every
-// covered pixel; each pixel of the range is then tested exactly.
+// Exact column range of box row r under one edge: T(c, r) = q + sx c >= 0
+// with q = base + sy r is c >= -q / sx (sx > 0) or c <= -q / sx (sx < 0);
+// sx = 0 makes the row all-in or all-out.  The bound is estimated in FP32
+// (relative error a few 2^-24: under 0.01 px for every bound inside a box of
+// at most 2^14 px, clamped to [-2, bw + 1] beyond it) and corrected by one
+// exact integer test on each side, so lo / hi are the exact first / last
+// columns the edge admits.
 template <typename I>
-__device__ __forceinline__ void span_edge(const EdgeT<I>& e, float inv_sx, int r, float& lo, float& hi,
-                                          bool& empty) {
+__device__ __forceinline__ void span_edge(const EdgeT<I>& e, float inv_sx, int r, int bw, int& lo, int& hi) {
     const I q = e.base + e.sy * I(r);
     if (e.sx == I(0)) {
-        empty |= q < I(0);
-    } else {
-        const float b = -float(q) * inv_sx;
-        if (e.sx > I(0))
-            lo = fmaxf(lo, b);
-        else
-            hi = fminf(hi, b);
-    }
-}
-
-// Count pass over a face whose box is under 64 px a side: box pixel k goes
-// to lane k mod 32, two pixels per lane per step.  Row of pixel k:
-// floor((k + 1/2) * rn(1/bw)) in FP32 -- k + 1/2 is exact (k < 2^12), the
-// product is within 2^-23 relative of (k + 1/2) / bw, i.e. within
-// rows * 2^-23 < 1/(4 bw) of it, while (k + 1/2) / bw is at least 1/(2 bw)
-// away from every integer.
-__device__ __forceinline__ void count_job_box(const RasterJob& J, int lane, uint32_t* __restrict__ counts) {
-    constexpr int U = 2;
-    EdgeT<int> e0, e1, e2;
-    e0.set(J.ax1, J.ay1, J.ax2, J.ay2);
-    e1.set(J.ax2, J.ay2, J.ax0, J.ay0);
-    e2.set(J.ax0, J.ay0, J.ax1, J.ay1);
-    const u64 pbase = J.pix_base + u64(J.py0) * u64(J.W) + u64(J.px0);
-    const float4 none = make_float4(0.f, 0.f, 0.f, 0.f);
-    const int area = J.bw * J.bh;
-    const float inv = __frcp_rn(float(J.bw));
-    for (int base = 0; base < area; base += 32 * U) {
-        int c[U], r[U];
-        bool valid[U];
-#pragma unroll
-        for (int k = 0; k < U; ++k) {
-            const int idx = base + 32 * k + lane;
-            valid[k] = idx < area;
-            r[k] = __float2int_rz(__fmul_rn(__fadd_rn(float(idx), 0.5f), inv));
-            c[k] = idx - r[k] * J.bw;
+        if (q < I(0)) {
+            lo = bw;
+            hi = -1;
         }
-        raster_pixels<false, int, U>(J, c, r, valid, e0, e1, e2, pbase, none, none, none, counts, nullptr,
-                                     nullptr);
+        return;
+    }
+    const float b = fminf(fmaxf(-float(q) * inv_sx, -2.f), float(bw) + 1.f);
+    if (e.sx > I(0)) {
+        int c = int(ceilf(b));  // first column with T >= 0, up to one off
+        if (q + e.sx * I(c - 1) >= I(0))
+            --c;
+        else if (q + e.sx * I(c) < I(0))
+            ++c;
+        lo = max(lo, c);
+    } else {
+        int c = int(floorf(b));  // last column with T >= 0, up to one off
+        if (q + e.sx * I(c + 1) >= I(0))
+            ++c;
+        else if (q + e.sx * I(c) < I(0))
+            --c;
+        hi = min(hi, c);
     }
 }
 
-// One face: the warp takes the box rows 32 at a time (lane = row), finds each
-// row's candidate span, and spreads the concatenated spans over its lanes
-// (slot s -> row by a binary search of the spans' exclusive prefix sums).
-// Fewer slots than the whole box (about the covered pixels plus two per row)
-// for more work per face: used by the fill, whose covered pixels dominate,
-// and for 64-bit faces; the count of 32-bit faces walks the box.
+// Covered columns [xl, xl + len) of box row r (len 0: none): exactly the
+// pixels whose centres pass all three edge tests, since a row meets a
+// triangle in one interval.
+template <typename I>
+__device__ __forceinline__ int row_span(const EdgeT<I>& e0, const EdgeT<I>& e1, const EdgeT<I>& e2, float i0,
+                                        float i1, float i2, int r, int bw, int& xl) {
+    int lo = 0, hi = bw - 1;
+    span_edge(e0, i0, r, bw, lo, hi);
+    span_edge(e1, i1, r, bw, lo, hi);
+    span_edge(e2, i2, r, bw, lo, hi);
+    xl = lo;
+    return max(0, hi - lo + 1);
+}
+
+struct FaceEdges {
+    // Counter-clockwise edges e0: 1 -> 2, e1: 2 -> 0, e2: 0 -> 1, and their
+    // column-step reciprocals for the FP32 span estimates.
+    template <typename I>
+    __device__ __forceinline__ static void make(const RasterJob& J, EdgeT<I>& e0, EdgeT<I>& e1, EdgeT<I>& e2,
+                                                float& i0, float& i1, float& i2) {
+        e0.set(I(J.ax1), I(J.ay1), I(J.ax2), I(J.ay2));
+        e1.set(I(J.ax2), I(J.ay2), I(J.ax0), I(J.ay0));
+        e2.set(I(J.ax0), I(J.ay0), I(J.ax1), I(J.ay1));
+        i0 = e0.sx != I(0) ? __frcp_rn(float(e0.sx)) : 0.f;
+        i1 = e1.sx != I(0) ? __frcp_rn(float(e1.sx)) : 0.f;
+        i2 = e2.sx != I(0) ? __frcp_rn(float(e2.sx)) : 0.f;
+    }
+};
+
+// Count pass over one face: lane = box row, 32 rows at a time; each row's
+// exact span adds +1 at its first pixel and -1 after its last one (when that
+// is still in the image row) to a per-row difference array held in `counts`
+// (u32, modulo 2^32); row_prefix_counts turns it into per-pixel counts.  Two
+// atomics per face row instead of one per covered pixel.
+template <typename I>
+__device__ __forceinline__ void count_job_rows(const RasterJob& J, int lane, uint32_t* __restrict__ counts) {
+    EdgeT<I> e0, e1, e2;
+    float i0, i1, i2;
+    FaceEdges::make(J, e0, e1, e2, i0, i1, i2);
+    const u64 pbase = J.pix_base + u64(J.py0) * u64(J.W) + u64(J.px0);
+    for (int r = lane; r < J.bh; r += 32) {
+        int xl;
+        const int len = row_span(e0, e1, e2, i0, i1, i2, r, J.bw, xl);
+        if (len > 0) {
+            uint32_t* row = counts + pbase + u64(r) * u64(J.W);
+            atomicAdd(row + xl, 1u);
+            if (J.px0 + xl + len < J.W) atomicAdd(row + xl + len, 0xffffffffu);
+        }
+    }
+}
+
+// Per-row inclusive prefix, in place, of the count pass's difference array
+// (u32 arithmetic modulo 2^32, so the -1 entries wrap and the sums come out
+// exact): one warp per image row.
+__device__ __forceinline__ void row_prefix_warp(uint32_t* row, int W, int lane) {
+    uint32_t carry = 0;
+    for (int x0 = 0; x0 < W; x0 += 32) {
+        const int x = x0 + lane;
+        uint32_t v = x < W ? row[x] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane >= o) v += t;
+        }
+        v += carry;
+        if (x < W) row[x] = v;
+        carry = __shfl_sync(0xffffffffu, v, 31);
+    }
+}
+
+// Fill of U covered pixels per lane per step: offset loads, counter atomics
+// and depth keys of all U before the stores.  A counter already at zero
+// (which matching count and fill spans never leave) skips the store, so a
+// record is never written outside its list.
+template <typename I, int U>
+__device__ __forceinline__ void fill_pixels(const RasterJob& J, const int (&c)[U], const int (&r)[U],
+                                            const bool (&valid)[U], u64 pbase, const float4& va, const float4& vb,
+                                            const float4& vc, uint32_t* __restrict__ counts,
+                                            const u64* __restrict__ offsets, u64* __restrict__ records) {
+    uint32_t slot[U];
+    u64 off[U];
+    float z[U];
+#pragma unroll
+    for (int k = 0; k < U; ++k) {
+        if (valid[k]) {
+            const u64 p = pbase + uint32_t(r[k] * J.W + c[k]);
+            off[k] = offsets[p];
+            slot[k] = atomicSub(&counts[p], 1u);
+            z[k] = depth_key(va, vb, vc, float(J.px0 + c[k]) + 0.5f, float(J.py0 + r[k]) + 0.5f);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < U; ++k)
+        if (valid[k] && slot[k] != 0u) records[off[k] + slot[k] - 1u] = (u64(__float_as_uint(z[k])) << 32) | J.bits;
+}
+
+// One face: the count walks its rows (count_job_rows); the fill takes the box
+// rows 32 at a time (lane = row), finds each row's exact span, and spreads the
+// concatenated spans over its lanes (slot s -> row by a binary search of the
+// spans' exclusive prefix sums), so every lane slot is a covered pixel.
 template <bool FILL, typename I>
 __device__ __forceinline__ void raster_job(const RasterJob& J, int lane, const float4* __restrict__ vproj,
                                            uint32_t* __restrict__ counts, const u64* __restrict__ offsets,
                                            u64* __restrict__ records) {
-    if (!FILL && sizeof(I) == 4) {
-        count_job_box(J, lane, counts);
-        return;
-    }
-    constexpr int U = sizeof(I) == 4 ? 2 : 1;  // one pixel per step on the rare 64-bit path
-    // Counter-clockwise edges e0: 1 -> 2, e1: 2 -> 0, e2: 0 -> 1.
-    EdgeT<I> e0, e1, e2;
-    e0.set(I(J.ax1), I(J.ay1), I(J.ax2), I(J.ay2));
-    e1.set(I(J.ax2), I(J.ay2), I(J.ax0), I(J.ay0));
-    e2.set(I(J.ax0), I(J.ay0), I(J.ax1), I(J.ay1));
-    const float i0 = e0.sx != I(0) ? __frcp_rn(float(e0.sx)) : 0.f;
-    const float i1 = e1.sx != I(0) ? __frcp_rn(float(e1.sx)) : 0.f;
-    const float i2 = e2.sx != I(0) ? __frcp_rn(float(e2.sx)) : 0.f;
-    const u64 pbase = J.pix_base + u64(J.py0) * u64(J.W) + u64(J.px0);
-    float4 va = make_float4(0.f, 0.f, 0.f, 0.f), vb = va, vc = va;
-    if (FILL) {
-        va = vproj[J.v0];
-        vb = vproj[J.v1];
-        vc = vproj[J.v2];
-    }
-    const float wmax = float(J.bw - 1);
-    for (int r0 = 0; r0 < J.bh; r0 += 32) {
-        const int r = r0 + lane;
-        int xl = 0, len = 0;
-        if (r < J.bh) {
-            float lo = 0.f, hi = wmax;
-            bool empty = false;
-            span_edge(e0, i0, r, lo, hi, empty);
-            span_edge(e1, i1, r, lo, hi, empty);
-            span_edge(e2, i2, r, lo, hi, empty);
-            if (!empty) {
-                xl = max(0, int(fminf(lo, wmax + 1.f)) - 1);               // lo >= 0: int() is floor
-                const int xr = min(J.bw - 1, int(floorf(fmaxf(hi, -1.f))) + 1);
-                len = max(0, xr - xl + 1);
+    if constexpr (!FILL) {
+        count_job_rows<I>(J, lane, counts);
+    } else {
+        constexpr int U = sizeof(I) == 4 ? 2 : 1;  // one pixel per step on the rare 64-bit path
+        EdgeT<I> e0, e1, e2;
+        float i0, i1, i2;
+        FaceEdges::make(J, e0, e1, e2, i0, i1, i2);
+        const u64 pbase = J.pix_base + u64(J.py0) * u64(J.W) + u64(J.px0);
+        const float4 va = vproj[J.v0], vb = vproj[J.v1], vc = vproj[J.v2];
+        for (int r0 = 0; r0 < J.bh; r0 += 32) {
+            const int r = r0 + lane;
+            int xl = 0, len = 0;
+            if (r < J.bh) len = row_span(e0, e1, e2, i0, i1, i2, r, J.bw, xl);
+            int incl = len;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += t;
             }
-        }
-        int incl = len;
+            const int excl = incl - len;
+            const int total = __shfl_sync(0xffffffffu, incl, 31);
+            for (int s0 = 0; s0 < total; s0 += 32 * U) {
+                int c[U], rr[U];
+                bool valid[U];
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int t = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += t;
-        }
-        const int excl = incl - len;
-        const int total = __shfl_sync(0xffffffffu, incl, 31);
-        for (int s0 = 0; s0 < total; s0 += 32 * U) {
-            int c[U], rr[U];
-            bool valid[U];
+                for (int k = 0; k < U; ++k) {
+                    const int sl = s0 + 32 * k + lane;
+                    int i = 0;  // last row whose span starts at or before slot sl
 #pragma unroll
-            for (int k = 0; k < U; ++k) {
-                const int sl = s0 + 32 * k + lane;
-                int i = 0;  // last row whose span starts at or before slot sl
-#pragma unroll
-                for (int step = 16; step >= 1; step >>= 1)
-                    if (__shfl_sync(0xffffffffu, excl, i + step) <= sl) i += step;
-                valid[k] = sl < total;
-                rr[k] = r0 + i;
-                c[k] = __shfl_sync(0xffffffffu, xl, i) + (sl - __shfl_sync(0xffffffffu, excl, i));
+                    for (int step = 16; step >= 1; step >>= 1)
+                        if (__shfl_sync(0xffffffffu, excl, i + step) <= sl) i += step;
+                    valid[k] = sl < total;
+                    rr[k] = r0 + i;
+                    c[k] = __shfl_sync(0xffffffffu, xl, i) + (sl - __shfl_sync(0xffffffffu, excl, i));
+                }
+                fill_pixels<I, U>(J, c, rr, valid, pbase, va, vb, vc, counts, offsets, records);
             }
-            raster_pixels<FILL, I, U>(J, c, rr, valid, e0, e1, e2, pbase, va, vb, vc, counts, offsets, records);
         }
     }
 }
