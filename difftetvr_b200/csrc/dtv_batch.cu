@@ -108,8 +108,6 @@ __global__ void __launch_bounds__(128) kb_raster(const BatchView* __restrict__ v
                                                  uint32_t* __restrict__ counts, const u64* __restrict__ offsets,
                                                  u64* __restrict__ records, const uint32_t* __restrict__ ok) {
     if (FILL && !batch_ok(ok)) return;
-    __shared__ RasterJob jobs[4][32];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const u64 first = u64(blockIdx.x) * blockDim.x;
     const u64 g = first + threadIdx.x;
     bool live = false;
@@ -121,8 +119,14 @@ __global__ void __launch_bounds__(128) kb_raster(const BatchView* __restrict__ v
                             int(bv.W), 0, int(bv.H), bv.pix_base, J) &&
                (J.wide != 0) == WIDE;
     }
-    if (live) jobs[w][lane] = J;
-    raster_warp<FILL, WIDE>(jobs[w], __ballot_sync(0xffffffffu, live), lane, vproj, counts, offsets, records);
+    if constexpr (!FILL) {
+        if (live) count_face<typename std::conditional<WIDE, long long, int>::type>(J, counts);
+    } else {
+        __shared__ RasterJob jobs[4][32];
+        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+        if (live) jobs[w][lane] = J;
+        raster_warp<FILL, WIDE>(jobs[w], __ballot_sync(0xffffffffu, live), lane, vproj, counts, offsets, records);
+    }
 }
 
 // Per-row prefix of the count pass's difference arrays, one view per grid row.

@@ -45,13 +45,17 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster(const uint4* __res
                                                               uint32_t* __restrict__ counts,
                                                               const u64* __restrict__ offsets,
                                                               u64* __restrict__ records) {
-    __shared__ RasterJob jobs[kRasterWarps][32];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t f = blockIdx.x * blockDim.x + threadIdx.x;
     RasterJob J;
     const bool live = f < F && raster_setup(f, faces, vfix, 0u, W, row0, row1, 0ull, J) && (J.wide != 0) == WIDE;
-    if (live) jobs[w][lane] = J;
-    raster_warp<FILL, WIDE>(jobs[w], __ballot_sync(kFull, live), lane, vproj, counts, offsets, records);
+    if constexpr (!FILL) {
+        if (live) count_face<typename std::conditional<WIDE, long long, int>::type>(J, counts);
+    } else {
+        __shared__ RasterJob jobs[kRasterWarps][32];
+        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+        if (live) jobs[w][lane] = J;
+        raster_warp<FILL, WIDE>(jobs[w], __ballot_sync(kFull, live), lane, vproj, counts, offsets, records);
+    }
 }
 
 // Difference array of the count pass -> per-pixel counts, rows [row0, row1).

@@ -15,10 +15,11 @@ constexpr int kTile = 16;  // composite / adjoint pixel tile (16 x 16 threads)
 // one face (projected fixed-point vertices, orientation, clipped bounding box)
 // into shared memory; the warp then takes the faces one at a time.  Each box
 // row of a face meets it in one interval of pixel centres, found exactly per
-// row (row_span).  COUNT mode adds +1 / -1 at the ends of each row's interval
-// to a per-row difference array in `counts`, which row_prefix_counts turns
-// into per-pixel counts; FILL mode spreads the covered pixels of the face over
-// the warp's lanes and writes each record at offsets[p] + (--counts[p]),
+// row (row_span).  The count (one thread per face) adds +1 / -1 at the ends of
+// each row's interval to a per-row difference array in `counts`, which
+// row_prefix_warp turns into per-pixel counts; the fill (one warp per face)
+// spreads the covered pixels of the face over the warp's lanes and writes
+// each record at offsets[p] + (--counts[p]),
 // leaving counts zeroed for the next render.  Only pixel rows [row0, row1) are
 // visited (row bands of a render whose lists do not fit the fragment budget at
 // once).
@@ -166,22 +167,22 @@ struct FaceEdges {
     }
 };
 
-// Count pass over one face: lane = box row, 32 rows at a time; each row's
-// exact span adds +1 at its first pixel and -1 after its last one (when that
-// is still in the image row) to a per-row difference array held in `counts`
-// (u32, modulo 2^32); row_prefix_counts turns it into per-pixel counts.  Two
-// atomics per face row instead of one per covered pixel.
+// Count pass over one face, one thread: each box row's exact span adds +1 at
+// its first pixel and -1 after its last one (when that is still in the image
+// row) to a per-row difference array held in `counts` (u32, modulo 2^32);
+// row_prefix_warp turns it into per-pixel counts.  Two atomics per face row
+// instead of one per covered pixel, and no per-face warp work: a face has
+// about eleven rows at the path's sizes.
 template <typename I>
-__device__ __forceinline__ void count_job_rows(const RasterJob& J, int lane, uint32_t* __restrict__ counts) {
+__device__ __forceinline__ void count_face(const RasterJob& J, uint32_t* __restrict__ counts) {
     EdgeT<I> e0, e1, e2;
     float i0, i1, i2;
     FaceEdges::make(J, e0, e1, e2, i0, i1, i2);
-    const u64 pbase = J.pix_base + u64(J.py0) * u64(J.W) + u64(J.px0);
-    for (int r = lane; r < J.bh; r += 32) {
+    uint32_t* row = counts + J.pix_base + u64(J.py0) * u64(J.W) + u64(J.px0);
+    for (int r = 0; r < J.bh; ++r, row += J.W) {
         int xl;
         const int len = row_span(e0, e1, e2, i0, i1, i2, r, J.bw, xl);
         if (len > 0) {
-            uint32_t* row = counts + pbase + u64(r) * u64(J.W);
             atomicAdd(row + xl, 1u);
             if (J.px0 + xl + len < J.W) atomicAdd(row + xl + len, 0xffffffffu);
         }
@@ -233,17 +234,16 @@ __device__ __forceinline__ void fill_pixels(const RasterJob& J, const int (&c)[U
         if (valid[k] && slot[k] != 0u) records[off[k] + slot[k] - 1u] = (u64(__float_as_uint(z[k])) << 32) | J.bits;
 }
 
-// One face: the count walks its rows (count_job_rows); the fill takes the box
-// rows 32 at a time (lane = row), finds each row's exact span, and spreads the
-// concatenated spans over its lanes (slot s -> row by a binary search of the
-// spans' exclusive prefix sums), so every lane slot is a covered pixel.
+// Fill of one face by the warp: it takes the box rows 32 at a time (lane =
+// row), finds each row's exact span, and spreads the concatenated spans over
+// its lanes (slot s -> row by a binary search of the spans' exclusive prefix
+// sums), so every lane slot is a covered pixel.
 template <bool FILL, typename I>
 __device__ __forceinline__ void raster_job(const RasterJob& J, int lane, const float4* __restrict__ vproj,
                                            uint32_t* __restrict__ counts, const u64* __restrict__ offsets,
                                            u64* __restrict__ records) {
-    if constexpr (!FILL) {
-        count_job_rows<I>(J, lane, counts);
-    } else {
+    static_assert(FILL, "the count pass runs one face per thread (count_face)");
+    {
         constexpr int U = sizeof(I) == 4 ? 2 : 1;  // one pixel per step on the rare 64-bit path
         EdgeT<I> e0, e1, e2;
         float i0, i1, i2;
