@@ -27,6 +27,12 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "fwd+adj iter/s at 1.57M tets 1024²"
+# Kernels of this library per timed step of the plain method: project 1,
+# count 2 (32- and 64-bit faces) + row prefix 1, scan 3, fill 2, sort 8
+# (classify, five register / distribution classes, shared-memory and block
+# classes), composite 1; adjoint 1 + scatter 1; l2 loss 1; Adam 2 (colours,
+# positions).
+LIST_STEP_LAUNCHES = 1 + 3 + 3 + 2 + 8 + 1 + 2 + 1 + 2
 LR_COL, LR_POS = 1e-2, 1e-4
 
 
@@ -315,7 +321,7 @@ def run_ours(args, rank, world):
                    "fragments_per_step": nf, "views": len(views), "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (fragment records ~%.1f GB per step)" % (8 * nf / 1e9)},
         "e2e": e2e,
-        "gpu_launches": 13 * K,
+        "gpu_launches": LIST_STEP_LAUNCHES * K,
         "stage_ms": {k: round(v, 4) for k, v in avg.items()},
         "fragments_per_s": nf * value / world * world,
         "roofline": roofline,
