@@ -206,6 +206,11 @@ __global__ void __launch_bounds__(256) kb_loss(const BatchView* __restrict__ vie
     }
 }
 
+// SCREEN: each view adds screen-space adjoint rows of its own camera into
+// view_rows (at its vert_base), which kb_view_rows projects and adds into the
+// slots' rows; otherwise world-space rows go straight to the slot (views of
+// one mesh share them).
+template <bool SCREEN>
 __global__ void __launch_bounds__(kTile * kTile, 2) kb_adjoint(const BatchView* __restrict__ views, int nviews,
                                                             const u64* __restrict__ offsets,
                                                             const u64* __restrict__ records,
@@ -213,6 +218,7 @@ __global__ void __launch_bounds__(kTile * kTile, 2) kb_adjoint(const BatchView* 
                                                             const float* __restrict__ tfinal,
                                                             const uint32_t* __restrict__ term,
                                                             float4* __restrict__ grad_rows,
+                                                            float4* __restrict__ view_rows,
                                                             const uint32_t* __restrict__ ok) {
     __shared__ float4 vcache4[3 * kTile * kTile];
     __shared__ float vcache1[3 * kTile * kTile];
@@ -221,9 +227,32 @@ __global__ void __launch_bounds__(kTile * kTile, 2) kb_adjoint(const BatchView* 
     if (!tile_pixel(views, nviews, v, px, py)) return;
     const BatchView& bv = views[v];
     if (bv.grad_slot < 0 || bv.dimage == nullptr) return;
-    VertCache acc{grad_rows + 2 * bv.grad_base, vcache4 + threadIdx.x, vcache1 + threadIdx.x, kTile * kTile};
-    adjoint_pixel(px, py, offsets + bv.pix_base, records, bv.faces, vgeo + bv.vert_base, bv.colors, int(bv.W),
-                  bv.cam, sh, bv.dimage, tfinal + bv.pix_base, term + bv.pix_base, acc);
+    float4* rows = SCREEN ? view_rows + 2 * bv.vert_base : grad_rows + 2 * bv.grad_base;
+    VertCache acc{rows, vcache4 + threadIdx.x, vcache1 + threadIdx.x, kTile * kTile};
+    adjoint_pixel<VertCache, SCREEN>(px, py, offsets + bv.pix_base, records, bv.faces, vgeo + bv.vert_base,
+                                     bv.colors, int(bv.W), bv.cam, sh, bv.dimage, tfinal + bv.pix_base,
+                                     term + bv.pix_base, acc);
+}
+
+// Screen-space rows of every view with a gradient slot -> world-space rows
+// of the slot (one thread per view vertex; untouched vertices skipped).
+__global__ void __launch_bounds__(256) kb_view_rows(const BatchView* __restrict__ views, int nviews, u64 total,
+                                                    const VGeo* __restrict__ vgeo,
+                                                    const float4* __restrict__ view_rows,
+                                                    float4* __restrict__ grad_rows, const uint32_t* __restrict__ ok) {
+    if (!batch_ok(ok)) return;
+    const u64 first = u64(blockIdx.x) * blockDim.x;
+    const u64 g = first + threadIdx.x;
+    if (g >= total) return;
+    const int v = view_of_item(g, first, nviews, [&](int i) { return views[i].vert_base; });
+    const BatchView& bv = views[v];
+    if (bv.grad_slot < 0 || bv.dimage == nullptr) return;
+    const float4 a = view_rows[2 * g], c = view_rows[2 * g + 1];
+    if (a.x == 0.f && a.y == 0.f && a.z == 0.f && c.x == 0.f && c.y == 0.f && c.z == 0.f && c.w == 0.f) return;
+    const float3 w = screen_to_world(a, vgeo[g], bv.cam);
+    float4* row = grad_rows + 2 * (bv.grad_base + (g - bv.vert_base));
+    atomicAdd(row, make_float4(w.x, w.y, w.z, 0.f));
+    atomicAdd(row + 1, c);
 }
 
 // Adds each slot's accumulated rows into its gradient buffers.
@@ -354,6 +383,7 @@ struct dtv_batch {
     DevBuf<uint32_t> ok;
     DevBuf<u64> total;
     DevBuf<float4> grad_rows;
+    DevBuf<float4> view_rows;  // [tot_verts][2]: screen-space adjoint rows of each view (at its vert_base)
     DevBuf<float4> dimage_internal;
     DevBuf<float> loss;
     DevBuf<int> step;
@@ -445,6 +475,7 @@ void ensure_scratch(dtv_batch* b, cudaStream_t s) {
     b->vproj.ensure(b->tot_verts ? b->tot_verts : 1, s);
     b->vfix.ensure(b->tot_verts ? b->tot_verts : 1, s);
     b->vgeo.ensure(b->tot_verts ? b->tot_verts : 1, s);
+    b->view_rows.ensure(2 * (b->tot_verts ? b->tot_verts : 1), s);
     b->counts.ensure(b->tot_pixels, s, /*zero_new=*/true);
     b->offsets.ensure(b->tot_pixels + 1, s);
     b->scan.ensure(dtv::scan_scratch_elems(b->tot_pixels), s);
@@ -485,6 +516,25 @@ void launch_kb_raster(dtv_batch* b, const uint32_t* okp, cudaStream_t s) {
         dim3 grid(unsigned(b->max_height + 7) / 8, unsigned(b->nviews));
         kb_row_prefix<<<grid, 256, 0, s>>>(b->d_views.ptr, b->counts.ptr);
     }
+}
+
+// Adjoint of every view with a gradient slot into the slots' rows (which the
+// caller has cleared): screen-space view rows projected per vertex, or
+// world-space rows directly for absolute-value gradients.
+void enqueue_adjoint(dtv_batch* b, const dtv::ShadeDev& sh, const uint32_t* okp, cudaStream_t s) {
+    using namespace dtv;
+    if (sh.use_abs_grad) {
+        kb_adjoint<false><<<unsigned(b->tot_tiles), kTile * kTile, 0, s>>>(
+            b->d_views.ptr, b->nviews, b->offsets.ptr, b->records.ptr, b->vgeo.ptr, sh, b->tfinal.ptr, b->term.ptr,
+            b->grad_rows.ptr, b->view_rows.ptr, okp);
+        return;
+    }
+    DTV_CK(cudaMemsetAsync(b->view_rows.ptr, 0, sizeof(float4) * 2 * size_t(b->tot_verts), s));
+    kb_adjoint<true><<<unsigned(b->tot_tiles), kTile * kTile, 0, s>>>(
+        b->d_views.ptr, b->nviews, b->offsets.ptr, b->records.ptr, b->vgeo.ptr, sh, b->tfinal.ptr, b->term.ptr,
+        b->grad_rows.ptr, b->view_rows.ptr, okp);
+    kb_view_rows<<<grid_for(b->tot_verts, 256, 0x7fffffffu), 256, 0, s>>>(
+        b->d_views.ptr, b->nviews, b->tot_verts, b->vgeo.ptr, b->view_rows.ptr, b->grad_rows.ptr, okp);
 }
 
 // Enqueues project, count, scan, [capacity guard], fill, sort, composite.
@@ -559,6 +609,7 @@ int32_t dtv_batch_reserve(dtv_batch* b, uint64_t max_views, uint64_t max_vertice
         b->vproj.ensure(V, s);
         b->vfix.ensure(V, s);
         b->vgeo.ensure(V, s);
+        b->view_rows.ensure(2 * V, s);
         b->counts.ensure(P, s, /*zero_new=*/true);
         b->offsets.ensure(P + 1, s);
         b->scan.ensure(dtv::scan_scratch_elems(P), s);
@@ -606,6 +657,7 @@ int32_t dtv_batch_destroy(dtv_batch* b) {
     b->ok.release();
     b->total.release();
     b->grad_rows.release();
+    b->view_rows.release();
     b->dimage_internal.release();
     b->loss.release();
     b->step.release();
@@ -793,10 +845,8 @@ int32_t dtv_batch_render_adjoint(dtv_batch* b, int32_t num_views, const dtv_batc
         dtv::ShadeDev sh = b->sh;
         sh.use_abs_grad = use_abs_grad ? 1 : 0;
         using namespace dtv;
-        kb_adjoint<<<unsigned(b->tot_tiles), kTile * kTile, 0, s>>>(b->d_views.ptr, b->nviews, b->offsets.ptr,
-                                                                    b->records.ptr, b->vgeo.ptr, sh, b->tfinal.ptr,
-                                                                    b->term.ptr, b->grad_rows.ptr,
-                                                                    b->async_render ? b->ok.ptr : nullptr);
+        const uint32_t* okp = b->async_render ? b->ok.ptr : nullptr;
+        enqueue_adjoint(b, sh, okp, s);
         if (rows)
             kb_scatter<<<grid_for(rows, 256, 148 * 16), 256, 0, s>>>(b->d_slots.ptr, num_slots, rows,
                                                                      b->grad_rows.ptr);
@@ -816,9 +866,7 @@ void enqueue_train_body(dtv_batch* b, const dtv::AdamConst& ac, int nslots, cuda
     kb_loss<<<grid_for(b->tot_pixels, 256, 148 * 8), 256, 0, s>>>(b->d_views.ptr, b->nviews, b->tot_pixels,
                                                                   b->loss.ptr, b->ok.ptr);
     DTV_CK(cudaMemsetAsync(b->grad_rows.ptr, 0, sizeof(float4) * 2 * size_t(b->tot_rows), s));
-    kb_adjoint<<<unsigned(b->tot_tiles), kTile * kTile, 0, s>>>(b->d_views.ptr, b->nviews, b->offsets.ptr,
-                                                                b->records.ptr, b->vgeo.ptr, b->sh, b->tfinal.ptr,
-                                                                b->term.ptr, b->grad_rows.ptr, b->ok.ptr);
+    enqueue_adjoint(b, b->sh, b->ok.ptr, s);
     kb_adam_rows<<<grid_for(b->tot_rows, 256, 148 * 16), 256, 0, s>>>(b->d_slots.ptr, nslots, b->tot_rows,
                                                                       b->grad_rows.ptr, ac, b->step.ptr, b->ok.ptr);
     kb_step_increment<<<1, 1, 0, s>>>(b->step.ptr, b->ok.ptr);
@@ -829,7 +877,8 @@ std::vector<u64> train_signature(const dtv_batch* b, const dtv::AdamConst& ac, i
     std::vector<u64> sig = {u64(b->nviews), b->tot_verts, b->tot_faces, b->tot_pixels, b->tot_tiles, b->tot_rows,
                             u64(b->max_height),
                             b->capacity, u64(nslots), u64(uintptr_t(b->records.ptr)),
-                            u64(uintptr_t(b->dimage_internal.ptr)), u64(uintptr_t(b->grad_rows.ptr))};
+                            u64(uintptr_t(b->dimage_internal.ptr)), u64(uintptr_t(b->grad_rows.ptr)),
+                            u64(uintptr_t(b->view_rows.ptr))};
     const uint32_t* shw = reinterpret_cast<const uint32_t*>(&b->sh);
     for (size_t i = 0; i < sizeof(b->sh) / 4; ++i) sig.push_back(shw[i]);
     const uint32_t* acw = reinterpret_cast<const uint32_t*>(&ac);
