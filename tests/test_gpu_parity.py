@@ -74,6 +74,31 @@ def test_long_lists_bit_exact_and_composited(oracle):
     assert np.abs(img - img_o).max() < 1e-4
 
 
+def test_list_over_block_cap_is_reported():
+    """A 1 x 1 x 6000-cell column seen end-on puts about 18,000 fragments in
+    the centre pixels' lists, over the 16,384 the block sort takes: the render
+    completes and the next call reports the overflow."""
+    import difftetvr_b200 as d
+    from difftetvr_b200 import synthetic as S
+    from difftetvr_b200._lib import DtvError
+    cells, pos = d.build_hex_mesh((-0.05, -0.05, -1.0), (0.05, 0.05, 1.0), 2, 2, 6001)
+    col = S.gaussian_colors(pos, seed=5)
+    col[:, 3] *= 1e-3
+    mesh = d.TetMesh()
+    mesh.set_tet_mesh_data(cells, pos, col)
+    r = d.Renderer(d.RendererType.PPLL)
+    r.set_tet_mesh(mesh)
+    r.set_viewport_size(64, 64)
+    r.set_camera_fovy(S.FOVY_45)
+    r.set_view_matrix(S.look_at_view([0.001, 0.002, 2.5]))
+    r.set_attenuation(1.0)
+    r.render()
+    torch.cuda.synchronize()
+    with pytest.raises(DtvError, match="exceeded 16384"):
+        r.render()
+    torch.cuda.synchronize()
+
+
 def test_mesh_faces_match_oracle(oracle):
     sc = Scene(8, 64, seed=3)
     mesh, r = sc.make_renderer()
