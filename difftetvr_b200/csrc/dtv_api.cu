@@ -62,6 +62,7 @@ struct dtv_mesh {
     // Ray-tet path: per-tet face ids and the boundary faces as their own
     // face set (rasterised alone; record face field k -> global face bf_global[k]).
     uint32_t* d_tet_faces = nullptr;   // 4T
+    uint8_t* d_tet_flip = nullptr;     // T (MeshHost::tet_flip)
     uint4* d_bfaces = nullptr;         // Nb
     uint32_t* d_bf_global = nullptr;   // Nb
     std::vector<uint32_t> bf_global;   // host copy
@@ -330,6 +331,7 @@ int32_t dtv_mesh_create(const uint32_t* h_cells, uint64_t num_cells, uint64_t nu
                 }
             const uint64_t Nb = m->bf_global.size();
             DTV_CK(cudaMalloc(&m->d_tet_faces, sizeof(uint32_t) * (4 * num_cells ? 4 * num_cells : 1)));
+            DTV_CK(cudaMalloc(&m->d_tet_flip, num_cells ? num_cells : 1));
             DTV_CK(cudaMalloc(&m->d_bfaces, sizeof(uint4) * (Nb ? Nb : 1)));
             DTV_CK(cudaMalloc(&m->d_bf_global, sizeof(uint32_t) * (Nb ? Nb : 1)));
             if (Nb) {
@@ -337,9 +339,11 @@ int32_t dtv_mesh_create(const uint32_t* h_cells, uint64_t num_cells, uint64_t nu
                 DTV_CK(cudaMemcpy(m->d_bf_global, m->bf_global.data(), sizeof(uint32_t) * Nb,
                                   cudaMemcpyHostToDevice));
             }
-            if (num_cells)
+            if (num_cells) {
                 DTV_CK(cudaMemcpy(m->d_tet_faces, m->host.tet_faces.data(), sizeof(uint32_t) * 4 * num_cells,
                                   cudaMemcpyHostToDevice));
+                DTV_CK(cudaMemcpy(m->d_tet_flip, m->host.tet_flip.data(), num_cells, cudaMemcpyHostToDevice));
+            }
             if (F) {
                 DTV_CK(cudaMemcpy(m->d_faces, faces.data(), sizeof(uint4) * F, cudaMemcpyHostToDevice));
                 DTV_CK(cudaMemcpy(m->d_face_to_tet, m->host.face_to_tet.data(), sizeof(uint32_t) * 2 * F,
@@ -365,6 +369,7 @@ int32_t dtv_mesh_destroy(dtv_mesh* m) {
     cudaFree(m->d_face_to_tet);
     cudaFree(m->d_cells);
     cudaFree(m->d_tet_faces);
+    cudaFree(m->d_tet_flip);
     cudaFree(m->d_bfaces);
     cudaFree(m->d_bf_global);
     delete m;
@@ -548,7 +553,8 @@ int32_t render_common(dtv_renderer* r, const dtv_mesh* mesh, const float* d_posi
         rec_event(r, 5, s);
         if (raytet) {
             dtv::launch_walk_composite(r->offsets.ptr, r->records.ptr, mesh->d_bf_global, mesh->d_faces,
-                                       mesh->d_face_to_tet, mesh->d_tet_faces, uint32_t(mesh->host.num_cells),
+                                       mesh->d_face_to_tet, mesh->d_tet_faces, mesh->d_cells, mesh->d_tet_flip,
+                                       uint32_t(mesh->host.num_cells),
                                        r->vfix.ptr, r->vgeo.ptr, reinterpret_cast<const float4*>(d_colors), cam, sh,
                                        reinterpret_cast<float4*>(d_image), r->tfinal.ptr, r->wstate.ptr, s);
             check_launch("ray-tet walk");
@@ -594,7 +600,8 @@ int32_t adjoint_common(dtv_renderer* r, const dtv_mesh* mesh, const float* d_pos
             adjoint_banded(r, mesh, d_colors, d_image_adjoint, sh, d_grad_positions, d_grad_colors, s);
         } else if (r->type == DTV_RENDERER_INTERSECTION) {
             dtv::launch_walk_adjoint(r->offsets.ptr, r->records.ptr, mesh->d_bf_global, mesh->d_faces,
-                                     mesh->d_face_to_tet, mesh->d_tet_faces, uint32_t(mesh->host.num_cells),
+                                     mesh->d_face_to_tet, mesh->d_tet_faces, mesh->d_cells, mesh->d_tet_flip,
+                                     uint32_t(mesh->host.num_cells),
                                      r->vfix.ptr, r->vgeo.ptr, reinterpret_cast<const float4*>(d_colors), r->cam, sh,
                                      reinterpret_cast<const float4*>(d_image_adjoint), r->tfinal.ptr,
                                      r->wstate.ptr, uint32_t(r->V), r->grad_rows.ptr, d_grad_positions,

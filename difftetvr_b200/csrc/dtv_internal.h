@@ -19,6 +19,11 @@ struct MeshHost {
     std::vector<uint32_t> vertex_boundary;// V
     std::vector<uint32_t> cells;          // 4T
     std::vector<uint32_t> tet_faces;      // 4T: unique face index of face j of tet c (TetFaceTable order)
+    // T: bit j set when face j's side seen from tet c is not given by the
+    // winding of c's own vertex order (the shared face's stored winding, as
+    // read with the owner rule, disagrees with c's order: inconsistently
+    // oriented neighbours); 0 for a consistently oriented mesh.
+    std::vector<uint8_t> tet_flip;
 };
 
 // Builds faces from cells (restates buildFacesSlim, TetMesh.cpp:1218-1268).
@@ -94,12 +99,14 @@ void launch_scatter_positions(const float4* grad_rows, uint32_t V, float* grad_p
 // Ray-tet path (dtv_raytet.cu).
 void launch_walk_composite(const unsigned long long* b_offsets, const unsigned long long* b_records,
                            const uint32_t* bf_global, const uint4* faces, const uint32_t* face_to_tet,
-                           const uint32_t* tet_faces, uint32_t num_tets, const int2* vfix, const VGeo* vgeo,
+                           const uint32_t* tet_faces, const uint32_t* cells, const uint8_t* tet_flip,
+                           uint32_t num_tets, const int2* vfix, const VGeo* vgeo,
                            const float4* colors, const CamDev& cam, const ShadeDev& sh, float4* image,
                            float* tfinal, uint4* wstate, cudaStream_t s);
 void launch_walk_adjoint(const unsigned long long* b_offsets, const unsigned long long* b_records,
                          const uint32_t* bf_global, const uint4* faces, const uint32_t* face_to_tet,
-                         const uint32_t* tet_faces, uint32_t num_tets, const int2* vfix, const VGeo* vgeo,
+                         const uint32_t* tet_faces, const uint32_t* cells, const uint8_t* tet_flip,
+                         uint32_t num_tets, const int2* vfix, const VGeo* vgeo,
                          const float4* colors, const CamDev& cam, const ShadeDev& sh, const float4* dimage,
                          const float* tfinal, const uint4* wstate, uint32_t V, float4* grad_rows, float* grad_pos,
                          float4* grad_col, cudaStream_t s);

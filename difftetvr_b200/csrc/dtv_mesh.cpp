@@ -90,6 +90,28 @@ void build_faces(const uint32_t* cells, uint64_t T, uint64_t V, MeshHost& out) {
         if (out.face_boundary[f])
             for (int k = 0; k < 3; ++k) out.vertex_boundary[out.tri[3 * f + k]] = 1u;
     out.cells.assign(cells, cells + 4 * T);
+    // Per tet and face j: is face j camera-facing for tet c when c's own
+    // vertex order (kTetFaceTable) winds clockwise on screen?  The ray-tet walk
+    // classifies faces by the stored winding of the unique face and whether c
+    // owns it (owner: same order; other tet: the stored order read reversed);
+    // k_j = !(odd_j ^ owner_j), odd_j = the stored order is an odd permutation
+    // of c's order, turns that rule into one on c's own order.
+    out.tet_flip.assign(T, 0u);
+    for (uint64_t c = 0; c < T; ++c) {
+        uint8_t mask = 0;
+        for (int j = 0; j < 4; ++j) {
+            const uint32_t f = out.tet_faces[4 * c + uint64_t(j)];
+            const bool owner = out.face_to_tet[2 * uint64_t(f)] == uint32_t(c);
+            const uint32_t a = cells[4 * c + kTetFaceTable[j][0]], b = cells[4 * c + kTetFaceTable[j][1]],
+                           d = cells[4 * c + kTetFaceTable[j][2]];
+            const uint32_t* s = &out.tri[3 * uint64_t(f)];
+            const bool even = (s[0] == a && s[1] == b && s[2] == d) || (s[0] == b && s[1] == d && s[2] == a) ||
+                              (s[0] == d && s[1] == a && s[2] == b);
+            const bool odd = !even;
+            if (!(odd ^ owner)) mask |= uint8_t(1u << j);
+        }
+        out.tet_flip[c] = mask;
+    }
 }
 
 }  // namespace dtv

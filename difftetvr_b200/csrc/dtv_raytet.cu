@@ -26,12 +26,12 @@ namespace dtv {
 
 constexpr uint32_t kNoTet = 0xffffffffu;
 
-// Exact coverage of the pixel centre by face f (the rule of raster_face);
-// *front_stored: the face's stored winding faces the camera.  The edge
-// functions are taken relative to the pixel centre: with every vertex within
-// 2^14 fixed-point units (64 px) of it they are exact in 32-bit integers,
-// otherwise in 64 bits; both give the raster's coverage.  No early exits, so
-// a warp's lanes stay together.
+// Exact coverage of the pixel centre by a triangle (the rasteriser's rule),
+// vertices relative to the pixel centre, `swap`: the given order winds
+// clockwise.  With every vertex within 2^14 fixed-point units (64 px) of the
+// centre the edge functions are exact in 32-bit integers, otherwise in 64
+// bits; both give the raster's coverage.  No early exits, so a warp's lanes
+// stay together.
 template <typename I>
 __device__ __forceinline__ bool covers_rel(I r0x, I r0y, I r1x, I r1y, I r2x, I r2y, bool swap) {
     // Vertices relative to the pixel centre; the orientation-normalised order
@@ -48,44 +48,56 @@ __device__ __forceinline__ bool covers_rel(I r0x, I r0y, I r1x, I r1y, I r2x, I 
     return edge_in<I>(E0, dx0, dy0) & edge_in<I>(E1, dx1, dy1) & edge_in<I>(E2, dx2, dy2);
 }
 
-__device__ __forceinline__ bool face_covers_px(const uint4* __restrict__ faces, const int2* __restrict__ vfix,
-                                               uint32_t f, int px, int py, bool* front_stored) {
-    const uint4 fc = faces[f];
-    const int2 q0 = vfix[fc.x], q1 = vfix[fc.y], q2 = vfix[fc.z];
-    const bool valid = q0.x != kInvalidFix && q1.x != kInvalidFix && q2.x != kInvalidFix;
-    const long long X0 = q0.x, Y0 = q0.y, X1 = q1.x, Y1 = q1.y, X2 = q2.x, Y2 = q2.y;
-    const long long area2 = (X1 - X0) * (Y2 - Y0) - (Y1 - Y0) * (X2 - X0);
-    *front_stored = area2 < 0;
-    const long long Xc = 256LL * px + 128, Yc = 256LL * py + 128;
-    const long long r0x = X0 - Xc, r0y = Y0 - Yc, r1x = X1 - Xc, r1y = Y1 - Yc, r2x = X2 - Xc, r2y = Y2 - Yc;
-    const long long m = max(max(max(llabs(r0x), llabs(r0y)), max(llabs(r1x), llabs(r1y))),
-                            max(llabs(r2x), llabs(r2y)));
-    bool in;
-    if (m < (1LL << 14))
-        in = covers_rel<int>(int(r0x), int(r0y), int(r1x), int(r1y), int(r2x), int(r2y), area2 < 0);
-    else
-        in = covers_rel<long long>(r0x, r0y, r1x, r1y, r2x, r2y, area2 < 0);
-    return valid && area2 != 0 && in;
-}
+// Per-tet topology for the walk: the unique face ids of a tet's four faces
+// (face j = local vertices kTetFaceTable[j] = {0,1,2}, {1,0,3}, {0,2,3},
+// {2,1,3}), its vertex ids, and per face the bit that turns the on-screen
+// winding of the tet's own vertex order into "faces the camera as seen from
+// this tet" (the mesh builder's tet_flip; 0 for consistently oriented meshes).
+struct TetTopo {
+    const uint4* tet_faces;
+    const uint4* cells;
+    const uint8_t* flip;
+};
 
 // Face of tet t (not `skip`) covering the pixel that faces the camera
 // (want_front) or away from it with respect to t's outward normal; the first
-// such face in the tet's face order.  All four faces are evaluated.
-__device__ __forceinline__ uint32_t tet_face_at(const uint32_t* __restrict__ tet_faces,
-                                                const uint4* __restrict__ faces,
-                                                const uint32_t* __restrict__ f2t, const int2* __restrict__ vfix,
-                                                uint32_t t, uint32_t skip, bool want_front, int px, int py) {
-    const uint4 tf = reinterpret_cast<const uint4*>(tet_faces)[t];
+// such face in the tet's face order.  All four faces are evaluated from the
+// tet's four projected vertices (4 vertex loads instead of 12, and no face or
+// face->tet loads); coverage is the rasteriser's rule (covers_rel normalises
+// the winding, and the normalised triangle's directed edges do not depend on
+// the starting vertex).
+__device__ __forceinline__ uint32_t tet_face_at(const TetTopo& tt, const int2* __restrict__ vfix, uint32_t t,
+                                                uint32_t skip, bool want_front, int px, int py) {
+    const uint4 tf = tt.tet_faces[t];
+    const uint4 cv = tt.cells[t];
+    const uint32_t flip = tt.flip[t];
     const uint32_t fs[4] = {tf.x, tf.y, tf.z, tf.w};
+    const int2 q[4] = {vfix[cv.x], vfix[cv.y], vfix[cv.z], vfix[cv.w]};
+    const long long Xc = 256LL * px + 128, Yc = 256LL * py + 128;
+    long long rx[4], ry[4];
+    bool ok[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        ok[k] = q[k].x != kInvalidFix;
+        rx[k] = (long long)q[k].x - Xc;
+        ry[k] = (long long)q[k].y - Yc;
+    }
+    constexpr int A[4] = {0, 1, 0, 2}, B[4] = {1, 0, 2, 1}, C[4] = {2, 3, 3, 3};
     uint32_t found = kNoTet;
 #pragma unroll
     for (int j = 3; j >= 0; --j) {
-        const uint32_t f = fs[j];
-        bool front_stored;
-        const bool cov = face_covers_px(faces, vfix, f, px, py, &front_stored);
-        const bool owner = f2t[2 * size_t(f)] == t;  // stored winding is outward for the face's first tet
-        const bool match = f != skip && cov && ((front_stored == owner) == want_front);
-        found = match ? f : found;  // descending j: the smallest matching j wins
+        const int a = A[j], b = B[j], c = C[j];
+        const long long area2 = (rx[b] - rx[a]) * (ry[c] - ry[a]) - (ry[b] - ry[a]) * (rx[c] - rx[a]);
+        const long long m = max(max(max(llabs(rx[a]), llabs(ry[a])), max(llabs(rx[b]), llabs(ry[b]))),
+                                max(llabs(rx[c]), llabs(ry[c])));
+        bool in;
+        if (m < (1LL << 14))
+            in = covers_rel<int>(int(rx[a]), int(ry[a]), int(rx[b]), int(ry[b]), int(rx[c]), int(ry[c]), area2 < 0);
+        else
+            in = covers_rel<long long>(rx[a], ry[a], rx[b], ry[b], rx[c], ry[c], area2 < 0);
+        const bool front = (area2 < 0) != (((flip >> j) & 1u) != 0u);
+        const bool match = fs[j] != skip && ok[a] && ok[b] && ok[c] && area2 != 0 && in && front == want_front;
+        found = match ? fs[j] : found;  // descending j: the smallest matching j wins
     }
     return found;
 }
@@ -103,8 +115,7 @@ __device__ __forceinline__ float ray_scale(const CamDev& cam, float qx, float qy
 
 __global__ void __launch_bounds__(kTile * kTile, 2) k_walk_composite(
     const u64* __restrict__ b_offsets, const u64* __restrict__ b_records, const uint32_t* __restrict__ bf_global,
-    const uint4* __restrict__ faces, const uint32_t* __restrict__ f2t, const uint32_t* __restrict__ tet_faces,
-    uint32_t num_tets, const int2* __restrict__ vfix, const VGeo* __restrict__ vgeo,
+    const uint4* __restrict__ faces, const uint32_t* __restrict__ f2t, TetTopo tt, uint32_t num_tets, const int2* __restrict__ vfix, const VGeo* __restrict__ vgeo,
     const float4* __restrict__ colors, CamDev cam, ShadeDev sh, float4* __restrict__ image,
     float* __restrict__ tfinal, uint4* __restrict__ wstate) {
     const int px = blockIdx.x * kTile + (threadIdx.x % kTile);
@@ -125,7 +136,7 @@ __global__ void __launch_bounds__(kTile * kTile, 2) k_walk_composite(
         uint32_t t = f2t[2 * size_t(fe)];
         FragV f0 = load_frag(u64(fe) << 2, qx, qy, faces, vgeo, colors);
         for (uint32_t step = 0; step <= num_tets; ++step) {
-            const uint32_t fx = tet_face_at(tet_faces, faces, f2t, vfix, t, fe, false, px, py);
+            const uint32_t fx = tet_face_at(tt, vfix, t, fe, false, px, py);
             if (fx == kNoTet) break;
             if (sh.use_ert && T < sh.ert_thresh) {
                 stop = true;
@@ -154,8 +165,7 @@ __global__ void __launch_bounds__(kTile * kTile, 2) k_walk_composite(
 template <bool SCREEN>
 __global__ void __launch_bounds__(kTile * kTile, 2) k_walk_adjoint(
     const u64* __restrict__ b_offsets, const u64* __restrict__ b_records, const uint32_t* __restrict__ bf_global,
-    const uint4* __restrict__ faces, const uint32_t* __restrict__ f2t, const uint32_t* __restrict__ tet_faces,
-    uint32_t num_tets, const int2* __restrict__ vfix, const VGeo* __restrict__ vgeo,
+    const uint4* __restrict__ faces, const uint32_t* __restrict__ f2t, TetTopo tt, uint32_t num_tets, const int2* __restrict__ vfix, const VGeo* __restrict__ vgeo,
     const float4* __restrict__ colors, CamDev cam, ShadeDev sh, const float4* __restrict__ dimage,
     const float* __restrict__ tfinal, const uint4* __restrict__ wstate, float4* __restrict__ grad_rows) {
     const int px = blockIdx.x * kTile + (threadIdx.x % kTile);
@@ -176,7 +186,7 @@ __global__ void __launch_bounds__(kTile * kTile, 2) k_walk_adjoint(
     float T = tfinal[p];
     uint32_t t = ws.x, fe = ws.y;
     int b = int(ws.z);
-    uint32_t fx = tet_face_at(tet_faces, faces, f2t, vfix, t, fe, false, px, py);
+    uint32_t fx = tet_face_at(tt, vfix, t, fe, false, px, py);
     if (fx == kNoTet) return;
     // Vertex rows straight to global memory: the shared-memory vertex cache of
     // the list path measured slower here (register spills in the walk).
@@ -208,7 +218,7 @@ __global__ void __launch_bounds__(kTile * kTile, 2) k_walk_adjoint(
             if (bb < 0) break;
             fx = bf_global[uint32_t(b_records[beg + bb]) >> 2];
             t = f2t[2 * size_t(fx)];
-            fe = tet_face_at(tet_faces, faces, f2t, vfix, t, fx, true, px, py);
+            fe = tet_face_at(tt, vfix, t, fx, true, px, py);
             if (fe == kNoTet) break;
             int be = bb - 1;
             while (be >= 0 && !(uint32_t(b_records[beg + be]) & 1u)) --be;
@@ -220,7 +230,7 @@ __global__ void __launch_bounds__(kTile * kTile, 2) k_walk_adjoint(
         }
         const uint32_t tprev = other_tet(f2t, fe, t);
         if (tprev == kNoTet) break;
-        const uint32_t feprev = tet_face_at(tet_faces, faces, f2t, vfix, tprev, fe, true, px, py);
+        const uint32_t feprev = tet_face_at(tt, vfix, tprev, fe, true, px, py);
         if (feprev == kNoTet) break;
         fx = fe;
         gz_x = gz_e;
@@ -234,30 +244,33 @@ __global__ void __launch_bounds__(kTile * kTile, 2) k_walk_adjoint(
 
 void launch_walk_composite(const u64* b_offsets, const u64* b_records, const uint32_t* bf_global,
                            const uint4* faces, const uint32_t* face_to_tet, const uint32_t* tet_faces,
-                           uint32_t num_tets, const int2* vfix, const VGeo* vgeo, const float4* colors,
+                           const uint32_t* cells, const uint8_t* tet_flip, uint32_t num_tets, const int2* vfix, const VGeo* vgeo, const float4* colors,
                            const CamDev& cam, const ShadeDev& sh, float4* image, float* tfinal, uint4* wstate,
                            cudaStream_t s) {
     dim3 grid((cam.W + kTile - 1) / kTile, (cam.H + kTile - 1) / kTile);
-    k_walk_composite<<<grid, kTile * kTile, 0, s>>>(b_offsets, b_records, bf_global, faces, face_to_tet, tet_faces,
+    const TetTopo tt{reinterpret_cast<const uint4*>(tet_faces), reinterpret_cast<const uint4*>(cells), tet_flip};
+    k_walk_composite<<<grid, kTile * kTile, 0, s>>>(b_offsets, b_records, bf_global, faces, face_to_tet, tt,
                                                     num_tets, vfix, vgeo, colors, cam, sh, image, tfinal, wstate);
 }
 
 void launch_walk_adjoint(const u64* b_offsets, const u64* b_records, const uint32_t* bf_global, const uint4* faces,
-                         const uint32_t* face_to_tet, const uint32_t* tet_faces, uint32_t num_tets,
+                         const uint32_t* face_to_tet, const uint32_t* tet_faces, const uint32_t* cells,
+                         const uint8_t* tet_flip, uint32_t num_tets,
                          const int2* vfix, const VGeo* vgeo, const float4* colors, const CamDev& cam,
                          const ShadeDev& sh, const float4* dimage, const float* tfinal, const uint4* wstate,
                          uint32_t V, float4* grad_rows, float* grad_pos, float4* grad_col, cudaStream_t s) {
     cudaMemsetAsync(grad_rows, 0, sizeof(float4) * 2 * size_t(V), s);
     dim3 grid((cam.W + kTile - 1) / kTile, (cam.H + kTile - 1) / kTile);
+    const TetTopo tt{reinterpret_cast<const uint4*>(tet_faces), reinterpret_cast<const uint4*>(cells), tet_flip};
     // Screen-space position rows unless absolute gradients are asked for
     // (frag_vertex_grads); the scatter converts them per vertex.
     if (sh.use_abs_grad)
         k_walk_adjoint<false><<<grid, kTile * kTile, 0, s>>>(b_offsets, b_records, bf_global, faces, face_to_tet,
-                                                             tet_faces, num_tets, vfix, vgeo, colors, cam, sh, dimage,
+                                                             tt, num_tets, vfix, vgeo, colors, cam, sh, dimage,
                                                              tfinal, wstate, grad_rows);
     else
         k_walk_adjoint<true><<<grid, kTile * kTile, 0, s>>>(b_offsets, b_records, bf_global, faces, face_to_tet,
-                                                            tet_faces, num_tets, vfix, vgeo, colors, cam, sh, dimage,
+                                                            tt, num_tets, vfix, vgeo, colors, cam, sh, dimage,
                                                             tfinal, wstate, grad_rows);
     launch_scatter_grads(grad_rows, V, grad_pos, grad_col, s, sh.use_abs_grad ? nullptr : vgeo, &cam);
 }
