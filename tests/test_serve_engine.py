@@ -55,6 +55,12 @@ def test_all_requests_complete_in_arrival_order_within_budget():
     assert max(len(ids) for _, ids in be.launched) <= 3  # memory budget respected
     st = eng.latency_stats()
     assert st["requests"] == 20 and st["p99_ms"] >= st["p50_ms"] > 0
+    # Latency = queueing + service; the slowest requests come with their batch.
+    assert st["queue_p50_ms"] >= 0 and st["service_p50_ms"] > 0
+    assert st["service_p99_ms"] <= st["p99_ms"] + 1e-9
+    slow = st["slowest"]
+    assert len(slow) == 3 and slow[0]["ms"] >= slow[1]["ms"] >= slow[2]["ms"]
+    assert all(0 <= x["queue_ms"] <= x["ms"] and 1 <= x["batch_size"] <= 3 for x in slow)
 
 
 def test_requests_arriving_during_a_batch_start_on_the_free_slot():
