@@ -47,7 +47,8 @@ def parse_args():
     ap.add_argument("--n", type=int, default=64, help="Kuhn grid cubes per axis")
     ap.add_argument("--res", type=int, default=1024)
     ap.add_argument("--views", type=int, default=16)
-    ap.add_argument("--cpu-rows", type=int, default=32, help="rows of the CPU baseline sample")
+    ap.add_argument("--cpu-rows", type=int, default=64, help="rows of one band of the CPU baseline sample")
+    ap.add_argument("--cpu-bands", type=int, default=4, help="bands timed for the CPU baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
@@ -708,17 +709,15 @@ def run_serving(args):
     return out
 
 
-def cpu_port_sample(args, sc, rows=None):
-    """Time the oracle's FP32 port (all host threads) on a band of rows of one
-    forward + adjoint view of the same workload; returns (iter/s extrapolated
-    to the full image, seconds, description)."""
+def cpu_port_band(args, sc, r0, rows):
+    """Seconds the oracle's FP32 port (all host threads) takes for forward +
+    adjoint of one view of the workload restricted to pixel rows [r0, r0+rows)
+    (every face is still projected, set up and clipped to the band)."""
     import numpy as np
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
 
-    rows = rows or args.cpu_rows
     res = args.res
-    r0 = res // 2 - rows // 2
     fa = O.Faces(sc["cells"], sc["pos"].shape[0])
     cam = O.make_camera(sc["views"][0], __import__("math").radians(45.0), res, res)
     prm = O.make_params(attenuation=1.0, use_ert=True, ert_thresh=1e-4, rows=(r0, r0 + rows))
@@ -727,10 +726,58 @@ def cpu_port_sample(args, sc, rows=None):
     t = time.perf_counter()
     O.render(fa, sc["pos"], sc["col"], cam, prm, precision=32)
     O.adjoint(fa, sc["pos"], sc["col"], cam, prm, w, precision=32)
-    sec = time.perf_counter() - t
-    frac = rows / res
-    return frac / sec, sec, (f"rows [{r0},{r0 + rows}) of {res} ({frac:.4f} of the pixels; faces are rasterised "
-                              f"in full), forward + adjoint of one view, FP32 port, extrapolated to the image")
+    return time.perf_counter() - t
+
+
+def cpu_port_strata(res, rows):
+    """Start rows of the res // rows horizontal strata of `rows` rows, in
+    van der Corput order, so that any prefix spreads over the whole image."""
+    count = max(1, res // rows)
+    order, seen = [], set()
+    for i in range(1, 4 * count + 1):
+        x, f, j = 0.0, 0.5, i
+        while j:
+            x += f * (j & 1)
+            j >>= 1
+            f *= 0.5
+        k = min(int(x * count), count - 1)
+        if k not in seen:
+            seen.add(k)
+            order.append(k)
+    order += [k for k in range(count) if k not in seen]
+    return [k * rows for k in order]
+
+
+class CpuPortEstimate:
+    """Full-image seconds of the oracle's FP32 port (all host threads) for
+    forward + adjoint of one view, from a one-row pass (the per-view part that
+    does not scale with rows: projection and the loop over all faces) and
+    bands of `rows` rows taken from the image's strata in van der Corput order
+    (the per-row part, which varies with how much of the mesh a row crosses):
+    full = fixed + strata * mean(band - fixed)."""
+
+    def __init__(self, args, sc, rows=None):
+        self.args, self.sc = args, sc
+        self.rows = min(rows or args.cpu_rows, args.res)
+        self.starts = cpu_port_strata(args.res, self.rows)
+        self.fixed = cpu_port_band(args, sc, 0, 1)
+        self.bands = []
+
+    def step(self):
+        r0 = self.starts[len(self.bands) % len(self.starts)]
+        t = cpu_port_band(self.args, self.sc, r0, self.rows)
+        self.bands.append(t)
+        return t
+
+    def seconds(self):
+        mean = sum(max(t - self.fixed, 0.0) for t in self.bands) / len(self.bands)
+        return self.fixed + len(self.starts) * mean
+
+    def describe(self):
+        full = self.seconds()
+        return (f"one-row pass ({self.fixed:.3f} s) + {len(self.bands)} bands of {self.rows} rows from the "
+                f"{len(self.starts)} strata of {self.args.res} rows (van der Corput order), forward + adjoint "
+                f"of one view, FP32 port; full image = fixed + {len(self.starts)} x mean band excess = {full:.2f} s")
 
 
 def run_reference(args, rank, world):
@@ -747,21 +794,19 @@ def run_reference(args, rank, world):
     views = [S.sphere_camera(100 + i) for i in range(args.views)]
     sc = {"cells": cells, "pos": pos, "col": col, "views": views, "np": np}
     for _ in range(args.warmup):
-        cpu_port_sample(args, sc, rows=8)
-    secs = []
+        cpu_port_band(args, sc, args.res // 2 - args.cpu_rows // 2, args.cpu_rows)
+    est = CpuPortEstimate(args, sc)
     for _ in range(args.steps):
-        _, s, desc = cpu_port_sample(args, sc, rows=8)
-        secs.append(s)
-    frac = 8 / args.res
-    value = frac / (sum(secs) / len(secs))
+        est.step()
+    value = 1.0 / est.seconds()
+    desc = est.describe()
     cores = O.num_threads()
     return {
         "metric": METRIC, "value": value, "unit": "iter/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
         "config": {"workload": f"plain method, Kuhn {args.n}^3, {args.res}x{args.res}, fwd+adj (CPU port)"},
-        "cpu_baseline": {"value": value, "unit": "iter/s", "cores": cores, "kind": "port",
-                         "sample": desc.replace(f"rows [{args.res // 2 - args.cpu_rows // 2}", "rows [")},
+        "cpu_baseline": {"value": value, "unit": "iter/s", "cores": cores, "kind": "port", "sample": desc},
         "e2e": {"value": value, "unit": "iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "the reference's Vulkan renderer (and lavapipe) is unavailable on this box; the timed CPU "
                 "implementation is this repository's FP32 restatement of its algorithm",
@@ -836,7 +881,10 @@ def main():
         torch.cuda.empty_cache()
         result["served"] = run_serving(args)
     if rank == 0 and not args.no_cpu_baseline:
-        v, s, desc = cpu_port_sample(args, sc)
+        est = CpuPortEstimate(args, sc)
+        for _ in range(args.cpu_bands):
+            est.step()
+        v, s, desc = 1.0 / est.seconds(), est.fixed + sum(est.bands), est.describe()
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import oracle as O
         result["cpu_baseline"] = {"value": v, "unit": "iter/s", "cores": O.num_threads(), "kind": "port",
