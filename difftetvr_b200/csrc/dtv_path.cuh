@@ -347,20 +347,40 @@ __device__ __forceinline__ uint32_t record_lo(const u64* __restrict__ records, u
 // per sub-segment, colour and density linear along the segment), front to
 // back.  Per sub-segment starting at fraction s, c0 = cf + s (cb - cf) and
 // c1 - c0 = (cb - cf) / 4, so C += T ((1 - A) c0 - (K / 4) (cb - cf)).
+// When every sub-segment has a > 0 and a t < 1/8 (nearly all of them at the
+// path's densities) the four sets of terms are independent straight-line code
+// (seg_terms_short, the same arithmetic seg_terms picks for that tier), which
+// the scheduler interleaves; otherwise each sub-segment takes seg_terms.
 __device__ __forceinline__ void segment_composite(float tSeg, const float4& cf, const float4& cb, float atten,
                                                   float& C0, float& C1, float& C2, float& T) {
     const float d0 = cb.x - cf.x, d1 = cb.y - cf.y, d2 = cb.z - cf.z, dw = cb.w - cf.w;
+    float av[kNumSubdivs];
+    bool short_tier = true;
 #pragma unroll
     for (int s = 0; s < kNumSubdivs; ++s) {
-        const float fs = 0.25f * s, fm = 0.25f * (s + 0.5f);
-        const float a = (cf.w + dw * fm) * atten;
-        if (!(a > 0.f)) continue;  // a <= 0 contributes nothing
-        const SegTerms st = seg_terms(tSeg, a);
+        av[s] = (cf.w + dw * (0.25f * (s + 0.5f))) * atten;
+        short_tier &= (av[s] > 0.f) & (av[s] * tSeg < 0.125f);
+    }
+    auto accumulate = [&](int s, const SegTerms& st) {
+        const float fs = 0.25f * s;
         const float w = T * st.omA, k = T * (0.25f * st.K);
         C0 += w * (cf.x + d0 * fs) - k * d0;
         C1 += w * (cf.y + d1 * fs) - k * d1;
         C2 += w * (cf.z + d2 * fs) - k * d2;
         T *= st.A;
+    };
+    if (short_tier) {
+        SegTerms st[kNumSubdivs];
+#pragma unroll
+        for (int s = 0; s < kNumSubdivs; ++s) st[s] = seg_terms_short(tSeg, av[s]);
+#pragma unroll
+        for (int s = 0; s < kNumSubdivs; ++s) accumulate(s, st[s]);
+        return;
+    }
+#pragma unroll
+    for (int s = 0; s < kNumSubdivs; ++s) {
+        if (!(av[s] > 0.f)) continue;  // a <= 0 contributes nothing
+        accumulate(s, seg_terms(tSeg, av[s]));
     }
 }
 
@@ -597,18 +617,24 @@ __device__ __forceinline__ void frag_vertex_grads(const FragV& fr, float qx, flo
 // (BackwardCommon.glsl:121-125) so a density clamped at zero can grow again.
 // Outputs (added): g_tot = dL/d(segment length), the colour weights wf / wb and
 // the alpha adjoints af / ab of the front / back fragment.
-__device__ __forceinline__ void segment_adjoint(float tSeg, const float4& cf, const float4& cb, float pf, float pb,
-                                                float atten, float& T, float& gT, float& g_tot, float& wf,
-                                                float& wb, float& af, float& ab) {
-    const float dp = pb - pf, D = 0.25f * dp, dw = cb.w - cf.w;
+__device__ __forceinline__ void segment_adjoint(float tSeg, float cfw, float cbw, float pf, float pb, float atten,
+                                                float& T, float& gT, float& g_tot, float& wf, float& wb, float& af,
+                                                float& ab) {
+    const float dp = pb - pf, D = 0.25f * dp, dw = cbw - cfw;
+    float av[kNumSubdivs];
+    bool short_tier = true;
 #pragma unroll
-    for (int s = kNumSubdivs - 1; s >= 0; --s) {
+    for (int s = 0; s < kNumSubdivs; ++s) {
+        av[s] = (cfw + dw * (0.25f * (s + 0.5f))) * atten;
+        short_tier &= (av[s] > 0.f) & (av[s] * tSeg < 0.125f);
+    }
+    // One sub-segment, back to front; st is used only when a > 0.
+    auto step = [&](int s, const SegTerms& st, bool dense) {
         const float fs = 0.25f * s, fm = 0.25f * (s + 0.5f);
         const float P0 = pf + fs * dp;
-        const float a = (cf.w + dw * fm) * atten;
+        const float a = av[s];
         float g_a;
-        if (a > 0.f) {
-            const SegTerms st = seg_terms_adj(tSeg, a);
+        if (dense) {
             const float Tin = __fdividef(T, st.A);
             const float gTo = gT;
             gT = st.omA * P0 - st.K * D + gTo * st.A;
@@ -623,7 +649,30 @@ __device__ __forceinline__ void segment_adjoint(float tSeg, const float4& cf, co
         }
         af += (1.f - fm) * g_a * atten;
         ab += fm * g_a * atten;
+    };
+    // Same tiers as segment_composite: straight-line terms when all four
+    // sub-segments are in the short tier (seg_terms_adj's arithmetic there).
+    if (short_tier) {
+        SegTerms st[kNumSubdivs];
+#pragma unroll
+        for (int s = 0; s < kNumSubdivs; ++s) st[s] = seg_terms_adj_short(tSeg, av[s]);
+#pragma unroll
+        for (int s = kNumSubdivs - 1; s >= 0; --s) step(s, st[s], true);
+        return;
     }
+#pragma unroll
+    for (int s = kNumSubdivs - 1; s >= 0; --s) {
+        if (av[s] > 0.f)
+            step(s, seg_terms_adj(tSeg, av[s]), true);
+        else
+            step(s, SegTerms{}, false);
+    }
+}
+
+__device__ __forceinline__ void segment_adjoint(float tSeg, const float4& cf, const float4& cb, float pf, float pb,
+                                                float atten, float& T, float& gT, float& g_tot, float& wf,
+                                                float& wb, float& af, float& ab) {
+    segment_adjoint(tSeg, cf.w, cb.w, pf, pb, atten, T, gT, g_tot, wf, wb, af, ab);
 }
 
 // Position gradients of one fragment from its depth adjoint alone (per-cell
@@ -691,12 +740,164 @@ __device__ __forceinline__ float3 screen_to_world(const float4& a, const VGeo& P
                        V[8] * gxv + V[9] * gyv + V[10] * gzv);
 }
 
+// A fragment of the screen-space adjoint with what its vertex gradients need:
+// the interpolation state of face_interp and its vertices' colours reduced by
+// the pixel's colour adjoint gC.  A fragment's gradients are taken one step
+// after it is loaded (its back segment and its front segment must both be
+// done), so carrying this state spares the second gather of its three
+// vertices and the second FP64 solve.  Its depth, alpha and colour are those
+// of load_frag_face (same expressions), so the adjoint walks the forward's
+// values.
+struct FragG {
+    uint32_t v[3];
+    uint32_t bits;
+    float z, alpha, pcol;            // depth, alpha, gC . colour.rgb
+    float lam[3], iz[3], dx[3], dy[3];
+    float invA, zb, zz;              // 1 / sum(E), 1 / sum(lam iz), zb^2 (0 when the depth is clamped)
+    float pc[3], cw[3];              // gC . vertex colour rgb, vertex alpha
+};
+
+__device__ __forceinline__ FragG load_frag_g(uint32_t lo, const uint4& fc, float qx, float qy,
+                                             const VGeo* __restrict__ vgeo, const float4* __restrict__ colors,
+                                             float gC0, float gC1, float gC2) {
+    FragG f;
+    f.bits = lo & 3u;
+    f.v[0] = fc.x;
+    f.v[1] = fc.y;
+    f.v[2] = fc.z;
+    const VGeo a = vgeo[fc.x], b = vgeo[fc.y], c = vgeo[fc.z];
+    FaceInterp fi;
+    face_interp(a, b, c, qx, qy, fi);
+    const float4 c0 = colors[fc.x], c1 = colors[fc.y], c2 = colors[fc.z];
+    const float* bary = fi.bary;
+    const float4 col = make_float4(bary[0] * c0.x + bary[1] * c1.x + bary[2] * c2.x,
+                                   bary[0] * c0.y + bary[1] * c1.y + bary[2] * c2.y,
+                                   bary[0] * c0.z + bary[1] * c1.z + bary[2] * c2.z,
+                                   bary[0] * c0.w + bary[1] * c1.w + bary[2] * c2.w);
+    f.z = fi.z;
+    f.alpha = col.w;
+    f.pcol = gC0 * col.x + gC1 * col.y + gC2 * col.z;
+    f.iz[0] = a.iz;
+    f.iz[1] = b.iz;
+    f.iz[2] = c.iz;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        f.lam[j] = fi.lam[j];
+        f.dx[j] = fi.dx[j];
+        f.dy[j] = fi.dy[j];
+    }
+    f.invA = __fdividef(1.0f, fi.A);
+    f.zb = fi.zb;
+    f.zz = fi.clamped ? 0.f : fi.zb * fi.zb;
+    f.pc[0] = gC0 * c0.x + gC1 * c0.y + gC2 * c0.z;
+    f.pc[1] = gC0 * c1.x + gC1 * c1.y + gC2 * c1.z;
+    f.pc[2] = gC0 * c2.x + gC1 * c2.y + gC2 * c2.z;
+    f.cw[0] = c0.w;
+    f.cw[1] = c1.w;
+    f.cw[2] = c2.w;
+    return f;
+}
+
+// frag_vertex_grads with SCREEN from a carried fragment: depth adjoint gz,
+// colour weight w (colour adjoint = gC w) and alpha adjoint ga.
+template <class Acc>
+__device__ __forceinline__ void frag_grads_carried(const FragG& f, float gz, float w, float ga, Acc& acc) {
+    float bary[3], gb[3], sb = 0.f;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        bary[j] = (f.lam[j] * f.iz[j]) * f.zb;
+        gb[j] = w * f.pc[j] + ga * f.cw[j];
+        sb += gb[j] * bary[j];
+    }
+    const float gzz = gz * f.zz;
+    float glam[3], giz[3], sl = 0.f;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        const float gu = f.zb * (gb[j] - sb) - gzz;
+        glam[j] = gu * f.iz[j];
+        giz[j] = gu * f.lam[j];
+        sl += glam[j] * f.lam[j];
+    }
+    float gE[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) gE[j] = (glam[j] - sl) * f.invA;
+    const float* dx = f.dx;
+    const float* dy = f.dy;
+    float4 gpv[3];
+    float gav[3];
+    gpv[0] = make_float4(-gE[1] * dy[2] + gE[2] * dy[1], gE[1] * dx[2] - gE[2] * dx[1], giz[0], w * bary[0]);
+    gpv[1] = make_float4(gE[0] * dy[2] - gE[2] * dy[0], -gE[0] * dx[2] + gE[2] * dx[0], giz[1], w * bary[1]);
+    gpv[2] = make_float4(-gE[0] * dy[1] + gE[1] * dy[0], gE[0] * dx[1] - gE[1] * dx[0], giz[2], w * bary[2]);
+#pragma unroll
+    for (int j = 0; j < 3; ++j) gav[j] = ga * bary[j];
+    acc.add_face(f.v, gpv, gav);
+}
+
+// adjoint_pixel for screen-space rows (no absolute gradients), on carried
+// fragments.
+template <class Acc>
+__device__ __forceinline__ void adjoint_pixel_carried(
+    int px, int py, const u64* __restrict__ offsets, const u64* __restrict__ records, const uint4* __restrict__ faces,
+    const VGeo* __restrict__ vgeo, const float4* __restrict__ colors, int W, const ShadeDev& sh,
+    const float4* __restrict__ dimage, const float* __restrict__ tfinal, const uint32_t* __restrict__ term,
+    Acc& acc) {
+    const size_t p = size_t(py) * W + px;
+    const u64 beg = offsets[p];
+    const uint32_t n = uint32_t(offsets[p + 1] - beg);
+    if (n < 2) return;
+    const float4 g = dimage[p];
+    if (g.x == 0.f && g.y == 0.f && g.z == 0.f && g.w == 0.f) return;
+    const float qx = float(px) + 0.5f, qy = float(py) + 0.5f;
+    const float gC0 = g.x, gC1 = g.y, gC2 = g.z;
+    float gT = g.x * sh.clear[0] + g.y * sh.clear[1] + g.z * sh.clear[2] + g.w * (sh.clear[3] - 1.f);
+    float T = tfinal[p];
+    const int last = sh.use_ert ? int(term[p]) - 1 : int(n) - 1;
+    if (last < 1) return;
+    const float atten = sh.atten;
+    acc.set_pixel(gC0, gC1, gC2);
+    // Dependent loads record -> face -> vertex rows software-pipelined as in
+    // adjoint_pixel.
+    const uint32_t lo_b = record_lo(records, beg + last);
+    FragG fb = load_frag_g(lo_b, faces[lo_b >> 2], qx, qy, vgeo, colors, gC0, gC1, gC2);
+    uint32_t lo_f = record_lo(records, beg + last - 1);
+    uint4 fc_f = faces[lo_f >> 2];
+    uint32_t lo_n = last >= 2 ? record_lo(records, beg + last - 2) : 0u;
+    float gz_b = 0.f, wb = 0.f, ab = 0.f;
+    for (int i = last; i >= 1; --i) {
+        const FragG ff = load_frag_g(lo_f, fc_f, qx, qy, vgeo, colors, gC0, gC1, gC2);
+        if (i >= 2) {
+            fc_f = faces[lo_n >> 2];
+            lo_f = lo_n;
+            if (i >= 3) lo_n = record_lo(records, beg + i - 3);
+        }
+        float gz_f = 0.f, wf = 0.f, af = 0.f;
+        if (!skip_pair(ff.bits, fb.bits)) {
+            float g_tot = 0.f;
+            segment_adjoint((fb.z - ff.z) * 0.25f, ff.alpha, fb.alpha, ff.pcol, fb.pcol, atten, T, gT, g_tot, wf,
+                            wb, af, ab);
+            gz_f -= g_tot;
+            gz_b += g_tot;
+        }
+        frag_grads_carried(fb, gz_b, wb, ab, acc);
+        fb = ff;
+        gz_b = gz_f;
+        wb = wf;
+        ab = af;
+    }
+    frag_grads_carried(fb, gz_b, wb, ab, acc);
+    acc.flush();
+}
+
 template <class Acc, bool SCREEN = false>
 __device__ __forceinline__ void adjoint_pixel(
     int px, int py, const u64* __restrict__ offsets, const u64* __restrict__ records, const uint4* __restrict__ faces,
     const VGeo* __restrict__ vgeo, const float4* __restrict__ colors, int W, const CamDev& cam, const ShadeDev& sh,
     const float4* __restrict__ dimage, const float* __restrict__ tfinal, const uint32_t* __restrict__ term,
     Acc& acc) {
+    if constexpr (SCREEN) {
+        adjoint_pixel_carried(px, py, offsets, records, faces, vgeo, colors, W, sh, dimage, tfinal, term, acc);
+        return;
+    }
     const size_t p = size_t(py) * W + px;
     const u64 beg = offsets[p];
     const uint32_t n = uint32_t(offsets[p + 1] - beg);

@@ -107,16 +107,36 @@ __device__ __forceinline__ float series_chi_short(float x) {
     return p;
 }
 
-// Forward terms; caller guarantees a > 0.  (The reference drops a < 1e-6; the
-// continuous value kept here differs from that by at most a t.)
-__device__ __forceinline__ SegTerms seg_terms(float t, float a) {
+// The x = a t < 1/8 tier of seg_terms / seg_terms_adj alone (no branch), for
+// callers that have checked the tier for several sub-segments at once.
+__device__ __forceinline__ SegTerms seg_terms_short(float t, float a) {
     SegTerms s;
     const float x = a * t;
     s.A = __expf(-x);
-    if (x < 0.125f) {
-        s.omA = x * series_phi1_short(x);
-        s.K = -t * x * series_psi_short(x);
-    } else if (x < 0.5f) {
+    s.omA = x * series_phi1_short(x);
+    s.K = -t * x * series_psi_short(x);
+    s.dK = 0.f;
+    return s;
+}
+
+__device__ __forceinline__ SegTerms seg_terms_adj_short(float t, float a) {
+    SegTerms s;
+    const float x = a * t;
+    s.A = __expf(-x);
+    s.omA = x * series_phi1_short(x);
+    s.K = -t * x * series_psi_short(x);
+    s.dK = t * t * series_chi_short(x);
+    return s;
+}
+
+// Forward terms; caller guarantees a > 0.  (The reference drops a < 1e-6; the
+// continuous value kept here differs from that by at most a t.)
+__device__ __forceinline__ SegTerms seg_terms(float t, float a) {
+    const float x = a * t;
+    if (x < 0.125f) return seg_terms_short(t, a);
+    SegTerms s;
+    s.A = __expf(-x);
+    if (x < 0.5f) {
         s.omA = x * series_phi1(x);
         s.K = -t * x * series_psi(x);
     } else {
@@ -130,15 +150,12 @@ __device__ __forceinline__ SegTerms seg_terms(float t, float a) {
 
 // Forward terms and dK/da in one pass (adjoint); caller guarantees a > 0.
 __device__ __forceinline__ SegTerms seg_terms_adj(float t, float a) {
-    SegTerms s;
     const float x = a * t;
+    if (x < 0.125f) return seg_terms_adj_short(t, a);
+    SegTerms s;
     s.A = __expf(-x);
     float chi;
-    if (x < 0.125f) {
-        s.omA = x * series_phi1_short(x);
-        s.K = -t * x * series_psi_short(x);
-        chi = series_chi_short(x);
-    } else if (x < 0.5f) {
+    if (x < 0.5f) {
         s.omA = x * series_phi1(x);
         s.K = -t * x * series_psi(x);
         chi = series_chi(x);
