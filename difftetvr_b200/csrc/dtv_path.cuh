@@ -466,40 +466,52 @@ struct VertCache {
     __device__ __forceinline__ void set_pixel(float a0, float a1, float a2) { g0 = a0; g1 = a1; g2 = a2; }
     __device__ __forceinline__ void spill(int s, uint32_t v) const {
         if (v == kNone) return;
+        spill_held(s, v);
+    }
+    __device__ __forceinline__ void spill_held(int s, uint32_t v) const {
         const float4 q = c4[s * stride];
         const float a = c1[s * stride];
         atomicAdd(rows + 2 * size_t(v), make_float4(q.x, q.y, q.z, 0.f));
         atomicAdd(rows + 2 * size_t(v) + 1, make_float4(g0 * q.w, g1 * q.w, g2 * q.w, a));
     }
+    // The same steps for every lane (no branch on which slot a vertex is in):
+    // the retired slots are spilled in a loop over the retire mask (one pass
+    // on most fragments: each new face usually retires one vertex), and each
+    // of the face's vertices adds into its slot, a new one into the lowest
+    // free slot (the load of its old value predicated off).
     __device__ __forceinline__ void add_face(const uint32_t (&v)[3], const float4 (&gp)[3], const float (&s2)[3]) {
         int m[3];  // cache slot holding each vertex of the face, -1 if none
-#pragma unroll
-        for (int k = 0; k < 3; ++k) m[k] = v[k] == id0 ? 0 : (v[k] == id1 ? 1 : (v[k] == id2 ? 2 : -1));
-        bool u0 = m[0] == 0 || m[1] == 0 || m[2] == 0;
-        bool u1 = m[0] == 1 || m[1] == 1 || m[2] == 1;
-        bool u2 = m[0] == 2 || m[1] == 2 || m[2] == 2;
-        // Retire the cached vertices the face does not have.
-        if (!u0) { spill(0, id0); id0 = kNone; }
-        if (!u1) { spill(1, id1); id1 = kNone; }
-        if (!u2) { spill(2, id2); id2 = kNone; }
+        uint32_t used = 0u;
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            if (m[k] >= 0) {
-                const int o = m[k] * stride;
-                const float4 q = c4[o];
-                c4[o] = make_float4(q.x + gp[k].x, q.y + gp[k].y, q.z + gp[k].z, q.w + gp[k].w);
-                c1[o] += s2[k];
-            } else {
-                const int s = !u0 ? 0 : (!u1 ? 1 : 2);
-                u0 |= s == 0;
-                u1 |= s == 1;
-                u2 |= s == 2;
-                if (s == 0) id0 = v[k];
-                else if (s == 1) id1 = v[k];
-                else id2 = v[k];
-                c4[s * stride] = gp[k];
-                c1[s * stride] = s2[k];
+            m[k] = v[k] == id0 ? 0 : (v[k] == id1 ? 1 : (v[k] == id2 ? 2 : -1));
+            used |= m[k] >= 0 ? (1u << m[k]) : 0u;
+        }
+        const uint32_t held = uint32_t(id0 != kNone) | (uint32_t(id1 != kNone) << 1) | (uint32_t(id2 != kNone) << 2);
+        uint32_t retire = held & ~used;
+        while (retire) {
+            const int s = __ffs(retire) - 1;
+            retire &= retire - 1u;
+            spill_held(s, s == 0 ? id0 : (s == 1 ? id1 : id2));
+        }
+        uint32_t free = ~used & 7u;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const bool hit = m[k] >= 0;
+            const int s = hit ? m[k] : __ffs(free) - 1;
+            free = hit ? free : (free & (free - 1u));
+            const int o = s * stride;
+            float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
+            float a = 0.f;
+            if (hit) {
+                q = c4[o];
+                a = c1[o];
             }
+            c4[o] = make_float4(q.x + gp[k].x, q.y + gp[k].y, q.z + gp[k].z, q.w + gp[k].w);
+            c1[o] = a + s2[k];
+            id0 = (!hit && s == 0) ? v[k] : id0;
+            id1 = (!hit && s == 1) ? v[k] : id1;
+            id2 = (!hit && s == 2) ? v[k] : id2;
         }
     }
     __device__ __forceinline__ void flush() {
