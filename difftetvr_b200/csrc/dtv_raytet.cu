@@ -162,6 +162,62 @@ __global__ void __launch_bounds__(kTile * kTile, 2) k_walk_composite(
     wstate[p] = make_uint4(last_tet, last_entry, last_b, nseg);
 }
 
+// The walk adjoint with screen-space rows on carried fragments (FragG): the
+// exit fragment of a tet is the entry fragment of the one walked before it,
+// so each step loads and solves one face, and a fragment's gradients are taken
+// from the state kept since its load.  Same steps and values as the general
+// loop in k_walk_adjoint.
+template <class Acc>
+__device__ __forceinline__ void walk_adjoint_carried(
+    const u64* __restrict__ b_records, u64 beg, const uint32_t* __restrict__ bf_global,
+    const uint4* __restrict__ faces, const uint32_t* __restrict__ f2t, const TetTopo& tt, uint32_t num_tets,
+    const int2* __restrict__ vfix, const VGeo* __restrict__ vgeo, const float4* __restrict__ colors, int px, int py,
+    float scale, float atten, float gC0, float gC1, float gC2, float T, float gT, uint32_t t, uint32_t fe,
+    uint32_t fx, int b, Acc& acc) {
+    const float qx = float(px) + 0.5f, qy = float(py) + 0.5f;
+    FragG fX = load_frag_g(fx << 2, faces[fx], qx, qy, vgeo, colors, gC0, gC1, gC2);
+    float gz_x = 0.f, wx = 0.f, ax = 0.f;
+    for (uint32_t step = 0; step <= num_tets; ++step) {
+        const FragG fE = load_frag_g(fe << 2, faces[fe], qx, qy, vgeo, colors, gC0, gC1, gC2);
+        const float tSeg = (fX.z - fE.z) * scale * 0.25f;
+        float g_tot = 0.f, we = 0.f, ae = 0.f;
+        segment_adjoint(tSeg, fE.alpha, fX.alpha, fE.pcol, fX.pcol, atten, T, gT, g_tot, we, wx, ae, ax);
+        const float gz_e = -g_tot * scale;
+        gz_x += g_tot * scale;
+        frag_grads_carried(fX, gz_x, wx, ax, acc);
+        if (faces[fe].w & 1u) {
+            frag_grads_carried(fE, gz_e, we, ae, acc);
+            // Previous interval: its exit is the last back-facing boundary fragment before b.
+            int bb = b - 1;
+            while (bb >= 0 && (uint32_t(b_records[beg + bb]) & 1u)) --bb;
+            if (bb < 0) break;
+            fx = bf_global[uint32_t(b_records[beg + bb]) >> 2];
+            t = f2t[2 * size_t(fx)];
+            fe = tet_face_at(tt, vfix, t, fx, true, px, py);
+            if (fe == kNoTet) break;
+            int be = bb - 1;
+            while (be >= 0 && !(uint32_t(b_records[beg + be]) & 1u)) --be;
+            b = be < 0 ? 0 : be;
+            fX = load_frag_g(fx << 2, faces[fx], qx, qy, vgeo, colors, gC0, gC1, gC2);
+            gz_x = 0.f;
+            wx = 0.f;
+            ax = 0.f;
+            continue;
+        }
+        const uint32_t tprev = other_tet(f2t, fe, t);
+        if (tprev == kNoTet) break;
+        const uint32_t feprev = tet_face_at(tt, vfix, tprev, fe, true, px, py);
+        if (feprev == kNoTet) break;
+        fX = fE;
+        gz_x = gz_e;
+        wx = we;
+        ax = ae;
+        t = tprev;
+        fe = feprev;
+    }
+    acc.flush();
+}
+
 template <bool SCREEN>
 __global__ void __launch_bounds__(kTile * kTile, 2) k_walk_adjoint(
     const u64* __restrict__ b_offsets, const u64* __restrict__ b_records, const uint32_t* __restrict__ bf_global,
@@ -188,8 +244,16 @@ __global__ void __launch_bounds__(kTile * kTile, 2) k_walk_adjoint(
     int b = int(ws.z);
     uint32_t fx = tet_face_at(tt, vfix, t, fe, false, px, py);
     if (fx == kNoTet) return;
-    // Vertex rows straight to global memory: the shared-memory vertex cache of
-    // the list path measured slower here (register spills in the walk).
+    if constexpr (SCREEN) {
+        __shared__ float4 vcache4[3 * kTile * kTile];
+        __shared__ float vcache1[3 * kTile * kTile];
+        VertCache acc{grad_rows, vcache4 + threadIdx.x, vcache1 + threadIdx.x, kTile * kTile};
+        acc.set_pixel(gC0, gC1, gC2);
+        walk_adjoint_carried(b_records, beg, bf_global, faces, f2t, tt, num_tets, vfix, vgeo, colors, px, py, scale,
+                             atten, gC0, gC1, gC2, T, gT, t, fe, fx, b, acc);
+        return;
+    }
+    // Vertex rows straight to global memory (absolute gradients, world rows).
     GradAcc acc{grad_rows};
     if (use_abs)
         acc.set_pixel(fabsf(gC0), fabsf(gC1), fabsf(gC2));
