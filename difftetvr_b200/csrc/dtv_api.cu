@@ -90,6 +90,8 @@ struct dtv_renderer {
     dtv_tuning tuning{0, 0, dtv::kSortSurrogateDefault, dtv::kSortBucketDefault};
     u64* h_rowoff = nullptr;      // pinned row-start offsets (H+1)
     size_t h_rowoff_cap = 0;
+    DevBuf<uint32_t> fill_order;    // faces in row-band order for the fill
+    DevBuf<uint32_t> band_scratch;  // band counts and cursors of fill_order
     DevBuf<uint4> wstate;         // ray-tet path: (last tet, its entry face, boundary entry index, segments)
     u64* h_nf = nullptr;          // pinned
     uint32_t* h_flags = nullptr;  // pinned
@@ -157,14 +159,15 @@ uint64_t plan_bands(dtv_renderer* r, int W, int H, uint64_t cap, cudaStream_t s)
 }
 
 // Builds the sorted lists of rows [y0, y1) into the records buffer (band-local
-// offsets): scan of the band's counts, fill, per-pixel sort.  The band's
-// counts must hold the rasterised counts; the fill leaves them zero.
+// offsets): scan of the band's counts, fill (faces in the render's fill_order),
+// per-pixel sort.  The band's counts must hold the rasterised counts; the fill
+// leaves them zero.
 void build_band_lists(dtv_renderer* r, const dtv_mesh* mesh, int W, int H, int y0, int y1, cudaStream_t s) {
     const uint64_t p0 = uint64_t(y0) * W, pb = uint64_t(y1 - y0) * W;
     dtv::launch_scan(r->counts.ptr + p0, pb, r->offsets.ptr + p0, r->scan_scratch.ptr, s);
     check_launch("band scan");
     dtv::launch_raster_fill(mesh->d_faces, uint32_t(mesh->host.num_faces), r->vproj.ptr, r->vfix.ptr, W, H,
-                            r->counts.ptr, r->offsets.ptr, r->records.ptr, s, y0, y1);
+                            r->counts.ptr, r->offsets.ptr, r->records.ptr, s, y0, y1, r->fill_order.ptr);
     check_launch("band fill");
     dtv::launch_sort(r->offsets.ptr + p0, r->records.ptr, uint32_t(pb), r->long_list.ptr, r->flags.ptr, s, nullptr,
                      r->tuning.sort_surrogate_classes, r->tuning.sort_bucket_classes);
@@ -440,6 +443,8 @@ int32_t dtv_renderer_destroy(dtv_renderer* r) {
     r->flags.release();
     r->grad_rows.release();
     r->wstate.release();
+    r->fill_order.release();
+    r->band_scratch.release();
     if (r->h_nf) cudaFreeHost(r->h_nf);
     if (r->h_flags) cudaFreeHost(r->h_flags);
     if (r->h_rowoff) cudaFreeHost(r->h_rowoff);
@@ -521,6 +526,10 @@ int32_t render_common(dtv_renderer* r, const dtv_mesh* mesh, const float* d_posi
                                                    " bytes), over the budget of " + std::to_string(budget) +
                                                    " bytes");
             }
+            r->fill_order.ensure(size_t(F), s);
+            r->band_scratch.ensure(2 * dtv::kFillBands, s);
+            dtv::launch_fill_order(rfaces, uint32_t(F), r->vfix.ptr, H, nf, r->fill_order.ptr, r->band_scratch.ptr,
+                                   s);
             render_banded(r, mesh, d_colors, cam, sh, d_image, budget / sizeof(u64), s);
             r->adjoint_timed = false;
             r->have_render = true;
@@ -539,8 +548,11 @@ int32_t render_common(dtv_renderer* r, const dtv_mesh* mesh, const float* d_posi
             throw;
         }
         rec_event(r, 3, s);
+        r->fill_order.ensure(size_t(F), s);
+        r->band_scratch.ensure(2 * dtv::kFillBands, s);
+        dtv::launch_fill_order(rfaces, uint32_t(F), r->vfix.ptr, H, nf, r->fill_order.ptr, r->band_scratch.ptr, s);
         dtv::launch_raster_fill(rfaces, uint32_t(F), r->vproj.ptr, r->vfix.ptr, W, H, r->counts.ptr,
-                                r->offsets.ptr, r->records.ptr, s);
+                                r->offsets.ptr, r->records.ptr, s, 0, -1, r->fill_order.ptr);
         check_launch("raster fill");
         rec_event(r, 4, s);
         DTV_CK(cudaMemsetAsync(r->flags.ptr, 0, 2 * sizeof(uint32_t), s));

@@ -37,7 +37,14 @@ void launch_raster_count(const uint4* faces, uint32_t F, const float4* vproj, co
                          uint32_t* counts, cudaStream_t s, int row0 = 0, int row1 = -1);
 void launch_raster_fill(const uint4* faces, uint32_t F, const float4* vproj, const int2* vfix, int W, int H,
                         uint32_t* counts, const unsigned long long* offsets, unsigned long long* records,
-                        cudaStream_t s, int row0 = 0, int row1 = -1);
+                        cudaStream_t s, int row0 = 0, int row1 = -1, const uint32_t* order = nullptr);
+// Order of the faces for the fill, grouped by row bands of about
+// kFillBandBytes of records each (nf records over H rows; order: F entries;
+// band_scratch: 2 * kFillBands entries).
+constexpr int kFillBands = 512;
+constexpr uint64_t kFillBandBytes = 24ull << 20;
+void launch_fill_order(const uint4* faces, uint32_t F, const int2* vfix, int H, uint64_t nf, uint32_t* order,
+                       uint32_t* band_scratch, cudaStream_t s);
 // Exclusive scan of counts[n] into offsets[n+1]; scratch must hold scan_scratch_elems(n) u64.
 size_t scan_scratch_elems(uint64_t n);
 void launch_scan(const uint32_t* counts, uint64_t n, unsigned long long* offsets, unsigned long long* scratch,

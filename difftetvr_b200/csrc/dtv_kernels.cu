@@ -44,10 +44,12 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster(const uint4* __res
                                                               const int2* __restrict__ vfix, int W, int row0, int row1,
                                                               uint32_t* __restrict__ counts,
                                                               const u64* __restrict__ offsets,
-                                                              u64* __restrict__ records) {
-    const uint32_t f = blockIdx.x * blockDim.x + threadIdx.x;
+                                                              u64* __restrict__ records,
+                                                              const uint32_t* __restrict__ order) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t f = (order && i < F) ? order[i] : i;
     RasterJob J;
-    const bool live = f < F && raster_setup(f, faces, vfix, 0u, W, row0, row1, 0ull, J) && (J.wide != 0) == WIDE;
+    const bool live = i < F && raster_setup(f, faces, vfix, 0u, W, row0, row1, 0ull, J) && (J.wide != 0) == WIDE;
     if constexpr (!FILL) {
         if (live) count_face<typename std::conditional<WIDE, long long, int>::type>(J, counts);
     } else {
@@ -71,21 +73,112 @@ void launch_raster_count(const uint4* faces, uint32_t F, const float4* vproj, co
     if (row1 <= row0) return;
     const unsigned blocks = (F + 32 * kRasterWarps - 1) / (32 * kRasterWarps);
     k_raster<false, false><<<blocks, 32 * kRasterWarps, 0, s>>>(faces, F, vproj, vfix, W, row0, row1, counts, nullptr,
-                                                                nullptr);
+                                                                nullptr, nullptr);
     k_raster<false, true><<<blocks, 32 * kRasterWarps, 0, s>>>(faces, F, vproj, vfix, W, row0, row1, counts, nullptr,
-                                                               nullptr);
+                                                               nullptr, nullptr);
     k_row_prefix<<<unsigned(row1 - row0 + 7) / 8, 256, 0, s>>>(counts, W, row0, row1);
 }
 
 void launch_raster_fill(const uint4* faces, uint32_t F, const float4* vproj, const int2* vfix, int W, int H,
-                        uint32_t* counts, const u64* offsets, u64* records, cudaStream_t s, int row0, int row1) {
+                        uint32_t* counts, const u64* offsets, u64* records, cudaStream_t s, int row0, int row1,
+                        const uint32_t* order) {
     if (F == 0) return;
     if (row1 < 0) row1 = H;
     const unsigned blocks = (F + 32 * kRasterWarps - 1) / (32 * kRasterWarps);
     k_raster<true, false><<<blocks, 32 * kRasterWarps, 0, s>>>(faces, F, vproj, vfix, W, row0, row1, counts, offsets,
-                                                               records);
+                                                               records, order);
     k_raster<true, true><<<blocks, 32 * kRasterWarps, 0, s>>>(faces, F, vproj, vfix, W, row0, row1, counts, offsets,
-                                                              records);
+                                                              records, order);
+}
+
+// ---------------------------------------------------------------------------
+// Face order of the fill: faces grouped by the band of 2^shift image rows
+// that holds their first covered row.  In face-index order every pixel's list
+// receives records throughout the fill, so each 32-byte sector of the record
+// buffer (four records) is written piecemeal and leaves L2 partly written
+// (a DRAM read to merge, and the sector written again).  Band by band, the
+// lists being written at any time belong to a few bands whose records fit in
+// L2 until their sectors are complete.  The order within a band is arbitrary:
+// the per-pixel sort makes the lists canonical.
+__device__ __forceinline__ int fill_band(uint32_t f, const uint4* __restrict__ faces, const int2* __restrict__ vfix,
+                                         int H, int shift) {
+    const uint4 fc = faces[f];
+    const int2 q0 = vfix[fc.x], q1 = vfix[fc.y], q2 = vfix[fc.z];
+    if (q0.x == kInvalidFix || q1.x == kInvalidFix || q2.x == kInvalidFix) return 0;
+    const long long minY = min(q0.y, min(q1.y, q2.y));
+    const long long py0 = ceil_div256(minY - 128);
+    return int(min((long long)H - 1, max(0LL, py0))) >> shift;
+}
+
+__global__ void __launch_bounds__(256) k_band_count(const uint4* __restrict__ faces, uint32_t F,
+                                                    const int2* __restrict__ vfix, int H, int shift,
+                                                    uint32_t* __restrict__ hist) {
+    __shared__ uint32_t h[kFillBands];
+    for (int b = threadIdx.x; b < kFillBands; b += blockDim.x) h[b] = 0u;
+    __syncthreads();
+    const uint32_t f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f < F) atomicAdd(&h[fill_band(f, faces, vfix, H, shift)], 1u);
+    __syncthreads();
+    for (int b = threadIdx.x; b < kFillBands; b += blockDim.x)
+        if (h[b]) atomicAdd(&hist[b], h[b]);
+}
+
+// hist[b] -> exclusive prefix in cursor[b] (one warp).
+__global__ void k_band_scan(const uint32_t* __restrict__ hist, uint32_t* __restrict__ cursor) {
+    const int lane = threadIdx.x;
+    uint32_t carry = 0;
+    for (int b0 = 0; b0 < kFillBands; b0 += 32) {
+        const uint32_t v = hist[b0 + lane];
+        uint32_t incl = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(kFull, incl, o);
+            if (lane >= o) incl += t;
+        }
+        cursor[b0 + lane] = carry + incl - v;
+        carry += __shfl_sync(kFull, incl, 31);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_band_scatter(const uint4* __restrict__ faces, uint32_t F,
+                                                      const int2* __restrict__ vfix, int H, int shift,
+                                                      uint32_t* __restrict__ cursor, uint32_t* __restrict__ order) {
+    __shared__ uint32_t h[kFillBands], base[kFillBands];
+    for (int b = threadIdx.x; b < kFillBands; b += blockDim.x) h[b] = 0u;
+    __syncthreads();
+    const uint32_t f = blockIdx.x * blockDim.x + threadIdx.x;
+    int band = 0;
+    uint32_t rank = 0;
+    if (f < F) {
+        band = fill_band(f, faces, vfix, H, shift);
+        rank = atomicAdd(&h[band], 1u);
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < kFillBands; b += blockDim.x)
+        if (h[b]) base[b] = atomicAdd(&cursor[b], h[b]);
+    __syncthreads();
+    if (f < F) order[base[band] + rank] = f;
+}
+
+// Largest band of 2^shift rows whose records (nf over H rows on average) stay
+// under kFillBandBytes, with at most kFillBands bands.
+int fill_band_shift(int H, uint64_t nf) {
+    const double per_row = double(nf) * sizeof(u64) / double(H > 0 ? H : 1);
+    int shift = 0;
+    while (shift < 30 && per_row * double(2u << shift) <= double(kFillBandBytes)) ++shift;
+    while (((H - 1) >> shift) >= kFillBands) ++shift;
+    return shift;
+}
+
+void launch_fill_order(const uint4* faces, uint32_t F, const int2* vfix, int H, uint64_t nf, uint32_t* order,
+                       uint32_t* band_scratch, cudaStream_t s) {
+    if (F == 0) return;
+    const int shift = fill_band_shift(H, nf);
+    const unsigned blocks = (F + 255) / 256;
+    cudaMemsetAsync(band_scratch, 0, kFillBands * sizeof(uint32_t), s);
+    k_band_count<<<blocks, 256, 0, s>>>(faces, F, vfix, H, shift, band_scratch);
+    k_band_scan<<<1, 32, 0, s>>>(band_scratch, band_scratch + kFillBands);
+    k_band_scatter<<<blocks, 256, 0, s>>>(faces, F, vfix, H, shift, band_scratch + kFillBands, order);
 }
 
 // ---------------------------------------------------------------------------
