@@ -102,18 +102,81 @@ __global__ void __launch_bounds__(256) kb_project(const BatchView* __restrict__ 
     }
 }
 
+// Row-band order of the batch fill (launch_fill_order for one view): items
+// (view faces) grouped by the band of 2^shift pixels of the concatenated
+// views' pixels that holds the start of the face's first covered row, the
+// shift putting about kFillBandBytes of records in a band.  The shift comes
+// from the scanned total on the device (no host read in a captured step).
+__device__ __forceinline__ int kb_band_shift(const u64* __restrict__ offsets, u64 tot_pixels) {
+    const u64 nf = offsets[tot_pixels];
+    const u64 target = nf ? (kFillBandBytes / sizeof(u64)) * tot_pixels / nf : tot_pixels;
+    int shift = target ? 63 - __clzll((long long)target) : 0;
+    while (((tot_pixels - 1) >> shift) >= u64(kFillBands)) ++shift;
+    return shift;
+}
+
+__device__ __forceinline__ int kb_face_band(const BatchView* __restrict__ views, int nviews, u64 g,
+                                            const int2* __restrict__ vfix, int shift) {
+    const int v = find_index(g, nviews, [&](int i) { return views[i].face_base; });
+    const BatchView& bv = views[v];
+    const uint4 fc = bv.faces[g - bv.face_base];
+    const int2* vf = vfix + bv.vert_base;
+    const int2 q0 = vf[fc.x], q1 = vf[fc.y], q2 = vf[fc.z];
+    if (q0.x == kInvalidFix || q1.x == kInvalidFix || q2.x == kInvalidFix) return 0;
+    const long long minY = min(q0.y, min(q1.y, q2.y));
+    const long long py0 = min((long long)bv.H - 1, max(0LL, ceil_div256(minY - 128)));
+    return int(min(u64(kFillBands - 1), (bv.pix_base + u64(py0) * bv.W) >> shift));
+}
+
+__global__ void __launch_bounds__(256) kb_band_count(const BatchView* __restrict__ views, int nviews, u64 total,
+                                                     const int2* __restrict__ vfix, const u64* __restrict__ offsets,
+                                                     u64 tot_pixels, uint32_t* __restrict__ hist) {
+    __shared__ uint32_t h[kFillBands];
+    for (int b = threadIdx.x; b < kFillBands; b += blockDim.x) h[b] = 0u;
+    __syncthreads();
+    const u64 g = u64(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (g < total) atomicAdd(&h[kb_face_band(views, nviews, g, vfix, kb_band_shift(offsets, tot_pixels))], 1u);
+    __syncthreads();
+    for (int b = threadIdx.x; b < kFillBands; b += blockDim.x)
+        if (h[b]) atomicAdd(&hist[b], h[b]);
+}
+
+__global__ void __launch_bounds__(256) kb_band_scatter(const BatchView* __restrict__ views, int nviews, u64 total,
+                                                       const int2* __restrict__ vfix, const u64* __restrict__ offsets,
+                                                       u64 tot_pixels, uint32_t* __restrict__ cursor,
+                                                       uint32_t* __restrict__ order) {
+    __shared__ uint32_t h[kFillBands], base[kFillBands];
+    for (int b = threadIdx.x; b < kFillBands; b += blockDim.x) h[b] = 0u;
+    __syncthreads();
+    const u64 g = u64(blockIdx.x) * blockDim.x + threadIdx.x;
+    int band = 0;
+    uint32_t rank = 0;
+    if (g < total) {
+        band = kb_face_band(views, nviews, g, vfix, kb_band_shift(offsets, tot_pixels));
+        rank = atomicAdd(&h[band], 1u);
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < kFillBands; b += blockDim.x)
+        if (h[b]) base[b] = atomicAdd(&cursor[b], h[b]);
+    __syncthreads();
+    if (g < total) order[base[band] + rank] = uint32_t(g);
+}
+
 template <bool FILL, bool WIDE>
 __global__ void __launch_bounds__(128) kb_raster(const BatchView* __restrict__ views, int nviews, u64 total,
                                                  const float4* __restrict__ vproj, const int2* __restrict__ vfix,
                                                  uint32_t* __restrict__ counts, const u64* __restrict__ offsets,
-                                                 u64* __restrict__ records, const uint32_t* __restrict__ ok) {
+                                                 u64* __restrict__ records, const uint32_t* __restrict__ ok,
+                                                 const uint32_t* __restrict__ order) {
     if (FILL && !batch_ok(ok)) return;
     const u64 first = u64(blockIdx.x) * blockDim.x;
-    const u64 g = first + threadIdx.x;
+    const u64 i = first + threadIdx.x;
     bool live = false;
     RasterJob J;
-    if (g < total) {
-        const int v = view_of_item(g, first, nviews, [&](int i) { return views[i].face_base; });
+    if (i < total) {
+        const u64 g = order ? u64(order[i]) : i;
+        const int v = order ? find_index(g, nviews, [&](int k) { return views[k].face_base; })
+                            : view_of_item(g, first, nviews, [&](int k) { return views[k].face_base; });
         const BatchView& bv = views[v];
         live = raster_setup(uint32_t(g - bv.face_base), bv.faces, vfix + bv.vert_base, uint32_t(bv.vert_base),
                             int(bv.W), 0, int(bv.H), bv.pix_base, J) &&
@@ -383,6 +446,8 @@ struct dtv_batch {
     DevBuf<uint32_t> ok;
     DevBuf<u64> total;
     DevBuf<float4> grad_rows;
+    DevBuf<uint32_t> fill_order;    // items (view faces) in row-band order for the fill
+    DevBuf<uint32_t> band_scratch;  // band counts and cursors of fill_order
     DevBuf<float4> view_rows;  // [tot_verts][2]: screen-space adjoint rows of each view (at its vert_base)
     DevBuf<float4> dimage_internal;
     DevBuf<float> loss;
@@ -460,6 +525,7 @@ void build_views(dtv_batch* b, int nviews, const dtv_batch_view* views, bool tra
     }
     (void)internal_dimage;
     require(vb < (u64(1) << 32), "a batch holds fewer than 2^32 vertices in total");
+    require(fb < (u64(1) << 32), "a batch holds fewer than 2^32 faces in total");
     b->nviews = nviews;
     b->tot_verts = vb;
     b->tot_faces = fb;
@@ -476,6 +542,8 @@ void ensure_scratch(dtv_batch* b, cudaStream_t s) {
     b->vfix.ensure(b->tot_verts ? b->tot_verts : 1, s);
     b->vgeo.ensure(b->tot_verts ? b->tot_verts : 1, s);
     b->view_rows.ensure(2 * (b->tot_verts ? b->tot_verts : 1), s);
+    b->fill_order.ensure(b->tot_faces ? b->tot_faces : 1, s);
+    b->band_scratch.ensure(2 * dtv::kFillBands, s);
     b->counts.ensure(b->tot_pixels, s, /*zero_new=*/true);
     b->offsets.ensure(b->tot_pixels + 1, s);
     b->scan.ensure(dtv::scan_scratch_elems(b->tot_pixels), s);
@@ -506,12 +574,23 @@ template <bool FILL>
 void launch_kb_raster(dtv_batch* b, const uint32_t* okp, cudaStream_t s) {
     using namespace dtv;
     const unsigned blocks = grid_for(b->tot_faces, 128, 0x7fffffffu);
+    const uint32_t* order = nullptr;
+    if (FILL && b->tot_faces) {
+        const unsigned ob = grid_for(b->tot_faces, 256, 0x7fffffffu);
+        DTV_CK(cudaMemsetAsync(b->band_scratch.ptr, 0, kFillBands * sizeof(uint32_t), s));
+        kb_band_count<<<ob, 256, 0, s>>>(b->d_views.ptr, b->nviews, b->tot_faces, b->vfix.ptr, b->offsets.ptr,
+                                         b->tot_pixels, b->band_scratch.ptr);
+        launch_band_scan(b->band_scratch.ptr, b->band_scratch.ptr + kFillBands, s);
+        kb_band_scatter<<<ob, 256, 0, s>>>(b->d_views.ptr, b->nviews, b->tot_faces, b->vfix.ptr, b->offsets.ptr,
+                                           b->tot_pixels, b->band_scratch.ptr + kFillBands, b->fill_order.ptr);
+        order = b->fill_order.ptr;
+    }
     kb_raster<FILL, false><<<blocks, 128, 0, s>>>(b->d_views.ptr, b->nviews, b->tot_faces, b->vproj.ptr,
                                                   b->vfix.ptr, b->counts.ptr, FILL ? b->offsets.ptr : nullptr,
-                                                  FILL ? b->records.ptr : nullptr, okp);
+                                                  FILL ? b->records.ptr : nullptr, okp, order);
     kb_raster<FILL, true><<<blocks, 128, 0, s>>>(b->d_views.ptr, b->nviews, b->tot_faces, b->vproj.ptr,
                                                  b->vfix.ptr, b->counts.ptr, FILL ? b->offsets.ptr : nullptr,
-                                                 FILL ? b->records.ptr : nullptr, okp);
+                                                 FILL ? b->records.ptr : nullptr, okp, order);
     if (!FILL) {
         dim3 grid(unsigned(b->max_height + 7) / 8, unsigned(b->nviews));
         kb_row_prefix<<<grid, 256, 0, s>>>(b->d_views.ptr, b->counts.ptr);
@@ -610,6 +689,10 @@ int32_t dtv_batch_reserve(dtv_batch* b, uint64_t max_views, uint64_t max_vertice
         b->vfix.ensure(V, s);
         b->vgeo.ensure(V, s);
         b->view_rows.ensure(2 * V, s);
+        // Fill order: a Kuhn-grid tet mesh has about 12 faces per vertex; a
+        // batch with more faces grows it at its first render.
+        b->fill_order.ensure(13 * V, s);
+        b->band_scratch.ensure(2 * dtv::kFillBands, s);
         b->counts.ensure(P, s, /*zero_new=*/true);
         b->offsets.ensure(P + 1, s);
         b->scan.ensure(dtv::scan_scratch_elems(P), s);
@@ -658,6 +741,8 @@ int32_t dtv_batch_destroy(dtv_batch* b) {
     b->total.release();
     b->grad_rows.release();
     b->view_rows.release();
+    b->fill_order.release();
+    b->band_scratch.release();
     b->dimage_internal.release();
     b->loss.release();
     b->step.release();

@@ -45,6 +45,8 @@ constexpr int kFillBands = 512;
 constexpr uint64_t kFillBandBytes = 24ull << 20;
 void launch_fill_order(const uint4* faces, uint32_t F, const int2* vfix, int H, uint64_t nf, uint32_t* order,
                        uint32_t* band_scratch, cudaStream_t s);
+// Exclusive prefix of kFillBands band counts (one warp).
+void launch_band_scan(const uint32_t* hist, uint32_t* cursor, cudaStream_t s);
 // Exclusive scan of counts[n] into offsets[n+1]; scratch must hold scan_scratch_elems(n) u64.
 size_t scan_scratch_elems(uint64_t n);
 void launch_scan(const uint32_t* counts, uint64_t n, unsigned long long* offsets, unsigned long long* scratch,

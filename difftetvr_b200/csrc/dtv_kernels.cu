@@ -162,6 +162,10 @@ __global__ void __launch_bounds__(256) k_band_scatter(const uint4* __restrict__ 
 
 // Largest band of 2^shift rows whose records (nf over H rows on average) stay
 // under kFillBandBytes, with at most kFillBands bands.
+void launch_band_scan(const uint32_t* hist, uint32_t* cursor, cudaStream_t s) {
+    k_band_scan<<<1, 32, 0, s>>>(hist, cursor);
+}
+
 int fill_band_shift(int H, uint64_t nf) {
     const double per_row = double(nf) * sizeof(u64) / double(H > 0 ? H : 1);
     int shift = 0;
@@ -177,7 +181,7 @@ void launch_fill_order(const uint4* faces, uint32_t F, const int2* vfix, int H, 
     const unsigned blocks = (F + 255) / 256;
     cudaMemsetAsync(band_scratch, 0, kFillBands * sizeof(uint32_t), s);
     k_band_count<<<blocks, 256, 0, s>>>(faces, F, vfix, H, shift, band_scratch);
-    k_band_scan<<<1, 32, 0, s>>>(band_scratch, band_scratch + kFillBands);
+    launch_band_scan(band_scratch, band_scratch + kFillBands, s);
     k_band_scatter<<<blocks, 256, 0, s>>>(faces, F, vfix, H, shift, band_scratch + kFillBands, order);
 }
 
