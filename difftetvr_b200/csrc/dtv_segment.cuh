@@ -10,9 +10,9 @@
 //   K     = (t + 1/a) A - 1/a = -t x psi(x),   psi(x) = (phi1(x) - e^-x) / x
 //   dK/da = t^2 chi(x),       chi(x) = (1 - e^-x (1 + x + x^2)) / x^2
 // For x < 0.5 phi1, psi and chi come from their Taylor series (derived from
-// the exponential series; coefficients below; degree 5 below x = 1/8, degree
-// 8-9 above), which avoids the cancellation of the direct form (~1e-3
-// relative error in FP32 at a t ~ 1e-4).
+// the exponential series; coefficients below; below x = 1/8 from the one
+// series of phi2, degree 8-9 series above), which avoids the cancellation of
+// the direct form (~1e-3 relative error in FP32 at a t ~ 1e-4).
 // exp and the divisions use the fast hardware approximations (__expf,
 // __fdividef: a few ulp), well inside the path's 1e-5 image / 1e-4 gradient
 // tolerances; the discrete depth key never goes through this file.
@@ -72,38 +72,23 @@ __device__ __forceinline__ float series_chi(float x) {
     return p;
 }
 
-// The same series to degree 5, for x < 1/8: the first omitted term at x = 1/8
-// is x^6/7! = 7.6e-10 for phi1, 7 x^6/8! = 6.6e-10 for psi and
-// 49 x^6/8! = 4.6e-9 for chi, at most about 1e-8 of the value (under one
-// FP32 ulp).  At the path's densities and segment lengths nearly every
-// sub-segment has x < 1/8.
-__device__ __forceinline__ float series_phi1_short(float x) {
-    float p = -1.38888889e-3f;
-    p = fmaf(p, x, 8.33333333e-3f);
-    p = fmaf(p, x, -4.16666667e-2f);
-    p = fmaf(p, x, 0.166666667f);
-    p = fmaf(p, x, -0.5f);
-    p = fmaf(p, x, 1.0f);
-    return p;
-}
-
-__device__ __forceinline__ float series_psi_short(float x) {
-    float p = -1.19047619e-3f;
-    p = fmaf(p, x, 6.94444444e-3f);
-    p = fmaf(p, x, -3.33333333e-2f);
-    p = fmaf(p, x, 0.125f);
-    p = fmaf(p, x, -0.333333333f);
+// Below x = 1/8 one series serves all three: with
+//   phi2(x) = (e^-x - 1 + x) / x^2 = sum_j (-x)^j / (j+2)!,
+// phi1 = 1 - x phi2, psi = phi1 - phi2 (the series of psi is the difference
+// of those of phi1 and phi2 term by term) and chi = psi - e^-x (likewise).
+// phi2 to degree 5: the first omitted term at x = 1/8 is x^6/8! = 9.5e-11,
+// 2e-10 of the value.  Both differences are exact in FP32 (Sterbenz: phi1/2
+// <= phi2 <= phi1 and A/2 <= psi <= A for 0 <= x <= 1/8), so psi and chi
+// carry only the rounding of their operands (chi: that of __expf too).  At
+// the path's densities and segment lengths nearly every sub-segment has
+// x < 1/8.
+__device__ __forceinline__ float series_phi2_short(float x) {
+    float p = -1.98412698e-4f;
+    p = fmaf(p, x, 1.38888889e-3f);
+    p = fmaf(p, x, -8.33333333e-3f);
+    p = fmaf(p, x, 4.16666667e-2f);
+    p = fmaf(p, x, -0.166666667f);
     p = fmaf(p, x, 0.5f);
-    return p;
-}
-
-__device__ __forceinline__ float series_chi_short(float x) {
-    float p = 7.14285714e-3f;
-    p = fmaf(p, x, -3.47222222e-2f);
-    p = fmaf(p, x, 0.133333333f);
-    p = fmaf(p, x, -0.375f);
-    p = fmaf(p, x, 0.666666667f);
-    p = fmaf(p, x, -0.5f);
     return p;
 }
 
@@ -113,8 +98,10 @@ __device__ __forceinline__ SegTerms seg_terms_short(float t, float a) {
     SegTerms s;
     const float x = a * t;
     s.A = __expf(-x);
-    s.omA = x * series_phi1_short(x);
-    s.K = -t * x * series_psi_short(x);
+    const float phi2 = series_phi2_short(x);
+    const float phi1 = fmaf(-x, phi2, 1.0f);
+    s.omA = x * phi1;
+    s.K = -t * x * (phi1 - phi2);
     s.dK = 0.f;
     return s;
 }
@@ -123,9 +110,12 @@ __device__ __forceinline__ SegTerms seg_terms_adj_short(float t, float a) {
     SegTerms s;
     const float x = a * t;
     s.A = __expf(-x);
-    s.omA = x * series_phi1_short(x);
-    s.K = -t * x * series_psi_short(x);
-    s.dK = t * t * series_chi_short(x);
+    const float phi2 = series_phi2_short(x);
+    const float phi1 = fmaf(-x, phi2, 1.0f);
+    const float psi = phi1 - phi2;
+    s.omA = x * phi1;
+    s.K = -t * x * psi;
+    s.dK = t * t * (psi - s.A);
     return s;
 }
 
