@@ -664,12 +664,39 @@ __device__ __forceinline__ void segment_adjoint(float tSeg, float cfw, float cbw
     };
     // Same tiers as segment_composite: straight-line terms when all four
     // sub-segments are in the short tier (seg_terms_adj's arithmetic there).
+    // There every A > 0.88, so the transmittance in front of the segment is
+    // T / (A0 A1 A2 A3) (one division; the product cannot underflow) and each
+    // sub-segment's entry transmittance follows front to back by products.
+    // The constant factors (1/4 of the length adjoint, the attenuation of the
+    // alpha adjoints) are applied once per segment.
     if (short_tier) {
         SegTerms st[kNumSubdivs];
 #pragma unroll
         for (int s = 0; s < kNumSubdivs; ++s) st[s] = seg_terms_adj_short(tSeg, av[s]);
+        float Tin[kNumSubdivs];
+        Tin[0] = __fdividef(T, (st[0].A * st[1].A) * (st[2].A * st[3].A));
 #pragma unroll
-        for (int s = kNumSubdivs - 1; s >= 0; --s) step(s, st[s], true);
+        for (int s = 1; s < kNumSubdivs; ++s) Tin[s] = Tin[s - 1] * st[s - 1].A;
+        float gl = 0.f, gaf = 0.f, gab = 0.f;
+#pragma unroll
+        for (int s = kNumSubdivs - 1; s >= 0; --s) {
+            const float fs = 0.25f * s, fm = 0.25f * (s + 0.5f);
+            const float P0 = pf + fs * dp;
+            const float Tout = s == kNumSubdivs - 1 ? T : Tin[s + 1];
+            const float gTo = gT;
+            gT = st[s].omA * P0 - st[s].K * D + gTo * st[s].A;
+            gl += (av[s] * Tout) * (P0 + tSeg * D - gTo);
+            const float g_a = Tin[s] * (tSeg * st[s].A * (P0 - gTo) - st[s].dK * D);
+            const float qK = 0.25f * st[s].K, tw = Tin[s] * st[s].omA;
+            wf += (1.f - fs) * tw + Tin[s] * qK;
+            wb += fs * tw - Tin[s] * qK;
+            gaf += (1.f - fm) * g_a;
+            gab += fm * g_a;
+        }
+        T = Tin[0];
+        g_tot += 0.25f * gl;
+        af += gaf * atten;
+        ab += gab * atten;
         return;
     }
 #pragma unroll
