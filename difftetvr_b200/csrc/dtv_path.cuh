@@ -361,27 +361,28 @@ __device__ __forceinline__ void segment_composite(float tSeg, const float4& cf, 
         av[s] = (cf.w + dw * (0.25f * (s + 0.5f))) * atten;
         short_tier &= (av[s] > 0.f) & (av[s] * tSeg < 0.125f);
     }
-    auto accumulate = [&](int s, const SegTerms& st) {
-        const float fs = 0.25f * s;
-        const float w = T * st.omA, k = T * (0.25f * st.K);
-        C0 += w * (cf.x + d0 * fs) - k * d0;
-        C1 += w * (cf.y + d1 * fs) - k * d1;
-        C2 += w * (cf.z + d2 * fs) - k * d2;
-        T *= st.A;
-    };
+    // Sub-segment s adds w (cf + fs d) - k d per channel; summed over the
+    // sub-segments that is cf sum(w) + d sum(w fs - k), two scalars.
+    float ws = 0.f, ds = 0.f;
+    SegTerms st[kNumSubdivs];
     if (short_tier) {
-        SegTerms st[kNumSubdivs];
 #pragma unroll
         for (int s = 0; s < kNumSubdivs; ++s) st[s] = seg_terms_short(tSeg, av[s]);
+    } else {
+        // a <= 0 contributes nothing: A = 1, 1 - A = K = 0.
 #pragma unroll
-        for (int s = 0; s < kNumSubdivs; ++s) accumulate(s, st[s]);
-        return;
+        for (int s = 0; s < kNumSubdivs; ++s) st[s] = av[s] > 0.f ? seg_terms(tSeg, av[s]) : SegTerms{1.f, 0.f, 0.f, 0.f};
     }
 #pragma unroll
     for (int s = 0; s < kNumSubdivs; ++s) {
-        if (!(av[s] > 0.f)) continue;  // a <= 0 contributes nothing
-        accumulate(s, seg_terms(tSeg, av[s]));
+        const float w = T * st[s].omA, k = T * (0.25f * st[s].K);
+        ws += w;
+        ds += w * (0.25f * s) - k;
+        T *= st[s].A;
     }
+    C0 += cf.x * ws + d0 * ds;
+    C1 += cf.y * ws + d1 * ds;
+    C2 += cf.z * ws + d2 * ds;
 }
 
 // ---------------------------------------------------------------------------
