@@ -84,6 +84,30 @@ __device__ __forceinline__ uint32_t tet_face_at(const TetTopo& tt, const int2* _
     }
     constexpr int A[4] = {0, 1, 0, 2}, B[4] = {1, 0, 2, 1}, C[4] = {2, 3, 3, 3};
     uint32_t found = kNoTet;
+    // All four vertices within 2^14 units of the centre (nearly every step):
+    // every face's area and edge functions are exact in 32 bits, which is the
+    // per-face test below decided for the whole tet at once.
+    long long mm = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) mm = max(mm, max(llabs(rx[k]), llabs(ry[k])));
+    if (mm < (1LL << 14)) {
+        int ix[4], iy[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            ix[k] = int(rx[k]);
+            iy[k] = int(ry[k]);
+        }
+#pragma unroll
+        for (int j = 3; j >= 0; --j) {
+            const int a = A[j], b = B[j], c = C[j];
+            const int area2 = (ix[b] - ix[a]) * (iy[c] - iy[a]) - (iy[b] - iy[a]) * (ix[c] - ix[a]);
+            const bool in = covers_rel<int>(ix[a], iy[a], ix[b], iy[b], ix[c], iy[c], area2 < 0);
+            const bool front = (area2 < 0) != (((flip >> j) & 1u) != 0u);
+            const bool match = fs[j] != skip && area2 != 0 && in && front == want_front;
+            found = match ? fs[j] : found;
+        }
+        return found;
+    }
 #pragma unroll
     for (int j = 3; j >= 0; --j) {
         const int a = A[j], b = B[j], c = C[j];
