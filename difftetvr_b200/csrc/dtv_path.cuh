@@ -678,7 +678,9 @@ __device__ __forceinline__ void segment_adjoint(float tSeg, float cfw, float cbw
         Tin[0] = __fdividef(T, (st[0].A * st[1].A) * (st[2].A * st[3].A));
 #pragma unroll
         for (int s = 1; s < kNumSubdivs; ++s) Tin[s] = Tin[s - 1] * st[s - 1].A;
-        float gl = 0.f, gaf = 0.f, gab = 0.f;
+        // Colour weights: front += sum((1 - fs) tw + Tin K / 4), back +=
+        // sum(fs tw - Tin K / 4), from three sums.
+        float gl = 0.f, gaf = 0.f, gab = 0.f, stw = 0.f, sftw = 0.f, sk = 0.f;
 #pragma unroll
         for (int s = kNumSubdivs - 1; s >= 0; --s) {
             const float fs = 0.25f * s, fm = 0.25f * (s + 0.5f);
@@ -688,14 +690,17 @@ __device__ __forceinline__ void segment_adjoint(float tSeg, float cfw, float cbw
             gT = st[s].omA * P0 - st[s].K * D + gTo * st[s].A;
             gl += (av[s] * Tout) * (P0 + tSeg * D - gTo);
             const float g_a = Tin[s] * (tSeg * st[s].A * (P0 - gTo) - st[s].dK * D);
-            const float qK = 0.25f * st[s].K, tw = Tin[s] * st[s].omA;
-            wf += (1.f - fs) * tw + Tin[s] * qK;
-            wb += fs * tw - Tin[s] * qK;
+            const float tw = Tin[s] * st[s].omA;
+            stw += tw;
+            sftw += fs * tw;
+            sk += Tin[s] * st[s].K;
             gaf += (1.f - fm) * g_a;
             gab += fm * g_a;
         }
         T = Tin[0];
         g_tot += 0.25f * gl;
+        wf += (stw - sftw) + 0.25f * sk;
+        wb += sftw - 0.25f * sk;
         af += gaf * atten;
         ab += gab * atten;
         return;
@@ -785,9 +790,10 @@ __device__ __forceinline__ float3 screen_to_world(const float4& a, const VGeo& P
 // the pixel's colour adjoint gC.  A fragment's gradients are taken one step
 // after it is loaded (its back segment and its front segment must both be
 // done), so carrying this state spares the second gather of its three
-// vertices and the second FP64 solve.  Its depth, alpha and colour are those
-// of load_frag_face (same expressions), so the adjoint walks the forward's
-// values.
+// vertices and the second FP64 solve.  Its depth and alpha are those of
+// load_frag_face (same expressions), so the adjoint walks the forward's
+// transmittances; gC . colour is the barycentric sum of the reduced vertex
+// colours.
 struct FragG {
     uint32_t v[3];
     uint32_t bits;
@@ -810,13 +816,8 @@ __device__ __forceinline__ FragG load_frag_g(uint32_t lo, const uint4& fc, float
     face_interp(a, b, c, qx, qy, fi);
     const float4 c0 = colors[fc.x], c1 = colors[fc.y], c2 = colors[fc.z];
     const float* bary = fi.bary;
-    const float4 col = make_float4(bary[0] * c0.x + bary[1] * c1.x + bary[2] * c2.x,
-                                   bary[0] * c0.y + bary[1] * c1.y + bary[2] * c2.y,
-                                   bary[0] * c0.z + bary[1] * c1.z + bary[2] * c2.z,
-                                   bary[0] * c0.w + bary[1] * c1.w + bary[2] * c2.w);
     f.z = fi.z;
-    f.alpha = col.w;
-    f.pcol = gC0 * col.x + gC1 * col.y + gC2 * col.z;
+    f.alpha = bary[0] * c0.w + bary[1] * c1.w + bary[2] * c2.w;
     f.iz[0] = a.iz;
     f.iz[1] = b.iz;
     f.iz[2] = c.iz;
@@ -832,6 +833,7 @@ __device__ __forceinline__ FragG load_frag_g(uint32_t lo, const uint4& fc, float
     f.pc[0] = gC0 * c0.x + gC1 * c0.y + gC2 * c0.z;
     f.pc[1] = gC0 * c1.x + gC1 * c1.y + gC2 * c1.z;
     f.pc[2] = gC0 * c2.x + gC1 * c2.y + gC2 * c2.z;
+    f.pcol = bary[0] * f.pc[0] + bary[1] * f.pc[1] + bary[2] * f.pc[2];
     f.cw[0] = c0.w;
     f.cw[1] = c1.w;
     f.cw[2] = c2.w;
