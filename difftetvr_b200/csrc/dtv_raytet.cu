@@ -66,11 +66,23 @@ struct TetTopo {
 // face->tet loads); coverage is the rasteriser's rule (covers_rel normalises
 // the winding, and the normalised triangle's directed edges do not depend on
 // the starting vertex).
-__device__ __forceinline__ uint32_t tet_face_at(const TetTopo& tt, const int2* __restrict__ vfix, uint32_t t,
-                                                uint32_t skip, bool want_front, int px, int py) {
-    const uint4 tf = tt.tet_faces[t];
-    const uint4 cv = tt.cells[t];
-    const uint32_t flip = tt.flip[t];
+// A tet's row of the walk tables (loaded ahead of its face search by the
+// walks, so that the loads overlap the previous segment's work).
+struct TetRow {
+    uint4 tf;       // face ids
+    uint4 cv;       // vertex ids
+    uint32_t flip;  // face-side bits
+};
+
+__device__ __forceinline__ TetRow load_tet(const TetTopo& tt, uint32_t t) {
+    return TetRow{tt.tet_faces[t], tt.cells[t], uint32_t(tt.flip[t])};
+}
+
+__device__ __forceinline__ uint32_t tet_face_of(const TetRow& tr, const int2* __restrict__ vfix, uint32_t skip,
+                                                bool want_front, int px, int py) {
+    const uint4 tf = tr.tf;
+    const uint4 cv = tr.cv;
+    const uint32_t flip = tr.flip;
     const uint32_t fs[4] = {tf.x, tf.y, tf.z, tf.w};
     const int2 q[4] = {vfix[cv.x], vfix[cv.y], vfix[cv.z], vfix[cv.w]};
     const long long Xc = 256LL * px + 128, Yc = 256LL * py + 128;
@@ -126,6 +138,11 @@ __device__ __forceinline__ uint32_t tet_face_at(const TetTopo& tt, const int2* _
     return found;
 }
 
+__device__ __forceinline__ uint32_t tet_face_at(const TetTopo& tt, const int2* __restrict__ vfix, uint32_t t,
+                                                uint32_t skip, bool want_front, int px, int py) {
+    return tet_face_of(load_tet(tt, t), vfix, skip, want_front, px, py);
+}
+
 __device__ __forceinline__ uint32_t other_tet(const uint32_t* __restrict__ f2t, uint32_t f, uint32_t t) {
     const uint32_t a = f2t[2 * size_t(f)], b = f2t[2 * size_t(f) + 1];
     return a == t ? b : a;
@@ -159,25 +176,32 @@ __global__ void __launch_bounds__(kTile * kTile, 2) k_walk_composite(
         uint32_t fe = bf_global[bits >> 2];
         uint32_t t = f2t[2 * size_t(fe)];
         FragV f0 = load_frag(u64(fe) << 2, qx, qy, faces, vgeo, colors);
+        TetRow tr = load_tet(tt, t);
         for (uint32_t step = 0; step <= num_tets; ++step) {
-            const uint32_t fx = tet_face_at(tt, vfix, t, fe, false, px, py);
+            const uint32_t fx = tet_face_of(tr, vfix, fe, false, px, py);
             if (fx == kNoTet) break;
             if (sh.use_ert && T < sh.ert_thresh) {
                 stop = true;
                 break;
             }
-            const FragV f1 = load_frag(u64(fx) << 2, qx, qy, faces, vgeo, colors);
+            // The next tet and its table row are fetched before this segment
+            // is composited, so their loads overlap the exit face's vertex loads.
+            const uint4 fcx = faces[fx];
+            const uint32_t tn = other_tet(f2t, fx, t);
+            const bool more = !(fcx.w & 1u) && tn != kNoTet;  // not leaving the mesh
+            TetRow tr_next{};
+            if (more) tr_next = load_tet(tt, tn);
+            const FragV f1 = load_frag_face(fx << 2, fcx, qx, qy, vgeo, colors);
             segment_composite((f1.z - f0.z) * scale * 0.25f, f0.col, f1.col, sh.atten, C0, C1, C2, T);
             last_tet = t;
             last_entry = fe;
             last_b = b;
             ++nseg;
-            if (faces[fx].w & 1u) break;  // left the mesh
-            const uint32_t tn = other_tet(f2t, fx, t);
-            if (tn == kNoTet) break;
+            if (!more) break;
             t = tn;
             fe = fx;
             f0 = f1;
+            tr = tr_next;
         }
     }
     image[p] = make_float4(C0 + T * sh.clear[0], C1 + T * sh.clear[1], C2 + T * sh.clear[2],
@@ -202,14 +226,21 @@ __device__ __forceinline__ void walk_adjoint_carried(
     FragG fX = load_frag_g(fx << 2, faces[fx], qx, qy, vgeo, colors, gC0, gC1, gC2);
     float gz_x = 0.f, wx = 0.f, ax = 0.f;
     for (uint32_t step = 0; step <= num_tets; ++step) {
-        const FragG fE = load_frag_g(fe << 2, faces[fe], qx, qy, vgeo, colors, gC0, gC1, gC2);
+        // The tet behind the entry face and its table row are fetched first, so
+        // their loads overlap the entry face's vertex loads and this step's math.
+        const uint4 fce = faces[fe];
+        const uint32_t tprev = other_tet(f2t, fe, t);
+        const bool inner = !(fce.w & 1u) && tprev != kNoTet;
+        TetRow trp{};
+        if (inner) trp = load_tet(tt, tprev);
+        const FragG fE = load_frag_g(fe << 2, fce, qx, qy, vgeo, colors, gC0, gC1, gC2);
         const float tSeg = (fX.z - fE.z) * scale * 0.25f;
         float g_tot = 0.f, we = 0.f, ae = 0.f;
         segment_adjoint(tSeg, fE.alpha, fX.alpha, fE.pcol, fX.pcol, atten, T, gT, g_tot, we, wx, ae, ax);
         const float gz_e = -g_tot * scale;
         gz_x += g_tot * scale;
         frag_grads_carried(fX, gz_x, wx, ax, acc);
-        if (faces[fe].w & 1u) {
+        if (fce.w & 1u) {
             frag_grads_carried(fE, gz_e, we, ae, acc);
             // Previous interval: its exit is the last back-facing boundary fragment before b.
             int bb = b - 1;
@@ -228,9 +259,8 @@ __device__ __forceinline__ void walk_adjoint_carried(
             ax = 0.f;
             continue;
         }
-        const uint32_t tprev = other_tet(f2t, fe, t);
-        if (tprev == kNoTet) break;
-        const uint32_t feprev = tet_face_at(tt, vfix, tprev, fe, true, px, py);
+        if (!inner) break;
+        const uint32_t feprev = tet_face_of(trp, vfix, fe, true, px, py);
         if (feprev == kNoTet) break;
         fX = fE;
         gz_x = gz_e;
