@@ -30,11 +30,11 @@ sys.path.insert(0, ROOT)
 
 METRIC = "fwd+adj iter/s at 1.57M tets 1024²"
 # Kernels of this library per timed step of the plain method: project 1,
-# count 2 (32- and 64-bit faces) + row prefix 1, scan 3, fill 2, sort 8
-# (classify, five register / distribution classes, shared-memory and block
-# classes), composite 1; adjoint 1 + scatter 1; l2 loss 1; Adam 2 (colours,
-# positions).
-LIST_STEP_LAUNCHES = 1 + 3 + 3 + 2 + 8 + 1 + 2 + 1 + 2
+# count 2 (32- and 64-bit faces) + row prefix 1, scan 3, fill order 3 (band
+# count, scan, scatter) + fill 2, sort 8 (classify, five register /
+# distribution classes, shared-memory and block classes), composite 1;
+# adjoint 1 + scatter 1; l2 loss 1; Adam 2 (colours, positions).
+LIST_STEP_LAUNCHES = 1 + 3 + 3 + 3 + 2 + 8 + 1 + 2 + 1 + 2
 LR_COL, LR_POS = 1e-2, 1e-4
 
 
