@@ -27,9 +27,12 @@ thread_local std::string g_last_error;
 dtv::CamDev make_cam(const dtv_camera& c) {
     dtv::CamDev k;
     std::memcpy(k.V, c.view, sizeof(k.V));
+    // Host set-up: the focal constant in double, split into an FP32 pair for
+    // the device (the discrete path uses f alone).
     const double tanh = std::tan(0.5 * double(c.fovy));
-    k.fd = 0.5 * double(c.height) / tanh;
-    k.f = float(k.fd);
+    const double fd = 0.5 * double(c.height) / tanh;
+    k.f = float(fd);
+    k.f_lo = float(fd - double(k.f));
     k.cx = 0.5f * float(c.width);
     k.cy = 0.5f * float(c.height);
     k.znear = c.znear;
@@ -80,7 +83,6 @@ struct dtv_renderer {
     DevBuf<float> tfinal;
     DevBuf<uint32_t> term;
     DevBuf<uint32_t> long_list;     // sort scratch (length classes)
-    DevBuf<uint32_t> flags;
     DevBuf<float4> grad_rows;     // [V][2] interleaved vertex gradient accumulator
     // Row bands [row0, row1) of the last render when its lists exceeded the
     // fragment budget (each band's lists are rebuilt by the adjoint); empty
@@ -94,9 +96,6 @@ struct dtv_renderer {
     DevBuf<uint32_t> band_scratch;  // band counts and cursors of fill_order
     DevBuf<uint4> wstate;         // ray-tet path: (last tet, its entry face, boundary entry index, segments)
     u64* h_nf = nullptr;          // pinned
-    uint32_t* h_flags = nullptr;  // pinned
-    bool flags_pending = false;
-    cudaEvent_t flags_event = nullptr;
     // State of the last render.
     bool have_render = false;
     const dtv_mesh* mesh = nullptr;
@@ -111,16 +110,6 @@ struct dtv_renderer {
 };
 
 namespace {
-
-void check_pending_flags(dtv_renderer* r) {
-    if (!r->flags_pending) return;
-    DTV_CK(cudaEventSynchronize(r->flags_event));
-    r->flags_pending = false;
-    if (r->h_flags[1] != 0u)
-        throw DtvError(DTV_ERR_BUDGET, "a per-pixel fragment list exceeded " +
-                                           std::to_string(dtv::kSortBlockCap) +
-                                           " entries in the previous render; its order is undefined");
-}
 
 void rec_event(dtv_renderer* r, int idx, cudaStream_t s) {
     if (r->timing) DTV_CK(cudaEventRecord(r->ev[idx], s));
@@ -169,15 +158,9 @@ void build_band_lists(dtv_renderer* r, const dtv_mesh* mesh, int W, int H, int y
     dtv::launch_raster_fill(mesh->d_faces, uint32_t(mesh->host.num_faces), r->vproj.ptr, r->vfix.ptr, W, H,
                             r->counts.ptr, r->offsets.ptr, r->records.ptr, s, y0, y1, r->fill_order.ptr);
     check_launch("band fill");
-    dtv::launch_sort(r->offsets.ptr + p0, r->records.ptr, uint32_t(pb), r->long_list.ptr, r->flags.ptr, s, nullptr,
+    dtv::launch_sort(r->offsets.ptr + p0, r->records.ptr, uint32_t(pb), r->long_list.ptr, s, nullptr,
                      r->tuning.sort_surrogate_classes, r->tuning.sort_bucket_classes);
     check_launch("band sort");
-}
-
-void record_flags(dtv_renderer* r, cudaStream_t s) {
-    DTV_CK(cudaMemcpyAsync(r->h_flags, r->flags.ptr, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-    DTV_CK(cudaEventRecord(r->flags_event, s));
-    r->flags_pending = true;
 }
 
 // Composite of rows [y0, y1) with the stored lists: per-vertex colours
@@ -240,13 +223,11 @@ void render_banded(dtv_renderer* r, const dtv_mesh* mesh, const float* d_colors,
         throw;
     }
     rec_event(r, 3, s);
-    DTV_CK(cudaMemsetAsync(r->flags.ptr, 0, 2 * sizeof(uint32_t), s));
     for (const auto& b : r->bands) {
         build_band_lists(r, mesh, W, H, b.first, b.second, s);
         composite_rows(r, mesh, d_colors, cam, sh, d_image, b.first, b.second, s);
         check_launch("band composite");
     }
-    record_flags(r, s);
     rec_event(r, 4, s);
     rec_event(r, 5, s);
     rec_event(r, 6, s);
@@ -259,7 +240,6 @@ void adjoint_banded(dtv_renderer* r, const dtv_mesh* mesh, const float* d_colors
                     const dtv::ShadeDev& sh, float* d_grad_positions, float* d_grad_colors, cudaStream_t s) {
     const int W = r->cam.W, H = r->cam.H;
     DTV_CK(cudaMemsetAsync(r->grad_rows.ptr, 0, sizeof(float4) * 2 * size_t(r->V ? r->V : 1), s));
-    DTV_CK(cudaMemsetAsync(r->flags.ptr, 0, 2 * sizeof(uint32_t), s));
     for (const auto& b : r->bands) {
         dtv::launch_raster_count(mesh->d_faces, uint32_t(mesh->host.num_faces), r->vproj.ptr, r->vfix.ptr, W, H,
                                  r->counts.ptr, s, b.first, b.second);
@@ -270,7 +250,6 @@ void adjoint_banded(dtv_renderer* r, const dtv_mesh* mesh, const float* d_colors
     }
     scatter_rows(r, sh, d_grad_positions, d_grad_colors, s);
     check_launch("scatter gradients");
-    record_flags(r, s);
 }
 
 }  // namespace
@@ -416,8 +395,6 @@ int32_t dtv_renderer_create(int32_t type, dtv_renderer** out) {
         r->type = type;
         try {
             DTV_CK(cudaMallocHost(&r->h_nf, sizeof(u64)));
-            DTV_CK(cudaMallocHost(&r->h_flags, 2 * sizeof(uint32_t)));
-            DTV_CK(cudaEventCreateWithFlags(&r->flags_event, cudaEventDisableTiming));
             for (auto& e : r->ev) DTV_CK(cudaEventCreate(&e));
         } catch (...) {
             dtv_renderer_destroy(r);
@@ -440,15 +417,12 @@ int32_t dtv_renderer_destroy(dtv_renderer* r) {
     r->tfinal.release();
     r->term.release();
     r->long_list.release();
-    r->flags.release();
     r->grad_rows.release();
     r->wstate.release();
     r->fill_order.release();
     r->band_scratch.release();
     if (r->h_nf) cudaFreeHost(r->h_nf);
-    if (r->h_flags) cudaFreeHost(r->h_flags);
     if (r->h_rowoff) cudaFreeHost(r->h_rowoff);
-    if (r->flags_event) cudaEventDestroy(r->flags_event);
     for (auto& e : r->ev)
         if (e) cudaEventDestroy(e);
     delete r;
@@ -476,7 +450,6 @@ int32_t render_common(dtv_renderer* r, const dtv_mesh* mesh, const float* d_posi
         require(camera->znear > 0.f && camera->zfar > camera->znear, "need 0 < znear < zfar");
         require(camera->fovy > 0.f && camera->fovy < 3.14159f, "fovy must be in (0, pi)");
         cudaStream_t s = static_cast<cudaStream_t>(stream);
-        check_pending_flags(r);
         r->have_render = false;
         r->cells = cells;
         const bool raytet = r->type == DTV_RENDERER_INTERSECTION;
@@ -501,7 +474,6 @@ int32_t render_common(dtv_renderer* r, const dtv_mesh* mesh, const float* d_posi
         else
             r->term.ensure(P, s);
         r->long_list.ensure(dtv::sort_scratch_elems(P), s);
-        r->flags.ensure(2, s);
 
         rec_event(r, 0, s);
         dtv::launch_project(d_positions, uint32_t(V), cam, r->vproj.ptr, r->vfix.ptr, r->vgeo.ptr, s);
@@ -555,13 +527,9 @@ int32_t render_common(dtv_renderer* r, const dtv_mesh* mesh, const float* d_posi
                                 r->offsets.ptr, r->records.ptr, s, 0, -1, r->fill_order.ptr);
         check_launch("raster fill");
         rec_event(r, 4, s);
-        DTV_CK(cudaMemsetAsync(r->flags.ptr, 0, 2 * sizeof(uint32_t), s));
-        dtv::launch_sort(r->offsets.ptr, r->records.ptr, uint32_t(P), r->long_list.ptr, r->flags.ptr, s, nullptr,
+        dtv::launch_sort(r->offsets.ptr, r->records.ptr, uint32_t(P), r->long_list.ptr, s, nullptr,
                          r->tuning.sort_surrogate_classes, r->tuning.sort_bucket_classes);
         check_launch("sort");
-        DTV_CK(cudaMemcpyAsync(r->h_flags, r->flags.ptr, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-        DTV_CK(cudaEventRecord(r->flags_event, s));
-        r->flags_pending = true;
         rec_event(r, 5, s);
         if (raytet) {
             dtv::launch_walk_composite(r->offsets.ptr, r->records.ptr, mesh->d_bf_global, mesh->d_faces,
@@ -603,7 +571,6 @@ int32_t adjoint_common(dtv_renderer* r, const dtv_mesh* mesh, const float* d_pos
             throw DtvError(DTV_ERR_STATE, cells ? "dtv_renderer_render_adjoint_cells after a per-vertex render"
                                                 : "dtv_renderer_render_adjoint after a per-cell render");
         cudaStream_t s = static_cast<cudaStream_t>(stream);
-        check_pending_flags(r);
         dtv::ShadeDev sh = r->sh;
         sh.use_abs_grad = use_abs_grad ? 1 : 0;
         r->grad_rows.ensure(2 * (r->V ? r->V : 1), s);

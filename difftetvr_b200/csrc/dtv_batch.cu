@@ -98,7 +98,7 @@ __global__ void __launch_bounds__(256) kb_project(const BatchView* __restrict__ 
         int2 fx;
         vproj[g] = project_vertex(bv.cam, x, y, z, fx);
         vfix[g] = fx;
-        vgeo[g] = project_vertex_geo(bv.cam, x, y, z);
+        vgeo[g] = project_vertex_geo(bv.cam, x, y, z, fx);
     }
 }
 
@@ -442,7 +442,6 @@ struct dtv_batch {
     DevBuf<float> tfinal;
     DevBuf<uint32_t> term;
     DevBuf<uint32_t> long_list;
-    DevBuf<uint32_t> sort_flags;
     DevBuf<uint32_t> ok;
     DevBuf<u64> total;
     DevBuf<float4> grad_rows;
@@ -550,7 +549,6 @@ void ensure_scratch(dtv_batch* b, cudaStream_t s) {
     b->tfinal.ensure(b->tot_pixels, s);
     b->term.ensure(b->tot_pixels, s);
     b->long_list.ensure(dtv::sort_scratch_elems(b->tot_pixels), s);
-    b->sort_flags.ensure(2, s);
     b->ok.ensure(1, s);
     b->total.ensure(1, s);
     b->loss.ensure(1, s);
@@ -630,8 +628,7 @@ void enqueue_forward(dtv_batch* b, const dtv::ShadeDev& sh, bool guarded, cudaSt
         kb_clear_counts<<<grid_for(b->tot_pixels, 256, 148 * 16), 256, 0, s>>>(b->counts.ptr, b->tot_pixels, okp);
     }
     launch_kb_raster<true>(b, okp, s);
-    DTV_CK(cudaMemsetAsync(b->sort_flags.ptr, 0, 2 * sizeof(uint32_t), s));
-    launch_sort(b->offsets.ptr, b->records.ptr, uint32_t(b->tot_pixels), b->long_list.ptr, b->sort_flags.ptr, s, okp,
+    launch_sort(b->offsets.ptr, b->records.ptr, uint32_t(b->tot_pixels), b->long_list.ptr, s, okp,
                 b->sort_surrogate_classes, b->sort_bucket_classes);
     kb_composite<<<unsigned(b->tot_tiles), kTile * kTile, 0, s>>>(b->d_views.ptr, b->nviews, b->offsets.ptr,
                                                                   b->records.ptr, b->vgeo.ptr, sh, b->tfinal.ptr,
@@ -701,7 +698,6 @@ int32_t dtv_batch_reserve(dtv_batch* b, uint64_t max_views, uint64_t max_vertice
         b->long_list.ensure(dtv::sort_scratch_elems(P), s);
         b->records.ensure(max_fragments ? max_fragments : 1, s);
         b->grad_rows.ensure(2 * (max_grad_vertices ? max_grad_vertices : 1), s);
-        b->sort_flags.ensure(2, s);
         b->ok.ensure(1, s);
         b->total.ensure(1, s);
         b->loss.ensure(1, s);
@@ -736,7 +732,6 @@ int32_t dtv_batch_destroy(dtv_batch* b) {
     b->tfinal.release();
     b->term.release();
     b->long_list.release();
-    b->sort_flags.release();
     b->ok.release();
     b->total.release();
     b->grad_rows.release();
@@ -833,9 +828,7 @@ int32_t dtv_batch_render(dtv_batch* b, int32_t num_views, const dtv_batch_view* 
             throw;
         }
         launch_kb_raster<true>(b, nullptr, s);
-        DTV_CK(cudaMemsetAsync(b->sort_flags.ptr, 0, 2 * sizeof(uint32_t), s));
-        launch_sort(b->offsets.ptr, b->records.ptr, uint32_t(b->tot_pixels), b->long_list.ptr, b->sort_flags.ptr, s,
-                    nullptr, b->sort_surrogate_classes, b->sort_bucket_classes);
+        launch_sort(b->offsets.ptr, b->records.ptr, uint32_t(b->tot_pixels), b->long_list.ptr, s, nullptr, b->sort_surrogate_classes, b->sort_bucket_classes);
         kb_composite<<<unsigned(b->tot_tiles), kTile * kTile, 0, s>>>(b->d_views.ptr, b->nviews, b->offsets.ptr,
                                                                       b->records.ptr, b->vgeo.ptr, b->sh,
                                                                       b->tfinal.ptr, b->term.ptr, nullptr);

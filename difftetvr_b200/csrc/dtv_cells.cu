@@ -46,30 +46,28 @@ __global__ void __launch_bounds__(kTile * kTile) k_composite_cells(
     const u64 beg = offsets[p];
     const uint32_t n = uint32_t(offsets[p + 1] - beg);
     const float qx = float(px) + 0.5f, qy = float(py) + 0.5f;
-    float C0 = 0.f, C1 = 0.f, C2 = 0.f, T = 1.f, zprev = 0.f;
+    float C0 = 0.f, C1 = 0.f, C2 = 0.f, zprev = 0.f;
+    TransF T{1.f, 0.f};  // float-float transmittance (dtv_segment.cuh)
     uint2 prev = make_uint2(kInvalidCell, kInvalidCell);
     uint32_t i = 0;
     for (; i < n; ++i) {
-        if (sh.use_ert && T < sh.ert_thresh) break;
+        if (sh.use_ert && T.hi < sh.ert_thresh) break;
         const uint32_t face = uint32_t(records[beg + i]) >> 2;
         const float z = face_depth(faces[face], vgeo, qx, qy);
         const uint2 cur = f2t[face];
         const uint32_t open = tet_union(cur, prev);
         if (open != kInvalidCell) {
             const float4 c = cell_colors[open];
-            const float A = __expf(-(c.w * sh.atten) * (z - zprev));
-            const float w = T * (1.f - A);
+            const float w = T.hi * one_minus_exp((c.w * sh.atten) * (z - zprev));
             C0 += w * c.x;
             C1 += w * c.y;
             C2 += w * c.z;
-            T *= A;
+            trans_add(T, -w);
         }
         prev = cur;
         zprev = z;
     }
-    image[p] = make_float4(C0 + T * sh.clear[0], C1 + T * sh.clear[1], C2 + T * sh.clear[2],
-                           (1.f - T) + T * sh.clear[3]);
-    tfinal[p] = T;
+    write_pixel(image, tfinal, p, C0, C1, C2, T, sh);
     term[p] = i;
 }
 
@@ -91,8 +89,9 @@ __global__ void __launch_bounds__(kTile * kTile) k_adjoint_cells(
     const float qx = float(px) + 0.5f, qy = float(py) + 0.5f;
     const bool use_abs = sh.use_abs_grad != 0;
     const float atten = sh.atten;
-    float gT = g.x * sh.clear[0] + g.y * sh.clear[1] + g.z * sh.clear[2] + g.w * (sh.clear[3] - 1.f);
-    float T = tfinal[p];
+    // Float-float transmittance and its adjoint (dtv_segment.cuh).
+    TransF gT{g.x * sh.clear[0] + g.y * sh.clear[1] + g.z * sh.clear[2] + g.w * (sh.clear[3] - 1.f), 0.f};
+    TransF T{tfinal[p], 0.f};
     uint32_t fbi = uint32_t(records[beg + last]) >> 2;
     uint4 fb = faces[fbi];
     uint2 pb = f2t[fbi];
@@ -107,13 +106,13 @@ __global__ void __launch_bounds__(kTile * kTile) k_adjoint_cells(
         if (open != kInvalidCell) {
             const float4 c = cell_colors[open];
             const float a = c.w * atten, t = zb - zf;
-            const float A = __expf(-a * t);
-            const float Tin = __fdividef(T, A);
-            const float oma = 1.f - A;
+            const float x = a * t;
+            const float oma = one_minus_exp(x), A = fabsf(x) < 0.125f ? 1.f - oma : __expf(-x);
+            trans_add(T, T.hi * expm1_signed(x));  // T_in = T_out / A
+            const float Tin = T.hi;
             const float gx = Tin * g.x, gy = Tin * g.y, gzc = Tin * g.z;
-            const float gA = Tin * gT - (gx * c.x + gy * c.y + gzc * c.z);
-            gT = oma * (g.x * c.x + g.y * c.y + g.z * c.z) + gT * A;
-            T = Tin;
+            const float gA = Tin * gT.hi - (gx * c.x + gy * c.y + gzc * c.z);
+            trans_add(gT, oma * ((g.x * c.x + g.y * c.y + g.z * c.z) - gT.hi));  // gT A + (1 - A) gC . c
             const float g_t = gA * (-a * A), g_a = gA * (-t * A);
             float4 gc = make_float4(gx * oma, gy * oma, gzc * oma, g_a * atten);
             if (use_abs) gc = make_float4(fabsf(gc.x), fabsf(gc.y), fabsf(gc.z), fabsf(gc.w));

@@ -3,7 +3,9 @@
 // point, the edge-function coverage rule, the FP32 depth key) use explicitly
 // rounded FP32 intrinsics so they are bit-reproducible; the continuous parts
 // (barycentrics, colours, segment integrals, adjoints) use ordinary FP32 with
-// the fast reciprocal (__fdividef) where a quotient feeds only them.
+// the fast reciprocal (__fdividef) where a quotient feeds only them, on
+// screen positions kept as snapped fixed point plus an FP32 residual.  No
+// FP64 arithmetic runs on the device.
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -32,22 +34,82 @@ __device__ __forceinline__ float4 project_vertex(const CamDev& c, float x, float
     return make_float4(sx, sy, iz, ze);
 }
 
-// FP64 projection of the same vertex (continuous path).
-__device__ __forceinline__ VGeo project_vertex_geo(const CamDev& c, float x, float y, float z) {
+// Float-float arithmetic (an unevaluated sum hi + lo of two FP32 values) for
+// the continuous path's projection: error-free sum and product (Knuth's
+// TwoSum, the FMA product error), so a screen position is carried to about
+// 2^-44 relative without FP64.
+struct F2 {
+    float hi, lo;
+};
+
+__device__ __forceinline__ F2 two_sum(float a, float b) {
+    const float s = __fadd_rn(a, b);
+    const float bb = __fsub_rn(s, a);
+    return F2{s, __fadd_rn(__fsub_rn(a, __fsub_rn(s, bb)), __fsub_rn(b, bb))};
+}
+
+__device__ __forceinline__ F2 fast_two_sum(float a, float b) {  // |a| >= |b|
+    const float s = __fadd_rn(a, b);
+    return F2{s, __fsub_rn(b, __fsub_rn(s, a))};
+}
+
+__device__ __forceinline__ F2 two_prod(float a, float b) {
+    const float p = __fmul_rn(a, b);
+    return F2{p, __fmaf_rn(a, b, -p)};
+}
+
+// m0 x + m1 y + m2 z + m3 (one row of the view matrix applied to a point).
+__device__ __forceinline__ F2 row_dot_ff(float m0, float m1, float m2, float m3, float x, float y, float z) {
+    const F2 p0 = two_prod(m0, x), p1 = two_prod(m1, y), p2 = two_prod(m2, z);
+    F2 s = two_sum(p0.hi, p1.hi);
+    float lo = __fadd_rn(__fadd_rn(p0.lo, p1.lo), s.lo);
+    s = two_sum(s.hi, p2.hi);
+    lo = __fadd_rn(lo, __fadd_rn(p2.lo, s.lo));
+    s = two_sum(s.hi, m3);
+    lo = __fadd_rn(lo, s.lo);
+    return fast_two_sum(s.hi, lo);
+}
+
+// a / b: the remainder a.hi - q b.hi of the correctly rounded quotient is
+// exact in FP32 (one FMA), the rest of the remainder is added before the
+// correction term is divided out.
+__device__ __forceinline__ F2 div_ff(const F2& a, const F2& b) {
+    const float q = __fdiv_rn(a.hi, b.hi);
+    float r = __fmaf_rn(-q, b.hi, a.hi);
+    r = __fadd_rn(r, __fmaf_rn(-q, b.lo, a.lo));
+    return fast_two_sum(q, __fdiv_rn(r, b.hi));
+}
+
+// Continuous-path projection of the vertex whose coverage-rule fixed point is
+// `fix`: x = cx + f xv / ze, y = cy - f yv / ze in float-float, stored as the
+// snapped position fix / 256 plus the residual (VGeo).  The oracle's FP64
+// projection and this one agree to ~1e-11 px.
+__device__ __forceinline__ VGeo project_vertex_geo(const CamDev& c, float x, float y, float z, int2 fix) {
     const float* V = c.V;
-    const double X = x, Y = y, Z = z;
-    const double xv = ((double(V[0]) * X + double(V[4]) * Y) + double(V[8]) * Z) + double(V[12]);
-    const double yv = ((double(V[1]) * X + double(V[5]) * Y) + double(V[9]) * Z) + double(V[13]);
-    const double zv = ((double(V[2]) * X + double(V[6]) * Y) + double(V[10]) * Z) + double(V[14]);
-    const double ze = -zv;
-    const double iz = 1.0 / ze;
+    const F2 xv = row_dot_ff(V[0], V[4], V[8], V[12], x, y, z);
+    const F2 yv = row_dot_ff(V[1], V[5], V[9], V[13], x, y, z);
+    const F2 zv = row_dot_ff(V[2], V[6], V[10], V[14], x, y, z);
+    const F2 ze{-zv.hi, -zv.lo};
+    const F2 qx = div_ff(xv, ze), qy = div_ff(yv, ze);
+    // f q in float-float (f = c.f + c.f_lo), then cx + f qx and cy - f qy.
+    const F2 mx = two_prod(c.f, qx.hi), my = two_prod(c.f, qy.hi);
+    const float mxl = __fadd_rn(mx.lo, __fmaf_rn(c.f, qx.lo, __fmul_rn(c.f_lo, qx.hi)));
+    const float myl = __fadd_rn(my.lo, __fmaf_rn(c.f, qy.lo, __fmul_rn(c.f_lo, qy.hi)));
+    const F2 sx = two_sum(c.cx, mx.hi), sy = two_sum(c.cy, -my.hi);
+    const float sxl = __fadd_rn(sx.lo, mxl), syl = __fsub_rn(sy.lo, myl);
     VGeo g;
-    g.sx = double(c.cx) + c.fd * (xv * iz);
-    g.sy = double(c.cy) - c.fd * (yv * iz);
-    g.iz = float(iz);
-    g.ze = float(ze);
-    g.xv = float(xv);
-    g.yv = float(yv);
+    const bool valid = fix.x != kInvalidFix;
+    g.sx = valid ? __fmul_rn(float(fix.x), 0.00390625f) : sx.hi;
+    g.sy = valid ? __fmul_rn(float(fix.y), 0.00390625f) : sy.hi;
+    g.rx = __fadd_rn(__fsub_rn(sx.hi, g.sx), sxl);  // the difference is exact (Sterbenz)
+    g.ry = __fadd_rn(__fsub_rn(sy.hi, g.sy), syl);
+    // 1 / ze with one Newton correction on the float-float depth.
+    const float i0 = __frcp_rn(ze.hi);
+    const float e = __fmaf_rn(-i0, ze.lo, __fmaf_rn(-i0, ze.hi, 1.0f));
+    g.iz = __fmaf_rn(i0, e, i0);
+    g.ze = ze.hi;
+    g.xv = xv.hi;
+    g.yv = yv.hi;
     return g;
 }
 
@@ -79,11 +141,11 @@ __device__ __forceinline__ float depth_key(const float4& a, const float4& b, con
 }
 
 // Continuous fragment values: perspective-correct barycentrics of the pixel
-// centre on the face, from the FP64 screen positions (edge functions in FP64,
-// so thin, nearly edge-on faces keep accurate weights).  Signed weights (a
-// pixel centre the fixed-point coverage rule places just outside the exact
-// projection extrapolates linearly); the depth is clamped to the face's vertex
-// depth range.  Depth and colour of a fragment come from the same weights.
+// centre on the face.  Signed weights (a pixel centre the fixed-point
+// coverage rule places just outside the exact projection extrapolates
+// linearly, which keeps the values smooth in the vertex positions for a fixed
+// list); the depth is clamped to the face's vertex depth range.  Depth and
+// colour of a fragment come from the same weights.
 struct FaceInterp {
     float lam[3];   // screen-space weights E_j / sum(E)
     float A;        // sum(E)
@@ -94,22 +156,43 @@ struct FaceInterp {
     float bary[3];  // perspective-correct weights
 };
 
+// Cross product (a + ar) x (b + br) of two vertex-to-pixel vectors, each the
+// exact difference of a snapped position and the pixel centre (a, b) plus its
+// residual (ar, br).  ax by - ay bx is formed with one rounding (the FMA
+// product error w - ay bx is exact), the residual terms are a few 2^-9 px of
+// the vertex distance and go through one FMA chain.  For a face w px wide and
+// L px long the edge function is kept to about 2^-24 (L / 256 + |E|), where
+// plain FP32 screen coordinates lose 2^-24 |x| L (|x| ~ 1000 px).
+__device__ __forceinline__ float cross_res(float ax, float ay, float arx, float ary, float bx, float by, float brx,
+                                           float bry) {
+    const float w = __fmul_rn(ay, bx);
+    const float e = __fmaf_rn(-ay, bx, w);
+    const float f = __fmaf_rn(ax, by, -w);
+    float t = __fmul_rn(arx, bry);
+    t = __fmaf_rn(-ary, brx, t);
+    t = __fmaf_rn(ax, bry, t);
+    t = __fmaf_rn(arx, by, t);
+    t = __fmaf_rn(-ay, brx, t);
+    t = __fmaf_rn(-ary, bx, t);
+    return __fadd_rn(f, __fadd_rn(e, t));
+}
+
 __device__ __forceinline__ void face_interp(const VGeo& a, const VGeo& b, const VGeo& c, float qx, float qy,
                                             FaceInterp& fi) {
-    const double d0x = a.sx - double(qx), d0y = a.sy - double(qy);
-    const double d1x = b.sx - double(qx), d1y = b.sy - double(qy);
-    const double d2x = c.sx - double(qx), d2y = c.sy - double(qy);
-    const double E0 = d1x * d2y - d1y * d2x;
-    const double E1 = d2x * d0y - d2y * d0x;
-    const double E2 = d0x * d1y - d0y * d1x;
-    const double A = E0 + E1 + E2;
-    fi.A = float(A);
+    // Snapped differences: multiples of 1/256 px below 2^16 px, exact.
+    const float d0x = a.sx - qx, d0y = a.sy - qy;
+    const float d1x = b.sx - qx, d1y = b.sy - qy;
+    const float d2x = c.sx - qx, d2y = c.sy - qy;
+    const float E0 = cross_res(d1x, d1y, b.rx, b.ry, d2x, d2y, c.rx, c.ry);
+    const float E1 = cross_res(d2x, d2y, c.rx, c.ry, d0x, d0y, a.rx, a.ry);
+    const float E2 = cross_res(d0x, d0y, a.rx, a.ry, d1x, d1y, b.rx, b.ry);
+    fi.A = E0 + E1 + E2;
     const float iA = __fdividef(1.0f, fi.A);
-    fi.lam[0] = float(E0) * iA;
-    fi.lam[1] = float(E1) * iA;
-    fi.lam[2] = float(E2) * iA;
-    fi.dx[0] = float(d0x); fi.dx[1] = float(d1x); fi.dx[2] = float(d2x);
-    fi.dy[0] = float(d0y); fi.dy[1] = float(d1y); fi.dy[2] = float(d2y);
+    fi.lam[0] = E0 * iA;
+    fi.lam[1] = E1 * iA;
+    fi.lam[2] = E2 * iA;
+    fi.dx[0] = d0x + a.rx; fi.dx[1] = d1x + b.rx; fi.dx[2] = d2x + c.rx;
+    fi.dy[0] = d0y + a.ry; fi.dy[1] = d1y + b.ry; fi.dy[2] = d2y + c.ry;
     const float u0 = fi.lam[0] * a.iz, u1 = fi.lam[1] * b.iz, u2 = fi.lam[2] * c.iz;
     fi.zb = __fdividef(1.0f, u0 + u1 + u2);
     fi.bary[0] = u0 * fi.zb;

@@ -48,24 +48,26 @@ void launch_fill_order(const uint4* faces, uint32_t F, const int2* vfix, int H, 
 // Exclusive prefix of kFillBands band counts (one warp).
 void launch_band_scan(const uint32_t* hist, uint32_t* cursor, cudaStream_t s);
 // Exclusive scan of counts[n] into offsets[n+1]; scratch must hold scan_scratch_elems(n) u64.
-size_t scan_scratch_elems(uint64_t n);
+constexpr uint64_t kScanTile = 4096;  // counts per scan block (1024 threads x 4)
+constexpr size_t scan_scratch_elems(uint64_t n) { return size_t((n + kScanTile - 1) / kScanTile) + 1; }
 void launch_scan(const uint32_t* counts, uint64_t n, unsigned long long* offsets, unsigned long long* scratch,
                  cudaStream_t s);
-// Per-pixel sort of the lists of P pixels.  scratch holds sort_scratch_elems(P)
-// u32 (length-class counts and lists); flags[1] is set when a list is longer
-// than the block sort capacity.  With a non-null `ok`, the sort does nothing
-// when *ok == 0 (batched steps whose records overflowed the buffer).
-size_t sort_scratch_elems(uint64_t P);
+// Per-pixel sort of the lists of P pixels, any length.  scratch holds
+// sort_scratch_elems(P) u32 (length-class counts and lists).  With a non-null
+// `ok`, the sort does nothing when *ok == 0 (batched steps whose records
+// overflowed the buffer).
+constexpr int kSortClasses = 8;  // list-length classes (dtv_kernels.cu)
+constexpr size_t sort_scratch_elems(uint64_t P) { return 16 + size_t(kSortClasses) * size_t(P); }
 // surrogate_classes: bit c set = list-length class c (1..4: up to 64, 128,
 // 256, 512 records) is sorted through 32-bit surrogate keys, else through the
 // 64-bit network (same result either way).
 constexpr uint32_t kSortSurrogateDefault = 0x1eu;
 constexpr uint32_t kSortBucketDefault = 0x1cu;  // classes sorted by distribution (bit c: class c, 2..4)
 void launch_sort(const unsigned long long* offsets, unsigned long long* records, uint32_t P, uint32_t* scratch,
-                 uint32_t* flags, cudaStream_t s, const uint32_t* ok = nullptr,
+                 cudaStream_t s, const uint32_t* ok = nullptr,
                  uint32_t surrogate_classes = kSortSurrogateDefault, uint32_t bucket_classes = kSortBucketDefault);
 constexpr uint32_t kSortWarpCap = 1024;    // elements per warp list sorted in shared memory
-constexpr uint32_t kSortBlockCap = 16384;  // elements per block-sorted list (128 KiB shared memory)
+constexpr uint32_t kSortBlockCap = 16384;  // elements per block-sorted list / chunk of a longer one (128 KiB shared memory)
 
 // tile: pixel tile of the 256-thread blocks (0: 16 x 16, 1: 32 x 8, 2: 8 x 32).
 void launch_composite(const unsigned long long* offsets, const unsigned long long* records, const uint4* faces,

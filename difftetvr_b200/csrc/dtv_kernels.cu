@@ -25,7 +25,7 @@ __global__ void __launch_bounds__(256) k_project(const float* __restrict__ pos, 
     int2 fx;
     vproj[v] = project_vertex(cam, x, y, z, fx);
     vfix[v] = fx;
-    vgeo[v] = project_vertex_geo(cam, x, y, z);
+    vgeo[v] = project_vertex_geo(cam, x, y, z, fx);
 }
 
 void launch_project(const float* pos, uint32_t V, const CamDev& cam, float4* vproj, int2* vfix, VGeo* vgeo,
@@ -189,7 +189,7 @@ void launch_fill_order(const uint4* faces, uint32_t F, const int2* vfix, int H, 
 // Exclusive scan of the per-pixel counts (u32) into u64 offsets[n+1].
 constexpr int kScanThreads = 1024;
 constexpr int kScanItems = 4;
-constexpr uint64_t kScanTile = uint64_t(kScanThreads) * kScanItems;
+static_assert(uint64_t(kScanThreads) * kScanItems == kScanTile, "scan tile and scan_scratch_elems disagree");
 
 __device__ __forceinline__ u64 block_exclusive_scan(u64 v, u64* sm, u64& total) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -265,8 +265,6 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_final(const uint32_t* __r
         run += v[k];
     }
 }
-
-size_t scan_scratch_elems(uint64_t n) { return size_t((n + kScanTile - 1) / kScanTile) + 1; }
 
 void launch_scan(const uint32_t* counts, uint64_t n, u64* offsets, u64* scratch, cudaStream_t s) {
     const uint64_t nb = (n + kScanTile - 1) / kScanTile;
@@ -505,9 +503,9 @@ constexpr int kSortWarps = 8;
 // with only the registers its class needs.  Classes 0..4: one warp per list,
 // 32 K records in registers (K = 1, 2, 4, 8, 16); class 5: one warp per list,
 // bitonic in shared memory (<= kSortWarpCap); class 6: one block per list
-// (<= kSortBlockCap).  Longer lists set flags[1].
+// (<= kSortBlockCap); class 7: one block per longer list, in place (merge
+// stages over global memory), so no list length is refused.
 // Scratch layout (u32): [0, 16) class counts, then kSortClasses lists of P.
-constexpr int kSortClasses = 7;
 constexpr int kSortGridBlocks = 148 * 8;
 
 __device__ __forceinline__ int sort_class(uint32_t n) {
@@ -521,17 +519,17 @@ __device__ __forceinline__ int sort_class(uint32_t n) {
 }
 
 __global__ void __launch_bounds__(256) k_sort_classify(const u64* __restrict__ offsets, uint32_t P,
-                                                       uint32_t* __restrict__ scratch, uint32_t* __restrict__ flags,
+                                                       uint32_t* __restrict__ scratch,
                                                        const uint32_t* __restrict__ ok) {
     if (ok && *ok == 0u) return;
     const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     int c = -1;
     if (p < P) {
-        const uint32_t n = uint32_t(offsets[p + 1] - offsets[p]);
+        const u64 n = offsets[p + 1] - offsets[p];
         if (n > kSortBlockCap)
-            atomicExch(&flags[1], 1u);
+            c = 7;
         else if (n > 1)
-            c = sort_class(n);
+            c = sort_class(uint32_t(n));
     }
     const unsigned act = __ballot_sync(kFull, c >= 0);
     if (c < 0) return;
@@ -734,7 +732,90 @@ __global__ void __launch_bounds__(1024) k_sort_class_block(const u64* __restrict
     }
 }
 
-size_t sort_scratch_elems(uint64_t P) { return 16 + size_t(kSortClasses) * size_t(P); }
+// Class 7: lists longer than kSortBlockCap, one block per list, in place.
+// An ascending-only bitonic network over the list padded (in thought) with
+// +infinity to N = 2^m records: stage k compares i with i ^ (k - 1) (the
+// mirrored partner in its block of k), then i with i ^ j for j = k/4 .. 1.
+// Every comparator (i, l), i < l, keeps the smaller record at i, so the
+// padding never moves and comparators that reach past the list are skipped.
+// Chunks of C = kSortBlockCap records are sorted whole in shared memory;
+// each later stage (k = 2C .. N) runs its comparators of distance >= C over
+// global memory and the rest chunk by chunk in shared memory.  Records are
+// distinct (a face meets a pixel once), so the order is the total order of
+// the 64-bit values.
+__device__ __forceinline__ void cmpswap_global(u64* r, u64 i, u64 l) {
+    const u64 a = r[i], b = r[l];
+    if (a > b) {
+        r[i] = b;
+        r[l] = a;
+    }
+}
+
+__global__ void __launch_bounds__(1024) k_sort_class_long(const u64* __restrict__ offsets, u64* records,
+                                                          const uint32_t* __restrict__ items,
+                                                          const uint32_t* __restrict__ count,
+                                                          const uint32_t* __restrict__ ok) {
+    if (ok && *ok == 0u) return;
+    extern __shared__ u64 sm_sort[];
+    constexpr u64 C = kSortBlockCap;
+    const uint32_t num = *count;
+    const uint32_t tid = threadIdx.x, nthr = blockDim.x;
+    for (uint32_t it = blockIdx.x; it < num; it += gridDim.x) {
+        const uint32_t p = items[it];
+        const u64 beg = offsets[p];
+        const u64 n = offsets[p + 1] - beg;
+        u64* r = records + beg;
+        u64 N = C;
+        while (N < n) N <<= 1;
+        // Stages k <= C: each chunk sorted in shared memory.
+        for (u64 c0 = 0; c0 < n; c0 += C) {
+            const u64 m = min(C, n - c0);
+            for (uint32_t j = tid; j < C; j += nthr) sm_sort[j] = j < m ? r[c0 + j] : ~0ull;
+            __syncthreads();
+            bitonic_smem<true>(sm_sort, uint32_t(C), tid, nthr);
+            for (uint32_t j = tid; j < m; j += nthr) r[c0 + j] = sm_sort[j];
+            __syncthreads();
+        }
+        for (u64 k = 2 * C; k <= N; k <<= 1) {
+            // Mirror step of stage k, then the half-cleaners of distance >= C.
+            const u64 h = k >> 1;
+            for (u64 t = tid; t < (N >> 1); t += nthr) {
+                const u64 b = (t & ~(h - 1)) << 1, o = t & (h - 1);  // block of k, offset in its lower half
+                const u64 l = b + (k - 1 - o);
+                if (l < n) cmpswap_global(r, b + o, l);
+            }
+            __syncthreads();
+            for (u64 j = k >> 2; j >= C; j >>= 1) {
+                for (u64 t = tid; t < (N >> 1); t += nthr) {
+                    const u64 i = ((t & ~(j - 1)) << 1) | (t & (j - 1));
+                    if (i + j < n) cmpswap_global(r, i, i + j);
+                }
+                __syncthreads();
+            }
+            // Half-cleaners of distance < C stay inside one chunk.
+            for (u64 c0 = 0; c0 < n; c0 += C) {
+                const u64 m = min(C, n - c0);
+                for (uint32_t j = tid; j < C; j += nthr) sm_sort[j] = j < m ? r[c0 + j] : ~0ull;
+                __syncthreads();
+                for (uint32_t j = uint32_t(C >> 1); j > 0; j >>= 1) {
+                    for (uint32_t t = tid; t < uint32_t(C >> 1); t += nthr) {
+                        const uint32_t i = ((t & ~(j - 1)) << 1) | (t & (j - 1));
+                        const u64 a = sm_sort[i], b = sm_sort[i + j];
+                        if (a > b) {
+                            sm_sort[i] = b;
+                            sm_sort[i + j] = a;
+                        }
+                    }
+                    __syncthreads();
+                }
+                for (uint32_t j = tid; j < m; j += nthr) r[c0 + j] = sm_sort[j];
+                __syncthreads();
+            }
+        }
+    }
+}
+
+static_assert(kSortClasses == 8, "k_sort_classify assigns classes 0..7");
 
 template <int K>
 void sort_class(int method, unsigned g, const u64* offsets, u64* records, const uint32_t* items,
@@ -747,7 +828,7 @@ void sort_class(int method, unsigned g, const u64* offsets, u64* records, const 
         k_sort_class_regs<K, false><<<g, kSortWarps * 32, 0, s>>>(offsets, records, items, count, redo_n, redo, ok);
 }
 
-void launch_sort(const u64* offsets, u64* records, uint32_t P, uint32_t* scratch, uint32_t* flags, cudaStream_t s,
+void launch_sort(const u64* offsets, u64* records, uint32_t P, uint32_t* scratch, cudaStream_t s,
                  const uint32_t* ok, uint32_t surrogate_classes, uint32_t bucket_classes) {
     static bool attr_set = false;
     const size_t smem_warp = size_t(kSortWarps) * kSortWarpCap * sizeof(u64);
@@ -755,11 +836,12 @@ void launch_sort(const u64* offsets, u64* records, uint32_t P, uint32_t* scratch
     if (!attr_set) {
         cudaFuncSetAttribute(k_sort_class_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_warp));
         cudaFuncSetAttribute(k_sort_class_block, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_block));
+        cudaFuncSetAttribute(k_sort_class_long, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_block));
         attr_set = true;
     }
     if (P == 0) return;
     cudaMemsetAsync(scratch, 0, 16 * sizeof(uint32_t), s);
-    k_sort_classify<<<(P + 255) / 256, 256, 0, s>>>(offsets, P, scratch, flags, ok);
+    k_sort_classify<<<(P + 255) / 256, 256, 0, s>>>(offsets, P, scratch, ok);
     auto items = [&](int c) { return scratch + 16 + size_t(c) * P; };
     const unsigned g = unsigned(std::min<uint64_t>(kSortGridBlocks, (uint64_t(P) + kSortWarps - 1) / kSortWarps));
     // Lists the register sorts leave unsettled join the block-sort class (6).
@@ -778,6 +860,7 @@ void launch_sort(const u64* offsets, u64* records, uint32_t P, uint32_t* scratch
     k_sort_class_smem<<<std::min(g, 296u), kSortWarps * 32, smem_warp, s>>>(offsets, records, items(5), scratch + 5,
                                                                             ok);
     k_sort_class_block<<<296, 1024, smem_block, s>>>(offsets, records, items(6), scratch + 6, ok);
+    k_sort_class_long<<<148, 1024, smem_block, s>>>(offsets, records, items(7), scratch + 7, ok);
 }
 
 // ---------------------------------------------------------------------------

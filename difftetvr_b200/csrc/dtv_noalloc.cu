@@ -23,9 +23,9 @@
 // that first call before any stream capture.
 //
 // All calls share the one array and it keeps the last call's contents: each
-// call clears what must start at zero (the per-pixel counters and the sort
-// flags).  Calls that overlap on the GPU (other streams, other host threads)
-// race on the array; serialise them.
+// call clears what must start at zero (the per-pixel counters; the sort
+// clears its own class counters).  Calls that overlap on the GPU (other
+// streams, other host threads) race on the array; serialise them.
 #include <cstring>
 #include <mutex>
 #include <stdexcept>
@@ -40,7 +40,10 @@ constexpr uint64_t kNaMaxPixels = 65536;
 constexpr uint64_t kNaMaxFragments = uint64_t(4) << 20;
 
 constexpr size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
-constexpr size_t kNaScanElems = kNaMaxPixels / 4096 + 2;  // >= scan_scratch_elems(kNaMaxPixels)
+// The scan and sort scratch sizes come from the same constexpr functions the
+// allocating path uses, so a change of their tiling cannot overrun a region.
+constexpr size_t kNaScanElems = dtv::scan_scratch_elems(kNaMaxPixels);
+constexpr size_t kNaSortElems = dtv::sort_scratch_elems(kNaMaxPixels);
 
 constexpr size_t kOffVproj = 0;
 constexpr size_t kOffVfix = align256(kOffVproj + sizeof(float4) * kNaMaxVertices);
@@ -51,10 +54,9 @@ constexpr size_t kOffScan = align256(kOffOffsets + sizeof(unsigned long long) * 
 constexpr size_t kOffTfinal = align256(kOffScan + sizeof(unsigned long long) * kNaScanElems);
 constexpr size_t kOffTerm = align256(kOffTfinal + sizeof(float) * kNaMaxPixels);
 constexpr size_t kOffLong = align256(kOffTerm + sizeof(uint32_t) * kNaMaxPixels);
-constexpr size_t kNaSortElems = 16 + 7 * kNaMaxPixels;  // >= sort_scratch_elems(kNaMaxPixels)
-constexpr size_t kOffFlags = align256(kOffLong + sizeof(uint32_t) * kNaSortElems);
-constexpr size_t kOffRecords = align256(kOffFlags + 2 * sizeof(uint32_t));
+constexpr size_t kOffRecords = align256(kOffLong + sizeof(uint32_t) * kNaSortElems);
 constexpr size_t kNaScratchBytes = align256(kOffRecords + sizeof(unsigned long long) * kNaMaxFragments);
+static_assert(kNaScratchBytes < (size_t(48) << 20), "fixed scratch of the allocation-free render grew past 48 MiB");
 
 }  // namespace
 
@@ -128,7 +130,6 @@ extern "C" int32_t dtv_render_noalloc(const dtv_mesh* mesh, const float* d_posit
         auto* tfinal = reinterpret_cast<float*>(base + kOffTfinal);
         auto* term = reinterpret_cast<uint32_t*>(base + kOffTerm);
         auto* long_list = reinterpret_cast<uint32_t*>(base + kOffLong);
-        auto* flags = reinterpret_cast<uint32_t*>(base + kOffFlags);
         auto* records = reinterpret_cast<unsigned long long*>(base + kOffRecords);
 
         const dtv::CamDev cam = dtv::camera_constants(*camera);
@@ -150,17 +151,10 @@ extern "C" int32_t dtv_render_noalloc(const dtv_mesh* mesh, const float* d_posit
         if (params->fragment_budget_bytes && nf * sizeof(unsigned long long) > params->fragment_budget_bytes)
             throw NaError(DTV_ERR_BUDGET, "dtv_render_noalloc: fragments exceed fragment_budget_bytes");
         dtv::launch_raster_fill(mv.faces, uint32_t(mv.num_faces), vproj, vfix, W, H, counts, offsets, records, s);
-        NA_CK(cudaMemsetAsync(flags, 0, 2 * sizeof(uint32_t), s));
-        dtv::launch_sort(offsets, records, uint32_t(P), long_list, flags, s);
+        dtv::launch_sort(offsets, records, uint32_t(P), long_list, s);
         dtv::launch_composite(offsets, records, mv.faces, vgeo, reinterpret_cast<const float4*>(d_colors), W, H, sh,
                               reinterpret_cast<float4*>(d_image), tfinal, term, s);
         NA_CK(cudaGetLastError());
-        uint32_t hflags[2] = {0, 0};
-        NA_CK(cudaMemcpyAsync(hflags, flags, sizeof(hflags), cudaMemcpyDeviceToHost, s));
-        NA_CK(cudaStreamSynchronize(s));
-        if (hflags[1] != 0u)
-            throw NaError(DTV_ERR_BUDGET, "dtv_render_noalloc: a per-pixel fragment list exceeded " +
-                                              std::to_string(dtv::kSortBlockCap) + " entries");
         return DTV_OK;
     } catch (const NaError& e) {
         dtv_set_last_error(e.what());

@@ -352,7 +352,7 @@ __device__ __forceinline__ uint32_t record_lo(const u64* __restrict__ records, u
 // (seg_terms_short, the same arithmetic seg_terms picks for that tier), which
 // the scheduler interleaves; otherwise each sub-segment takes seg_terms.
 __device__ __forceinline__ void segment_composite(float tSeg, const float4& cf, const float4& cb, float atten,
-                                                  float& C0, float& C1, float& C2, float& T) {
+                                                  float& C0, float& C1, float& C2, TransF& T) {
     const float d0 = cb.x - cf.x, d1 = cb.y - cf.y, d2 = cb.z - cf.z, dw = cb.w - cf.w;
     float av[kNumSubdivs];
     bool short_tier = true;
@@ -373,16 +373,33 @@ __device__ __forceinline__ void segment_composite(float tSeg, const float4& cf, 
 #pragma unroll
         for (int s = 0; s < kNumSubdivs; ++s) st[s] = av[s] > 0.f ? seg_terms(tSeg, av[s]) : SegTerms{1.f, 0.f, 0.f, 0.f};
     }
+    // Inside the segment the sub-segments' entry transmittances follow in
+    // FP32 from T.hi (Ts = Ts - Ts (1 - A) in one FMA); the segment lowers T
+    // by exactly the sum of its sub-segment weights ws, applied to the
+    // float-float T.
+    float Ts = T.hi;
 #pragma unroll
     for (int s = 0; s < kNumSubdivs; ++s) {
-        const float w = T * st[s].omA, k = T * (0.25f * st[s].K);
+        const float w = Ts * st[s].omA, k = Ts * (0.25f * st[s].K);
         ws += w;
         ds += w * (0.25f * s) - k;
-        T *= st[s].A;
+        Ts = __fmaf_rn(-Ts, st[s].omA, Ts);
     }
+    trans_add_small(T, -ws);
     C0 += cf.x * ws + d0 * ds;
     C1 += cf.y * ws + d1 * ds;
     C2 += cf.z * ws + d2 * ds;
+}
+
+// Final pixel value over the clear colour (alpha = 1 - T taken from the
+// float-float T, so a nearly transparent pixel keeps its small alpha) and the
+// final transmittance for the adjoint.
+__device__ __forceinline__ void write_pixel(float4* __restrict__ image, float* __restrict__ tfinal, size_t p,
+                                            float C0, float C1, float C2, const TransF& T, const ShadeDev& sh) {
+    const float alpha = __fsub_rn(__fsub_rn(1.f, T.hi), T.lo);
+    image[p] = make_float4(C0 + T.hi * sh.clear[0], C1 + T.hi * sh.clear[1], C2 + T.hi * sh.clear[2],
+                           alpha + T.hi * sh.clear[3]);
+    tfinal[p] = T.hi + T.lo;
 }
 
 // ---------------------------------------------------------------------------
@@ -397,21 +414,20 @@ __device__ __forceinline__ void composite_pixel(
     const u64 beg = offsets[p];
     const uint32_t n = uint32_t(offsets[p + 1] - beg);
     const float qx = float(px) + 0.5f, qy = float(py) + 0.5f;
-    float C0 = 0.f, C1 = 0.f, C2 = 0.f, T = 1.f;
+    float C0 = 0.f, C1 = 0.f, C2 = 0.f;
+    TransF T{1.f, 0.f};
     uint32_t i = n;
     if (n >= 2) {
         FragV f1 = load_frag(records[beg], qx, qy, faces, vgeo, colors), f0;
         for (i = 1; i < n; ++i) {
-            if (sh.use_ert && T < sh.ert_thresh) break;
+            if (sh.use_ert && T.hi < sh.ert_thresh) break;
             f0 = f1;
             f1 = load_frag(records[beg + i], qx, qy, faces, vgeo, colors);
             if (skip_pair(f0.bits, f1.bits)) continue;
             segment_composite((f1.z - f0.z) * 0.25f, f0.col, f1.col, sh.atten, C0, C1, C2, T);
         }
     }
-    image[p] = make_float4(C0 + T * sh.clear[0], C1 + T * sh.clear[1], C2 + T * sh.clear[2],
-                           (1.f - T) + T * sh.clear[3]);
-    tfinal[p] = T;
+    write_pixel(image, tfinal, p, C0, C1, C2, T, sh);
     term[p] = i;
 }
 
@@ -631,7 +647,7 @@ __device__ __forceinline__ void frag_vertex_grads(const FragV& fr, float qx, flo
 // Outputs (added): g_tot = dL/d(segment length), the colour weights wf / wb and
 // the alpha adjoints af / ab of the front / back fragment.
 __device__ __forceinline__ void segment_adjoint(float tSeg, float cfw, float cbw, float pf, float pb, float atten,
-                                                float& T, float& gT, float& g_tot, float& wf, float& wb, float& af,
+                                                TransF& T, TransF& gT, float& g_tot, float& wf, float& wb, float& af,
                                                 float& ab) {
     const float dp = pb - pf, D = 0.25f * dp, dw = cbw - cfw;
     float av[kNumSubdivs];
@@ -641,53 +657,67 @@ __device__ __forceinline__ void segment_adjoint(float tSeg, float cfw, float cbw
         av[s] = (cfw + dw * (0.25f * (s + 0.5f))) * atten;
         short_tier &= (av[s] > 0.f) & (av[s] * tSeg < 0.125f);
     }
-    // One sub-segment, back to front; st is used only when a > 0.
+    // One sub-segment, back to front; st is used only when a > 0.  (This
+    // path runs when some sub-segment of the segment has x >= 1/8: T and gT
+    // change by large steps there, taken on hi with lo scaled along.)
     auto step = [&](int s, const SegTerms& st, bool dense) {
         const float fs = 0.25f * s, fm = 0.25f * (s + 0.5f);
         const float P0 = pf + fs * dp;
         const float a = av[s];
         float g_a;
         if (dense) {
-            const float Tin = __fdividef(T, st.A);
-            const float gTo = gT;
-            gT = st.omA * P0 - st.K * D + gTo * st.A;
-            g_tot += 0.25f * (a * T) * (P0 + tSeg * D - gTo);
+            const float iA = __fdividef(1.f, st.A);
+            const float Tin = T.hi * iA;
+            const float gTo = gT.hi;
+            gT.hi = st.omA * P0 - st.K * D + gTo * st.A;
+            gT.lo *= st.A;
+            g_tot += 0.25f * (a * T.hi) * (P0 + tSeg * D - gTo);
             g_a = Tin * (tSeg * st.A * (P0 - gTo) - st.dK * D);
-            T = Tin;
+            T.hi = Tin;
+            T.lo *= iA;
             const float qK = 0.25f * st.K, tw = Tin * st.omA;
             wf += (1.f - fs) * tw + Tin * qK;
             wb += fs * tw - Tin * qK;
         } else {
-            g_a = T * (tSeg * (P0 - gT) + 0.5f * tSeg * tSeg * D);
+            g_a = T.hi * (tSeg * (P0 - gT.hi) + 0.5f * tSeg * tSeg * D);
         }
         af += (1.f - fm) * g_a * atten;
         ab += fm * g_a * atten;
     };
     // Same tiers as segment_composite: straight-line terms when all four
     // sub-segments are in the short tier (seg_terms_adj's arithmetic there).
-    // There every A > 0.88, so the transmittance in front of the segment is
-    // T / (A0 A1 A2 A3) (one division; the product cannot underflow) and each
-    // sub-segment's entry transmittance follows front to back by products.
-    // The constant factors (1/4 of the length adjoint, the attenuation of the
-    // alpha adjoints) are applied once per segment.
+    // There every x = a t < 1/8, so the transmittance in front of the segment
+    // is T e^X with X = x0 + x1 + x2 + x3 < 1/2: the float-float T grows by
+    // T expm1(X) (expm1 from its series), and each sub-segment's entry
+    // transmittance follows front to back by the forward's own FMA step.  The
+    // transmittance adjoint gT (= gTo A + (1 - A) P0 - K D per sub-segment)
+    // runs in FP32 from gT.hi inside the segment and its total change over the
+    // segment is added to the float-float gT.  The constant factors (1/4 of
+    // the length adjoint, the attenuation of the alpha adjoints) are applied
+    // once per segment.
     if (short_tier) {
         SegTerms st[kNumSubdivs];
 #pragma unroll
         for (int s = 0; s < kNumSubdivs; ++s) st[s] = seg_terms_adj_short(tSeg, av[s]);
+        const float Tout_seg = T.hi;
+        trans_add_small(T, T.hi * expm1_half((av[0] + av[1] + av[2] + av[3]) * tSeg));
         float Tin[kNumSubdivs];
-        Tin[0] = __fdividef(T, (st[0].A * st[1].A) * (st[2].A * st[3].A));
+        Tin[0] = T.hi;
 #pragma unroll
-        for (int s = 1; s < kNumSubdivs; ++s) Tin[s] = Tin[s - 1] * st[s - 1].A;
+        for (int s = 1; s < kNumSubdivs; ++s) Tin[s] = __fmaf_rn(-Tin[s - 1], st[s - 1].omA, Tin[s - 1]);
         // Colour weights: front += sum((1 - fs) tw + Tin K / 4), back +=
         // sum(fs tw - Tin K / 4), from three sums.
-        float gl = 0.f, gaf = 0.f, gab = 0.f, stw = 0.f, sftw = 0.f, sk = 0.f;
+        float gl = 0.f, gaf = 0.f, gab = 0.f, stw = 0.f, sftw = 0.f, sk = 0.f, dg = 0.f;
+        float g = gT.hi;
 #pragma unroll
         for (int s = kNumSubdivs - 1; s >= 0; --s) {
             const float fs = 0.25f * s, fm = 0.25f * (s + 0.5f);
             const float P0 = pf + fs * dp;
-            const float Tout = s == kNumSubdivs - 1 ? T : Tin[s + 1];
-            const float gTo = gT;
-            gT = st[s].omA * P0 - st[s].K * D + gTo * st[s].A;
+            const float Tout = s == kNumSubdivs - 1 ? Tout_seg : Tin[s + 1];
+            const float gTo = g;
+            const float c = st[s].omA * P0 - st[s].K * D;
+            g = __fmaf_rn(-gTo, st[s].omA, gTo) + c;
+            dg += __fmaf_rn(-gTo, st[s].omA, c);
             gl += (av[s] * Tout) * (P0 + tSeg * D - gTo);
             const float g_a = Tin[s] * (tSeg * st[s].A * (P0 - gTo) - st[s].dK * D);
             const float tw = Tin[s] * st[s].omA;
@@ -697,7 +727,7 @@ __device__ __forceinline__ void segment_adjoint(float tSeg, float cfw, float cbw
             gaf += (1.f - fm) * g_a;
             gab += fm * g_a;
         }
-        T = Tin[0];
+        trans_add(gT, dg);
         g_tot += 0.25f * gl;
         wf += (stw - sftw) + 0.25f * sk;
         wb += sftw - 0.25f * sk;
@@ -715,7 +745,7 @@ __device__ __forceinline__ void segment_adjoint(float tSeg, float cfw, float cbw
 }
 
 __device__ __forceinline__ void segment_adjoint(float tSeg, const float4& cf, const float4& cb, float pf, float pb,
-                                                float atten, float& T, float& gT, float& g_tot, float& wf,
+                                                float atten, TransF& T, TransF& gT, float& g_tot, float& wf,
                                                 float& wb, float& af, float& ab) {
     segment_adjoint(tSeg, cf.w, cb.w, pf, pb, atten, T, gT, g_tot, wf, wb, af, ab);
 }
@@ -790,7 +820,7 @@ __device__ __forceinline__ float3 screen_to_world(const float4& a, const VGeo& P
 // the pixel's colour adjoint gC.  A fragment's gradients are taken one step
 // after it is loaded (its back segment and its front segment must both be
 // done), so carrying this state spares the second gather of its three
-// vertices and the second FP64 solve.  Its depth and alpha are those of
+// vertices and the second solve.  Its depth and alpha are those of
 // load_frag_face (same expressions), so the adjoint walks the forward's
 // transmittances; gC . colour is the barycentric sum of the reduced vertex
 // colours.
@@ -807,13 +837,13 @@ __device__ __forceinline__ FragG load_frag_g(uint32_t lo, const uint4& fc, float
                                              const VGeo* __restrict__ vgeo, const float4* __restrict__ colors,
                                              float gC0, float gC1, float gC2) {
     FragG f;
-    f.bits = lo & 3u;
     f.v[0] = fc.x;
     f.v[1] = fc.y;
     f.v[2] = fc.z;
     const VGeo a = vgeo[fc.x], b = vgeo[fc.y], c = vgeo[fc.z];
     FaceInterp fi;
     face_interp(a, b, c, qx, qy, fi);
+    f.bits = lo & 3u;
     const float4 c0 = colors[fc.x], c1 = colors[fc.y], c2 = colors[fc.z];
     const float* bary = fi.bary;
     f.z = fi.z;
@@ -891,8 +921,8 @@ __device__ __forceinline__ void adjoint_pixel_carried(
     if (g.x == 0.f && g.y == 0.f && g.z == 0.f && g.w == 0.f) return;
     const float qx = float(px) + 0.5f, qy = float(py) + 0.5f;
     const float gC0 = g.x, gC1 = g.y, gC2 = g.z;
-    float gT = g.x * sh.clear[0] + g.y * sh.clear[1] + g.z * sh.clear[2] + g.w * (sh.clear[3] - 1.f);
-    float T = tfinal[p];
+    TransF gT{g.x * sh.clear[0] + g.y * sh.clear[1] + g.z * sh.clear[2] + g.w * (sh.clear[3] - 1.f), 0.f};
+    TransF T{tfinal[p], 0.f};
     const int last = sh.use_ert ? int(term[p]) - 1 : int(n) - 1;
     if (last < 1) return;
     const float atten = sh.atten;
@@ -948,8 +978,8 @@ __device__ __forceinline__ void adjoint_pixel(
     if (g.x == 0.f && g.y == 0.f && g.z == 0.f && g.w == 0.f) return;
     const float qx = float(px) + 0.5f, qy = float(py) + 0.5f;
     const float gC0 = g.x, gC1 = g.y, gC2 = g.z;
-    float gT = g.x * sh.clear[0] + g.y * sh.clear[1] + g.z * sh.clear[2] + g.w * (sh.clear[3] - 1.f);
-    float T = tfinal[p];
+    TransF gT{g.x * sh.clear[0] + g.y * sh.clear[1] + g.z * sh.clear[2] + g.w * (sh.clear[3] - 1.f), 0.f};
+    TransF T{tfinal[p], 0.f};
     const int last = sh.use_ert ? int(term[p]) - 1 : int(n) - 1;
     if (last < 1) return;
     const float atten = sh.atten;

@@ -167,7 +167,8 @@ __global__ void __launch_bounds__(kTile * kTile, 2) k_walk_composite(
     const uint32_t nb = uint32_t(b_offsets[p + 1] - beg);
     const float qx = float(px) + 0.5f, qy = float(py) + 0.5f;
     const float scale = ray_scale(cam, qx, qy);
-    float C0 = 0.f, C1 = 0.f, C2 = 0.f, T = 1.f;
+    float C0 = 0.f, C1 = 0.f, C2 = 0.f;
+    TransF T{1.f, 0.f};
     uint32_t last_tet = kNoTet, last_entry = kNoTet, last_b = 0, nseg = 0;
     bool stop = false;
     for (uint32_t b = 0; b < nb && !stop; ++b) {
@@ -180,7 +181,7 @@ __global__ void __launch_bounds__(kTile * kTile, 2) k_walk_composite(
         for (uint32_t step = 0; step <= num_tets; ++step) {
             const uint32_t fx = tet_face_of(tr, vfix, fe, false, px, py);
             if (fx == kNoTet) break;
-            if (sh.use_ert && T < sh.ert_thresh) {
+            if (sh.use_ert && T.hi < sh.ert_thresh) {
                 stop = true;
                 break;
             }
@@ -204,9 +205,7 @@ __global__ void __launch_bounds__(kTile * kTile, 2) k_walk_composite(
             tr = tr_next;
         }
     }
-    image[p] = make_float4(C0 + T * sh.clear[0], C1 + T * sh.clear[1], C2 + T * sh.clear[2],
-                           (1.f - T) + T * sh.clear[3]);
-    tfinal[p] = T;
+    write_pixel(image, tfinal, p, C0, C1, C2, T, sh);
     wstate[p] = make_uint4(last_tet, last_entry, last_b, nseg);
 }
 
@@ -220,7 +219,7 @@ __device__ __forceinline__ void walk_adjoint_carried(
     const u64* __restrict__ b_records, u64 beg, const uint32_t* __restrict__ bf_global,
     const uint4* __restrict__ faces, const uint32_t* __restrict__ f2t, const TetTopo& tt, uint32_t num_tets,
     const int2* __restrict__ vfix, const VGeo* __restrict__ vgeo, const float4* __restrict__ colors, int px, int py,
-    float scale, float atten, float gC0, float gC1, float gC2, float T, float gT, uint32_t t, uint32_t fe,
+    float scale, float atten, float gC0, float gC1, float gC2, TransF T, TransF gT, uint32_t t, uint32_t fe,
     uint32_t fx, int b, Acc& acc) {
     const float qx = float(px) + 0.5f, qy = float(py) + 0.5f;
     FragG fX = load_frag_g(fx << 2, faces[fx], qx, qy, vgeo, colors, gC0, gC1, gC2);
@@ -292,8 +291,8 @@ __global__ void __launch_bounds__(kTile * kTile, 2) k_walk_adjoint(
     const float scale = ray_scale(cam, qx, qy);
     const float atten = sh.atten;
     const float gC0 = g.x, gC1 = g.y, gC2 = g.z;
-    float gT = g.x * sh.clear[0] + g.y * sh.clear[1] + g.z * sh.clear[2] + g.w * (sh.clear[3] - 1.f);
-    float T = tfinal[p];
+    TransF gT{g.x * sh.clear[0] + g.y * sh.clear[1] + g.z * sh.clear[2] + g.w * (sh.clear[3] - 1.f), 0.f};
+    TransF T{tfinal[p], 0.f};
     uint32_t t = ws.x, fe = ws.y;
     int b = int(ws.z);
     uint32_t fx = tet_face_at(tt, vfix, t, fe, false, px, py);

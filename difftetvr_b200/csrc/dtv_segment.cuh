@@ -79,7 +79,7 @@ __device__ __forceinline__ float series_chi(float x) {
 // phi2 to degree 5: the first omitted term at x = 1/8 is x^6/8! = 9.5e-11,
 // 2e-10 of the value.  Both differences are exact in FP32 (Sterbenz: phi1/2
 // <= phi2 <= phi1 and A/2 <= psi <= A for 0 <= x <= 1/8), so psi and chi
-// carry only the rounding of their operands (chi: that of __expf too).  At
+// carry only the rounding of their operands (chi: that of A too).  At
 // the path's densities and segment lengths nearly every sub-segment has
 // x < 1/8.
 __device__ __forceinline__ float series_phi2_short(float x) {
@@ -92,15 +92,32 @@ __device__ __forceinline__ float series_phi2_short(float x) {
     return p;
 }
 
+// e^x - 1 for |x| < 1/2 from its Taylor series to degree 9 (the first
+// omitted term at |x| = 1/2 is x^10 / 10! = 2.7e-10, under 7e-10 of the value).
+__device__ __forceinline__ float expm1_half(float x) {
+    float p = 2.75573192e-6f;             // 1/9!
+    p = fmaf(p, x, 2.48015873e-5f);       // 1/8!
+    p = fmaf(p, x, 1.98412698e-4f);       // 1/7!
+    p = fmaf(p, x, 1.38888889e-3f);       // 1/6!
+    p = fmaf(p, x, 8.33333333e-3f);       // 1/5!
+    p = fmaf(p, x, 4.16666667e-2f);       // 1/4!
+    p = fmaf(p, x, 0.166666667f);         // 1/3!
+    p = fmaf(p, x, 0.5f);                 // 1/2!
+    p = fmaf(p, x, 1.0f);
+    return x * p;
+}
+
 // The x = a t < 1/8 tier of seg_terms / seg_terms_adj alone (no branch), for
 // callers that have checked the tier for several sub-segments at once.
+// Here A = 1 - (1 - A): one rounding of a value near 1 (within 2^-25), no
+// exp evaluation.
 __device__ __forceinline__ SegTerms seg_terms_short(float t, float a) {
     SegTerms s;
     const float x = a * t;
-    s.A = __expf(-x);
     const float phi2 = series_phi2_short(x);
     const float phi1 = fmaf(-x, phi2, 1.0f);
     s.omA = x * phi1;
+    s.A = 1.0f - s.omA;
     s.K = -t * x * (phi1 - phi2);
     s.dK = 0.f;
     return s;
@@ -109,14 +126,56 @@ __device__ __forceinline__ SegTerms seg_terms_short(float t, float a) {
 __device__ __forceinline__ SegTerms seg_terms_adj_short(float t, float a) {
     SegTerms s;
     const float x = a * t;
-    s.A = __expf(-x);
     const float phi2 = series_phi2_short(x);
     const float phi1 = fmaf(-x, phi2, 1.0f);
     const float psi = phi1 - phi2;
     s.omA = x * phi1;
+    s.A = 1.0f - s.omA;
     s.K = -t * x * psi;
     s.dK = t * t * (psi - s.A);
     return s;
+}
+
+// 1 - e^-x without cancellation (x phi1(x) for |x| < 1/8).
+__device__ __forceinline__ float one_minus_exp(float x) {
+    if (fabsf(x) < 0.125f) return x * fmaf(-x, series_phi2_short(x), 1.0f);
+    return 1.0f - __expf(-x);
+}
+
+// e^x - 1 without cancellation (series for |x| < 1/2).
+__device__ __forceinline__ float expm1_signed(float x) {
+    if (fabsf(x) < 0.5f) return expm1_half(x);
+    return __expf(x) - 1.0f;
+}
+
+// Transmittance carried along a pixel ray as an unevaluated float-float sum
+// hi + lo.  A segment of optical depth x lowers T by T (1 - e^-x); at low
+// density that is far below the spacing of FP32 values near T (2^-24 T): a
+// plain FP32 T would round each decrement, or lose it entirely once it is
+// under half that spacing (a ray through thousands of nearly transparent
+// segments would keep T = 1).  Each segment's decrement (or, back to front,
+// increment) is applied with an error-free sum, the error kept in lo.
+struct TransF {
+    float hi, lo;
+};
+
+// T += d for |d| <= |T.hi| (Fast2Sum), renormalised.
+__device__ __forceinline__ void trans_add_small(TransF& T, float d) {
+    const float s = __fadd_rn(T.hi, d);
+    const float e = __fadd_rn(__fsub_rn(T.hi, s), d);
+    const float lo = __fadd_rn(T.lo, e);
+    T.hi = __fadd_rn(s, lo);
+    T.lo = __fsub_rn(lo, __fsub_rn(T.hi, s));
+}
+
+// T += d for any d (TwoSum), renormalised.
+__device__ __forceinline__ void trans_add(TransF& T, float d) {
+    const float s = __fadd_rn(T.hi, d);
+    const float bb = __fsub_rn(s, T.hi);
+    const float e = __fadd_rn(__fsub_rn(T.hi, __fsub_rn(s, bb)), __fsub_rn(d, bb));
+    const float lo = __fadd_rn(T.lo, e);
+    T.hi = __fadd_rn(s, lo);
+    T.lo = __fsub_rn(lo, __fsub_rn(T.hi, s));
 }
 
 // Forward terms; caller guarantees a > 0.  (The reference drops a < 1e-6; the

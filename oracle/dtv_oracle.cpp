@@ -1218,6 +1218,21 @@ int64_t orc_fragments(const uint32_t* tri, const uint32_t* fbits, int64_t F, con
     return nf;
 }
 
+// Fragment lists of pixel rows [row_begin, row_end) only (offsets over all
+// P + 1 pixels, zero-length lists outside the rows): bounded checks of large
+// images.
+int64_t orc_fragments_rows(const uint32_t* tri, const uint32_t* fbits, int64_t F, const float* pos, int64_t V,
+                           const Camera* camp, int32_t row_begin, int32_t row_end, int64_t* offsets,
+                           uint64_t* records, int64_t records_cap) {
+    CamConst cam = make_cam(*camp);
+    auto pf = project_all_f(pos, V, cam);
+    FragLists fl = build_fragments(tri, fbits, F, pf, cam, row_begin, row_end);
+    int64_t nf = int64_t(fl.records.size());
+    if (offsets) std::memcpy(offsets, fl.offsets.data(), sizeof(int64_t) * fl.offsets.size());
+    if (records && records_cap >= nf) std::memcpy(records, fl.records.data(), sizeof(uint64_t) * size_t(nf));
+    return nf;
+}
+
 // FP32 projection of vertices (sx, sy, ze per vertex) and the snapped coords.
 void orc_project_f32(const float* pos, int64_t V, const Camera* camp, float* sxsyze, int32_t* XY,
                      uint8_t* valid) {

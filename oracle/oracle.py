@@ -51,6 +51,9 @@ def load():
         lib.orc_fragments.restype = ctypes.c_int64
         lib.orc_fragments.argtypes = [_vp, _vp, ctypes.c_int64, _vp, ctypes.c_int64, ctypes.POINTER(Camera), _vp,
                                       _vp, ctypes.c_int64]
+        lib.orc_fragments_rows.restype = ctypes.c_int64
+        lib.orc_fragments_rows.argtypes = [_vp, _vp, ctypes.c_int64, _vp, ctypes.c_int64, ctypes.POINTER(Camera),
+                                           ctypes.c_int32, ctypes.c_int32, _vp, _vp, ctypes.c_int64]
         lib.orc_project_f32.restype = None
         lib.orc_project_f32.argtypes = [_vp, ctypes.c_int64, ctypes.POINTER(Camera), _vp, _vp, _vp]
         for name in ("orc_render_f64", "orc_render_f32"):
@@ -142,6 +145,21 @@ def fragments(faces: Faces, positions: np.ndarray, cam: Camera):
     rec = np.empty(max(nf, 1), np.uint64)
     lib.orc_fragments(_p(faces.tri), _p(faces.face_boundary), faces.num_faces, _p(pos), pos.shape[0],
                       ctypes.byref(cam), _p(off), _p(rec), rec.shape[0])
+    return off, rec[:nf]
+
+
+def fragments_rows(faces: Faces, positions: np.ndarray, cam: Camera, row_begin: int, row_end: int):
+    """fragments() restricted to pixel rows [row_begin, row_end): offsets i64[P+1]
+    (empty lists outside the rows), records u64 of those rows."""
+    lib = load()
+    pos = np.ascontiguousarray(positions, dtype=np.float32)
+    P = cam.width * cam.height
+    off = np.empty(P + 1, np.int64)
+    args = (_p(faces.tri), _p(faces.face_boundary), faces.num_faces, _p(pos), pos.shape[0], ctypes.byref(cam),
+            int(row_begin), int(row_end), _p(off))
+    nf = lib.orc_fragments_rows(*args, None, 0)
+    rec = np.empty(max(nf, 1), np.uint64)
+    lib.orc_fragments_rows(*args, _p(rec), rec.shape[0])
     return off, rec[:nf]
 
 

@@ -58,7 +58,11 @@ def test_inconsistently_oriented_tets_walk_like_the_oracle(oracle):
     img_o, _, nseg_o = oracle.raytet(fa, sc.pos, sc.col, sc.oracle_camera(oracle), sc.oracle_params(oracle))
     assert np.array_equal(nseg_g, nseg_o)
     assert (nseg_o > 0).sum() > 0.1 * 96 * 96
-    assert np.abs(img - img_o).max() < IMG_TOL
+    # Walks through mis-oriented tets take segments of negative length, so T
+    # grows above 1 (to about 7) and pixel values reach -6: the FP32 depth
+    # difference of a segment carries ~2^-24 |z| of error into the optical
+    # depth, scaled by T.  The image tolerance is taken relative to the value.
+    assert (np.abs(img - img_o) / np.maximum(1.0, np.abs(img_o))).max() < IMG_TOL
 
 
 @pytest.mark.parametrize("kind,n,res,clear", [("cube", 8, 128, (0, 0, 0, 0)), ("cube", 16, 256, (0, 0, 0, 0)),

@@ -71,3 +71,40 @@ def test_noalloc_rejects_sizes_beyond_its_limits():
     torch.cuda.synchronize()
     assert float((out - ref).abs().max()) <= IMG_TOL
     assert np.isfinite(out.cpu().numpy()).all()
+
+
+def test_noalloc_fragment_and_vertex_limits_then_valid_call():
+    """The fragment limit (4,194,304 records) is checked after the exact count
+    of the scan, once the per-pixel counters are written; the budget of the
+    call's parameters likewise.  The next valid call must clear what the
+    rejected one left and match dtv_renderer_render."""
+    from difftetvr_b200._lib import DTV_ERR_ARG, DTV_ERR_BUDGET
+    sc = Scene(32, 256, seed=3)  # 35,937 vertices, about 6.4 M fragments at 256 x 256
+    mesh, r = sc.make_renderer()
+    pos = mesh.get_vertex_positions().detach()
+    col = mesh.get_vertex_colors().detach()
+    with pytest.raises(_lib.DtvError) as e:
+        _noalloc_render(mesh, r, pos, col)
+    assert e.value.code == DTV_ERR_BUDGET and "fragments exceed" in str(e.value)
+    r.set_viewport_size(128, 128)
+    ref = r.render().clone()
+    out = _noalloc_render(mesh, r, pos, col)
+    torch.cuda.synchronize()
+    assert float((out - ref).abs().max()) <= IMG_TOL
+
+    # The caller's own fragment budget, then a valid call again.
+    r.set_fragment_budget_bytes(1024)
+    with pytest.raises(_lib.DtvError) as e:
+        _noalloc_render(mesh, r, pos, col)
+    assert e.value.code == DTV_ERR_BUDGET and "fragment_budget_bytes" in str(e.value)
+    r.set_fragment_budget_bytes(0)
+    out = _noalloc_render(mesh, r, pos, col)
+    torch.cuda.synchronize()
+    assert float((out - ref).abs().max()) <= IMG_TOL
+
+    # Vertex limit (65,536): a 40^3 mesh has 68,921 vertices.
+    big = Scene(40, 64, seed=4)
+    mesh_b, r_b = big.make_renderer()
+    with pytest.raises(_lib.DtvError) as e:
+        _noalloc_render(mesh_b, r_b, mesh_b.get_vertex_positions().detach(), mesh_b.get_vertex_colors().detach())
+    assert e.value.code == DTV_ERR_ARG and "vertices exceed" in str(e.value)
