@@ -47,8 +47,7 @@ def parse_args():
     ap.add_argument("--n", type=int, default=64, help="Kuhn grid cubes per axis")
     ap.add_argument("--res", type=int, default=1024)
     ap.add_argument("--views", type=int, default=16)
-    ap.add_argument("--cpu-rows", type=int, default=64, help="rows of one band of the CPU baseline sample")
-    ap.add_argument("--cpu-bands", type=int, default=4, help="bands timed for the CPU baseline")
+    ap.add_argument("--cpu-steps", type=int, default=2, help="whole CPU-port steps timed for cpu_baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
@@ -709,107 +708,81 @@ def run_serving(args):
     return out
 
 
-def cpu_port_band(args, sc, r0, rows):
-    """Seconds the oracle's FP32 port (all host threads) takes for forward +
-    adjoint of one view of the workload restricted to pixel rows [r0, r0+rows)
-    (every face is still projected, set up and clipped to the band)."""
-    import numpy as np
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O
+class CpuPortLoop:
+    """The workload's iteration on the host cores: the oracle's FP32 port
+    (all threads) renders the whole image, the L2 loss adjoint is taken
+    against a target image of the seed-1 mesh, the port's adjoint gives the
+    vertex position / colour gradients and a host Adam (lr 1e-2 colours
+    clamped at zero, 1e-4 positions) updates them.  Inputs come from
+    oracle/scene.py, so no product code is loaded.  One camera
+    (sphere_camera(100), the first of the GPU loop's cameras) for every step;
+    its target image is rendered once, untimed."""
 
-    res = args.res
-    fa = O.Faces(sc["cells"], sc["pos"].shape[0])
-    cam = O.make_camera(sc["views"][0], __import__("math").radians(45.0), res, res)
-    prm = O.make_params(attenuation=1.0, use_ert=True, ert_thresh=1e-4, rows=(r0, r0 + rows))
-    w = np.zeros((res, res, 4), np.float32)
-    w[r0:r0 + rows] = 1e-6
-    t = time.perf_counter()
-    O.render(fa, sc["pos"], sc["col"], cam, prm, precision=32)
-    O.adjoint(fa, sc["pos"], sc["col"], cam, prm, w, precision=32)
-    return time.perf_counter() - t
+    def __init__(self, n: int, res: int):
+        import numpy as np
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        import scene as OS
 
+        self.np, self.O, self.res = np, O, res
+        cells, pos = OS.kuhn_mesh(n, seed=0)
+        self.pos = pos.copy()
+        self.col = OS.gaussian_colors(pos, seed=0)
+        _, pos_t = OS.kuhn_mesh(n, seed=1)
+        col_t = OS.gaussian_colors(pos_t, seed=1)
+        self.faces = O.Faces(cells, pos.shape[0])
+        self.cam = O.make_camera(OS.sphere_camera(100), OS.FOVY_45, res, res)
+        self.prm = O.make_params(attenuation=1.0, use_ert=True, ert_thresh=1e-4)
+        self.target = O.render(self.faces, pos_t, col_t, self.cam, self.prm, precision=32)[0]
+        self.opt_col = OS.Adam(self.col, LR_COL, clamp_nonnegative=True)
+        self.opt_pos = OS.Adam(self.pos, LR_POS)
+        self.times = []
 
-def cpu_port_strata(res, rows):
-    """Start rows of the res // rows horizontal strata of `rows` rows, in
-    van der Corput order, so that any prefix spreads over the whole image."""
-    count = max(1, res // rows)
-    order, seen = [], set()
-    for i in range(1, 4 * count + 1):
-        x, f, j = 0.0, 0.5, i
-        while j:
-            x += f * (j & 1)
-            j >>= 1
-            f *= 0.5
-        k = min(int(x * count), count - 1)
-        if k not in seen:
-            seen.add(k)
-            order.append(k)
-    order += [k for k in range(count) if k not in seen]
-    return [k * rows for k in order]
+    def step(self) -> float:
+        np, O = self.np, self.O
+        t = time.perf_counter()
+        img = O.render(self.faces, self.pos, self.col, self.cam, self.prm, precision=32)[0]
+        gimg = (2.0 / img.size) * (img - self.target)
+        gp, gc = O.adjoint(self.faces, self.pos, self.col, self.cam, self.prm, gimg, precision=32)
+        self.opt_col.step(gc.astype(np.float32))
+        self.opt_pos.step(gp.astype(np.float32))
+        dt = time.perf_counter() - t
+        self.times.append(dt)
+        return dt
 
-
-class CpuPortEstimate:
-    """Full-image seconds of the oracle's FP32 port (all host threads) for
-    forward + adjoint of one view, from a one-row pass (the per-view part that
-    does not scale with rows: projection and the loop over all faces) and
-    bands of `rows` rows taken from the image's strata in van der Corput order
-    (the per-row part, which varies with how much of the mesh a row crosses):
-    full = fixed + strata * mean(band - fixed)."""
-
-    def __init__(self, args, sc, rows=None):
-        self.args, self.sc = args, sc
-        self.rows = min(rows or args.cpu_rows, args.res)
-        self.starts = cpu_port_strata(args.res, self.rows)
-        self.fixed = cpu_port_band(args, sc, 0, 1)
-        self.bands = []
-
-    def step(self):
-        r0 = self.starts[len(self.bands) % len(self.starts)]
-        t = cpu_port_band(self.args, self.sc, r0, self.rows)
-        self.bands.append(t)
-        return t
-
-    def seconds(self):
-        mean = sum(max(t - self.fixed, 0.0) for t in self.bands) / len(self.bands)
-        return self.fixed + len(self.starts) * mean
-
-    def describe(self):
-        full = self.seconds()
-        return (f"one-row pass ({self.fixed:.3f} s) + {len(self.bands)} bands of {self.rows} rows from the "
-                f"{len(self.starts)} strata of {self.args.res} rows (van der Corput order), forward + adjoint "
-                f"of one view, FP32 port; full image = fixed + {len(self.starts)} x mean band excess = {full:.2f} s")
+    def describe(self, n: int) -> str:
+        return (f"{len(self.times)} whole steps (forward + L2 adjoint + adjoint + Adam) of one view "
+                f"(Kuhn {n}^3 at {self.res}x{self.res}, sphere_camera(100)) on the oracle's FP32 port, "
+                f"{self.O.num_threads()} threads, mean {sum(self.times) / len(self.times):.2f} s per step")
 
 
 def run_reference(args, rank, world):
-    """CPU implementation of the path (the oracle's FP32 port; the reference's
-    own Vulkan path is unavailable on this box) timed on host cores."""
-    import numpy as np
-
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O
-
-    from difftetvr_b200 import synthetic as S
-    cells, pos = S.kuhn_mesh(args.n, seed=0)
-    col = S.gaussian_colors(pos, seed=0)
-    views = [S.sphere_camera(100 + i) for i in range(args.views)]
-    sc = {"cells": cells, "pos": pos, "col": col, "views": views, "np": np}
+    """The CPU implementation of the path (the oracle's FP32 port: the
+    reference's own Vulkan path is unavailable on this box and its build
+    needs the un-vendored sgl framework) timed on the host cores: W untimed
+    and K timed whole steps of the workload."""
+    loop = CpuPortLoop(args.n, args.res)
     for _ in range(args.warmup):
-        cpu_port_band(args, sc, args.res // 2 - args.cpu_rows // 2, args.cpu_rows)
-    est = CpuPortEstimate(args, sc)
+        loop.step()
+    loop.times.clear()
+    t0 = time.perf_counter()
     for _ in range(args.steps):
-        est.step()
-    value = 1.0 / est.seconds()
-    desc = est.describe()
-    cores = O.num_threads()
+        loop.step()
+    total = time.perf_counter() - t0
+    value = args.steps / total
+    cores = loop.O.num_threads()
     return {
         "metric": METRIC, "value": value, "unit": "iter/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
-        "config": {"workload": f"plain method, Kuhn {args.n}^3, {args.res}x{args.res}, fwd+adj (CPU port)"},
-        "cpu_baseline": {"value": value, "unit": "iter/s", "cores": cores, "kind": "port", "sample": desc},
+        "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+        "config": {"workload": f"plain method, Kuhn {args.n}^3 ({6 * args.n ** 3} tets), {args.res}x{args.res}, "
+                               "one camera per step, fwd+adj+Adam (CPU port)", "res": args.res},
+        "cpu_baseline": {"value": value, "unit": "iter/s", "cores": cores, "kind": "port",
+                         "sample": loop.describe(args.n)},
         "e2e": {"value": value, "unit": "iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "the reference's Vulkan renderer (and lavapipe) is unavailable on this box; the timed CPU "
-                "implementation is this repository's FP32 restatement of its algorithm",
+                "implementation is this repository's FP32 restatement of its algorithm (oracle/), fed by "
+                "oracle/scene.py so that no product code is loaded",
     }
 
 
@@ -881,14 +854,12 @@ def main():
         torch.cuda.empty_cache()
         result["served"] = run_serving(args)
     if rank == 0 and not args.no_cpu_baseline:
-        est = CpuPortEstimate(args, sc)
-        for _ in range(args.cpu_bands):
-            est.step()
-        v, s, desc = 1.0 / est.seconds(), est.fixed + sum(est.bands), est.describe()
-        sys.path.insert(0, os.path.join(ROOT, "oracle"))
-        import oracle as O
-        result["cpu_baseline"] = {"value": v, "unit": "iter/s", "cores": O.num_threads(), "kind": "port",
-                                  "sample": desc, "seconds": s}
+        loop = CpuPortLoop(args.n, args.res)
+        for _ in range(args.cpu_steps):
+            loop.step()
+        v = len(loop.times) / sum(loop.times)
+        result["cpu_baseline"] = {"value": v, "unit": "iter/s", "cores": loop.O.num_threads(), "kind": "port",
+                                  "sample": loop.describe(args.n), "seconds": sum(loop.times)}
     if rank == 0:
         print(json.dumps(result))
     if world > 1:
