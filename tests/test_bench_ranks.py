@@ -50,33 +50,3 @@ def test_max_over_ranks_and_rank0_output():
         assert ms == pytest.approx(15.0)
         assert rate == pytest.approx(2 * 20 / 0.015)
     assert res[1][3] == 0 and res[1][4] == ""
-
-
-def test_cpu_strata_cover_the_image_and_prefixes_spread():
-    sys.path.insert(0, ROOT)
-    import bench
-    starts = bench.cpu_port_strata(1024, 64)
-    assert sorted(starts) == list(range(0, 1024, 64))
-    # every prefix of length 2^k holds one band in each of the 2^k equal parts
-    for k in (1, 2, 3, 4):
-        parts = sorted(s * (1 << k) // 1024 for s in starts[:1 << k])
-        assert parts == list(range(1 << k))
-    assert bench.cpu_port_strata(100, 64) == [0]
-
-
-def test_cpu_estimate_arithmetic(monkeypatch):
-    sys.path.insert(0, ROOT)
-    import bench
-
-    class A:
-        res, cpu_rows = 256, 64
-    # a synthetic port: 0.1 s per view plus a cost per row that peaks at the centre
-    cost = lambda r: 0.001 * (1.0 + (r < 192) * (r >= 64))
-    monkeypatch.setattr(bench, "cpu_port_band",
-                        lambda args, sc, r0, rows: 0.1 + sum(cost(r) for r in range(r0, r0 + rows)))
-    est = bench.CpuPortEstimate(A, None)
-    for _ in range(4):
-        est.step()
-    full = 0.1 + sum(cost(r) for r in range(256))
-    # the one-row pass also holds row 0's cost, subtracted once per stratum
-    assert abs(est.seconds() - full) < 4 * 0.001 + 1e-9
