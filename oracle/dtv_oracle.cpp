@@ -1161,6 +1161,434 @@ struct TempFace {
 
 }  // namespace
 
+// ---------------------------------------------------------------------------
+// Reference mode: the reference's own formulas of the PPLL path, as its GLSL
+// states them, on the same fragment sets (this file's fixed-point coverage,
+// since the reference's rasteriser is the GPU's).  Used to measure how far
+// the exact path (above; the CUDA library follows it) is from what the
+// reference computes on the same inputs.  Evaluated in double; the FP32
+// storage of the depth buffer value is reproduced.
+//
+// Forward (Data/Shaders/PPLL/Forward.glsl:35-105, 159-211):
+//  - each fragment stores gl_FragCoord.z, the NDC depth interpolated affinely
+//    in screen space, as a 32-bit float (LinkedListGather.glsl:97); lists are
+//    ordered by it (the 4-ary heap, Forward.glsl:107-114; ties here by face);
+//  - depthLinear = zNear zFar / (zFar + z_ndc (zNear - zFar))
+//    (Utils/DepthHelper.glsl:72-75);
+//  - the world point is the inverse view-projection of (ndc.xy, z_ndc), and
+//    the colour weights are unsigned cross-product ratios u = |d21 x (p - p1)|
+//    / A, v = |(p - p0) x d20| / A, w = 1 - u - v, A = max(|d20 x d21|, 1e-5)
+//    (Forward.glsl:80-103);
+//  - accumulateLinearConst returns 0 when a < 1e-6 (ForwardCommon.glsl:42-49);
+//  - opacity is blended front to back and the ray stops once
+//    alpha > 1 - thresh (Forward.glsl:169-173).
+// Adjoint (PPLL/Backward.glsl:107-512, Common/BackwardCommon.glsl:95-251):
+//  - back to front from the termination index; per segment only
+//    sub-segments s = 3, 2, 1 (Backward.glsl:222), each inverted with
+//    alpha_in = (C.a - alpha_out) / (C.a - 1) (:232) and differentiated by
+//    accumulateLinearConstAdjoint (:116-133; its getNextFragment clamps the
+//    area at 1e-6, Backward.glsl:98);
+//  - segmentLengthAdjoint differentiates the Euclidean distance between the
+//    two fragments' world points (BackwardCommon.glsl:139-181);
+//  - baryAdjoint differentiates u, v with the world point held fixed
+//    (:183-251).
+namespace refmode {
+
+struct V3 {
+    double x, y, z;
+};
+inline V3 operator+(V3 a, V3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+inline V3 operator-(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline V3 operator*(double s, V3 a) { return {s * a.x, s * a.y, s * a.z}; }
+inline double dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+inline V3 cross(V3 a, V3 b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+inline double len(V3 a) { return std::sqrt(dot(a, a)); }
+
+struct Cam {
+    CamConst c;
+    double inv_view[16];  // column-major inverse of the view matrix
+    double zn, zf;
+};
+
+inline void invert4(const float* m, double* out) {
+    // Gauss-Jordan on a row-major copy of the column-major matrix.
+    double a[4][8];
+    for (int r = 0; r < 4; ++r)
+        for (int k = 0; k < 4; ++k) {
+            a[r][k] = double(m[k * 4 + r]);
+            a[r][4 + k] = r == k ? 1.0 : 0.0;
+        }
+    for (int c = 0; c < 4; ++c) {
+        int piv = c;
+        for (int r = c + 1; r < 4; ++r)
+            if (std::fabs(a[r][c]) > std::fabs(a[piv][c])) piv = r;
+        for (int k = 0; k < 8; ++k) std::swap(a[c][k], a[piv][k]);
+        const double d = a[c][c];
+        for (int k = 0; k < 8; ++k) a[c][k] /= d;
+        for (int r = 0; r < 4; ++r) {
+            if (r == c) continue;
+            const double f = a[r][c];
+            for (int k = 0; k < 8; ++k) a[r][k] -= f * a[c][k];
+        }
+    }
+    for (int r = 0; r < 4; ++r)
+        for (int k = 0; k < 4; ++k) out[k * 4 + r] = a[r][4 + k];
+}
+
+Cam make(const Camera& camera) {
+    Cam k;
+    k.c = make_cam(camera);
+    invert4(camera.view, k.inv_view);
+    k.zn = camera.znear;
+    k.zf = camera.zfar;
+    return k;
+}
+
+// NDC depth of view depth ze (perspectiveRH_ZO): zFar (ze - zNear) / ((zFar - zNear) ze).
+inline double ndc_of_ze(const Cam& k, double ze) { return k.zf * (ze - k.zn) / ((k.zf - k.zn) * ze); }
+inline double lin_depth(const Cam& k, double zndc) { return k.zn * k.zf / (k.zf + zndc * (k.zn - k.zf)); }
+
+// World point of pixel centre (px, py) at NDC depth zndc.
+inline V3 unproject(const Cam& k, int px, int py, double zndc) {
+    const double ze = lin_depth(k, zndc);
+    const double sx = double(px) + 0.5, sy = double(py) + 0.5;
+    const double xv = (sx - k.c.cxd) * ze / k.c.fd, yv = -(sy - k.c.cyd) * ze / k.c.fd, zv = -ze;
+    const double* M = k.inv_view;
+    return {M[0] * xv + M[4] * yv + M[8] * zv + M[12], M[1] * xv + M[5] * yv + M[9] * zv + M[13],
+            M[2] * xv + M[6] * yv + M[10] * zv + M[14]};
+}
+
+struct Mesh {
+    const uint32_t* tri;
+    const double* pos;
+    const double* col;
+    std::vector<ProjR<double>> proj;
+};
+
+inline V3 vpos(const Mesh& m, uint32_t v) { return {m.pos[3 * v], m.pos[3 * v + 1], m.pos[3 * v + 2]}; }
+
+struct Frag {
+    float zndc;          // the stored depth buffer value
+    double depth;        // depthLinear
+    V3 p;                // world point
+    V3 pv[3];            // face vertices
+    double c[3][4];      // vertex colours
+    uint32_t vi[3];
+    double u, v;
+    double col[4];
+    bool boundary, front;
+};
+
+// gl_FragCoord.z of face f at the pixel centre (screen-affine interpolation
+// of the vertices' NDC depths), as stored: a 32-bit float.
+inline float frag_zndc(const Mesh& m, const Cam& k, uint32_t f, int px, int py) {
+    const ProjR<double>& a = m.proj[m.tri[3 * f]];
+    const ProjR<double>& b = m.proj[m.tri[3 * f + 1]];
+    const ProjR<double>& c = m.proj[m.tri[3 * f + 2]];
+    const double qx = px + 0.5, qy = py + 0.5;
+    const double d0x = a.sx - qx, d0y = a.sy - qy, d1x = b.sx - qx, d1y = b.sy - qy, d2x = c.sx - qx,
+                 d2y = c.sy - qy;
+    const double E0 = d1x * d2y - d1y * d2x, E1 = d2x * d0y - d2y * d0x, E2 = d0x * d1y - d0y * d1x;
+    const double A = E0 + E1 + E2;
+    return float((E0 * ndc_of_ze(k, a.ze) + E1 * ndc_of_ze(k, b.ze) + E2 * ndc_of_ze(k, c.ze)) / A);
+}
+
+inline Frag eval(const Mesh& m, const Cam& k, uint32_t bits, float zndc, int px, int py, double area_floor) {
+    Frag fr;
+    const uint32_t f = bits >> 2;
+    fr.boundary = (bits >> 1) & 1u;
+    fr.front = bits & 1u;
+    fr.zndc = zndc;
+    fr.depth = lin_depth(k, double(zndc));
+    fr.p = unproject(k, px, py, double(zndc));
+    for (int j = 0; j < 3; ++j) {
+        fr.vi[j] = m.tri[3 * f + j];
+        fr.pv[j] = vpos(m, fr.vi[j]);
+        for (int q = 0; q < 4; ++q) fr.c[j][q] = m.col[4 * size_t(fr.vi[j]) + q];
+    }
+    const V3 d20 = fr.pv[2] - fr.pv[0], d21 = fr.pv[2] - fr.pv[1];
+    const double area = std::max(len(cross(d20, d21)), area_floor);
+    fr.u = len(cross(d21, fr.p - fr.pv[1])) / area;
+    fr.v = len(cross(fr.p - fr.pv[0], d20)) / area;
+    const double w = 1.0 - fr.u - fr.v;
+    for (int q = 0; q < 4; ++q) fr.col[q] = fr.c[0][q] * fr.u + fr.c[1][q] * fr.v + fr.c[2][q] * w;
+    return fr;
+}
+
+// Records of one pixel re-keyed by the stored NDC depth (ties by face).
+inline std::vector<std::pair<float, uint32_t>> pixel_list(const Mesh& m, const Cam& k, const uint64_t* recs,
+                                                          int64_t n, int px, int py) {
+    std::vector<std::pair<float, uint32_t>> l{};
+    l.resize(size_t(n));
+    for (int64_t i = 0; i < n; ++i) {
+        const uint32_t bits = uint32_t(recs[i] & 0xffffffffu);
+        l[size_t(i)] = {frag_zndc(m, k, bits >> 2, px, py), bits};
+    }
+    std::sort(l.begin(), l.end(), [](const std::pair<float, uint32_t>& a, const std::pair<float, uint32_t>& b) {
+        return a.first < b.first || (a.first == b.first && (a.second >> 2) < (b.second >> 2));
+    });
+    return l;
+}
+
+// accumulateLinearConst (ForwardCommon.glsl:42-49 / BackwardCommon.glsl:103-110).
+inline void acc_lin_const(double t, const double c0[3], const double c1[3], double a, double out[4], double& A) {
+    A = std::exp(-a * t);
+    if (a < 1e-6) {
+        out[0] = out[1] = out[2] = out[3] = 0.0;
+        return;
+    }
+    const double K = (t + 1.0 / a) * A - 1.0 / a;
+    for (int q = 0; q < 3; ++q) out[q] = (1.0 - A) * c0[q] + K * (c0[q] - c1[q]);
+    out[3] = 1.0 - A;
+}
+
+inline bool skip(const Frag& f0, const Frag& f1) {
+    return (f0.boundary && !f0.front) && (f1.boundary && f1.front);
+}
+
+// Forward of one pixel: premultiplied colour and opacity, termination index.
+inline void composite(const Mesh& m, const Cam& k, const Params& prm, const std::vector<std::pair<float, uint32_t>>& l,
+                      int px, int py, double ray[4], uint32_t& term) {
+    ray[0] = ray[1] = ray[2] = ray[3] = 0.0;
+    const size_t n = l.size();
+    size_t i = n;
+    if (n >= 1) {
+        Frag f1 = eval(m, k, l[0].second, l[0].first, px, py, 1e-5), f0;
+        for (i = 1; i < n; ++i) {
+            if (prm.use_ert && ray[3] > 1.0 - double(prm.ert_thresh)) break;
+            f0 = f1;
+            f1 = eval(m, k, l[i].second, l[i].first, px, py, 1e-5);
+            if (skip(f0, f1)) continue;
+            const double tSeg = (f1.depth - f0.depth) / kNumSubdivs;
+            for (int s = 0; s < kNumSubdivs; ++s) {
+                const double fb = double(s) / kNumSubdivs, fm = (s + 0.5) / kNumSubdivs,
+                             fe = (s + 1.0) / kNumSubdivs;
+                double c0[3], c1[3], acc[4], A;
+                for (int q = 0; q < 3; ++q) {
+                    c0[q] = f0.col[q] + (f1.col[q] - f0.col[q]) * fb;
+                    c1[q] = f0.col[q] + (f1.col[q] - f0.col[q]) * fe;
+                }
+                const double alpha = f0.col[3] + (f1.col[3] - f0.col[3]) * fm;
+                acc_lin_const(tSeg, c0, c1, alpha * prm.attenuation, acc, A);
+                for (int q = 0; q < 3; ++q) ray[q] += (1.0 - ray[3]) * acc[q];
+                ray[3] += (1.0 - ray[3]) * acc[3];
+            }
+        }
+    }
+    term = uint32_t(i);
+}
+
+// d/dp_k of (n . (a x b)) with da/dp_k = al I, db/dp_k = be I: al (b x n) + be (n x a).
+inline V3 dcross(V3 n, V3 a, V3 b, double al, double be) { return al * cross(b, n) + be * cross(n, a); }
+
+// baryAdjoint (BackwardCommon.glsl:183-251), world point p fixed.
+inline void bary_adjoint(const Frag& fr, const double dc[4], double du, double dv, V3 dp[3], double dcol[3][4]) {
+    const V3 p = fr.p, p0 = fr.pv[0], p1 = fr.pv[1], p2 = fr.pv[2];
+    du += dc[0] * (fr.c[0][0] - fr.c[2][0]) + dc[1] * (fr.c[0][1] - fr.c[2][1]) + dc[2] * (fr.c[0][2] - fr.c[2][2]) +
+          dc[3] * (fr.c[0][3] - fr.c[2][3]);
+    dv += dc[0] * (fr.c[1][0] - fr.c[2][0]) + dc[1] * (fr.c[1][1] - fr.c[2][1]) + dc[2] * (fr.c[1][2] - fr.c[2][2]) +
+          dc[3] * (fr.c[1][3] - fr.c[2][3]);
+    const double w = 1.0 - fr.u - fr.v;
+    for (int q = 0; q < 4; ++q) {
+        dcol[0][q] = dc[q] * fr.u;
+        dcol[1][q] = dc[q] * fr.v;
+        dcol[2][q] = dc[q] * w;
+    }
+    // u = |n1| / |n0|, v = |n2| / |n0| with n0 = (p0 - p2) x (p1 - p2),
+    // n1 = (p - p1) x (p1 - p2), n2 = (p - p0) x (p0 - p2); the denominators
+    // clamped as in the GLSL (max(f0^1.5, 1e-6), max(sqrt(f), 1e-6)).
+    const V3 a0 = p0 - p2, b0 = p1 - p2, n0 = cross(a0, b0);
+    const V3 a1 = p - p1, b1 = p1 - p2, n1 = cross(a1, b1);
+    const V3 a2 = p - p0, b2 = p0 - p2, n2 = cross(a2, b2);
+    const double f0 = dot(n0, n0), f1 = dot(n1, n1), f2 = dot(n2, n2);
+    const double den0 = std::max(std::pow(f0, 1.5), 1e-6), den1 = std::max(std::sqrt(f1), 1e-6),
+                 den2 = std::max(std::sqrt(f2), 1e-6);
+    // n . dn/dp_k for the three vertices.
+    const V3 g0[3] = {dcross(n0, a0, b0, 1, 0), dcross(n0, a0, b0, 0, 1), dcross(n0, a0, b0, -1, -1)};
+    const V3 g1[3] = {V3{0, 0, 0}, dcross(n1, a1, b1, -1, 1), dcross(n1, a1, b1, 0, -1)};
+    const V3 g2[3] = {dcross(n2, a2, b2, -1, 1), V3{0, 0, 0}, dcross(n2, a2, b2, 0, -1)};
+    for (int j = 0; j < 3; ++j) {
+        const V3 du_dp = (1.0 / (den1 * den0)) * (f0 * g1[j] - f1 * g0[j]);
+        const V3 dv_dp = (1.0 / (den2 * den0)) * (f0 * g2[j] - f2 * g0[j]);
+        dp[j] = dp[j] + du * du_dp + dv * dv_dp;
+    }
+}
+
+// segmentLengthAdjoint (BackwardCommon.glsl:139-181): t = |P0 - P1| with
+// P_k = u_k p_k0 + v_k p_k1 + w_k p_k2.
+inline void seglen_adjoint(const Frag& f0, const Frag& f1, double g, double& du0, double& dv0, double& du1,
+                           double& dv1, V3 dp0[3], V3 dp1[3]) {
+    const double w0 = 1.0 - f0.u - f0.v, w1 = 1.0 - f1.u - f1.v;
+    const V3 P0 = f0.u * f0.pv[0] + f0.v * f0.pv[1] + w0 * f0.pv[2];
+    const V3 P1 = f1.u * f1.pv[0] + f1.v * f1.pv[1] + w1 * f1.pv[2];
+    const V3 D = P0 - P1;
+    const double inv = 1.0 / std::sqrt(std::max(dot(D, D), 1e-6));
+    du0 = g * dot(f0.pv[0] - f0.pv[2], D) * inv;
+    dv0 = g * dot(f0.pv[1] - f0.pv[2], D) * inv;
+    du1 = -g * dot(f1.pv[0] - f1.pv[2], D) * inv;
+    dv1 = -g * dot(f1.pv[1] - f1.pv[2], D) * inv;
+    dp0[0] = (g * f0.u * inv) * D;
+    dp0[1] = (g * f0.v * inv) * D;
+    dp0[2] = (g * w0 * inv) * D;
+    dp1[0] = (-g * f1.u * inv) * D;
+    dp1[1] = (-g * f1.v * inv) * D;
+    dp1[2] = (-g * w1 * inv) * D;
+}
+
+// Adjoint of one pixel (Backward.glsl:107-512, PER_VERTEX_COLORS).
+// skip0: reproduce the loop bound s > 0 of Backward.glsl:222 (false: s >= 0,
+// for checks of this restatement).
+inline void adjoint(const Mesh& m, const Cam& k, const Params& prm, const std::vector<std::pair<float, uint32_t>>& l,
+                    int px, int py, const double ray_out[4], uint32_t term, const double g_in[4], double* grad_pos,
+                    double* grad_col, bool skip0) {
+    const int64_t n = int64_t(l.size());
+    if (n < 2) return;
+    const int64_t tidx = prm.use_ert ? n - int64_t(term) : 0;  // farthest layers the forward did not reach
+    double ray[4] = {ray_out[0], ray_out[1], ray_out[2], ray_out[3]};
+    double dout[4] = {g_in[0], g_in[1], g_in[2], g_in[3]};
+    const double inv_n = 1.0 / kNumSubdivs;
+    // Back to front: backward index b is forward index n - 1 - b.
+    auto frag_b = [&](int64_t b) {
+        const auto& e = l[size_t(n - 1 - b)];
+        return eval(m, k, e.second, e.first, px, py, 1e-6);
+    };
+    Frag fr0 = frag_b(0), fr1;
+    for (int64_t i = 1; i < n; ++i) {
+        if (i > tidx) fr1 = fr0;
+        fr0 = frag_b(i);
+        if (i <= tidx) continue;
+        if (skip(fr0, fr1)) continue;
+        double dcf0[4] = {0, 0, 0, 0}, dcf1[4] = {0, 0, 0, 0}, dt = 0.0;
+        const double t = fr1.depth - fr0.depth, tSeg = t / kNumSubdivs;
+        for (int s = kNumSubdivs - 1; s >= (skip0 ? 1 : 0); --s) {
+            const double fb = s * inv_n, fm = (s + 0.5) * inv_n, fe = (s + 1.0) * inv_n;
+            double c0[3], c1[3], acc[4], A;
+            for (int q = 0; q < 3; ++q) {
+                c0[q] = fr0.col[q] + (fr1.col[q] - fr0.col[q]) * fb;
+                c1[q] = fr0.col[q] + (fr1.col[q] - fr0.col[q]) * fe;
+            }
+            const double alpha = fr0.col[3] + (fr1.col[3] - fr0.col[3]) * fm;
+            const double a = alpha * prm.attenuation;
+            acc_lin_const(tSeg, c0, c1, a, acc, A);
+            const double a_in = (acc[3] - ray[3]) / (acc[3] - 1.0);
+            double dacc[4];
+            for (int q = 0; q < 3; ++q) {
+                ray[q] = ray[q] - (1.0 - a_in) * acc[q];
+                dacc[q] = (1.0 - a_in) * dout[q];
+            }
+            dacc[3] = (1.0 - a_in) * dout[3];
+            dout[3] = dout[3] * (1.0 - acc[3]) - (dout[0] * acc[0] + dout[1] * acc[1] + dout[2] * acc[2]);
+            ray[3] = a_in;
+            // accumulateLinearConstAdjoint (BackwardCommon.glsl:116-133), tf = 1 / NUM_SUBDIVS.
+            const double tt = tSeg;
+            double dot_t = 0.0;
+            for (int q = 0; q < 3; ++q) dot_t += dacc[q] * (a * c0[q] + (a * c1[q] - a * c0[q]) * tt) * A;
+            dt += inv_n * (dot_t + dacc[3] * a * A);
+            double dc0[3], dc1[3], da;
+            if (a < 1e-6) {
+                da = dacc[3] * tt;
+                for (int q = 0; q < 3; ++q) {
+                    dc0[q] = dc1[q] = 0.0;
+                    da += dacc[q] * (tt * c0[q] + 0.5 * tt * tt * (c1[q] - c0[q]));
+                }
+            } else {
+                const double ia = 1.0 / a, K = (tt + ia) * A - ia;
+                da = dacc[3] * tt * A;
+                for (int q = 0; q < 3; ++q) {
+                    dc0[q] = ((1.0 - A) + K) * dacc[q];
+                    dc1[q] = -K * dacc[q];
+                    da += dacc[q] * (tt * A * c0[q] + (ia * ia - (tt * tt + ia * ia + tt * ia) * A) * (c0[q] - c1[q]));
+                }
+            }
+            da *= prm.attenuation;
+            for (int q = 0; q < 3; ++q) {
+                dcf0[q] += (1.0 - fb) * dc0[q] + (1.0 - fe) * dc1[q];
+                dcf1[q] += fb * dc0[q] + fe * dc1[q];
+            }
+            dcf0[3] += (1.0 - fm) * da;
+            dcf1[3] += fm * da;
+        }
+        double du0, dv0, du1, dv1;
+        V3 dp0[3], dp1[3];
+        seglen_adjoint(fr0, fr1, dt, du0, dv0, du1, dv1, dp0, dp1);
+        double dcol0[3][4], dcol1[3][4];
+        bary_adjoint(fr0, dcf0, du0, dv0, dp0, dcol0);
+        bary_adjoint(fr1, dcf1, du1, dv1, dp1, dcol1);
+        const bool ab = prm.use_abs_grad != 0;
+        for (int j = 0; j < 3; ++j) {
+            const V3 q0 = dp0[j], q1 = dp1[j];
+            const double g0[3] = {q0.x, q0.y, q0.z}, g1[3] = {q1.x, q1.y, q1.z};
+            for (int c = 0; c < 3; ++c) {
+                grad_pos[3 * size_t(fr0.vi[j]) + c] += ab ? std::fabs(g0[c]) : g0[c];
+                grad_pos[3 * size_t(fr1.vi[j]) + c] += ab ? std::fabs(g1[c]) : g1[c];
+            }
+            for (int c = 0; c < 4; ++c) {
+                grad_col[4 * size_t(fr0.vi[j]) + c] += ab ? std::fabs(dcol0[j][c]) : dcol0[j][c];
+                grad_col[4 * size_t(fr1.vi[j]) + c] += ab ? std::fabs(dcol1[j][c]) : dcol1[j][c];
+            }
+        }
+    }
+}
+
+// Forward (and with image_adj, the adjoint) of pixel rows of the prm range.
+int run(const uint32_t* tri, const uint32_t* fbits, int64_t F, const float* pos_f, const double* pos,
+        const double* col, int64_t V, const Camera* camp, const Params* prm, double* image, uint32_t* term,
+        const double* image_adj, double* grad_pos, double* grad_col, bool skip0) {
+    const Cam k = make(*camp);
+    int r0, r1;
+    row_range(*prm, k.c.H, r0, r1);
+    auto pf = project_all_f(pos_f, V, k.c);
+    FragLists fl = build_fragments(tri, fbits, F, pf, k.c, r0, r1);
+    Mesh m{tri, pos, col, {}};
+    m.proj.resize(size_t(V));
+    for (int64_t v = 0; v < V; ++v) m.proj[size_t(v)] = project_r<double>(k.c, pos[3 * v], pos[3 * v + 1], pos[3 * v + 2]);
+    const int W = k.c.W;
+    int nthreads = 1;
+#ifdef _OPENMP
+    nthreads = omp_get_max_threads();
+#endif
+    std::vector<std::vector<double>> gp, gc;
+    if (image_adj) {
+        gp.assign(nthreads, std::vector<double>(3 * size_t(V), 0.0));
+        gc.assign(nthreads, std::vector<double>(4 * size_t(V), 0.0));
+    }
+#pragma omp parallel
+    {
+        int tid = 0;
+#ifdef _OPENMP
+        tid = omp_get_thread_num();
+#endif
+#pragma omp for schedule(dynamic, 4)
+        for (int py = r0; py < r1; ++py)
+            for (int px = 0; px < W; ++px) {
+                const int64_t p = int64_t(py) * W + px;
+                const auto l = pixel_list(m, k, fl.records.data() + fl.offsets[p], fl.offsets[p + 1] - fl.offsets[p],
+                                          px, py);
+                double ray[4];
+                uint32_t tm;
+                composite(m, k, *prm, l, px, py, ray, tm);
+                // Clear colour blended under the premultiplied result, as the exact path does.
+                const double T = 1.0 - ray[3];
+                if (image)
+                    for (int q = 0; q < 4; ++q) image[4 * p + q] = ray[q] + T * double(prm->clear_color[q]);
+                if (term) term[p] = tm;
+                if (image_adj) {
+                    const double g[4] = {image_adj[4 * p], image_adj[4 * p + 1], image_adj[4 * p + 2],
+                                         image_adj[4 * p + 3]};
+                    adjoint(m, k, *prm, l, px, py, ray, tm, g, gp[tid].data(), gc[tid].data(), skip0);
+                }
+            }
+    }
+    if (image_adj)
+        for (int t = 0; t < nthreads; ++t) {
+            for (int64_t i = 0; i < 3 * V; ++i) grad_pos[i] += gp[t][size_t(i)];
+            for (int64_t i = 0; i < 4 * V; ++i) grad_col[i] += gc[t][size_t(i)];
+        }
+    return 0;
+}
+
+}  // namespace refmode
+
 extern "C" {
 
 // buildFacesSlim, src/Tet/TetMesh.cpp:1218-1268 (with TempFace ordering
@@ -1397,6 +1825,48 @@ int orc_num_threads(void) {
 #else
     return 1;
 #endif
+}
+
+// Reference mode (namespace refmode): forward, and the adjoint when image_adj
+// is given.  pos_f: the FP32 positions of the coverage rule.  skip0 = 0 runs
+// the adjoint over all four sub-segments (a check of this restatement).
+int orc_refmode_f64(const uint32_t* tri, const uint32_t* fbits, int64_t F, const float* pos_f, const double* pos,
+                    const double* col, int64_t V, const Camera* cam, const Params* prm, double* image,
+                    uint32_t* term, const double* image_adj, double* grad_pos, double* grad_col, int32_t skip0) {
+    return refmode::run(tri, fbits, F, pos_f, pos, col, V, cam, prm, image, term, image_adj, grad_pos, grad_col,
+                        skip0 != 0);
+}
+
+// Check hook of the reference mode's baryAdjoint: u, v of world point p on
+// face (p0, p1, p2) and their gradients w.r.t. the vertices (p fixed):
+// du[3 j + c] = du / d p_j[c], likewise dv.
+void orc_refmode_bary_uv(const double* p, const double* p0, const double* p1, const double* p2, double* u,
+                         double* v, double* du, double* dv) {
+    refmode::Frag fr;
+    fr.p = {p[0], p[1], p[2]};
+    fr.pv[0] = {p0[0], p0[1], p0[2]};
+    fr.pv[1] = {p1[0], p1[1], p1[2]};
+    fr.pv[2] = {p2[0], p2[1], p2[2]};
+    for (int j = 0; j < 3; ++j)
+        for (int q = 0; q < 4; ++q) fr.c[j][q] = 0.0;
+    const refmode::V3 d20 = fr.pv[2] - fr.pv[0], d21 = fr.pv[2] - fr.pv[1];
+    const double area = std::max(refmode::len(refmode::cross(d20, d21)), 1e-6);
+    fr.u = refmode::len(refmode::cross(d21, fr.p - fr.pv[1])) / area;
+    fr.v = refmode::len(refmode::cross(fr.p - fr.pv[0], d20)) / area;
+    *u = fr.u;
+    *v = fr.v;
+    const double zero[4] = {0, 0, 0, 0};
+    for (int which = 0; which < 2; ++which) {
+        refmode::V3 dp[3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        double dcol[3][4];
+        refmode::bary_adjoint(fr, zero, which == 0 ? 1.0 : 0.0, which == 1 ? 1.0 : 0.0, dp, dcol);
+        double* out = which == 0 ? du : dv;
+        for (int j = 0; j < 3; ++j) {
+            out[3 * j] = dp[j].x;
+            out[3 * j + 1] = dp[j].y;
+            out[3 * j + 2] = dp[j].z;
+        }
+    }
 }
 
 }  // extern "C"

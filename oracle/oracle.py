@@ -69,6 +69,12 @@ def load():
         lib.orc_render_frozen_f64.restype = ctypes.c_int
         lib.orc_render_frozen_f64.argtypes = [_vp, _vp, ctypes.c_int64, _vp, _vp, _vp, ctypes.c_int64,
                                               ctypes.POINTER(Camera), ctypes.POINTER(Params), _vp]
+        lib.orc_refmode_f64.restype = ctypes.c_int
+        lib.orc_refmode_f64.argtypes = [_vp, _vp, ctypes.c_int64, _vp, _vp, _vp, ctypes.c_int64,
+                                        ctypes.POINTER(Camera), ctypes.POINTER(Params), _vp, _vp, _vp, _vp, _vp,
+                                        ctypes.c_int32]
+        lib.orc_refmode_bary_uv.restype = None
+        lib.orc_refmode_bary_uv.argtypes = [_vp] * 8
         lib.orc_tet_faces.restype = None
         lib.orc_tet_faces.argtypes = [_vp, ctypes.c_int64, _vp]
         for name in ("orc_raytet_f64", "orc_raytet_f32"):
@@ -243,6 +249,42 @@ def raytet(faces: Faces, positions, colors, cam: Camera, prm: Params, image_adjo
     H, W = cam.height, cam.width
     out = (img.reshape(H, W, 4), tf.reshape(H, W), nseg.reshape(H, W))
     return out if gimg is None else out + (gp, gc)
+
+
+def refmode(faces: Faces, positions, colors, cam: Camera, prm: Params, image_adjoint=None, skip0: bool = True):
+    """The reference's own formulas (dtv_oracle.cpp, namespace refmode) on this
+    oracle's fragment sets: (image [H,W,4], termination [H,W]) and, with
+    image_adjoint, also the reference adjoint's (grad_positions [V,3],
+    grad_colors [V,4]).  FP64 except the FP32 depth-buffer value.  skip0=False
+    differentiates all four sub-segments (the reference skips the first)."""
+    lib = load()
+    pf = np.ascontiguousarray(positions, dtype=np.float32)
+    pos = np.ascontiguousarray(positions, dtype=np.float64)
+    col = np.ascontiguousarray(colors, dtype=np.float64)
+    V = pos.shape[0]
+    P = cam.width * cam.height
+    img = np.zeros((P, 4))
+    term = np.zeros(P, np.uint32)
+    gimg = None if image_adjoint is None else np.ascontiguousarray(image_adjoint, np.float64).reshape(-1, 4)
+    gp = np.zeros((V, 3))
+    gc = np.zeros((V, 4))
+    lib.orc_refmode_f64(_p(faces.tri), _p(faces.face_boundary), faces.num_faces, _p(pf), _p(pos), _p(col), V,
+                        ctypes.byref(cam), ctypes.byref(prm), _p(img), _p(term),
+                        None if gimg is None else _p(gimg), _p(gp), _p(gc), int(bool(skip0)))
+    H, W = cam.height, cam.width
+    out = (img.reshape(H, W, 4), term.reshape(H, W))
+    return out if gimg is None else out + (gp, gc)
+
+
+def refmode_bary_uv(p, p0, p1, p2):
+    """(u, v, du [3,3], dv [3,3]) of the reference mode's unsigned weights of
+    world point p on face (p0, p1, p2), gradients w.r.t. the vertices."""
+    lib = load()
+    arr = [np.ascontiguousarray(x, np.float64) for x in (p, p0, p1, p2)]
+    u, v = np.zeros(1), np.zeros(1)
+    du, dv = np.zeros(9), np.zeros(9)
+    lib.orc_refmode_bary_uv(*[_p(a) for a in arr], _p(u), _p(v), _p(du), _p(dv))
+    return float(u[0]), float(v[0]), du.reshape(3, 3), dv.reshape(3, 3)
 
 
 def segment_integral(t, c0, c1, a):
