@@ -1,11 +1,20 @@
 """The C-ABI library loads and exports every symbol include/*.h declares (no GPU needed)."""
 import glob
+import importlib.util
 import os
 import re
 
 import difftetvr_b200._lib as L
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def load_cpp_build():
+    """tests/cpp/build.py (compiles the C++ check program)."""
+    spec = importlib.util.spec_from_file_location("cpp_check_build", os.path.join(ROOT, "tests", "cpp", "build.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
 
 
 def declared_symbols():
@@ -36,3 +45,14 @@ def test_version_and_error_path():
     code = lib.dtv_build_hex_mesh(None, None, 1, 1, 1, None, None)
     assert code == L.DTV_ERR_ARG
     assert b"null" in lib.dtv_last_error_string()
+
+
+def test_cpp_classes_compile_against_the_headers_and_reject_bad_input():
+    """include/difftetvr_b200.hpp (TetMesh / Renderer over the C ABI) compiles
+    into a program linked to the in-tree library; its error paths that need
+    no GPU throw difftetvr_b200::Error with the C ABI's codes."""
+    import subprocess
+    exe = load_cpp_build().build()
+    res = subprocess.run([exe, "errors"], capture_output=True, text=True, timeout=60)
+    assert res.returncode == 0, res.stdout + res.stderr
+    assert "OK errors" in res.stdout
