@@ -62,10 +62,13 @@ def parse_args():
     ap.add_argument("--scale-cap-gb", type=float, default=40.0)
     ap.add_argument("--scale-recompute-gb", type=float, default=4.0)
     ap.add_argument("--batched-res", type=str, default="512,1024")
-    ap.add_argument("--batched-steps", type=int, default=3)
+    ap.add_argument("--batched-steps", type=int, default=20)
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--serving-rates", type=str, default="50,200,500,1000,2000")
     ap.add_argument("--serving-requests", type=int, default=150)
+    ap.add_argument("--serving-slots", type=int, default=4)
+    ap.add_argument("--serving-policy", choices=["fifo", "sjf"], default="sjf")
+    ap.add_argument("--serving-isolated", type=int, default=500, help="requests timed alone for the isolated p99")
     return ap.parse_args()
 
 
@@ -142,6 +145,59 @@ def ncu_traffic_per_unit():
             return json.load(f)
     except (OSError, ValueError):
         return {}
+
+
+RED_PROBE_SRC = r"""
+extern "C" __global__ void red_probe(float4* rows, unsigned nrows, unsigned iters, unsigned seed) {
+    unsigned h = (blockIdx.x * blockDim.x + threadIdx.x) * 2654435761u + seed;
+    for (unsigned i = 0; i < iters; ++i) {
+        h = h * 1664525u + 1013904223u;
+        const unsigned r = (h >> 8) % nrows;
+        atomicAdd(rows + 2 * r, make_float4(1.f, 1.f, 1.f, 0.f));
+        atomicAdd(rows + 2 * r + 1, make_float4(1.f, 1.f, 1.f, 1.f));
+    }
+}
+"""
+
+
+def l2_red_peak(num_rows: int):
+    """Float4 atomic adds per second that the L2 reduction units take when
+    every lane adds two float4 (one 32-byte row) into random rows of a table of
+    num_rows rows: the pattern of the adjoint's vertex-row atomics with no
+    other work.  Compiled at run time (NVRTC, sm_100a), launched on torch's
+    current stream, timed with CUDA events (best of 3)."""
+    import ctypes
+    import torch
+    from cuda.bindings import driver, nvrtc
+
+    err, prog = nvrtc.nvrtcCreateProgram(RED_PROBE_SRC.encode(), b"red_probe.cu", 0, [], [])
+    opts = [b"--gpu-architecture=sm_100a", b"-std=c++17"]
+    (err,) = nvrtc.nvrtcCompileProgram(prog, len(opts), opts)
+    if err != nvrtc.nvrtcResult.NVRTC_SUCCESS:
+        raise RuntimeError(f"NVRTC: {err}")
+    err, size = nvrtc.nvrtcGetCUBINSize(prog)
+    cubin = b" " * size
+    (err,) = nvrtc.nvrtcGetCUBIN(prog, cubin)
+    torch.cuda.init()
+    err, mod = driver.cuModuleLoadData(cubin)
+    if err != driver.CUresult.CUDA_SUCCESS:
+        raise RuntimeError(f"cuModuleLoadData: {err}")
+    err, fn = driver.cuModuleGetFunction(mod, b"red_probe")
+    rows = torch.zeros(2 * num_rows, 4, device="cuda")
+    blocks, threads, iters = 148 * 8, 256, 128
+    stream = torch.cuda.current_stream().cuda_stream
+    args = ((rows.data_ptr(), num_rows, iters, 7), (ctypes.c_void_p, ctypes.c_uint, ctypes.c_uint, ctypes.c_uint))
+    best = None
+    for _ in range(4):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        (err,) = driver.cuLaunchKernel(fn, blocks, 1, 1, threads, 1, 1, 0, stream, args, 0)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        best = ms if best is None else min(best, ms)
+    driver.cuModuleUnload(mod)
+    return 2.0 * blocks * threads * iters / (best / 1e3)
 
 
 # ---------------------------------------------------------------------------
@@ -353,6 +409,30 @@ def run_ours(args, rank, world):
     roofline = {"bound": "hbm", "kernel": dominant, "achieved": round(achieved, 1), "peak": peak,
                 "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
                 "traffic": traffic, "algorithmic_bytes": algo[dominant], "kernel_ms": avg[dominant]}
+    # The adjoint is bound by instruction issue and its vertex-row atomics, not
+    # by HBM: its issue rate against 148 SMs x 4 schedulers x the sampled SM
+    # clock, and its float4 atomic rate against the probe's, from the
+    # per-fragment counts of one ncu capture (profiles/roofline_traffic.json).
+    prof = ncu_traffic_per_unit().get("adjoint", {})
+    t_adj = avg.get("adjoint", 0.0) / 1e3
+    if t_adj > 0 and "warp_inst_per_fragment" in prof:
+        sm_hz = (clk.get("sm_mhz") or 1965.0) * 1e6
+        inst = float(prof["warp_inst_per_fragment"]) * nf / t_adj
+        roofline["issue"] = {"kernel": "adjoint", "achieved_warp_inst_per_s": inst,
+                             "peak_warp_inst_per_s": 148 * 4 * sm_hz, "frac": round(inst / (148 * 4 * sm_hz), 4),
+                             "warp_inst_per_fragment": prof["warp_inst_per_fragment"]}
+    if t_adj > 0 and "red_float4_per_fragment" in prof:
+        try:
+            red_peak = l2_red_peak(V)
+        except Exception as exc:  # the probe is a report, not part of the step
+            red_peak = None
+            roofline["l2_red_error"] = str(exc)[:200]
+        if red_peak:
+            red = float(prof["red_float4_per_fragment"]) * nf / t_adj
+            roofline["l2_red"] = {"kernel": "adjoint", "achieved_float4_per_s": red, "peak_float4_per_s": red_peak,
+                                  "frac": round(red / red_peak, 4), "per_fragment": prof["red_float4_per_fragment"],
+                                  "peak_source": "float4 atomicAdd probe over random 32-byte rows of a "
+                                                 f"{V}-row table (bench.py l2_red_peak)"}
 
     result = {
         "metric": METRIC, "value": value, "unit": "iter/s", "n_gpus": world, "steps": K, "warmup": args.warmup,
@@ -561,8 +641,11 @@ def run_batched(args, res: int, steps: int, warmup: int = 2):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / n
 
+    from difftetvr_b200.autotune import autotune_batch, autotune_renderer
+
     meshes = [mk(n, 1 + i) for i, n in enumerate(sizes)]
     br = BatchRenderer(meshes, attenuation=1.0)
+    tuned_batch = autotune_batch(br, views)["tuning"]
     br.set_graph(True)
     ms_batched = timed(lambda i: br.train_step(views, lr_positions=LR_POS, lr_colors=LR_COL, clamp_colors=1), steps)
     info = br.info()
@@ -596,12 +679,46 @@ def run_batched(args, res: int, steps: int, warmup: int = 2):
         for o in opts:
             o.step()
 
+    # Each plain renderer tuned on its own mesh's first view, as the batch is.
+    for mi, r in enumerate(rends):
+        r.set_view_matrix(next(v.view_matrix for v in views if v.mesh == mi))
+        autotune_renderer(r)
     ms_plain = timed(plain_step, steps)
+    # Where the plain loop's time goes: one more step with per-view stage
+    # events.  busy = the sum of the stage times (device work); the rest of
+    # the step is launch and host time between views, which is what one launch
+    # per stage over all views can remove.  plain / busy bounds the speed-up
+    # of batching that keeps per-fragment work as it is.
+    for r in rends:
+        r.set_stage_timing(True)
+    busy = {f"{n}^3": 0.0 for n in sizes}
+    stage_busy = {}
+    for o in opts:
+        o.zero_grad(set_to_none=False)
+    for v in views:
+        r = rends[v.mesh]
+        r.set_view_matrix(v.view_matrix)
+        img = r.render()
+        _lib.call("dtv_loss_l2", img.data_ptr(), v.target.data_ptr(), n_img, 1.0 / n_img, adj.data_ptr(),
+                  loss.data_ptr(), stream.cuda_stream)
+        r.render_adjoint(adj)
+        st = r.get_stage_times()
+        busy[f"{sizes[v.mesh]}^3"] += sum(st.values())
+        for k2, v2 in st.items():
+            stage_busy[k2] = stage_busy.get(k2, 0.0) + v2
+    for r in rends:
+        r.set_stage_timing(False)
+    busy_total = sum(busy.values())
     nv = len(views)
     return {"res": res, "views": nv, "views_per_mesh": counts, "meshes": [f"{n}^3" for n in sizes],
             "batched_views_per_s": nv / (ms_batched / 1e3), "plain_views_per_s": nv / (ms_plain / 1e3),
             "batched_ms_per_step": ms_batched, "plain_ms_per_step": ms_plain,
             "speedup": ms_plain / ms_batched, "fragments_per_step": info["fragments"],
+            "plain_device_busy_ms": {k2: round(v2, 3) for k2, v2 in busy.items()},
+            "plain_stage_busy_ms": {k2: round(v2, 3) for k2, v2 in stage_busy.items()},
+            "plain_overhead_ms": round(ms_plain - busy_total, 3),
+            "speedup_bound_same_kernels": round(ms_plain / busy_total, 3) if busy_total > 0 else None,
+            "tuning_batch": tuned_batch,
             "graph": info["graph"], "steps": steps, "warmup": warmup}
 
 
@@ -609,9 +726,11 @@ def run_serving(args):
     """Serving config: Kuhn 16^3 / 32^3 / 64^3 meshes resident; Poisson arrivals
     at each rate; resolution 256^2 / 512^2 / 1024^2 with weights 0.5 / 0.3 / 0.2;
     70 % forward-only, 30 % forward + adjoint against a supplied target image.
-    Continuous batching over 2 slots, admission by fragment storage.  Reports
-    p50 / p99 latency and throughput per rate beside the latency of the same
-    kind of requests served alone (serial plain solves)."""
+    Continuous batching over --serving-slots slots, admission by fragment
+    storage (shortest estimate first with a 20 ms age bound, or arrival order).
+    Reports p50 / p99 latency and throughput per rate beside the latency of the
+    same kind of requests served alone (serial plain solves, --serving-isolated
+    of them)."""
     import numpy as np
     import torch
 
@@ -627,7 +746,7 @@ def run_serving(args):
         m.set_use_gradients(True)
         m.set_tet_mesh_data(cells, pos, S.gaussian_colors(pos, seed=20 + i))
         meshes[k] = m
-    be = GpuBackend(meshes, slots=2)
+    be = GpuBackend(meshes, slots=args.serving_slots)
     be.calibrate(S.sphere_camera(0), res=256)
     res_choices, res_w = [256, 512, 1024], [0.5, 0.3, 0.2]
     targets = {r: torch.rand(r, r, 4, device="cuda", generator=torch.Generator(device="cuda").manual_seed(r))
@@ -669,14 +788,15 @@ def run_serving(args):
             for mode in ("gradient", "forward"):
                 solve_alone(Request(mesh=k, view_matrix=S.sphere_camera(1), width=res, height=res, mode=mode,
                                     target=targets[res] if mode == "gradient" else None))
-    iso = np.array([solve_alone(q) for q in make_requests(np.random.default_rng(7), 80)])
+    iso = np.array([solve_alone(q) for q in make_requests(np.random.default_rng(7), args.serving_isolated)])
     out = {"meshes": list(names), "resolutions": res_choices, "resolution_weights": res_w, "gradient_fraction": 0.3,
-           "slots": be.slots, "isolated": {"p50_ms": float(np.percentile(iso, 50)),
-                                            "p99_ms": float(np.percentile(iso, 99))}, "rates": []}
+           "slots": be.slots, "policy": args.serving_policy,
+           "isolated": {"requests": int(iso.size), "p50_ms": float(np.percentile(iso, 50)),
+                        "p99_ms": float(np.percentile(iso, 99))}, "rates": []}
     budget = int(max(be.fragments_per_pixel(k) for k in names) * 1024 * 1024 * 4)
     be.reserve(32, max(res_choices) ** 2, int(1.5 * budget))
     # Warm-up pass (first batches of each slot), not reported.
-    eng = ServingEngine(be, budget_fragments=budget, max_batch=32)
+    eng = ServingEngine(be, budget_fragments=budget, max_batch=32, policy=args.serving_policy)
     eng.start()
     for f in [eng.submit(q) for q in make_requests(np.random.default_rng(3), 24)]:
         f.result(timeout=600)
@@ -685,7 +805,7 @@ def run_serving(args):
         rng = np.random.default_rng(int(rate))
         reqs = make_requests(rng, args.serving_requests)
         gaps = rng.exponential(1.0 / rate, size=len(reqs))
-        eng = ServingEngine(be, budget_fragments=budget, max_batch=32)
+        eng = ServingEngine(be, budget_fragments=budget, max_batch=32, policy=args.serving_policy)
         eng.start()
         t = time.perf_counter()
         # The client takes each result as it completes (so result tensors are
@@ -704,6 +824,7 @@ def run_serving(args):
         eng.stop()
         st = eng.latency_stats()
         st["rate_rps"] = rate
+        st["p99_over_isolated_p99"] = round(st["p99_ms"] / out["isolated"]["p99_ms"], 3)
         out["rates"].append(st)
     return out
 

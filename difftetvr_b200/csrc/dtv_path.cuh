@@ -342,6 +342,15 @@ __device__ __forceinline__ uint32_t record_lo(const u64* __restrict__ records, u
 }
 
 // ---------------------------------------------------------------------------
+// Whether every sub-segment of a segment has a > 0 and x = a t < 1/8 (the
+// short tier).  The sub-segment densities are affine in s, so their extremes
+// are at the end sub-segments (the inner ones can exceed them only by
+// rounding, where the series is still accurate).
+__device__ __forceinline__ bool short_tier_of(const float (&av)[kNumSubdivs], float tSeg) {
+    const float lo = fminf(av[0], av[kNumSubdivs - 1]), hi = fmaxf(av[0], av[kNumSubdivs - 1]);
+    return (lo > 0.f) & (hi * tSeg < 0.125f);
+}
+
 // One segment of a pixel's ray between a front fragment (colour cf) and a back
 // fragment (colour cb): the 4-sub-segment integral (ForwardCommon.glsl:42-49
 // per sub-segment, colour and density linear along the segment), front to
@@ -355,12 +364,9 @@ __device__ __forceinline__ void segment_composite(float tSeg, const float4& cf, 
                                                   float& C0, float& C1, float& C2, TransF& T) {
     const float d0 = cb.x - cf.x, d1 = cb.y - cf.y, d2 = cb.z - cf.z, dw = cb.w - cf.w;
     float av[kNumSubdivs];
-    bool short_tier = true;
 #pragma unroll
-    for (int s = 0; s < kNumSubdivs; ++s) {
-        av[s] = (cf.w + dw * (0.25f * (s + 0.5f))) * atten;
-        short_tier &= (av[s] > 0.f) & (av[s] * tSeg < 0.125f);
-    }
+    for (int s = 0; s < kNumSubdivs; ++s) av[s] = (cf.w + dw * (0.25f * (s + 0.5f))) * atten;
+    const bool short_tier = short_tier_of(av, tSeg);
     // Sub-segment s adds w (cf + fs d) - k d per channel; summed over the
     // sub-segments that is cf sum(w) + d sum(w fs - k), two scalars.
     float ws = 0.f, ds = 0.f;
@@ -651,12 +657,9 @@ __device__ __forceinline__ void segment_adjoint(float tSeg, float cfw, float cbw
                                                 float& ab) {
     const float dp = pb - pf, D = 0.25f * dp, dw = cbw - cfw;
     float av[kNumSubdivs];
-    bool short_tier = true;
 #pragma unroll
-    for (int s = 0; s < kNumSubdivs; ++s) {
-        av[s] = (cfw + dw * (0.25f * (s + 0.5f))) * atten;
-        short_tier &= (av[s] > 0.f) & (av[s] * tSeg < 0.125f);
-    }
+    for (int s = 0; s < kNumSubdivs; ++s) av[s] = (cfw + dw * (0.25f * (s + 0.5f))) * atten;
+    const bool short_tier = short_tier_of(av, tSeg);
     // One sub-segment, back to front; st is used only when a > 0.  (This
     // path runs when some sub-segment of the segment has x >= 1/8: T and gT
     // change by large steps there, taken on hi with lo scaled along.)
@@ -715,9 +718,9 @@ __device__ __forceinline__ void segment_adjoint(float tSeg, float cfw, float cbw
             const float P0 = pf + fs * dp;
             const float Tout = s == kNumSubdivs - 1 ? Tout_seg : Tin[s + 1];
             const float gTo = g;
-            const float c = st[s].omA * P0 - st[s].K * D;
-            g = __fmaf_rn(-gTo, st[s].omA, gTo) + c;
-            dg += __fmaf_rn(-gTo, st[s].omA, c);
+            const float dgs = __fmaf_rn(-gTo, st[s].omA, st[s].omA * P0 - st[s].K * D);  // gTo (A - 1) + ...
+            g = gTo + dgs;
+            dg += dgs;
             gl += (av[s] * Tout) * (P0 + tSeg * D - gTo);
             const float g_a = Tin[s] * (tSeg * st[s].A * (P0 - gTo) - st[s].dK * D);
             const float tw = Tin[s] * st[s].omA;

@@ -4,8 +4,9 @@ Requests (forward renders, or forward + adjoint against a supplied target
 image) of mixed resolution arrive at any time.  The engine batches them with
 continuous batching: it keeps a small number of execution slots (each a CUDA
 stream with its own batch renderer and fragment storage); whenever a slot is
-free it admits queued requests in arrival order while their estimated
-fragment storage fits the slot's budget, launches the batch asynchronously,
+free it admits queued requests (in arrival order, or smallest estimate first
+with an age bound) while their estimated fragment storage fits the slot's
+budget, launches the batch asynchronously,
 and goes back to admitting - so requests that arrive while other batches run
 on the GPU start as soon as a slot and memory are free, and the batches of
 different slots overlap on the device.  Results are delivered through
@@ -72,11 +73,20 @@ class ServingEngine:
       - observe(mesh, pixels, fragments) (optional; refines the estimate)
     """
 
-    def __init__(self, backend, budget_fragments: int, max_batch: int = 32, poll_s: float = 5e-5):
+    def __init__(self, backend, budget_fragments: int, max_batch: int = 32, poll_s: float = 5e-5,
+                 policy: str = "fifo", age_ms: float = 20.0):
+        """policy "fifo": admit in arrival order.  "sjf": requests queued for
+        at least age_ms first (in arrival order), then the rest by estimated
+        fragments, smallest first, so small requests do not wait behind large
+        ones and no request waits longer than about age_ms plus one batch."""
+        if policy not in ("fifo", "sjf"):
+            raise ValueError("policy must be 'fifo' or 'sjf'")
         self.backend = backend
         self.budget = int(budget_fragments)
         self.max_batch = int(max_batch)
         self.poll_s = poll_s
+        self.policy = policy
+        self.age_s = age_ms / 1e3
         self.queue: deque[Request] = deque()
         self.lock = threading.Lock()
         self.cv = threading.Condition(self.lock)
@@ -118,14 +128,33 @@ class ServingEngine:
 
     # -- engine ------------------------------------------------------------
     def admit(self) -> list[Request]:
-        """Requests for the next batch: arrival order, within the budget."""
+        """Requests for the next batch within the budget, in the policy's order."""
         batch, frags = [], 0.0
-        while self.queue and len(batch) < self.max_batch:
-            e = self.estimate(self.queue[0])
-            if batch and frags + e > self.budget:
+        if self.policy == "fifo":
+            while self.queue and len(batch) < self.max_batch:
+                e = self.estimate(self.queue[0])
+                if batch and frags + e > self.budget:
+                    break
+                batch.append(self.queue.popleft())
+                frags += e
+            return batch
+        now = time.perf_counter()
+        aged = [r for r in self.queue if now - r.t_arrival >= self.age_s]
+        fresh = sorted((r for r in self.queue if now - r.t_arrival < self.age_s), key=self.estimate)
+        taken = set()
+        for r in aged + fresh:
+            if len(batch) >= self.max_batch:
                 break
-            batch.append(self.queue.popleft())
+            e = self.estimate(r)
+            if batch and frags + e > self.budget:
+                if r in aged:
+                    break  # an aged request waits for the next batch, not behind younger ones
+                continue
+            batch.append(r)
+            taken.add(id(r))
             frags += e
+        if taken:
+            self.queue = deque(r for r in self.queue if id(r) not in taken)
         return batch
 
     def step(self) -> bool:

@@ -105,3 +105,36 @@ def test_cancel_pending_requests():
     assert n >= 3
     assert sum(f.cancelled() for f in futs) == n
     assert all(f.done() for f in futs)
+
+
+def test_sjf_admits_small_requests_first_and_aged_ones_before_them():
+    """Shortest-estimate-first admission with an age bound: among fresh
+    requests the smallest go first; a request queued longer than the age
+    bound goes before all fresh ones."""
+    be = FakeBackend(slots=1, delay=0.0)
+    eng = ServingEngine(be, budget_fragments=10 * 64 * 64 * 4, max_batch=2, policy="sjf", age_ms=1e6)
+    big, small1, small2 = req(64, 64), req(16, 16), req(16, 16)
+    for i, r in enumerate((big, small1, small2)):
+        r.id, r.t_arrival = i, time.perf_counter()
+        eng.queue.append(r)
+    first = eng.admit()
+    assert [r.id for r in first] == [1, 2]
+    assert [r.id for r in eng.queue] == [0]
+    # The same queue with the big request aged past the bound.
+    eng2 = ServingEngine(be, budget_fragments=10 * 64 * 64 * 4, max_batch=2, policy="sjf", age_ms=5.0)
+    big2, small3 = req(64, 64), req(16, 16)
+    big2.id, big2.t_arrival = 0, time.perf_counter() - 1.0
+    small3.id, small3.t_arrival = 1, time.perf_counter()
+    eng2.queue.extend([small3, big2])
+    assert [r.id for r in eng2.admit()] == [0, 1]
+    with pytest.raises(ValueError):
+        ServingEngine(be, budget_fragments=1, policy="lifo")
+
+
+def test_sjf_completes_every_request():
+    be = FakeBackend(slots=2, delay=0.002)
+    eng = ServingEngine(be, budget_fragments=10 * 32 * 32 * 3, max_batch=4, policy="sjf", age_ms=5.0)
+    eng.start()
+    futs = [eng.submit(req(16 if i % 3 else 32, 16 if i % 3 else 32)) for i in range(30)]
+    assert sorted(f.result(timeout=10).request_id for f in futs) == list(range(30))
+    eng.stop()
