@@ -65,8 +65,13 @@ def parse_args():
     ap.add_argument("--batched-steps", type=int, default=20)
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--serving-rates", type=str, default="50,200,500,1000,2000")
-    ap.add_argument("--serving-requests", type=int, default=150)
+    ap.add_argument("--serving-requests", type=int, default=150,
+                    help="requests per rate (at least one second of arrivals is used, up to 1000)")
     ap.add_argument("--serving-slots", type=int, default=4)
+    ap.add_argument("--serving-batch-mfrags", type=float, default=16.0,
+                    help="estimated fragments (millions) a serving batch is filled to")
+    ap.add_argument("--serving-priority-slots", type=int, default=0,
+                    help="slots on a high-priority stream taking the largest queued request alone")
     ap.add_argument("--serving-policy", choices=["fifo", "sjf"], default="sjf")
     ap.add_argument("--serving-isolated", type=int, default=500, help="requests timed alone for the isolated p99")
     return ap.parse_args()
@@ -580,11 +585,18 @@ def run_scale(args):
         nf = r.get_num_fragments()
         bands = r.get_num_bands()
         covered = int((img[..., 3] > 0).sum())
+        # Stage times from one more step with stage events (not in the timed loop).
+        r.set_stage_timing(True)
+        step()
+        torch.cuda.synchronize()
+        stage = {k: round(v, 3) for k, v in r.get_stage_times().items()}
+        r.set_stage_timing(False)
         out["modes"].append({
             "mode": name, "budget_bytes": budget, "bands": bands, "ms_per_step": ms, "iter_per_s": 1e3 / ms,
             "fragments": nf, "record_bytes": 8 * nf,
             "record_bytes_held": 8 * nf if bands == 0 else min(8 * nf, budget),
-            "mean_list_length_covered": nf / max(covered, 1), "fragments_per_s": nf / (ms / 1e3)})
+            "mean_list_length_covered": nf / max(covered, 1), "fragments_per_s": nf / (ms / 1e3),
+            "stage_ms": stage})
     del diff, r, mesh
     torch.cuda.empty_cache()
     return out
@@ -727,7 +739,9 @@ def run_serving(args):
     at each rate; resolution 256^2 / 512^2 / 1024^2 with weights 0.5 / 0.3 / 0.2;
     70 % forward-only, 30 % forward + adjoint against a supplied target image.
     Continuous batching over --serving-slots slots, admission by fragment
-    storage (shortest estimate first with a 20 ms age bound, or arrival order).
+    storage (shortest estimate first with a 20 ms age bound, or arrival order);
+    the first --serving-priority-slots slots run on a high-priority stream and
+    take the largest queued request alone.
     Reports p50 / p99 latency and throughput per rate beside the latency of the
     same kind of requests served alone (serial plain solves, --serving-isolated
     of them)."""
@@ -746,7 +760,7 @@ def run_serving(args):
         m.set_use_gradients(True)
         m.set_tet_mesh_data(cells, pos, S.gaussian_colors(pos, seed=20 + i))
         meshes[k] = m
-    be = GpuBackend(meshes, slots=args.serving_slots)
+    be = GpuBackend(meshes, slots=args.serving_slots, priority_slots=args.serving_priority_slots)
     be.calibrate(S.sphere_camera(0), res=256)
     res_choices, res_w = [256, 512, 1024], [0.5, 0.3, 0.2]
     targets = {r: torch.rand(r, r, 4, device="cuda", generator=torch.Generator(device="cuda").manual_seed(r))
@@ -790,22 +804,26 @@ def run_serving(args):
                                     target=targets[res] if mode == "gradient" else None))
     iso = np.array([solve_alone(q) for q in make_requests(np.random.default_rng(7), args.serving_isolated)])
     out = {"meshes": list(names), "resolutions": res_choices, "resolution_weights": res_w, "gradient_fraction": 0.3,
-           "slots": be.slots, "policy": args.serving_policy,
+           "slots": be.slots, "priority_slots": be.priority_slots, "policy": args.serving_policy,
+           "batch_fragments": int(args.serving_batch_mfrags * 1e6),
            "isolated": {"requests": int(iso.size), "p50_ms": float(np.percentile(iso, 50)),
                         "p99_ms": float(np.percentile(iso, 99))}, "rates": []}
     budget = int(max(be.fragments_per_pixel(k) for k in names) * 1024 * 1024 * 4)
     be.reserve(32, max(res_choices) ** 2, int(1.5 * budget))
     # Warm-up pass (first batches of each slot), not reported.
-    eng = ServingEngine(be, budget_fragments=budget, max_batch=32, policy=args.serving_policy)
+    batch_frags = int(args.serving_batch_mfrags * 1e6)
+    eng = ServingEngine(be, budget_fragments=budget, max_batch=32, policy=args.serving_policy,
+                        batch_fragments=batch_frags)
     eng.start()
     for f in [eng.submit(q) for q in make_requests(np.random.default_rng(3), 24)]:
         f.result(timeout=600)
     eng.stop()
     for rate in [float(x) for x in args.serving_rates.split(",") if x]:
         rng = np.random.default_rng(int(rate))
-        reqs = make_requests(rng, args.serving_requests)
+        reqs = make_requests(rng, max(args.serving_requests, min(int(rate), 1000)))
         gaps = rng.exponential(1.0 / rate, size=len(reqs))
-        eng = ServingEngine(be, budget_fragments=budget, max_batch=32, policy=args.serving_policy)
+        eng = ServingEngine(be, budget_fragments=budget, max_batch=32, policy=args.serving_policy,
+                            batch_fragments=batch_frags)
         eng.start()
         t = time.perf_counter()
         # The client takes each result as it completes (so result tensors are

@@ -10,8 +10,14 @@ from __future__ import annotations
 import torch
 
 TILES = (0, 1, 2)               # 16x16, 32x8, 8x32 pixels per 256-thread block
-SORT_CLASSES = (1, 2, 3, 4)     # lists of up to 64, 128, 256, 512 records
+SORT_CLASSES = (1, 2, 3, 4, 5)  # lists of up to 64, 128, 256, 512, 1024 records
 SORT_METHODS = ("bucket", "surrogate", "network")
+
+
+def methods_for(c: int) -> tuple:
+    """Sort methods available to list-length class c (no surrogate keys for
+    the shared-memory class 5)."""
+    return SORT_METHODS if c <= 4 else ("bucket", "network")
 
 
 def sort_method(tuning: dict, c: int) -> str:
@@ -96,7 +102,7 @@ def autotune_renderer(renderer, trials: int = 3, force: bool = False) -> dict:
             if ms < best_ms:
                 best, best_ms = cand, ms
     for c in SORT_CLASSES:
-        for method in SORT_METHODS:
+        for method in methods_for(c):
             if method == sort_method(best, c):
                 continue
             cand = with_sort_method(best, c, method)
@@ -128,7 +134,7 @@ def autotune_batch(batch_renderer, views, trials: int = 2, force: bool = False) 
     best = batch_renderer.get_tuning()
     best_ms = measure(best)
     for c in SORT_CLASSES:
-        for method in SORT_METHODS:
+        for method in methods_for(c):
             if method == sort_method(best, c):
                 continue
             cand = with_sort_method(best, c, method)

@@ -641,8 +641,8 @@ int32_t dtv_renderer_set_tuning(dtv_renderer* r, const dtv_tuning* t) {
         require(r && t, "null pointer");
         require(t->composite_tile >= 0 && t->composite_tile <= 2 && t->adjoint_tile >= 0 && t->adjoint_tile <= 2,
                 "tile index must be 0, 1 or 2");
-        require((t->sort_surrogate_classes & ~0x1eu) == 0 && (t->sort_bucket_classes & ~0x1eu) == 0,
-                "sort class masks use bits 1..4 only");
+        require((t->sort_surrogate_classes & ~0x1eu) == 0 && (t->sort_bucket_classes & ~0x3eu) == 0,
+                "sort class masks: surrogate bits 1..4, bucket bits 1..5");
         r->tuning = *t;
     });
 }

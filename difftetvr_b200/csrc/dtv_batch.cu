@@ -650,8 +650,8 @@ int32_t dtv_batch_create(dtv_batch** out) {
 int32_t dtv_batch_set_tuning(dtv_batch* b, const dtv_tuning* t) {
     return guarded([&] {
         require(b && t, "null pointer");
-        require((t->sort_surrogate_classes & ~0x1eu) == 0 && (t->sort_bucket_classes & ~0x1eu) == 0,
-                "sort class masks use bits 1..4 only");
+        require((t->sort_surrogate_classes & ~0x1eu) == 0 && (t->sort_bucket_classes & ~0x3eu) == 0,
+                "sort class masks: surrogate bits 1..4, bucket bits 1..5");
         if ((b->sort_surrogate_classes != t->sort_surrogate_classes ||
              b->sort_bucket_classes != t->sort_bucket_classes) && b->exec) {
             // The captured step holds the old sort launches.

@@ -62,7 +62,7 @@ constexpr size_t sort_scratch_elems(uint64_t P) { return 16 + size_t(kSortClasse
 // 256, 512 records) is sorted through 32-bit surrogate keys, else through the
 // 64-bit network (same result either way).
 constexpr uint32_t kSortSurrogateDefault = 0x1eu;
-constexpr uint32_t kSortBucketDefault = 0x1cu;  // classes sorted by distribution (bit c: class c, 2..4)
+constexpr uint32_t kSortBucketDefault = 0x3cu;  // classes sorted by distribution (bit c: class c, 2..5)
 void launch_sort(const unsigned long long* offsets, unsigned long long* records, uint32_t P, uint32_t* scratch,
                  cudaStream_t s, const uint32_t* ok = nullptr,
                  uint32_t surrogate_classes = kSortSurrogateDefault, uint32_t bucket_classes = kSortBucketDefault);

@@ -709,6 +709,109 @@ __global__ void __launch_bounds__(kSortWarps * 32) k_sort_class_smem(const u64* 
     }
 }
 
+// Class 5 by distribution: one warp per list of 513..1024 records in shared
+// memory.  Records are bucketed by depth over the list's range (n buckets,
+// bucket index monotone in the depth; equal depths share a bucket), the
+// buckets counted, scanned and scattered with shared-memory atomics, and each
+// bucket put in exact (depth, face) order by an insertion sort on the 64-bit
+// records.  Buckets hold about one record each; a list whose largest bucket
+// exceeds kBucketInsertMax records (depths clustered) is sorted by the
+// bitonic network instead.  O(n) work against the network's
+// O(n log^2 n).
+constexpr int kSortBucketWarps = 4;
+constexpr uint32_t kBucketInsertMax = 64;
+
+__global__ void __launch_bounds__(kSortBucketWarps * 32) k_sort_class_smem_bucket(
+    const u64* __restrict__ offsets, u64* records, const uint32_t* __restrict__ items,
+    const uint32_t* __restrict__ count, const uint32_t* __restrict__ ok) {
+    if (ok && *ok == 0u) return;
+    extern __shared__ u64 sm_sort[];
+    constexpr uint32_t C = kSortWarpCap;
+    const uint32_t num = *count;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    u64* in = sm_sort + size_t(warp) * (2 * C + C / 2);
+    u64* out = in + C;
+    uint32_t* cnt = reinterpret_cast<uint32_t*>(out + C);
+    for (uint32_t it = blockIdx.x * kSortBucketWarps + warp; it < num; it += gridDim.x * kSortBucketWarps) {
+        const uint32_t p = items[it];
+        const u64 beg = offsets[p];
+        const uint32_t n = uint32_t(offsets[p + 1] - beg);
+        u64* r = records + beg;
+        float dmin = 3.4e38f, dmax = 0.f;
+        for (uint32_t j = lane; j < n; j += 32) {
+            const u64 v = r[j];
+            in[j] = v;
+            const float d = __uint_as_float(uint32_t(v >> 32));
+            dmin = fminf(dmin, d);
+            dmax = fmaxf(dmax, d);
+            cnt[j] = 0u;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            dmin = fminf(dmin, __shfl_xor_sync(kFull, dmin, o));
+            dmax = fmaxf(dmax, __shfl_xor_sync(kFull, dmax, o));
+        }
+        const float scale = dmax > dmin ? float(n) / (dmax - dmin) : 0.f;
+        __syncwarp();
+        auto bucket = [&](u64 v) {
+            return min(uint32_t((__uint_as_float(uint32_t(v >> 32)) - dmin) * scale), n - 1u);
+        };
+        for (uint32_t j = lane; j < n; j += 32) atomicAdd(&cnt[bucket(in[j])], 1u);
+        __syncwarp();
+        // Exclusive scan of the counts; lane owns counters [lane * k, lane * k + k).
+        const uint32_t k = (n + 31) / 32, c0 = min(uint32_t(lane) * k, n), c1 = min(c0 + k, n);
+        uint32_t tot = 0, mx = 0;
+        for (uint32_t b = c0; b < c1; ++b) {
+            tot += cnt[b];
+            mx = max(mx, cnt[b]);
+        }
+        uint32_t incl = tot;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(kFull, incl, o);
+            if (lane >= o) incl += t;
+            mx = max(mx, __shfl_xor_sync(kFull, mx, o));
+        }
+        if (mx > kBucketInsertMax) {
+            // Clustered depths: the bitonic network on the list padded to 1024.
+            for (uint32_t j = n + lane; j < C; j += 32) in[j] = ~0ull;
+            __syncwarp();
+            bitonic_smem<false>(in, C, lane, 32);
+            for (uint32_t j = lane; j < n; j += 32) r[j] = in[j];
+            __syncwarp();
+            continue;
+        }
+        uint32_t run = incl - tot;
+        for (uint32_t b = c0; b < c1; ++b) {
+            const uint32_t c = cnt[b];
+            cnt[b] = run;
+            run += c;
+        }
+        __syncwarp();
+        for (uint32_t j = lane; j < n; j += 32) {
+            const u64 v = in[j];
+            out[atomicAdd(&cnt[bucket(v)], 1u)] = v;
+        }
+        __syncwarp();
+        // cnt[b] is now the end of bucket b (the start of bucket b + 1).
+        for (uint32_t b = lane; b < n; b += 32) {
+            const uint32_t s0 = b ? cnt[b - 1] : 0u, s1 = cnt[b];
+            for (uint32_t i = s0 + 1; i < s1; ++i) {
+                const u64 v = out[i];
+                uint32_t j = i;
+                while (j > s0 && out[j - 1] > v) {
+                    out[j] = out[j - 1];
+                    --j;
+                }
+                out[j] = v;
+            }
+        }
+        __syncwarp();
+        for (uint32_t j = lane; j < n; j += 32) r[j] = out[j];
+        __syncwarp();
+    }
+}
+
 // Class 6: one block per list.
 __global__ void __launch_bounds__(1024) k_sort_class_block(const u64* __restrict__ offsets, u64* records,
                                                            const uint32_t* __restrict__ items,
@@ -832,9 +935,12 @@ void launch_sort(const u64* offsets, u64* records, uint32_t P, uint32_t* scratch
                  const uint32_t* ok, uint32_t surrogate_classes, uint32_t bucket_classes) {
     static bool attr_set = false;
     const size_t smem_warp = size_t(kSortWarps) * kSortWarpCap * sizeof(u64);
+    const size_t smem_bucket = size_t(kSortBucketWarps) * (2 * kSortWarpCap + kSortWarpCap / 2) * sizeof(u64);
     const size_t smem_block = size_t(kSortBlockCap) * sizeof(u64);
     if (!attr_set) {
         cudaFuncSetAttribute(k_sort_class_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_warp));
+        cudaFuncSetAttribute(k_sort_class_smem_bucket, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(smem_bucket));
         cudaFuncSetAttribute(k_sort_class_block, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_block));
         cudaFuncSetAttribute(k_sort_class_long, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_block));
         attr_set = true;
@@ -857,8 +963,12 @@ void launch_sort(const u64* offsets, u64* records, uint32_t P, uint32_t* scratch
     sort_class<4>(q(2), g, offsets, records, items(2), scratch + 2, redo_n, redo, ok, s);
     sort_class<8>(q(3), g, offsets, records, items(3), scratch + 3, redo_n, redo, ok, s);
     sort_class<16>(q(4), g, offsets, records, items(4), scratch + 4, redo_n, redo, ok, s);
-    k_sort_class_smem<<<std::min(g, 296u), kSortWarps * 32, smem_warp, s>>>(offsets, records, items(5), scratch + 5,
-                                                                            ok);
+    if ((bucket_classes >> 5) & 1u)
+        k_sort_class_smem_bucket<<<296, kSortBucketWarps * 32, smem_bucket, s>>>(offsets, records, items(5),
+                                                                                 scratch + 5, ok);
+    else
+        k_sort_class_smem<<<std::min(g, 296u), kSortWarps * 32, smem_warp, s>>>(offsets, records, items(5),
+                                                                                scratch + 5, ok);
     k_sort_class_block<<<296, 1024, smem_block, s>>>(offsets, records, items(6), scratch + 6, ok);
     k_sort_class_long<<<148, 1024, smem_block, s>>>(offsets, records, items(7), scratch + 7, ok);
 }

@@ -66,6 +66,10 @@ class ServingEngine:
 
     backend: object with
       - slots (int): number of execution slots
+      - priority_slots (int, optional): slots 0 .. priority_slots-1 run on
+        high-priority streams; a free one takes the largest queued request
+        alone (the requests that set the latency tail), so its kernels are
+        scheduled ahead of the other slots' batches
       - launch(slot, requests) -> handle (asynchronous)
       - done(handle) -> bool
       - finish(handle) -> list[Result] (in request order)
@@ -74,15 +78,22 @@ class ServingEngine:
     """
 
     def __init__(self, backend, budget_fragments: int, max_batch: int = 32, poll_s: float = 5e-5,
-                 policy: str = "fifo", age_ms: float = 20.0):
+                 policy: str = "fifo", age_ms: float = 20.0, batch_fragments: int | None = None):
         """policy "fifo": admit in arrival order.  "sjf": requests queued for
         at least age_ms first (in arrival order), then the rest by estimated
         fragments, smallest first, so small requests do not wait behind large
-        ones and no request waits longer than about age_ms plus one batch."""
+        ones and no request waits longer than about age_ms plus one batch.
+        budget_fragments bounds a batch's fragment storage (a request over it
+        is rejected); batch_fragments (default: the budget) is the size a
+        batch is filled to: a batch's device time is about proportional to its
+        fragments and every request in it waits for all of them, so a smaller
+        batch keeps the latency of its requests near their own (a request
+        larger than batch_fragments runs alone)."""
         if policy not in ("fifo", "sjf"):
             raise ValueError("policy must be 'fifo' or 'sjf'")
         self.backend = backend
         self.budget = int(budget_fragments)
+        self.batch_fragments = self.budget if batch_fragments is None else min(int(batch_fragments), self.budget)
         self.max_batch = int(max_batch)
         self.poll_s = poll_s
         self.policy = policy
@@ -133,7 +144,7 @@ class ServingEngine:
         if self.policy == "fifo":
             while self.queue and len(batch) < self.max_batch:
                 e = self.estimate(self.queue[0])
-                if batch and frags + e > self.budget:
+                if batch and frags + e > self.batch_fragments:
                     break
                 batch.append(self.queue.popleft())
                 frags += e
@@ -146,7 +157,7 @@ class ServingEngine:
             if len(batch) >= self.max_batch:
                 break
             e = self.estimate(r)
-            if batch and frags + e > self.budget:
+            if batch and frags + e > self.batch_fragments:
                 if r in aged:
                     break  # an aged request waits for the next batch, not behind younger ones
                 continue
@@ -156,6 +167,14 @@ class ServingEngine:
         if taken:
             self.queue = deque(r for r in self.queue if id(r) not in taken)
         return batch
+
+    def admit_largest(self) -> list[Request]:
+        """The largest queued request alone (for a high-priority slot)."""
+        if not self.queue:
+            return []
+        r = max(self.queue, key=self.estimate)
+        self.queue.remove(r)
+        return [r]
 
     def step(self) -> bool:
         """One scheduling pass: finish completed batches, launch on free slots.
@@ -172,11 +191,12 @@ class ServingEngine:
                     self.completed.append(r)
                 del self.busy[slot]
                 progressed = True
+        prio = int(getattr(self.backend, "priority_slots", 0))
         for slot in range(self.backend.slots):
             if slot in self.busy:
                 continue
             with self.lock:
-                batch = self.admit()
+                batch = self.admit_largest() if slot < prio else self.admit()
             if not batch:
                 break
             t = time.perf_counter()
@@ -240,7 +260,9 @@ class GpuBackend:
     """Executes request batches with the batched CUDA path; one CUDA stream and
     one batch renderer (own fragment storage) per slot, meshes shared."""
 
-    def __init__(self, meshes: dict, slots: int = 2, attenuation: float = 1.0):
+    def __init__(self, meshes: dict, slots: int = 2, attenuation: float = 1.0, priority_slots: int = 0):
+        """priority_slots: the first slots run on the device's highest stream
+        priority (the engine gives each the largest queued request alone)."""
         import torch
 
         from .batch import BatchRenderer
@@ -249,7 +271,10 @@ class GpuBackend:
         self.meshes = [meshes[n] for n in self.names]
         self.index = {n: i for i, n in enumerate(self.names)}
         self.slots = int(slots)
-        self.streams = [torch.cuda.Stream() for _ in range(self.slots)]
+        self.priority_slots = min(int(priority_slots), self.slots)
+        high = torch.cuda.Stream.priority_range()[1] if hasattr(torch.cuda.Stream, "priority_range") else -1
+        self.streams = [torch.cuda.Stream(priority=high if i < self.priority_slots else 0)
+                        for i in range(self.slots)]
         self.renderers = [BatchRenderer(self.meshes, attenuation=attenuation, use_early_ray_termination=True)
                           for _ in range(self.slots)]
         self.fpp = {n: 64.0 for n in self.names}

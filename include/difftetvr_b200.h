@@ -22,7 +22,7 @@ extern "C" {
 
 #define DTV_OK 0
 #define DTV_ERR_ARG 1      /* invalid argument (bad pointer, size, alignment, enum) */
-#define DTV_ERR_BUDGET 2   /* fragment storage exceeds the configured memory budget or a list cap */
+#define DTV_ERR_BUDGET 2   /* fragment storage exceeds the configured memory budget or a fixed limit */
 #define DTV_ERR_CUDA 3     /* CUDA runtime error */
 #define DTV_ERR_TIMEOUT 4  /* a bounded device-side wait gave up */
 #define DTV_ERR_STATE 5    /* call out of order (e.g. adjoint before render) */
@@ -151,10 +151,10 @@ int32_t dtv_renderer_render_adjoint_cells(dtv_renderer* r, const dtv_mesh* mesh,
 /* Kernel configuration of a renderer (or batch): the pixel tile of the
  * composite and adjoint blocks (0: 16 x 16, 1: 32 x 8, 2: 8 x 32 pixels) and,
  * per list-length class c (bit c; 1..4 = lists of up to 64, 128, 256, 512
- * records), the per-pixel sort method: distribution into depth buckets plus
- * exact fix-up (bit c of sort_bucket_classes), else 32-bit surrogate keys
- * through a bitonic network (bit c of sort_surrogate_classes), else the
- * 64-bit bitonic network.  Every setting gives the same lists, images and
+ * records, 5 = up to 1024), the per-pixel sort method: distribution into
+ * depth buckets plus an exact fix-up (bit c of sort_bucket_classes, c = 1..5),
+ * else 32-bit surrogate keys through a bitonic network (bit c of
+ * sort_surrogate_classes, c = 1..4), else the 64-bit bitonic network.  Every setting gives the same lists, images and
  * gradients; they differ in speed only.  An autotuner (difftetvr_b200.autotune)
  * times them on the caller's workload.  Batches use only the sort fields. */
 typedef struct dtv_tuning {

@@ -66,8 +66,16 @@ def test_long_lists_bit_exact_and_composited(oracle):
     cam = oracle.make_camera(view, S.FOVY_45, 48, 48)
     off_o, rec_o = oracle.fragments(fa, pos, cam)
     lens = np.diff(off_o)
-    assert lens.max() > 1024 and ((lens > 32) & (lens <= 512)).any()
+    assert lens.max() > 1024 and ((lens > 32) & (lens <= 512)).any() and ((lens > 512) & (lens <= 1024)).any()
     assert np.array_equal(off_g.astype(np.int64), off_o) and np.array_equal(rec_g, rec_o)
+    # Every sort method of every list-length class (distribution sorts included).
+    for bucket in (0x00, 0x3e):
+        for surrogate in (0x00, 0x1e):
+            r.set_tuning(sort_bucket_classes=bucket, sort_surrogate_classes=surrogate)
+            img_t = r.render().cpu().numpy().astype(np.float64)
+            off_t, rec_t = r.get_fragment_lists()
+            assert np.array_equal(off_t, off_g) and np.array_equal(rec_t, rec_g), (bucket, surrogate)
+            assert np.array_equal(img_t, img)
     img_o = oracle.render(fa, pos, col, cam, oracle.make_params(attenuation=1.0))[0]
     # Thousands of segments per pixel: FP32 accumulation error of the
     # composite grows with the list length; this stress case is held to 1e-4.

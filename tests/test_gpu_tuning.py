@@ -15,7 +15,7 @@ CONFIGS = [dict(composite_tile=1, adjoint_tile=2, sort_surrogate_classes=0x00, s
            dict(composite_tile=0, adjoint_tile=0, sort_surrogate_classes=0x1e, sort_bucket_classes=0x00),
            dict(composite_tile=1, adjoint_tile=0, sort_surrogate_classes=0x00, sort_bucket_classes=0x1e),
            dict(composite_tile=0, adjoint_tile=1, sort_surrogate_classes=0x06, sort_bucket_classes=0x12)]
-DEFAULT = dict(composite_tile=0, adjoint_tile=0, sort_surrogate_classes=0x1e, sort_bucket_classes=0x1c)
+DEFAULT = dict(composite_tile=0, adjoint_tile=0, sort_surrogate_classes=0x1e, sort_bucket_classes=0x3c)
 
 
 def _run(mesh, r, w):
@@ -46,7 +46,7 @@ def test_every_configuration_gives_the_same_results():
     with pytest.raises(RuntimeError):
         r.set_tuning(sort_surrogate_classes=0x1)
     with pytest.raises(RuntimeError):
-        r.set_tuning(sort_bucket_classes=0x20)
+        r.set_tuning(sort_bucket_classes=0x40)
 
 
 def test_autotuner_sets_and_caches_a_configuration():
@@ -56,8 +56,8 @@ def test_autotuner_sets_and_caches_a_configuration():
     out = autotune.autotune_renderer(r, trials=2, force=True)
     t = out["tuning"]
     assert t["composite_tile"] in (0, 1, 2) and t["adjoint_tile"] in (0, 1, 2)
-    assert (t["sort_surrogate_classes"] & ~0x1e) == 0 and (t["sort_bucket_classes"] & ~0x1e) == 0
-    assert r.get_tuning() == t and len(out["timings"]) >= 13 and out["ms"] > 0
+    assert (t["sort_surrogate_classes"] & ~0x1e) == 0 and (t["sort_bucket_classes"] & ~0x3e) == 0
+    assert r.get_tuning() == t and len(out["timings"]) >= 14 and out["ms"] > 0
     r.set_tuning(composite_tile=(t["composite_tile"] + 1) % 3)
     again = autotune.autotune_renderer(r)  # cached: restores the chosen configuration
     assert again is out and r.get_tuning() == t
@@ -84,4 +84,4 @@ def test_batch_sort_configuration_and_autotune():
         for a, b in zip(br.render(views), ref):
             assert torch.equal(a, b)
     out = autotune.autotune_batch(br, views, trials=1, force=True)
-    assert br.get_tuning() == out["tuning"] and len(out["timings"]) == 9
+    assert br.get_tuning() == out["tuning"] and len(out["timings"]) == 10  # 1 + 4 classes x 2 + class 5 x 1

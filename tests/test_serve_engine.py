@@ -138,3 +138,34 @@ def test_sjf_completes_every_request():
     futs = [eng.submit(req(16 if i % 3 else 32, 16 if i % 3 else 32)) for i in range(30)]
     assert sorted(f.result(timeout=10).request_id for f in futs) == list(range(30))
     eng.stop()
+
+
+def test_priority_slot_takes_the_largest_request_alone():
+    """With a high-priority slot the largest queued request goes there alone
+    and the other slots take the rest in the engine's policy."""
+    be = FakeBackend(slots=2, delay=0.05)
+    be.priority_slots = 1
+    eng = ServingEngine(be, budget_fragments=10 * 64 * 64 * 4, max_batch=8, policy="sjf", age_ms=1e6)
+    reqs = [req(16, 16), req(64, 64), req(16, 16), req(32, 32)]
+    for i, r in enumerate(reqs):
+        r.id, r.t_arrival = i, time.perf_counter()
+        eng.queue.append(r)
+    eng.step()
+    by_slot = dict(be.launched)
+    assert by_slot[0] == [1]              # the 64 x 64 request, alone, on the priority slot
+    assert sorted(by_slot[1]) == [0, 2, 3]
+    eng.running = False
+    while eng.busy:
+        eng.step()
+        time.sleep(0.005)
+
+
+def test_batch_fragments_caps_the_batch_but_not_a_single_request():
+    be = FakeBackend(slots=1, delay=0.0)
+    eng = ServingEngine(be, budget_fragments=10 * 64 * 64 * 4, max_batch=8, batch_fragments=10 * 32 * 32 * 2)
+    for i, r in enumerate([req(32, 32), req(32, 32), req(32, 32), req(64, 64)]):
+        r.id, r.t_arrival = i, time.perf_counter()
+        eng.queue.append(r)
+    assert [r.id for r in eng.admit()] == [0, 1]   # two 32 x 32 fill the batch target
+    assert [r.id for r in eng.admit()] == [2]      # the 64 x 64 would overflow it
+    assert [r.id for r in eng.admit()] == [3]      # over the target, alone
