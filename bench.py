@@ -50,6 +50,7 @@ def parse_args():
     ap.add_argument("--cpu-steps", type=int, default=2, help="whole CPU-port steps timed for cpu_baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default kernel configuration")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-raytet", action="store_true")
     ap.add_argument("--profile", choices=["ppll", "intersection"], default=None,
@@ -276,6 +277,11 @@ def run_ours(args, rank, world):
     adj = torch.empty_like(targets[0])
     loss_acc = torch.zeros(1, device=device)
     stream = torch.cuda.current_stream(device)
+    # Kernel configuration from the library's autotuner on the first view
+    # (pixel tiles of composite / adjoint, sort method per list-length class).
+    from difftetvr_b200.autotune import autotune_renderer
+    r.set_view_matrix(views[0])
+    tuned = r.get_tuning() if args.no_autotune else autotune_renderer(r)["tuning"]
 
     def step(i):
         # Device-resident step: render, fused loss + image adjoint, adjoint, Adam.
@@ -447,6 +453,7 @@ def run_ours(args, rank, world):
                                f"{args.res}x{args.res}, one camera per step, fwd+adj+Adam",
                    "tets": 6 * args.n ** 3, "vertices": V, "faces": F, "res": args.res,
                    "fragments_per_step": nf, "views": len(views), "parallelism": f"replicas x{world}",
+                   "tuning": tuned,
                    "l2": "inputs larger than L2 (fragment records ~%.1f GB per step)" % (8 * nf / 1e9)},
         "e2e": e2e,
         "gpu_launches": LIST_STEP_LAUNCHES * K,
