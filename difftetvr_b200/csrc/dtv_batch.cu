@@ -291,10 +291,17 @@ __global__ void __launch_bounds__(kTile * kTile, 2) kb_adjoint(const BatchView* 
     const BatchView& bv = views[v];
     if (bv.grad_slot < 0 || bv.dimage == nullptr) return;
     float4* rows = SCREEN ? view_rows + 2 * bv.vert_base : grad_rows + 2 * bv.grad_base;
-    VertCache acc{rows, vcache4 + threadIdx.x, vcache1 + threadIdx.x, kTile * kTile};
-    adjoint_pixel<VertCache, SCREEN>(px, py, offsets + bv.pix_base, records, bv.faces, vgeo + bv.vert_base,
-                                     bv.colors, int(bv.W), bv.cam, sh, bv.dimage, tfinal + bv.pix_base,
-                                     term + bv.pix_base, acc);
+    if constexpr (SCREEN) {
+        OrderedRows acc{rows};
+        adjoint_pixel<OrderedRows, SCREEN>(px, py, offsets + bv.pix_base, records, bv.faces, vgeo + bv.vert_base,
+                                           bv.colors, int(bv.W), bv.cam, sh, bv.dimage, tfinal + bv.pix_base,
+                                           term + bv.pix_base, acc);
+    } else {
+        VertCache acc{rows, vcache4 + threadIdx.x, vcache1 + threadIdx.x, kTile * kTile};
+        adjoint_pixel<VertCache, SCREEN>(px, py, offsets + bv.pix_base, records, bv.faces, vgeo + bv.vert_base,
+                                         bv.colors, int(bv.W), bv.cam, sh, bv.dimage, tfinal + bv.pix_base,
+                                         term + bv.pix_base, acc);
+    }
 }
 
 // Screen-space rows of every view with a gradient slot -> world-space rows

@@ -1026,9 +1026,17 @@ __global__ void __launch_bounds__(256) k_adjoint(
     const int px = blockIdx.x * TX + (threadIdx.x % TX);
     const int py = row0 + int(blockIdx.y) * TY + int(threadIdx.x / TX);
     if (px >= W || py >= row1) return;
-    VertCache acc{grad_rows, vcache4 + threadIdx.x, vcache1 + threadIdx.x, 256};
-    adjoint_pixel<VertCache, SCREEN>(px, py, offsets, records, faces, vgeo, colors, W, cam, sh, dimage, tfinal, term,
-                                     acc);
+    // Screen-space rows: the ordered register cache (order_like); world-space
+    // rows (absolute gradients): the shared-memory cache.
+    if constexpr (SCREEN) {
+        OrderedRows acc{grad_rows};
+        adjoint_pixel<OrderedRows, SCREEN>(px, py, offsets, records, faces, vgeo, colors, W, cam, sh, dimage, tfinal,
+                                           term, acc);
+    } else {
+        VertCache acc{grad_rows, vcache4 + threadIdx.x, vcache1 + threadIdx.x, 256};
+        adjoint_pixel<VertCache, SCREEN>(px, py, offsets, records, faces, vgeo, colors, W, cam, sh, dimage, tfinal,
+                                         term, acc);
+    }
 }
 
 // Adds the interleaved rows into the caller's gradient buffers (SCREEN: the

@@ -452,6 +452,7 @@ __device__ __forceinline__ void composite_pixel(
 // and the alpha gradient s2; set_pixel() gives the sink gC (|gC| for absolute
 // gradients, whose s1 is then the absolute weight).
 struct GradAcc {
+    static constexpr bool kOrdered = false;
     float4* rows;   // [V][2]: position xyz, pad; colour rgba
     float g0 = 0.f, g1 = 0.f, g2 = 0.f;
 
@@ -478,6 +479,7 @@ struct GradAcc {
 // behind it, summing the tile's pixels with shared-memory atomics, and a
 // warp-wide merge of equal retired vertices both measured slower.)
 struct VertCache {
+    static constexpr bool kOrdered = false;
     static constexpr uint32_t kNone = 0xffffffffu;
     float4* rows;   // [V][2] global rows
     float4* c4;     // this thread's slot 0: position xyz, colour weight
@@ -542,6 +544,68 @@ struct VertCache {
         spill(1, id1);
         spill(2, id2);
         id0 = id1 = id2 = kNone;
+    }
+};
+
+// Vertex order of a fragment's face relative to the face processed just
+// before it (w, in its own order): each vertex the two faces share keeps its
+// position in w, and the face's other vertices take the remaining positions
+// in their order.  Returns the order in `out` and a 3-bit mask of the
+// positions whose vertex continues from w.  Consecutive fragments of a list
+// usually bound one tet and share an edge, so one position changes per
+// fragment and a cache of the three vertex rows needs no search.
+__device__ __forceinline__ uint32_t order_like(const uint32_t (&w)[3], uint32_t y0, uint32_t y1, uint32_t y2,
+                                               uint32_t (&out)[3]) {
+    const bool e00 = w[0] == y0, e01 = w[0] == y1, e02 = w[0] == y2;
+    const bool e10 = w[1] == y0, e11 = w[1] == y1, e12 = w[1] == y2;
+    const bool e20 = w[2] == y0, e21 = w[2] == y1, e22 = w[2] == y2;
+    const bool m0 = e00 | e01 | e02, m1 = e10 | e11 | e12, m2 = e20 | e21 | e22;
+    const bool u0 = e00 | e10 | e20, u1 = e01 | e11 | e21;
+    // The first and second of the face's vertices that w does not hold.
+    const uint32_t n1 = !u0 ? y0 : (!u1 ? y1 : y2);
+    const uint32_t n2 = (!u0 && !u1) ? y1 : y2;
+    out[0] = m0 ? w[0] : n1;
+    out[1] = m1 ? w[1] : (m0 ? n1 : n2);
+    const int free_before = int(!m0) + int(!m1);
+    out[2] = m2 ? w[2] : (free_before == 0 ? n1 : (free_before == 1 ? n2 : y2));
+    return uint32_t(m0) | (uint32_t(m1) << 1) | (uint32_t(m2) << 2);
+}
+
+// Vertex-row accumulator for faces given in order_like order: position s of
+// each face is cache slot s, so a face adds into its slots directly, and a
+// slot whose vertex does not continue is written to global memory (two float4
+// atomics) before the new vertex takes it.  Rows held in registers.
+struct OrderedRows {
+    static constexpr bool kOrdered = true;
+    static constexpr uint32_t kNone = 0xffffffffu;
+    float4* rows;   // [V][2] global rows
+    float g0 = 0.f, g1 = 0.f, g2 = 0.f;
+    uint32_t id[3] = {kNone, kNone, kNone};
+    float4 p[3];
+    float a[3];
+
+    __device__ __forceinline__ void set_pixel(float a0, float a1, float a2) { g0 = a0; g1 = a1; g2 = a2; }
+    __device__ __forceinline__ void put(uint32_t v, const float4& q, float al) const {
+        atomicAdd(rows + 2 * size_t(v), make_float4(q.x, q.y, q.z, 0.f));
+        atomicAdd(rows + 2 * size_t(v) + 1, make_float4(g0 * q.w, g1 * q.w, g2 * q.w, al));
+    }
+    __device__ __forceinline__ void add_ordered(const uint32_t (&v)[3], uint32_t keep, const float4 (&gp)[3],
+                                                const float (&s2)[3]) {
+#pragma unroll
+        for (int s = 0; s < 3; ++s) {
+            const bool k = (keep >> s) & 1u;
+            if (!k && id[s] != kNone) put(id[s], p[s], a[s]);
+            p[s] = k ? make_float4(p[s].x + gp[s].x, p[s].y + gp[s].y, p[s].z + gp[s].z, p[s].w + gp[s].w) : gp[s];
+            a[s] = k ? a[s] + s2[s] : s2[s];
+            id[s] = v[s];
+        }
+    }
+    __device__ __forceinline__ void flush() {
+#pragma unroll
+        for (int s = 0; s < 3; ++s) {
+            if (id[s] != kNone) put(id[s], p[s], a[s]);
+            id[s] = kNone;
+        }
     }
 };
 
@@ -629,7 +693,7 @@ __device__ __forceinline__ void frag_vertex_grads(const FragV& fr, float qx, flo
             gav[j] = s2;
         }
     }
-    acc.add_face(vi, gpv, gav);
+    if constexpr (!Acc::kOrdered) acc.add_face(vi, gpv, gav);  // ordered caches take carried fragments only
 }
 
 // Adjoint of one segment of a pixel's ray between a front fragment (colour
@@ -836,18 +900,18 @@ struct FragG {
     float pc[3], cw[3];              // gC . vertex colour rgb, vertex alpha
 };
 
-__device__ __forceinline__ FragG load_frag_g(uint32_t lo, const uint4& fc, float qx, float qy,
-                                             const VGeo* __restrict__ vgeo, const float4* __restrict__ colors,
-                                             float gC0, float gC1, float gC2) {
+__device__ __forceinline__ FragG load_frag_g(uint32_t lo, uint32_t v0, uint32_t v1, uint32_t v2, uint32_t keep,
+                                             float qx, float qy, const VGeo* __restrict__ vgeo,
+                                             const float4* __restrict__ colors, float gC0, float gC1, float gC2) {
     FragG f;
-    f.v[0] = fc.x;
-    f.v[1] = fc.y;
-    f.v[2] = fc.z;
-    const VGeo a = vgeo[fc.x], b = vgeo[fc.y], c = vgeo[fc.z];
+    f.v[0] = v0;
+    f.v[1] = v1;
+    f.v[2] = v2;
+    const VGeo a = vgeo[v0], b = vgeo[v1], c = vgeo[v2];
     FaceInterp fi;
     face_interp(a, b, c, qx, qy, fi);
-    f.bits = lo & 3u;
-    const float4 c0 = colors[fc.x], c1 = colors[fc.y], c2 = colors[fc.z];
+    f.bits = (lo & 3u) | (keep << 2);
+    const float4 c0 = colors[v0], c1 = colors[v1], c2 = colors[v2];
     const float* bary = fi.bary;
     f.z = fi.z;
     f.alpha = bary[0] * c0.w + bary[1] * c1.w + bary[2] * c2.w;
@@ -871,6 +935,12 @@ __device__ __forceinline__ FragG load_frag_g(uint32_t lo, const uint4& fc, float
     f.cw[1] = c1.w;
     f.cw[2] = c2.w;
     return f;
+}
+
+__device__ __forceinline__ FragG load_frag_g(uint32_t lo, const uint4& fc, float qx, float qy,
+                                             const VGeo* __restrict__ vgeo, const float4* __restrict__ colors,
+                                             float gC0, float gC1, float gC2) {
+    return load_frag_g(lo, fc.x, fc.y, fc.z, 0u, qx, qy, vgeo, colors, gC0, gC1, gC2);
 }
 
 // frag_vertex_grads with SCREEN from a carried fragment: depth adjoint gz,
@@ -905,7 +975,10 @@ __device__ __forceinline__ void frag_grads_carried(const FragG& f, float gz, flo
     gpv[2] = make_float4(-gE[0] * dy[1] + gE[1] * dy[0], gE[0] * dx[1] - gE[1] * dx[0], giz[2], w * bary[2]);
 #pragma unroll
     for (int j = 0; j < 3; ++j) gav[j] = ga * bary[j];
-    acc.add_face(f.v, gpv, gav);
+    if constexpr (Acc::kOrdered)
+        acc.add_ordered(f.v, f.bits >> 2, gpv, gav);
+    else
+        acc.add_face(f.v, gpv, gav);
 }
 
 // adjoint_pixel for screen-space rows (no absolute gradients), on carried
@@ -939,7 +1012,14 @@ __device__ __forceinline__ void adjoint_pixel_carried(
     uint32_t lo_n = last >= 2 ? record_lo(records, beg + last - 2) : 0u;
     float gz_b = 0.f, wb = 0.f, ab = 0.f;
     for (int i = last; i >= 1; --i) {
-        const FragG ff = load_frag_g(lo_f, fc_f, qx, qy, vgeo, colors, gC0, gC1, gC2);
+        FragG ff;
+        if constexpr (Acc::kOrdered) {
+            uint32_t pv[3];
+            const uint32_t keep = order_like(fb.v, fc_f.x, fc_f.y, fc_f.z, pv);
+            ff = load_frag_g(lo_f, pv[0], pv[1], pv[2], keep, qx, qy, vgeo, colors, gC0, gC1, gC2);
+        } else {
+            ff = load_frag_g(lo_f, fc_f, qx, qy, vgeo, colors, gC0, gC1, gC2);
+        }
         if (i >= 2) {
             fc_f = faces[lo_n >> 2];
             lo_f = lo_n;

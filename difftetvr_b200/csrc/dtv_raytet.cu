@@ -232,7 +232,11 @@ __device__ __forceinline__ void walk_adjoint_carried(
         const bool inner = !(fce.w & 1u) && tprev != kNoTet;
         TetRow trp{};
         if (inner) trp = load_tet(tt, tprev);
-        const FragG fE = load_frag_g(fe << 2, fce, qx, qy, vgeo, colors, gC0, gC1, gC2);
+        // The entry face shares an edge with the exit face (one tet): its
+        // vertices in the exit face's order for the ordered row cache.
+        uint32_t pv[3];
+        const uint32_t keep = order_like(fX.v, fce.x, fce.y, fce.z, pv);
+        const FragG fE = load_frag_g(fe << 2, pv[0], pv[1], pv[2], keep, qx, qy, vgeo, colors, gC0, gC1, gC2);
         const float tSeg = (fX.z - fE.z) * scale * 0.25f;
         float g_tot = 0.f, we = 0.f, ae = 0.f;
         segment_adjoint(tSeg, fE.alpha, fX.alpha, fE.pcol, fX.pcol, atten, T, gT, g_tot, we, wx, ae, ax);
@@ -298,9 +302,7 @@ __global__ void __launch_bounds__(kTile * kTile, 2) k_walk_adjoint(
     uint32_t fx = tet_face_at(tt, vfix, t, fe, false, px, py);
     if (fx == kNoTet) return;
     if constexpr (SCREEN) {
-        __shared__ float4 vcache4[3 * kTile * kTile];
-        __shared__ float vcache1[3 * kTile * kTile];
-        VertCache acc{grad_rows, vcache4 + threadIdx.x, vcache1 + threadIdx.x, kTile * kTile};
+        OrderedRows acc{grad_rows};
         acc.set_pixel(gC0, gC1, gC2);
         walk_adjoint_carried(b_records, beg, bf_global, faces, f2t, tt, num_tets, vfix, vgeo, colors, px, py, scale,
                              atten, gC0, gC1, gC2, T, gT, t, fe, fx, b, acc);
