@@ -1015,7 +1015,7 @@ void launch_composite(const u64* offsets, const u64* records, const uint4* faces
 // ---------------------------------------------------------------------------
 // (f) adjoint (adjoint_pixel).
 template <int TX, bool SCREEN>
-__global__ void __launch_bounds__(256) k_adjoint(
+__global__ void __launch_bounds__(256, 2) k_adjoint(
     const u64* __restrict__ offsets, const u64* __restrict__ records, const uint4* __restrict__ faces,
     const VGeo* __restrict__ vgeo, const float4* __restrict__ colors, int W, int row0, int row1, CamDev cam,
     ShadeDev sh, const float4* __restrict__ dimage, const float* __restrict__ tfinal,

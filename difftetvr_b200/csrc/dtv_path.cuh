@@ -370,11 +370,30 @@ __device__ __forceinline__ void segment_composite(float tSeg, const float4& cf, 
     // Sub-segment s adds w (cf + fs d) - k d per channel; summed over the
     // sub-segments that is cf sum(w) + d sum(w fs - k), two scalars.
     float ws = 0.f, ds = 0.f;
-    SegTerms st[kNumSubdivs];
     if (short_tier) {
-#pragma unroll
-        for (int s = 0; s < kNumSubdivs; ++s) st[s] = seg_terms_short(tSeg, av[s]);
-    } else {
+        // Two-wide: sub-segments (0, 1) and (2, 3).  Entry transmittances
+        // front to back by the FMA step, then the weights w = Ts (1 - A) and
+        // k = Ts K / 4 of both pairs.
+        const SegTerms2 s01 = seg_terms_short2<false>(tSeg, make_float2(av[0], av[1]));
+        const SegTerms2 s23 = seg_terms_short2<false>(tSeg, make_float2(av[2], av[3]));
+        const float T0 = T.hi;
+        const float T1 = __fmaf_rn(-T0, s01.omA.x, T0);
+        const float T2 = __fmaf_rn(-T1, s01.omA.y, T1);
+        const float T3 = __fmaf_rn(-T2, s23.omA.x, T2);
+        const float2 w01 = mul2(make_float2(T0, T1), s01.omA), w23 = mul2(make_float2(T2, T3), s23.omA);
+        const float2 k01 = mul2(make_float2(T0, T1), s01.K), k23 = mul2(make_float2(T2, T3), s23.K);
+        ws = hsum2(add2(w01, w23));
+        // sum(w fs) - sum(Ts K) / 4
+        const float2 wf = fma2(w23, make_float2(0.5f, 0.75f), mul2(w01, make_float2(0.f, 0.25f)));
+        ds = __fmaf_rn(hsum2(add2(k01, k23)), -0.25f, hsum2(wf));
+        trans_add_small(T, -ws);
+        C0 += cf.x * ws + d0 * ds;
+        C1 += cf.y * ws + d1 * ds;
+        C2 += cf.z * ws + d2 * ds;
+        return;
+    }
+    SegTerms st[kNumSubdivs];
+    {
         // a <= 0 contributes nothing: A = 1, 1 - A = K = 0.
 #pragma unroll
         for (int s = 0; s < kNumSubdivs; ++s) st[s] = av[s] > 0.f ? seg_terms(tSeg, av[s]) : SegTerms{1.f, 0.f, 0.f, 0.f};
@@ -763,43 +782,54 @@ __device__ __forceinline__ void segment_adjoint(float tSeg, float cfw, float cbw
     // the length adjoint, the attenuation of the alpha adjoints) are applied
     // once per segment.
     if (short_tier) {
-        SegTerms st[kNumSubdivs];
-#pragma unroll
-        for (int s = 0; s < kNumSubdivs; ++s) st[s] = seg_terms_adj_short(tSeg, av[s]);
+        // Two-wide: sub-segments (0, 1) and (2, 3) as pairs.
+        const float2 av01 = make_float2(av[0], av[1]), av23 = make_float2(av[2], av[3]);
+        const SegTerms2 s01 = seg_terms_short2<true>(tSeg, av01);
+        const SegTerms2 s23 = seg_terms_short2<true>(tSeg, av23);
         const float Tout_seg = T.hi;
         trans_add_small(T, T.hi * expm1_half((av[0] + av[1] + av[2] + av[3]) * tSeg));
-        float Tin[kNumSubdivs];
-        Tin[0] = T.hi;
-#pragma unroll
-        for (int s = 1; s < kNumSubdivs; ++s) Tin[s] = __fmaf_rn(-Tin[s - 1], st[s - 1].omA, Tin[s - 1]);
+        const float Tin0 = T.hi;
+        const float Tin1 = __fmaf_rn(-Tin0, s01.omA.x, Tin0);
+        const float Tin2 = __fmaf_rn(-Tin1, s01.omA.y, Tin1);
+        const float Tin3 = __fmaf_rn(-Tin2, s23.omA.x, Tin2);
+        const float2 Tin01 = make_float2(Tin0, Tin1), Tin23 = make_float2(Tin2, Tin3);
+        const float2 Tout01 = make_float2(Tin1, Tin2), Tout23 = make_float2(Tin3, Tout_seg);
+        // P0 = pf + fs dp and c = (1 - A) P0 - K D per sub-segment.
+        const float2 P01 = fma2(make_float2(0.f, 0.25f), bc2(dp), bc2(pf));
+        const float2 P23 = fma2(make_float2(0.5f, 0.75f), bc2(dp), bc2(pf));
+        const float2 c01 = fma2(s01.K, bc2(-D), mul2(s01.omA, P01));
+        const float2 c23 = fma2(s23.K, bc2(-D), mul2(s23.omA, P23));
+        // Transmittance adjoint back to front: gTo (A - 1) + c per sub-segment.
+        const float g3 = gT.hi;
+        const float d3 = __fmaf_rn(-g3, s23.omA.y, c23.y);
+        const float g2 = g3 + d3;
+        const float d2 = __fmaf_rn(-g2, s23.omA.x, c23.x);
+        const float g1 = g2 + d2;
+        const float d1 = __fmaf_rn(-g1, s01.omA.y, c01.y);
+        const float g0 = g1 + d1;
+        const float d0 = __fmaf_rn(-g0, s01.omA.x, c01.x);
+        const float2 gTo01 = make_float2(g0, g1), gTo23 = make_float2(g2, g3);
+        // Length adjoint: sum a Tout (P0 + t D - gTo).
+        const float tD = tSeg * D;
+        const float2 gl2 = fma2(mul2(av23, Tout23), sub2(add2(P23, bc2(tD)), gTo23),
+                                mul2(mul2(av01, Tout01), sub2(add2(P01, bc2(tD)), gTo01)));
+        // Alpha adjoints: Tin (t A (P0 - gTo) - dK D), split front / back.
+        const float2 ga01 = mul2(Tin01, fma2(s01.dK, bc2(-D), mul2(mul2(bc2(tSeg), s01.A), sub2(P01, gTo01))));
+        const float2 ga23 = mul2(Tin23, fma2(s23.dK, bc2(-D), mul2(mul2(bc2(tSeg), s23.A), sub2(P23, gTo23))));
+        const float2 gaf2 = fma2(make_float2(0.375f, 0.125f), ga23, mul2(make_float2(0.875f, 0.625f), ga01));
+        const float2 gab2 = fma2(make_float2(0.625f, 0.875f), ga23, mul2(make_float2(0.125f, 0.375f), ga01));
         // Colour weights: front += sum((1 - fs) tw + Tin K / 4), back +=
         // sum(fs tw - Tin K / 4), from three sums.
-        float gl = 0.f, gaf = 0.f, gab = 0.f, stw = 0.f, sftw = 0.f, sk = 0.f, dg = 0.f;
-        float g = gT.hi;
-#pragma unroll
-        for (int s = kNumSubdivs - 1; s >= 0; --s) {
-            const float fs = 0.25f * s, fm = 0.25f * (s + 0.5f);
-            const float P0 = pf + fs * dp;
-            const float Tout = s == kNumSubdivs - 1 ? Tout_seg : Tin[s + 1];
-            const float gTo = g;
-            const float dgs = __fmaf_rn(-gTo, st[s].omA, st[s].omA * P0 - st[s].K * D);  // gTo (A - 1) + ...
-            g = gTo + dgs;
-            dg += dgs;
-            gl += (av[s] * Tout) * (P0 + tSeg * D - gTo);
-            const float g_a = Tin[s] * (tSeg * st[s].A * (P0 - gTo) - st[s].dK * D);
-            const float tw = Tin[s] * st[s].omA;
-            stw += tw;
-            sftw += fs * tw;
-            sk += Tin[s] * st[s].K;
-            gaf += (1.f - fm) * g_a;
-            gab += fm * g_a;
-        }
-        trans_add(gT, dg);
-        g_tot += 0.25f * gl;
+        const float2 tw01 = mul2(Tin01, s01.omA), tw23 = mul2(Tin23, s23.omA);
+        const float stw = hsum2(add2(tw01, tw23));
+        const float sftw = hsum2(fma2(make_float2(0.5f, 0.75f), tw23, mul2(make_float2(0.f, 0.25f), tw01)));
+        const float sk = hsum2(fma2(Tin23, s23.K, mul2(Tin01, s01.K)));
+        trans_add(gT, ((d3 + d2) + d1) + d0);
+        g_tot += 0.25f * hsum2(gl2);
         wf += (stw - sftw) + 0.25f * sk;
         wb += sftw - 0.25f * sk;
-        af += gaf * atten;
-        ab += gab * atten;
+        af += hsum2(gaf2) * atten;
+        ab += hsum2(gab2) * atten;
         return;
     }
 #pragma unroll

@@ -136,6 +136,44 @@ __device__ __forceinline__ SegTerms seg_terms_adj_short(float t, float a) {
     return s;
 }
 
+// Two-wide FP32 arithmetic of sm_100: one FFMA2 / FMUL2 / FADD2 issues two
+// FP32 operations, each rounded as its scalar form.  The four sub-segments of
+// a segment have independent series terms, so they run as two pairs
+// (sub-segments 0,1 and 2,3) at half the issue slots.
+__device__ __forceinline__ float2 bc2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, bc2(-1.0f), a); }  // a - b
+__device__ __forceinline__ float hsum2(float2 a) { return a.x + a.y; }
+
+struct SegTerms2 {
+    float2 A, omA, K, dK;
+};
+
+// seg_terms_adj_short (DK: also dK) for two sub-segments: phi2 from its
+// series in -x (the same terms as in x with alternating signs, so the same
+// value), then phi1 = 1 - x phi2, psi = phi1 - phi2, 1 - A = x phi1,
+// K = -t x psi, dK = t^2 (psi - A).
+template <bool DK>
+__device__ __forceinline__ SegTerms2 seg_terms_short2(float t, float2 a) {
+    const float2 x = mul2(a, bc2(t)), nx = mul2(a, bc2(-t));
+    float2 p = bc2(1.98412698e-4f);
+    p = fma2(p, nx, bc2(1.38888889e-3f));
+    p = fma2(p, nx, bc2(8.33333333e-3f));
+    p = fma2(p, nx, bc2(4.16666667e-2f));
+    p = fma2(p, nx, bc2(0.166666667f));
+    p = fma2(p, nx, bc2(0.5f));
+    const float2 phi1 = fma2(nx, p, bc2(1.0f));
+    const float2 psi = sub2(phi1, p);
+    SegTerms2 s;
+    s.omA = mul2(x, phi1);
+    s.A = sub2(bc2(1.0f), s.omA);
+    s.K = mul2(mul2(bc2(-t), x), psi);
+    s.dK = DK ? mul2(bc2(t * t), sub2(psi, s.A)) : bc2(0.f);
+    return s;
+}
+
 // 1 - e^-x without cancellation (x phi1(x) for |x| < 1/8).
 __device__ __forceinline__ float one_minus_exp(float x) {
     if (fabsf(x) < 0.125f) return x * fmaf(-x, series_phi2_short(x), 1.0f);
