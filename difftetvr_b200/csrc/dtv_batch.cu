@@ -292,8 +292,8 @@ __global__ void __launch_bounds__(kTile * kTile, 2) kb_adjoint(const BatchView* 
     if (bv.grad_slot < 0 || bv.dimage == nullptr) return;
     float4* rows = SCREEN ? view_rows + 2 * bv.vert_base : grad_rows + 2 * bv.grad_base;
     if constexpr (SCREEN) {
-        OrderedRows acc{rows};
-        adjoint_pixel<OrderedRows, SCREEN>(px, py, offsets + bv.pix_base, records, bv.faces, vgeo + bv.vert_base,
+        OrderedRowsSmem acc{rows, vcache4 + threadIdx.x, vcache1 + threadIdx.x, kTile * kTile};
+        adjoint_pixel<OrderedRowsSmem, SCREEN>(px, py, offsets + bv.pix_base, records, bv.faces, vgeo + bv.vert_base,
                                            bv.colors, int(bv.W), bv.cam, sh, bv.dimage, tfinal + bv.pix_base,
                                            term + bv.pix_base, acc);
     } else {

@@ -591,15 +591,15 @@ __device__ __forceinline__ uint32_t order_like(const uint32_t (&w)[3], uint32_t 
 }
 
 // Vertex-row accumulator for faces given in order_like order: position s of
-// each face is cache slot s, so a face adds into its slots directly, and a
+// each face is cache slot s, so a face adds into its slots directly.  The
+// order of the next face is known when a face is added (its keep mask), so a
 // slot whose vertex does not continue is written to global memory (two float4
-// atomics) before the new vertex takes it.  Rows held in registers.
+// atomics) right after that add, with the face's own vertex ids; the cache
+// holds no ids.  Rows held in registers.
 struct OrderedRows {
     static constexpr bool kOrdered = true;
-    static constexpr uint32_t kNone = 0xffffffffu;
     float4* rows;   // [V][2] global rows
     float g0 = 0.f, g1 = 0.f, g2 = 0.f;
-    uint32_t id[3] = {kNone, kNone, kNone};
     float4 p[3];
     float a[3];
 
@@ -608,24 +608,70 @@ struct OrderedRows {
         atomicAdd(rows + 2 * size_t(v), make_float4(q.x, q.y, q.z, 0.f));
         atomicAdd(rows + 2 * size_t(v) + 1, make_float4(g0 * q.w, g1 * q.w, g2 * q.w, al));
     }
-    __device__ __forceinline__ void add_ordered(const uint32_t (&v)[3], uint32_t keep, const float4 (&gp)[3],
-                                                const float (&s2)[3]) {
+    // Face v (ordered; keep: the slots continuing from the previous face)
+    // adds its rows; slots not in keep_next (the next face's keep mask, 0 for
+    // the last face) are written out.
+    __device__ __forceinline__ void add_ordered(const uint32_t (&v)[3], uint32_t keep, uint32_t keep_next,
+                                                const float4 (&gp)[3], const float (&s2)[3]) {
 #pragma unroll
         for (int s = 0; s < 3; ++s) {
             const bool k = (keep >> s) & 1u;
-            if (!k && id[s] != kNone) put(id[s], p[s], a[s]);
             p[s] = k ? make_float4(p[s].x + gp[s].x, p[s].y + gp[s].y, p[s].z + gp[s].z, p[s].w + gp[s].w) : gp[s];
             a[s] = k ? a[s] + s2[s] : s2[s];
-            id[s] = v[s];
+            if (!((keep_next >> s) & 1u)) put(v[s], p[s], a[s]);
         }
     }
-    __device__ __forceinline__ void flush() {
+    // The slots a face added with keep_next left open, when no next face
+    // follows.
+    __device__ __forceinline__ void close(const uint32_t (&v)[3], uint32_t keep_next) const {
+#pragma unroll
+        for (int s = 0; s < 3; ++s)
+            if ((keep_next >> s) & 1u) put(v[s], p[s], a[s]);
+    }
+    __device__ __forceinline__ void flush() {}
+};
+
+// OrderedRows with the rows in shared memory (slot s of thread t at
+// c4[t + s * stride], c1[t + s * stride]), for kernels whose other state
+// leaves no registers for them.
+struct OrderedRowsSmem {
+    static constexpr bool kOrdered = true;
+    float4* rows;
+    float4* c4;
+    float* c1;
+    int stride;
+    float g0 = 0.f, g1 = 0.f, g2 = 0.f;
+
+    __device__ __forceinline__ void set_pixel(float a0, float a1, float a2) { g0 = a0; g1 = a1; g2 = a2; }
+    __device__ __forceinline__ void put(uint32_t v, const float4& q, float al) const {
+        atomicAdd(rows + 2 * size_t(v), make_float4(q.x, q.y, q.z, 0.f));
+        atomicAdd(rows + 2 * size_t(v) + 1, make_float4(g0 * q.w, g1 * q.w, g2 * q.w, al));
+    }
+    __device__ __forceinline__ void add_ordered(const uint32_t (&v)[3], uint32_t keep, uint32_t keep_next,
+                                                const float4 (&gp)[3], const float (&s2)[3]) {
 #pragma unroll
         for (int s = 0; s < 3; ++s) {
-            if (id[s] != kNone) put(id[s], p[s], a[s]);
-            id[s] = kNone;
+            float4 q = gp[s];
+            float al = s2[s];
+            if ((keep >> s) & 1u) {
+                const float4 o = c4[s * stride];
+                q = make_float4(o.x + q.x, o.y + q.y, o.z + q.z, o.w + q.w);
+                al += c1[s * stride];
+            }
+            if ((keep_next >> s) & 1u) {
+                c4[s * stride] = q;
+                c1[s * stride] = al;
+            } else {
+                put(v[s], q, al);
+            }
         }
     }
+    __device__ __forceinline__ void close(const uint32_t (&v)[3], uint32_t keep_next) const {
+#pragma unroll
+        for (int s = 0; s < 3; ++s)
+            if ((keep_next >> s) & 1u) put(v[s], c4[s * stride], c1[s * stride]);
+    }
+    __device__ __forceinline__ void flush() {}
 };
 
 // Vertex gradients of one fragment from its depth adjoint gz, its colour
@@ -976,7 +1022,8 @@ __device__ __forceinline__ FragG load_frag_g(uint32_t lo, const uint4& fc, float
 // frag_vertex_grads with SCREEN from a carried fragment: depth adjoint gz,
 // colour weight w (colour adjoint = gC w) and alpha adjoint ga.
 template <class Acc>
-__device__ __forceinline__ void frag_grads_carried(const FragG& f, float gz, float w, float ga, Acc& acc) {
+__device__ __forceinline__ void frag_grads_carried(const FragG& f, float gz, float w, float ga, uint32_t keep_next,
+                                                   Acc& acc) {
     float bary[3], gb[3], sb = 0.f;
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
@@ -1006,7 +1053,7 @@ __device__ __forceinline__ void frag_grads_carried(const FragG& f, float gz, flo
 #pragma unroll
     for (int j = 0; j < 3; ++j) gav[j] = ga * bary[j];
     if constexpr (Acc::kOrdered)
-        acc.add_ordered(f.v, f.bits >> 2, gpv, gav);
+        acc.add_ordered(f.v, f.bits >> 2, keep_next, gpv, gav);
     else
         acc.add_face(f.v, gpv, gav);
 }
@@ -1063,13 +1110,13 @@ __device__ __forceinline__ void adjoint_pixel_carried(
             gz_f -= g_tot;
             gz_b += g_tot;
         }
-        frag_grads_carried(fb, gz_b, wb, ab, acc);
+        frag_grads_carried(fb, gz_b, wb, ab, ff.bits >> 2, acc);
         fb = ff;
         gz_b = gz_f;
         wb = wf;
         ab = af;
     }
-    frag_grads_carried(fb, gz_b, wb, ab, acc);
+    frag_grads_carried(fb, gz_b, wb, ab, 0u, acc);
     acc.flush();
 }
 

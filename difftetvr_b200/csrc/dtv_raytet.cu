@@ -224,6 +224,10 @@ __device__ __forceinline__ void walk_adjoint_carried(
     const float qx = float(px) + 0.5f, qy = float(py) + 0.5f;
     FragG fX = load_frag_g(fx << 2, faces[fx], qx, qy, vgeo, colors, gC0, gC1, gC2);
     float gz_x = 0.f, wx = 0.f, ax = 0.f;
+    // Cache slots the last added fragment left open for the next one; shared
+    // vertices keep their slot, so fX (the last added fragment, or the one it
+    // was kept for) names them when the walk ends.
+    uint32_t open = 0u;
     for (uint32_t step = 0; step <= num_tets; ++step) {
         // The tet behind the entry face and its table row are fetched first, so
         // their loads overlap the entry face's vertex loads and this step's math.
@@ -242,9 +246,11 @@ __device__ __forceinline__ void walk_adjoint_carried(
         segment_adjoint(tSeg, fE.alpha, fX.alpha, fE.pcol, fX.pcol, atten, T, gT, g_tot, we, wx, ae, ax);
         const float gz_e = -g_tot * scale;
         gz_x += g_tot * scale;
-        frag_grads_carried(fX, gz_x, wx, ax, acc);
-        if (fce.w & 1u) {
-            frag_grads_carried(fE, gz_e, we, ae, acc);
+        const bool leaving = fce.w & 1u;
+        frag_grads_carried(fX, gz_x, wx, ax, keep, acc);
+        if (leaving) {
+            frag_grads_carried(fE, gz_e, we, ae, 0u, acc);
+            open = 0u;
             // Previous interval: its exit is the last back-facing boundary fragment before b.
             int bb = b - 1;
             while (bb >= 0 && (uint32_t(b_records[beg + bb]) & 1u)) --bb;
@@ -262,6 +268,7 @@ __device__ __forceinline__ void walk_adjoint_carried(
             ax = 0.f;
             continue;
         }
+        open = keep;
         if (!inner) break;
         const uint32_t feprev = tet_face_of(trp, vfix, fe, true, px, py);
         if (feprev == kNoTet) break;
@@ -272,6 +279,7 @@ __device__ __forceinline__ void walk_adjoint_carried(
         t = tprev;
         fe = feprev;
     }
+    acc.close(fX.v, open);
     acc.flush();
 }
 
@@ -302,7 +310,9 @@ __global__ void __launch_bounds__(kTile * kTile, 2) k_walk_adjoint(
     uint32_t fx = tet_face_at(tt, vfix, t, fe, false, px, py);
     if (fx == kNoTet) return;
     if constexpr (SCREEN) {
-        OrderedRows acc{grad_rows};
+        __shared__ float4 vcache4[3 * kTile * kTile];
+        __shared__ float vcache1[3 * kTile * kTile];
+        OrderedRowsSmem acc{grad_rows, vcache4 + threadIdx.x, vcache1 + threadIdx.x, kTile * kTile};
         acc.set_pixel(gC0, gC1, gC2);
         walk_adjoint_carried(b_records, beg, bf_global, faces, f2t, tt, num_tets, vfix, vgeo, colors, px, py, scale,
                              atten, gC0, gC1, gC2, T, gT, t, fe, fx, b, acc);
