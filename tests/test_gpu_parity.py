@@ -5,7 +5,7 @@ import numpy as np
 import pytest
 import torch
 
-from helpers import Scene, rel_err
+from helpers import Scene, rel_err, two_block_scene
 
 pytestmark = pytest.mark.gpu
 
@@ -155,9 +155,15 @@ def test_image_with_early_ray_termination(oracle):
     assert (term_g < np.diff(r.get_fragment_lists()[0]).reshape(256, 256)).sum() > 100  # ERT actually fired
 
 
-@pytest.mark.parametrize("n,res,ert", [(8, 128, False), (16, 256, False), (8, 128, True)])
-def test_gradients_match_fp64_oracle(oracle, n, res, ert):
-    sc = Scene(n, res, seed=20 + n, attenuation=2.0 if ert else 1.0, ert=ert)
+# two_blocks: rays leave one block and enter the other, so consecutive faces of
+# a list share no vertex there (every cached vertex row is written out).
+@pytest.mark.parametrize("kind,n,res,ert", [("cube", 8, 128, False), ("cube", 16, 256, False),
+                                            ("cube", 8, 128, True), ("two_blocks", 4, 128, False)])
+def test_gradients_match_fp64_oracle(oracle, kind, n, res, ert):
+    if kind == "two_blocks":
+        sc = two_block_scene(n, res, seed=20 + n)
+    else:
+        sc = Scene(n, res, seed=20 + n, attenuation=2.0 if ert else 1.0, ert=ert)
     mesh, r = sc.make_renderer()
     rng = np.random.default_rng(5)
     w = rng.normal(size=(res, res, 4)).astype(np.float32)
