@@ -85,6 +85,51 @@ __device__ __forceinline__ uint32_t tet_face_of(const TetRow& tr, const int2* __
     const uint32_t flip = tr.flip;
     const uint32_t fs[4] = {tf.x, tf.y, tf.z, tf.w};
     const int2 q[4] = {vfix[cv.x], vfix[cv.y], vfix[cv.z], vfix[cv.w]};
+    uint32_t found = kNoTet;
+    // All four vertices projected and within 2^14 units of the centre (nearly
+    // every step): 32-bit integers are exact.  The tet's four faces share its
+    // six edges, so six edge functions K_uv = r_u x r_v (vertex positions
+    // relative to the pixel centre, u < v) and their tie-rule bits decide all
+    // four faces: a face's doubled area is the sum of its three directed
+    // edges' functions, the reversed edge of a non-degenerate edge owns the
+    // centre exactly when the edge does not, and a face with a degenerate
+    // edge has zero area and is skipped.  Same values and decisions as
+    // covers_rel on each face.
+    const bool projected = (q[0].x != kInvalidFix) & (q[1].x != kInvalidFix) & (q[2].x != kInvalidFix) &
+                           (q[3].x != kInvalidFix) & (px < (1 << 22)) & (py < (1 << 22));
+    if (projected) {
+        const int Xc = 256 * px + 128, Yc = 256 * py + 128;
+        int ix[4], iy[4], mm = 0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            ix[k] = q[k].x - Xc;
+            iy[k] = q[k].y - Yc;
+            mm = max(mm, max(abs(ix[k]), abs(iy[k])));
+        }
+        if (mm < (1 << 14)) {
+            const int K01 = ix[0] * iy[1] - iy[0] * ix[1], K02 = ix[0] * iy[2] - iy[0] * ix[2];
+            const int K03 = ix[0] * iy[3] - iy[0] * ix[3], K12 = ix[1] * iy[2] - iy[1] * ix[2];
+            const int K13 = ix[1] * iy[3] - iy[1] * ix[3], K23 = ix[2] * iy[3] - iy[2] * ix[3];
+            const bool f01 = edge_in<int>(K01, ix[1] - ix[0], iy[1] - iy[0]);
+            const bool f02 = edge_in<int>(K02, ix[2] - ix[0], iy[2] - iy[0]);
+            const bool f03 = edge_in<int>(K03, ix[3] - ix[0], iy[3] - iy[0]);
+            const bool f12 = edge_in<int>(K12, ix[2] - ix[1], iy[2] - iy[1]);
+            const bool f13 = edge_in<int>(K13, ix[3] - ix[1], iy[3] - iy[1]);
+            const bool f23 = edge_in<int>(K23, ix[3] - ix[2], iy[3] - iy[2]);
+            // Face j = (A, B, C): directed edges B->C, C->A, A->B.
+            const int ar[4] = {K12 - K02 + K01, K03 - K13 - K01, K23 - K03 + K02, K13 - K23 - K12};
+            const bool e0[4] = {f12, f03, f23, f13}, e1[4] = {!f02, !f13, !f03, !f23}, e2[4] = {f01, !f01, f02, !f12};
+#pragma unroll
+            for (int j = 3; j >= 0; --j) {
+                const bool sw = ar[j] < 0;  // clockwise: every directed edge reversed
+                const bool in = sw ? !(e0[j] | e1[j] | e2[j]) : (e0[j] & e1[j] & e2[j]);
+                const bool front = sw != (((flip >> j) & 1u) != 0u);
+                const bool match = fs[j] != skip && ar[j] != 0 && in && front == want_front;
+                found = match ? fs[j] : found;  // descending j: the smallest matching j wins
+            }
+            return found;
+        }
+    }
     const long long Xc = 256LL * px + 128, Yc = 256LL * py + 128;
     long long rx[4], ry[4];
     bool ok[4];
@@ -95,31 +140,6 @@ __device__ __forceinline__ uint32_t tet_face_of(const TetRow& tr, const int2* __
         ry[k] = (long long)q[k].y - Yc;
     }
     constexpr int A[4] = {0, 1, 0, 2}, B[4] = {1, 0, 2, 1}, C[4] = {2, 3, 3, 3};
-    uint32_t found = kNoTet;
-    // All four vertices within 2^14 units of the centre (nearly every step):
-    // every face's area and edge functions are exact in 32 bits, which is the
-    // per-face test below decided for the whole tet at once.
-    long long mm = 0;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) mm = max(mm, max(llabs(rx[k]), llabs(ry[k])));
-    if (mm < (1LL << 14)) {
-        int ix[4], iy[4];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            ix[k] = int(rx[k]);
-            iy[k] = int(ry[k]);
-        }
-#pragma unroll
-        for (int j = 3; j >= 0; --j) {
-            const int a = A[j], b = B[j], c = C[j];
-            const int area2 = (ix[b] - ix[a]) * (iy[c] - iy[a]) - (iy[b] - iy[a]) * (ix[c] - ix[a]);
-            const bool in = covers_rel<int>(ix[a], iy[a], ix[b], iy[b], ix[c], iy[c], area2 < 0);
-            const bool front = (area2 < 0) != (((flip >> j) & 1u) != 0u);
-            const bool match = fs[j] != skip && area2 != 0 && in && front == want_front;
-            found = match ? fs[j] : found;
-        }
-        return found;
-    }
 #pragma unroll
     for (int j = 3; j >= 0; --j) {
         const int a = A[j], b = B[j], c = C[j];
