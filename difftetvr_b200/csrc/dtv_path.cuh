@@ -458,7 +458,7 @@ __device__ __forceinline__ void composite_pixel(
 
 // ---------------------------------------------------------------------------
 // (f) adjoint.  Back to front from the termination index; transmittance is
-// rebuilt from the final value (T_in = T_out / A); per fragment the depth and
+// rebuilt from the final value (T = T_final e^X, TransBack); per fragment the depth and
 // colour adjoints of its two segments are summed and pushed through the
 // screen-space barycentrics and the projection to the face's three vertices.
 // Vertex gradient accumulation: the 7 values of a vertex (position xyz, pad,
@@ -761,11 +761,27 @@ __device__ __forceinline__ void frag_vertex_grads(const FragV& fr, float qx, flo
     if constexpr (!Acc::kOrdered) acc.add_face(vi, gpv, gav);  // ordered caches take carried fragments only
 }
 
+// Transmittance rebuilt back to front for the adjoint: T = tf e^X, with tf the
+// pixel's final transmittance and X the optical depth between the current
+// point and the ray's end (the sum of the sub-segment optical depths a t,
+// a > 0, already walked).  A sum of non-negative terms keeps every small step
+// (a ray of thousands of nearly transparent segments keeps its increments),
+// and one exponential per segment replaces a compensated update.  `cur` is
+// the current value, tf e^X.
+struct TransBack {
+    float tf, X, cur;
+    __device__ __forceinline__ explicit TransBack(float t) : tf(t), X(0.f), cur(t) {}
+    __device__ __forceinline__ void advance(float dX) {
+        X += dX;
+        cur = tf * __expf(X);
+    }
+};
+
 // Adjoint of one segment of a pixel's ray between a front fragment (colour
 // cf) and a back fragment (colour cb), the 4-sub-segment integral taken back
-// to front.  T holds the transmittance after the segment and is rebuilt in
-// place to the one before it (T_in = T_out / A); gT is the running
-// transmittance adjoint.
+// to front.  T holds the transmittance after the segment and is advanced to
+// the one before it (its optical depth grows by the segment's); gT is the
+// running transmittance adjoint.
 //
 // The pixel's colour adjoint gC = dL/dC.rgb enters every colour term through
 // dot products, so the sub-segment math runs on scalars: P0 = gC . c0 and
@@ -782,8 +798,8 @@ __device__ __forceinline__ void frag_vertex_grads(const FragV& fr, float qx, flo
 // Outputs (added): g_tot = dL/d(segment length), the colour weights wf / wb and
 // the alpha adjoints af / ab of the front / back fragment.
 __device__ __forceinline__ void segment_adjoint(float tSeg, float cfw, float cbw, float pf, float pb, float atten,
-                                                TransF& T, TransF& gT, float& g_tot, float& wf, float& wb, float& af,
-                                                float& ab) {
+                                                TransBack& T, TransF& gT, float& g_tot, float& wf, float& wb,
+                                                float& af, float& ab) {
     const float dp = pb - pf, D = 0.25f * dp, dw = cbw - cfw;
     float av[kNumSubdivs];
 #pragma unroll
@@ -791,7 +807,9 @@ __device__ __forceinline__ void segment_adjoint(float tSeg, float cfw, float cbw
     const bool short_tier = short_tier_of(av, tSeg);
     // One sub-segment, back to front; st is used only when a > 0.  (This
     // path runs when some sub-segment of the segment has x >= 1/8: T and gT
-    // change by large steps there, taken on hi with lo scaled along.)
+    // change by large steps there; T steps by 1 / A inside the segment and is
+    // rebuilt from the optical depth at its end.)
+    float Th = T.cur, Xseg = 0.f;
     auto step = [&](int s, const SegTerms& st, bool dense) {
         const float fs = 0.25f * s, fm = 0.25f * (s + 0.5f);
         const float P0 = pf + fs * dp;
@@ -799,29 +817,29 @@ __device__ __forceinline__ void segment_adjoint(float tSeg, float cfw, float cbw
         float g_a;
         if (dense) {
             const float iA = __fdividef(1.f, st.A);
-            const float Tin = T.hi * iA;
+            const float Tin = Th * iA;
             const float gTo = gT.hi;
             gT.hi = st.omA * P0 - st.K * D + gTo * st.A;
             gT.lo *= st.A;
-            g_tot += 0.25f * (a * T.hi) * (P0 + tSeg * D - gTo);
+            g_tot += 0.25f * (a * Th) * (P0 + tSeg * D - gTo);
             g_a = Tin * (tSeg * st.A * (P0 - gTo) - st.dK * D);
-            T.hi = Tin;
-            T.lo *= iA;
+            Th = Tin;
+            Xseg += a * tSeg;
             const float qK = 0.25f * st.K, tw = Tin * st.omA;
             wf += (1.f - fs) * tw + Tin * qK;
             wb += fs * tw - Tin * qK;
         } else {
-            g_a = T.hi * (tSeg * (P0 - gT.hi) + 0.5f * tSeg * tSeg * D);
+            g_a = Th * (tSeg * (P0 - gT.hi) + 0.5f * tSeg * tSeg * D);
         }
         af += (1.f - fm) * g_a * atten;
         ab += fm * g_a * atten;
     };
     // Same tiers as segment_composite: straight-line terms when all four
     // sub-segments are in the short tier (seg_terms_adj's arithmetic there).
-    // There every x = a t < 1/8, so the transmittance in front of the segment
-    // is T e^X with X = x0 + x1 + x2 + x3 < 1/2: the float-float T grows by
-    // T expm1(X) (expm1 from its series), and each sub-segment's entry
-    // transmittance follows front to back by the forward's own FMA step.  The
+    // There every x = a t < 1/8: the optical depth grows by X = x0 + x1 + x2 +
+    // x3, giving the transmittance in front of the segment, and each
+    // sub-segment's entry transmittance follows front to back by the
+    // forward's own FMA step.  The
     // transmittance adjoint gT (= gTo A + (1 - A) P0 - K D per sub-segment)
     // runs in FP32 from gT.hi inside the segment and its total change over the
     // segment is added to the float-float gT.  The constant factors (1/4 of
@@ -832,9 +850,9 @@ __device__ __forceinline__ void segment_adjoint(float tSeg, float cfw, float cbw
         const float2 av01 = make_float2(av[0], av[1]), av23 = make_float2(av[2], av[3]);
         const SegTerms2 s01 = seg_terms_short2<true>(tSeg, av01);
         const SegTerms2 s23 = seg_terms_short2<true>(tSeg, av23);
-        const float Tout_seg = T.hi;
-        trans_add_small(T, T.hi * expm1_half((av[0] + av[1] + av[2] + av[3]) * tSeg));
-        const float Tin0 = T.hi;
+        const float Tout_seg = T.cur;
+        T.advance((av[0] + av[1] + av[2] + av[3]) * tSeg);
+        const float Tin0 = T.cur;
         const float Tin1 = __fmaf_rn(-Tin0, s01.omA.x, Tin0);
         const float Tin2 = __fmaf_rn(-Tin1, s01.omA.y, Tin1);
         const float Tin3 = __fmaf_rn(-Tin2, s23.omA.x, Tin2);
@@ -885,10 +903,11 @@ __device__ __forceinline__ void segment_adjoint(float tSeg, float cfw, float cbw
         else
             step(s, SegTerms{}, false);
     }
+    T.advance(Xseg);
 }
 
 __device__ __forceinline__ void segment_adjoint(float tSeg, const float4& cf, const float4& cb, float pf, float pb,
-                                                float atten, TransF& T, TransF& gT, float& g_tot, float& wf,
+                                                float atten, TransBack& T, TransF& gT, float& g_tot, float& wf,
                                                 float& wb, float& af, float& ab) {
     segment_adjoint(tSeg, cf.w, cb.w, pf, pb, atten, T, gT, g_tot, wf, wb, af, ab);
 }
@@ -1075,7 +1094,7 @@ __device__ __forceinline__ void adjoint_pixel_carried(
     const float qx = float(px) + 0.5f, qy = float(py) + 0.5f;
     const float gC0 = g.x, gC1 = g.y, gC2 = g.z;
     TransF gT{g.x * sh.clear[0] + g.y * sh.clear[1] + g.z * sh.clear[2] + g.w * (sh.clear[3] - 1.f), 0.f};
-    TransF T{tfinal[p], 0.f};
+    TransBack T(tfinal[p]);
     const int last = sh.use_ert ? int(term[p]) - 1 : int(n) - 1;
     if (last < 1) return;
     const float atten = sh.atten;
@@ -1139,7 +1158,7 @@ __device__ __forceinline__ void adjoint_pixel(
     const float qx = float(px) + 0.5f, qy = float(py) + 0.5f;
     const float gC0 = g.x, gC1 = g.y, gC2 = g.z;
     TransF gT{g.x * sh.clear[0] + g.y * sh.clear[1] + g.z * sh.clear[2] + g.w * (sh.clear[3] - 1.f), 0.f};
-    TransF T{tfinal[p], 0.f};
+    TransBack T(tfinal[p]);
     const int last = sh.use_ert ? int(term[p]) - 1 : int(n) - 1;
     if (last < 1) return;
     const float atten = sh.atten;

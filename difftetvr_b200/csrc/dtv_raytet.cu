@@ -239,7 +239,7 @@ __device__ __forceinline__ void walk_adjoint_carried(
     const u64* __restrict__ b_records, u64 beg, const uint32_t* __restrict__ bf_global,
     const uint4* __restrict__ faces, const uint32_t* __restrict__ f2t, const TetTopo& tt, uint32_t num_tets,
     const int2* __restrict__ vfix, const VGeo* __restrict__ vgeo, const float4* __restrict__ colors, int px, int py,
-    float scale, float atten, float gC0, float gC1, float gC2, TransF T, TransF gT, uint32_t t, uint32_t fe,
+    float scale, float atten, float gC0, float gC1, float gC2, TransBack T, TransF gT, uint32_t t, uint32_t fe,
     uint32_t fx, int b, Acc& acc) {
     const float qx = float(px) + 0.5f, qy = float(py) + 0.5f;
     FragG fX = load_frag_g(fx << 2, faces[fx], qx, qy, vgeo, colors, gC0, gC1, gC2);
@@ -324,7 +324,7 @@ __global__ void __launch_bounds__(kTile * kTile, 2) k_walk_adjoint(
     const float atten = sh.atten;
     const float gC0 = g.x, gC1 = g.y, gC2 = g.z;
     TransF gT{g.x * sh.clear[0] + g.y * sh.clear[1] + g.z * sh.clear[2] + g.w * (sh.clear[3] - 1.f), 0.f};
-    TransF T{tfinal[p], 0.f};
+    TransBack T(tfinal[p]);
     uint32_t t = ws.x, fe = ws.y;
     int b = int(ws.z);
     uint32_t fx = tet_face_at(tt, vfix, t, fe, false, px, py);
