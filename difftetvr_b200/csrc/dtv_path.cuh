@@ -496,7 +496,10 @@ struct GradAcc {
 // of thread t at c4[t + s * stride], c1[t + s * stride]; flush() writes the
 // remaining ones at the end of the pixel.  (A block-wide shared-memory table
 // behind it, summing the tile's pixels with shared-memory atomics, and a
-// warp-wide merge of equal retired vertices both measured slower.)
+// warp-wide merge of equal retired vertices both measured slower.)  It takes
+// faces in their stored vertex order and finds each vertex's slot by id; the
+// screen-space adjoints use the ordered caches below (no search), this one
+// serves the world-space rows of absolute-value gradients.
 struct VertCache {
     static constexpr bool kOrdered = false;
     static constexpr uint32_t kNone = 0xffffffffu;
