@@ -9,7 +9,7 @@ from __future__ import annotations
 
 import torch
 
-TILES = (0, 1, 2)               # 16x16, 32x8, 8x32 pixels per 256-thread block
+TILES = (0, 1, 2)               # composite 16x16, 32x8, 8x32 (256 threads); adjoint 16x8, 32x4, 8x16 (128)
 SORT_CLASSES = (1, 2, 3, 4, 5)  # lists of up to 64, 128, 256, 512, 1024 records
 SORT_METHODS = ("bucket", "surrogate", "network")
 

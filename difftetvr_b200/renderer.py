@@ -152,8 +152,8 @@ class Renderer:
 
     def set_tuning(self, composite_tile: int | None = None, adjoint_tile: int | None = None,
                    sort_surrogate_classes: int | None = None, sort_bucket_classes: int | None = None) -> None:
-        """Pixel tile of the composite / adjoint blocks (0: 16x16, 1: 32x8,
-        2: 8x32) and the sort method per list-length class c = 1..4: depth
+        """Pixel tile of the composite blocks (0: 16x16, 1: 32x8, 2: 8x32) and
+        of the adjoint blocks (0: 16x8, 1: 32x4, 2: 8x16), and the sort method per list-length class c = 1..4: depth
         buckets (bit c of sort_bucket_classes), else 32-bit surrogate keys (bit
         c of sort_surrogate_classes), else the 64-bit network.  Results are
         identical for every setting."""

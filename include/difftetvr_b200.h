@@ -149,7 +149,8 @@ int32_t dtv_renderer_render_adjoint_cells(dtv_renderer* r, const dtv_mesh* mesh,
                                           float* d_grad_cell_colors, dtv_stream stream);
 
 /* Kernel configuration of a renderer (or batch): the pixel tile of the
- * composite and adjoint blocks (0: 16 x 16, 1: 32 x 8, 2: 8 x 32 pixels) and,
+ * composite blocks (0: 16 x 16, 1: 32 x 8, 2: 8 x 32 pixels), of the adjoint
+ * blocks (0: 16 x 8, 1: 32 x 4, 2: 8 x 16) and,
  * per list-length class c (bit c; 1..4 = lists of up to 64, 128, 256, 512
  * records, 5 = up to 1024), the per-pixel sort method: distribution into
  * depth buckets plus an exact fix-up (bit c of sort_bucket_classes, c = 1..5),
