@@ -93,17 +93,21 @@ def autotune_renderer(renderer, trials: int = 3, force: bool = False) -> dict:
 
     best = renderer.get_tuning()
     best_ms = measure(**best)
+    # Each knob's starting value was measured with the configuration before
+    # it, so it is skipped even when another value has become the best.
     for knob, values in (("composite_tile", TILES), ("adjoint_tile", TILES if with_adjoint else (best["adjoint_tile"],))):
+        start = best[knob]
         for v in values:
-            if v == best[knob]:
+            if v == start:
                 continue
             cand = dict(best, **{knob: v})
             ms = measure(**cand)
             if ms < best_ms:
                 best, best_ms = cand, ms
     for c in SORT_CLASSES:
+        start = sort_method(best, c)
         for method in methods_for(c):
-            if method == sort_method(best, c):
+            if method == start:
                 continue
             cand = with_sort_method(best, c, method)
             ms = measure(**cand)
@@ -134,8 +138,9 @@ def autotune_batch(batch_renderer, views, trials: int = 2, force: bool = False) 
     best = batch_renderer.get_tuning()
     best_ms = measure(best)
     for c in SORT_CLASSES:
+        start = sort_method(best, c)  # measured already (see autotune_renderer)
         for method in methods_for(c):
-            if method == sort_method(best, c):
+            if method == start:
                 continue
             cand = with_sort_method(best, c, method)
             ms = measure(cand)
