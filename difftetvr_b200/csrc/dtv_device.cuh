@@ -219,14 +219,4 @@ __device__ __forceinline__ bool skip_pair(uint32_t bits0, uint32_t bits1) {
     return ((bits0 & 3u) == 2u) && ((bits1 & 3u) == 3u);
 }
 
-__device__ __forceinline__ float4 lerp4(const float4& a, const float4& b, float t) {
-    return make_float4(a.x + (b.x - a.x) * t, a.y + (b.y - a.y) * t, a.z + (b.z - a.z) * t, a.w + (b.w - a.w) * t);
-}
-
-__device__ __forceinline__ float4 f4add(float4 a, float4 b) {
-    return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w);
-}
-
-__device__ __forceinline__ float4 f4scale(float4 a, float s) { return make_float4(a.x * s, a.y * s, a.z * s, a.w * s); }
-
 }  // namespace dtv
