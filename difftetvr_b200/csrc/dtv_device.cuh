@@ -13,6 +13,15 @@
 
 namespace dtv {
 
+// Two-wide FP32 arithmetic of sm_100: one FFMA2 / FMUL2 / FADD2 issues two
+// FP32 operations, each rounded as its scalar form.
+__device__ __forceinline__ float2 bc2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, bc2(-1.0f), a); }  // a - b
+__device__ __forceinline__ float hsum2(float2 a) { return a.x + a.y; }
+
 // Projected vertex: screen position, 1/ze and ze (view depth).
 __device__ __forceinline__ float4 project_vertex(const CamDev& c, float x, float y, float z, int2& fix) {
     const float* V = c.V;
@@ -179,10 +188,12 @@ __device__ __forceinline__ float cross_res(float ax, float ay, float arx, float 
 
 __device__ __forceinline__ void face_interp(const VGeo& a, const VGeo& b, const VGeo& c, float qx, float qy,
                                             FaceInterp& fi) {
-    // Snapped differences: multiples of 1/256 px below 2^16 px, exact.
-    const float d0x = a.sx - qx, d0y = a.sy - qy;
-    const float d1x = b.sx - qx, d1y = b.sy - qy;
-    const float d2x = c.sx - qx, d2y = c.sy - qy;
+    // Snapped differences: multiples of 1/256 px below 2^16 px, exact (x and
+    // y as one FP32 pair).
+    const float2 nq = make_float2(-qx, -qy);
+    const float2 d0 = add2(make_float2(a.sx, a.sy), nq), d1 = add2(make_float2(b.sx, b.sy), nq),
+                 d2 = add2(make_float2(c.sx, c.sy), nq);
+    const float d0x = d0.x, d0y = d0.y, d1x = d1.x, d1y = d1.y, d2x = d2.x, d2y = d2.y;
     const float E0 = cross_res(d1x, d1y, b.rx, b.ry, d2x, d2y, c.rx, c.ry);
     const float E1 = cross_res(d2x, d2y, c.rx, c.ry, d0x, d0y, a.rx, a.ry);
     const float E2 = cross_res(d0x, d0y, a.rx, a.ry, d1x, d1y, b.rx, b.ry);
@@ -191,8 +202,10 @@ __device__ __forceinline__ void face_interp(const VGeo& a, const VGeo& b, const 
     fi.lam[0] = E0 * iA;
     fi.lam[1] = E1 * iA;
     fi.lam[2] = E2 * iA;
-    fi.dx[0] = d0x + a.rx; fi.dx[1] = d1x + b.rx; fi.dx[2] = d2x + c.rx;
-    fi.dy[0] = d0y + a.ry; fi.dy[1] = d1y + b.ry; fi.dy[2] = d2y + c.ry;
+    const float2 e0 = add2(d0, make_float2(a.rx, a.ry)), e1 = add2(d1, make_float2(b.rx, b.ry)),
+                 e2 = add2(d2, make_float2(c.rx, c.ry));
+    fi.dx[0] = e0.x; fi.dx[1] = e1.x; fi.dx[2] = e2.x;
+    fi.dy[0] = e0.y; fi.dy[1] = e1.y; fi.dy[2] = e2.y;
     const float u0 = fi.lam[0] * a.iz, u1 = fi.lam[1] * b.iz, u2 = fi.lam[2] * c.iz;
     fi.zb = __fdividef(1.0f, u0 + u1 + u2);
     fi.bary[0] = u0 * fi.zb;

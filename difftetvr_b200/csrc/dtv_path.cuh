@@ -323,10 +323,13 @@ __device__ __forceinline__ FragV load_frag_face(uint32_t lo, const uint4& fc, fl
     float bary[3];
     face_bary(a, b, c, qx, qy, bary, fr.z);  // depth and colour from the same weights
     const float4 c0 = colors[fc.x], c1 = colors[fc.y], c2 = colors[fc.z];
-    fr.col = make_float4(bary[0] * c0.x + bary[1] * c1.x + bary[2] * c2.x,
-                         bary[0] * c0.y + bary[1] * c1.y + bary[2] * c2.y,
-                         bary[0] * c0.z + bary[1] * c1.z + bary[2] * c2.z,
-                         bary[0] * c0.w + bary[1] * c1.w + bary[2] * c2.w);
+    // (r, g) and (b, a) as FP32 pairs.
+    const float2 b0 = bc2(bary[0]), b1 = bc2(bary[1]), b2 = bc2(bary[2]);
+    const float2 rg = fma2(b2, make_float2(c2.x, c2.y),
+                           fma2(b1, make_float2(c1.x, c1.y), mul2(b0, make_float2(c0.x, c0.y))));
+    const float2 ba = fma2(b2, make_float2(c2.z, c2.w),
+                           fma2(b1, make_float2(c1.z, c1.w), mul2(b0, make_float2(c0.z, c0.w))));
+    fr.col = make_float4(rg.x, rg.y, ba.x, ba.y);
     return fr;
 }
 

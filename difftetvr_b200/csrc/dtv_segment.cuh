@@ -136,17 +136,9 @@ __device__ __forceinline__ SegTerms seg_terms_adj_short(float t, float a) {
     return s;
 }
 
-// Two-wide FP32 arithmetic of sm_100: one FFMA2 / FMUL2 / FADD2 issues two
-// FP32 operations, each rounded as its scalar form.  The four sub-segments of
-// a segment have independent series terms, so they run as two pairs
-// (sub-segments 0,1 and 2,3) at half the issue slots.
-__device__ __forceinline__ float2 bc2(float a) { return make_float2(a, a); }
-__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
-__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
-__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
-__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, bc2(-1.0f), a); }  // a - b
-__device__ __forceinline__ float hsum2(float2 a) { return a.x + a.y; }
-
+// The four sub-segments of a segment have independent series terms, so they
+// run as two pairs (sub-segments 0,1 and 2,3) of sm_100's two-wide FP32
+// instructions (fma2 / mul2 / add2, dtv_device.cuh) at half the issue slots.
 struct SegTerms2 {
     float2 A, omA, K, dK;
 };
