@@ -728,6 +728,36 @@ def run_batched(args, res: int, steps: int, warmup: int = 2):
     for r in rends:
         r.set_stage_timing(False)
     busy_total = sum(busy.values())
+    # Each mesh's views alone: a batch of that mesh only (tuned, CUDA graph)
+    # against the plain loop over the same views, both device-timed.  The
+    # small meshes show how much launch and host time one launch per stage
+    # removes when per-view work is small.
+    per_mesh = {}
+    k_steps = max(5, steps // 2)
+    for mi, n in enumerate(sizes):
+        own = [v for v in views if v.mesh == mi]
+        vm = [View(mesh=0, view_matrix=v.view_matrix, width=res, height=res, target=v.target) for v in own]
+        bm = BatchRenderer([mk(n, 1 + mi)], attenuation=1.0)
+        autotune_batch(bm, vm)
+        bm.set_graph(True)
+        ms_b = timed(lambda i: bm.train_step(vm, lr_positions=LR_POS, lr_colors=LR_COL, clamp_colors=1), k_steps)
+        del bm
+
+        def plain_mesh(i, mi=mi, own=own):
+            opts[mi].zero_grad(set_to_none=False)
+            r = rends[mi]
+            for v in own:
+                r.set_view_matrix(v.view_matrix)
+                img = r.render()
+                _lib.call("dtv_loss_l2", img.data_ptr(), v.target.data_ptr(), n_img, 1.0 / n_img, adj.data_ptr(),
+                          loss.data_ptr(), stream.cuda_stream)
+                r.render_adjoint(adj)
+            opts[mi].step()
+
+        ms_p = timed(plain_mesh, k_steps)
+        per_mesh[f"{n}^3"] = {"views": len(own), "batched_views_per_s": round(len(own) / (ms_b / 1e3), 1),
+                              "plain_views_per_s": round(len(own) / (ms_p / 1e3), 1),
+                              "speedup": round(ms_p / ms_b, 3), "steps": k_steps}
     nv = len(views)
     return {"res": res, "views": nv, "views_per_mesh": counts, "meshes": [f"{n}^3" for n in sizes],
             "batched_views_per_s": nv / (ms_batched / 1e3), "plain_views_per_s": nv / (ms_plain / 1e3),
@@ -737,6 +767,7 @@ def run_batched(args, res: int, steps: int, warmup: int = 2):
             "plain_stage_busy_ms": {k2: round(v2, 3) for k2, v2 in stage_busy.items()},
             "plain_overhead_ms": round(ms_plain - busy_total, 3),
             "speedup_bound_same_kernels": round(ms_plain / busy_total, 3) if busy_total > 0 else None,
+            "per_mesh": per_mesh,
             "tuning_batch": tuned_batch,
             "graph": info["graph"], "steps": steps, "warmup": warmup}
 
