@@ -157,8 +157,11 @@ def test_image_with_early_ray_termination(oracle):
 
 # two_blocks: rays leave one block and enter the other, so consecutive faces of
 # a list share no vertex there (every cached vertex row is written out).
+# (16, 512): the 16^3 / 512^2 configuration the reference runs on the CPU,
+# with and without early ray termination.
 @pytest.mark.parametrize("kind,n,res,ert", [("cube", 8, 128, False), ("cube", 16, 256, False),
-                                            ("cube", 8, 128, True), ("two_blocks", 4, 128, False)])
+                                            ("cube", 8, 128, True), ("two_blocks", 4, 128, False),
+                                            ("cube", 16, 512, False), ("cube", 16, 512, True)])
 def test_gradients_match_fp64_oracle(oracle, kind, n, res, ert):
     if kind == "two_blocks":
         sc = two_block_scene(n, res, seed=20 + n)
