@@ -103,8 +103,10 @@ def test_image_with_early_ray_termination(oracle):
     assert (nseg_o < nseg_full).sum() > 100  # ERT actually fired
 
 
+# (16, 512): the 16^3 / 512^2 configuration the reference runs on the CPU.
 @pytest.mark.parametrize("kind,n,res,ert", [("cube", 8, 128, False), ("cube", 16, 256, False),
-                                            ("cube", 8, 128, True), ("two_blocks", 4, 128, False)])
+                                            ("cube", 8, 128, True), ("two_blocks", 4, 128, False),
+                                            ("cube", 16, 512, False), ("cube", 16, 512, True)])
 def test_gradients_match_fp64_oracle(oracle, kind, n, res, ert):
     sc = _scene(kind, n, res, seed=20 + n, attenuation=2.0 if ert else 1.0, ert=ert)
     mesh, r = sc.make_renderer(_intersection())
