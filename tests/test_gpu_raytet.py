@@ -127,6 +127,27 @@ def test_gradients_match_fp64_oracle(oracle, kind, n, res, ert):
     assert rel_err(gc, gc_o) < GRAD_TOL, rel_err(gc, gc_o)
 
 
+@pytest.mark.parametrize("kind,n,res", [("cube", 8, 128), ("two_blocks", 4, 128)])
+def test_absolute_gradients_match_fp64_oracle(oracle, kind, n, res):
+    """render_adjoint(use_abs_grad=True) on the walk: absolute value of each
+    fragment's contribution per vertex (world-space rows, straight atomics)."""
+    sc = _scene(kind, n, res, seed=40 + n)
+    mesh, r = sc.make_renderer(_intersection())
+    w = np.random.default_rng(6).normal(size=(res, res, 4)).astype(np.float32)
+    r.render()
+    pos, col = mesh.get_vertex_positions(), mesh.get_vertex_colors()
+    pos.grad.zero_()
+    col.grad.zero_()
+    r.render_adjoint(torch.from_numpy(w).cuda(), use_abs_grad=True)
+    gp, gc = pos.grad.cpu().numpy(), col.grad.cpu().numpy()
+    fa = oracle.Faces(sc.cells, sc.pos.shape[0])
+    _, _, _, gp_o, gc_o = oracle.raytet(fa, sc.pos.astype(np.float64), sc.col.astype(np.float64),
+                                        sc.oracle_camera(oracle), sc.oracle_params(oracle, use_abs_grad=True),
+                                        image_adjoint=w.astype(np.float64))
+    assert (gc >= 0).all() and rel_err(gp, gp_o) < GRAD_TOL and rel_err(gc, gc_o) < GRAD_TOL, \
+        (rel_err(gp, gp_o), rel_err(gc, gc_o))
+
+
 def test_gradients_vs_fp64_central_differences(oracle):
     """CUDA ray-tet adjoint vs FP64 central differences (step 1e-4,
     Richardson-refined) of the oracle's forward with frozen coverage: 64
