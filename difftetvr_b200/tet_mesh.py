@@ -61,6 +61,50 @@ def build_faces_host(cells: np.ndarray, num_vertices: int):
     return tri[:F].copy(), fb[:F].copy(), f2t[:F].copy(), vb
 
 
+def unlink_cells(cells: np.ndarray, positions: np.ndarray, vertex_colors: np.ndarray | None = None):
+    """TetMesh::unlinkTets (TetMesh.cpp:1950-1989) on host arrays: every cell
+    gets its own four vertices (vertex 4 t + k is corner k of cell t), so no
+    face is shared any more.
+
+    Returns (cells u32[T,4], positions f32[4T,3], vertex colours f32[4T,4] or None)."""
+    flat = np.asarray(cells, dtype=np.uint32).reshape(-1)
+    new_cells = np.arange(flat.size, dtype=np.uint32).reshape(-1, 4)
+    pos = np.ascontiguousarray(np.asarray(positions, dtype=np.float32)[flat])
+    col = None if vertex_colors is None else np.ascontiguousarray(np.asarray(vertex_colors, dtype=np.float32)[flat])
+    return new_cells, pos, col
+
+
+def remove_transparent_cells(cells: np.ndarray, positions: np.ndarray, vertex_colors: np.ndarray | None,
+                             cell_colors: np.ndarray | None, alpha_threshold: float):
+    """TetMesh::removeTransparentTets (TetMesh.cpp:1991-2084) on host arrays.
+
+    A cell stays when one of its vertices has alpha >= alpha_threshold
+    (per-vertex colours) or its own alpha is >= alpha_threshold (per-cell
+    colours).  The vertices the kept cells use stay, in their original order,
+    and the kept cells keep their order.
+
+    Returns (cells u32[T',4], positions f32[V',3], vertex colours or None,
+    cell colours or None)."""
+    cells = np.asarray(cells, dtype=np.uint32).reshape(-1, 4)
+    pos = np.asarray(positions, dtype=np.float32).reshape(-1, 3)
+    thr = np.float32(alpha_threshold)
+    if vertex_colors is not None:
+        vcol = np.asarray(vertex_colors, dtype=np.float32).reshape(-1, 4)
+        keep = (vcol[cells, 3] >= thr).any(axis=1)
+    else:
+        ccol = np.asarray(cell_colors, dtype=np.float32).reshape(-1, 4)
+        keep = ccol[:, 3] >= thr
+    kept = cells[keep]
+    used = np.zeros(pos.shape[0], dtype=bool)
+    used[kept.reshape(-1)] = True
+    new_index = (np.cumsum(used) - used).astype(np.uint32)  # rank among the used vertices
+    new_cells = np.ascontiguousarray(new_index[kept])
+    new_pos = np.ascontiguousarray(pos[used])
+    new_vcol = None if vertex_colors is None else np.ascontiguousarray(vcol[used])
+    new_ccol = None if vertex_colors is not None else np.ascontiguousarray(ccol[keep])
+    return new_cells, new_pos, new_vcol, new_ccol
+
+
 class NativeMesh:
     """Owner of a dtv_mesh handle (device face topology)."""
 
@@ -108,6 +152,7 @@ class TetMesh:
         self._color_storage = ColorStorage.PER_VERTEX
         self._native: NativeMesh | None = None
         self._vertex_boundary: torch.Tensor | None = None
+        self._force_ovm = False
 
     # -- construction ------------------------------------------------------
     def set_use_gradients(self, use_gradients: bool = True) -> None:
@@ -234,6 +279,45 @@ class TetMesh:
             self.set_tet_mesh_data(c2, p2, v2)
         if volume_renderer is not None:
             volume_renderer.set_tet_mesh(self)
+
+    def set_force_use_ovm_representation(self) -> None:
+        """TetMesh::setForceUseOvmRepresentation (Module.cpp:794): the
+        reference keeps an OpenVolumeMesh copy of the mesh for coarse-to-fine
+        splitting.  The split here works on the plain cell and vertex arrays
+        (dtv_mesh_subdivide_vertices), so the flag is only recorded."""
+        self._force_ovm = True
+
+    # -- topology edits (Module.cpp:816-819) ---------------------------------
+    def _host_arrays(self):
+        pos = self._positions.detach().cpu().numpy()
+        vcol = None if self._colors is None else self._colors.detach().cpu().numpy()
+        ccol = None if self._cell_colors is None else self._cell_colors.detach().cpu().numpy()
+        return pos, vcol, ccol
+
+    def unlink_tets(self) -> None:
+        """TetMesh::unlinkTets (TetMesh.cpp:1950-1989): every cell gets its
+        own four vertices (a shared-index mesh becomes a cell soup)."""
+        if self._cells is None:
+            raise RuntimeError("Missing valid tet mesh.")
+        pos, vcol, ccol = self._host_arrays()
+        cells, pos, vcol = unlink_cells(self._cells, pos, vcol)
+        if ccol is not None:
+            self.set_tet_mesh_data_cell(cells, pos, ccol)
+        else:
+            self.set_tet_mesh_data(cells, pos, vcol)
+
+    def remove_transparent_tets(self, alpha_threshold: float) -> None:
+        """TetMesh::removeTransparentTets (TetMesh.cpp:1991-2084): removes the
+        cells with no vertex alpha (per-cell colours: no cell alpha) >=
+        alpha_threshold, and the vertices no remaining cell uses."""
+        if self._cells is None:
+            raise RuntimeError("Missing valid tet mesh.")
+        pos, vcol, ccol = self._host_arrays()
+        cells, pos, vcol, ccol = remove_transparent_cells(self._cells, pos, vcol, ccol, alpha_threshold)
+        if ccol is not None:
+            self.set_tet_mesh_data_cell(cells, pos, ccol)
+        else:
+            self.set_tet_mesh_data(cells, pos, vcol)
 
     # -- files (Module.cpp:787-788) ------------------------------------------
     def load_from_file(self, file_path: str) -> bool:

@@ -73,3 +73,66 @@ def test_empty_mesh():
 def test_out_of_range_cell_rejected():
     with pytest.raises(RuntimeError):
         d.build_faces_host(np.array([[0, 1, 2, 9]], np.uint32), 4)
+
+
+def _remove_transparent_loops(cells, pos, vcol, ccol, thr):
+    """removeTransparentTets (TetMesh.cpp:1991-2084) restated with loops."""
+    used_v = [False] * pos.shape[0]
+    keep = []
+    for t, c in enumerate(cells):
+        above = any(vcol[v, 3] >= thr for v in c) if vcol is not None else ccol[t, 3] >= thr
+        if above:
+            keep.append(t)
+            for v in c:
+                used_v[v] = True
+    remap, k = [0] * pos.shape[0], 0
+    for v in range(pos.shape[0]):
+        remap[v] = k
+        k += used_v[v]
+    new_cells = np.array([[remap[v] for v in cells[t]] for t in keep], np.uint32).reshape(-1, 4)
+    sel = np.array(used_v, bool)
+    return (new_cells, pos[sel], None if vcol is None else vcol[sel],
+            None if ccol is None else ccol[np.array(keep, np.int64)])
+
+
+def test_unlink_cells_gives_each_cell_its_own_vertices():
+    from difftetvr_b200.tet_mesh import unlink_cells
+    cells, pos = S.kuhn_mesh(3, seed=4)
+    col = S.gaussian_colors(pos, seed=4)
+    c2, p2, v2 = unlink_cells(cells, pos, col)
+    assert c2.shape == cells.shape and p2.shape == (4 * cells.shape[0], 3)
+    np.testing.assert_array_equal(c2.reshape(-1), np.arange(c2.size))
+    np.testing.assert_array_equal(p2[c2], pos[cells])  # every corner in place
+    np.testing.assert_array_equal(v2[c2], col[cells])
+    tri, fb, _, _ = d.build_faces_host(c2, p2.shape[0])
+    assert tri.shape[0] == 4 * cells.shape[0] and fb.all()  # no face shared: all boundary
+
+
+@pytest.mark.parametrize("per_cell", [False, True])
+def test_remove_transparent_cells_matches_loop_restatement(per_cell):
+    from difftetvr_b200.tet_mesh import remove_transparent_cells
+    rng = np.random.default_rng(11)
+    cells, pos = S.kuhn_mesh(4, seed=2)
+    vcol = rng.uniform(0, 1, (pos.shape[0], 4)).astype(np.float32)
+    vcol[:, 3] = np.where(rng.uniform(size=pos.shape[0]) < 0.8, 0.05, 0.9)
+    ccol = rng.uniform(0, 1, (cells.shape[0], 4)).astype(np.float32)
+    if per_cell:
+        vcol = None
+    else:
+        ccol = None
+    for thr in (0.0, 0.05, 0.5, 2.0):
+        got = remove_transparent_cells(cells, pos, vcol, ccol, thr)
+        want = _remove_transparent_loops(cells, pos, vcol, ccol, thr)
+        for g, w in zip(got, want):
+            if w is None:
+                assert g is None
+            else:
+                np.testing.assert_array_equal(g, w)
+        if thr == 0.0:
+            np.testing.assert_array_equal(got[0], cells)  # nothing removed
+        if thr == 0.05 and not per_cell:  # alpha == threshold keeps a cell
+            np.testing.assert_array_equal(got[0], cells)
+        if thr == 0.5:
+            assert 0 < got[0].shape[0] < cells.shape[0]
+        if thr == 2.0:
+            assert got[0].shape == (0, 4) and got[1].shape == (0, 3)
