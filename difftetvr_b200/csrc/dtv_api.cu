@@ -94,6 +94,7 @@ struct dtv_renderer {
     size_t h_rowoff_cap = 0;
     DevBuf<uint32_t> fill_order;    // faces in row-band order for the fill
     DevBuf<uint32_t> band_scratch;  // band counts and cursors of fill_order
+    DevBuf<uint32_t> wide_list;     // [0] = n, then the faces of the 64-bit raster path (count -> fill)
     DevBuf<uint4> wstate;         // ray-tet path: (last tet, its entry face, boundary entry index, segments)
     u64* h_nf = nullptr;          // pinned
     // State of the last render.
@@ -156,7 +157,8 @@ void build_band_lists(dtv_renderer* r, const dtv_mesh* mesh, int W, int H, int y
     dtv::launch_scan(r->counts.ptr + p0, pb, r->offsets.ptr + p0, r->scan_scratch.ptr, s);
     check_launch("band scan");
     dtv::launch_raster_fill(mesh->d_faces, uint32_t(mesh->host.num_faces), r->vproj.ptr, r->vfix.ptr, W, H,
-                            r->counts.ptr, r->offsets.ptr, r->records.ptr, s, y0, y1, r->fill_order.ptr);
+                            r->counts.ptr, r->offsets.ptr, r->records.ptr, s, y0, y1, r->fill_order.ptr,
+                            r->wide_list.ptr);
     check_launch("band fill");
     dtv::launch_sort(r->offsets.ptr + p0, r->records.ptr, uint32_t(pb), r->long_list.ptr, s, nullptr,
                      r->tuning.sort_surrogate_classes, r->tuning.sort_bucket_classes);
@@ -240,9 +242,10 @@ void adjoint_banded(dtv_renderer* r, const dtv_mesh* mesh, const float* d_colors
                     const dtv::ShadeDev& sh, float* d_grad_positions, float* d_grad_colors, cudaStream_t s) {
     const int W = r->cam.W, H = r->cam.H;
     DTV_CK(cudaMemsetAsync(r->grad_rows.ptr, 0, sizeof(float4) * 2 * size_t(r->V ? r->V : 1), s));
+    r->wide_list.ensure(size_t(mesh->host.num_faces) + 1, s);
     for (const auto& b : r->bands) {
         dtv::launch_raster_count(mesh->d_faces, uint32_t(mesh->host.num_faces), r->vproj.ptr, r->vfix.ptr, W, H,
-                                 r->counts.ptr, s, b.first, b.second);
+                                 r->counts.ptr, s, b.first, b.second, r->wide_list.ptr);
         check_launch("band count");
         build_band_lists(r, mesh, W, H, b.first, b.second, s);
         adjoint_rows(r, mesh, d_colors, d_image_adjoint, sh, b.first, b.second, d_grad_colors, s);
@@ -421,6 +424,7 @@ int32_t dtv_renderer_destroy(dtv_renderer* r) {
     r->wstate.release();
     r->fill_order.release();
     r->band_scratch.release();
+    r->wide_list.release();
     if (r->h_nf) cudaFreeHost(r->h_nf);
     if (r->h_rowoff) cudaFreeHost(r->h_rowoff);
     for (auto& e : r->ev)
@@ -479,7 +483,9 @@ int32_t render_common(dtv_renderer* r, const dtv_mesh* mesh, const float* d_posi
         dtv::launch_project(d_positions, uint32_t(V), cam, r->vproj.ptr, r->vfix.ptr, r->vgeo.ptr, s);
         check_launch("project");
         rec_event(r, 1, s);
-        dtv::launch_raster_count(rfaces, uint32_t(F), r->vproj.ptr, r->vfix.ptr, W, H, r->counts.ptr, s);
+        r->wide_list.ensure(size_t(F) + 1, s);
+        dtv::launch_raster_count(rfaces, uint32_t(F), r->vproj.ptr, r->vfix.ptr, W, H, r->counts.ptr, s, 0, -1,
+                                 r->wide_list.ptr);
         check_launch("raster count");
         rec_event(r, 2, s);
         dtv::launch_scan(r->counts.ptr, P, r->offsets.ptr, r->scan_scratch.ptr, s);
@@ -524,7 +530,7 @@ int32_t render_common(dtv_renderer* r, const dtv_mesh* mesh, const float* d_posi
         r->band_scratch.ensure(2 * dtv::kFillBands, s);
         dtv::launch_fill_order(rfaces, uint32_t(F), r->vfix.ptr, H, nf, r->fill_order.ptr, r->band_scratch.ptr, s);
         dtv::launch_raster_fill(rfaces, uint32_t(F), r->vproj.ptr, r->vfix.ptr, W, H, r->counts.ptr,
-                                r->offsets.ptr, r->records.ptr, s, 0, -1, r->fill_order.ptr);
+                                r->offsets.ptr, r->records.ptr, s, 0, -1, r->fill_order.ptr, r->wide_list.ptr);
         check_launch("raster fill");
         rec_event(r, 4, s);
         dtv::launch_sort(r->offsets.ptr, r->records.ptr, uint32_t(P), r->long_list.ptr, s, nullptr,

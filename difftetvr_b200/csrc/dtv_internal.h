@@ -32,12 +32,17 @@ void build_faces(const uint32_t* cells, uint64_t T, uint64_t V, MeshHost& out);
 // Launch wrappers (dtv_kernels.cu).  All run on `s`.
 void launch_project(const float* pos, uint32_t V, const CamDev& cam, float4* vproj, int2* vfix, VGeo* vgeo,
                     cudaStream_t s);
-// Pixel rows [row0, row1) only (row1 < 0: all rows).
+// Pixel rows [row0, row1) only (row1 < 0: all rows).  wide_list (u32[F + 1],
+// optional): the count lists the faces of the 64-bit path there, and the
+// 64-bit count and the fill that follows (same rows) walk that list instead of
+// setting up every face again; without it both 64-bit launches cover all F.
 void launch_raster_count(const uint4* faces, uint32_t F, const float4* vproj, const int2* vfix, int W, int H,
-                         uint32_t* counts, cudaStream_t s, int row0 = 0, int row1 = -1);
+                         uint32_t* counts, cudaStream_t s, int row0 = 0, int row1 = -1,
+                         uint32_t* wide_list = nullptr);
 void launch_raster_fill(const uint4* faces, uint32_t F, const float4* vproj, const int2* vfix, int W, int H,
                         uint32_t* counts, const unsigned long long* offsets, unsigned long long* records,
-                        cudaStream_t s, int row0 = 0, int row1 = -1, const uint32_t* order = nullptr);
+                        cudaStream_t s, int row0 = 0, int row1 = -1, const uint32_t* order = nullptr,
+                        const uint32_t* wide_list = nullptr);
 // Order of the faces for the fill, grouped by row bands of about
 // kFillBandBytes of records each (nf records over H rows; order: F entries;
 // band_scratch: 2 * kFillBands entries).

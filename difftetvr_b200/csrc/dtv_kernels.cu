@@ -45,13 +45,28 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster(const uint4* __res
                                                               uint32_t* __restrict__ counts,
                                                               const u64* __restrict__ offsets,
                                                               u64* __restrict__ records,
-                                                              const uint32_t* __restrict__ order) {
+                                                              const uint32_t* __restrict__ order,
+                                                              uint32_t* __restrict__ wide_list) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t f = (order && i < F) ? order[i] : i;
     RasterJob J;
-    const bool live = i < F && raster_setup(f, faces, vfix, 0u, W, row0, row1, 0ull, J) && (J.wide != 0) == WIDE;
+    const bool set = i < F && raster_setup(f, faces, vfix, 0u, W, row0, row1, 0ull, J);
+    const bool live = set && (J.wide != 0) == WIDE;
     if constexpr (!FILL) {
         if (live) count_face<typename std::conditional<WIDE, long long, int>::type>(J, counts);
+        if (!WIDE && wide_list) {
+            // The faces of the 64-bit path, for its count and fill launches
+            // (wide_list[0] = how many, then the face ids).
+            const bool wide = set && J.wide != 0;
+            const unsigned m = __ballot_sync(kFull, wide);
+            if (m) {
+                const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
+                uint32_t base = 0;
+                if (lane == leader) base = atomicAdd(wide_list, uint32_t(__popc(m)));
+                base = __shfl_sync(kFull, base, leader);
+                if (wide) wide_list[1 + base + __popc(m & ((1u << lane) - 1u))] = f;
+            }
+        }
     } else {
         __shared__ RasterJob jobs[kRasterWarps][32];
         const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -60,6 +75,37 @@ __global__ void __launch_bounds__(32 * kRasterWarps) k_raster(const uint4* __res
     }
 }
 
+// The 64-bit faces listed by the count (wide_list), 32 per warp and step over
+// a fixed grid: the count (one thread per face) or the fill (raster_warp).
+template <bool FILL>
+__global__ void __launch_bounds__(32 * kRasterWarps) k_raster_listed(const uint4* __restrict__ faces,
+                                                                     const float4* __restrict__ vproj,
+                                                                     const int2* __restrict__ vfix, int W, int row0,
+                                                                     int row1, uint32_t* __restrict__ counts,
+                                                                     const u64* __restrict__ offsets,
+                                                                     u64* __restrict__ records,
+                                                                     const uint32_t* __restrict__ wide_list) {
+    __shared__ RasterJob jobs[kRasterWarps][32];
+    const uint32_t n = wide_list[0];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x + uint32_t(w) * 32u; base < n; base += stride) {
+        const uint32_t i = base + uint32_t(lane);
+        RasterJob J;
+        const bool live = i < n && raster_setup(wide_list[1 + i], faces, vfix, 0u, W, row0, row1, 0ull, J) &&
+                          J.wide != 0;
+        if constexpr (!FILL) {
+            if (live) count_face<long long>(J, counts);
+        } else {
+            if (live) jobs[w][lane] = J;
+            raster_warp<FILL, true>(jobs[w], __ballot_sync(kFull, live), lane, vproj, counts, offsets, records);
+            __syncwarp();  // every lane is done with this step's jobs before the next step writes them
+        }
+    }
+}
+
+constexpr unsigned kListedBlocks = 148;
+
 // Difference array of the count pass -> per-pixel counts, rows [row0, row1).
 __global__ void __launch_bounds__(256) k_row_prefix(uint32_t* __restrict__ counts, int W, int row0, int row1) {
     const int row = row0 + int(blockIdx.x) * 8 + int(threadIdx.x >> 5);
@@ -67,28 +113,37 @@ __global__ void __launch_bounds__(256) k_row_prefix(uint32_t* __restrict__ count
 }
 
 void launch_raster_count(const uint4* faces, uint32_t F, const float4* vproj, const int2* vfix, int W, int H,
-                         uint32_t* counts, cudaStream_t s, int row0, int row1) {
+                         uint32_t* counts, cudaStream_t s, int row0, int row1, uint32_t* wide_list) {
     if (F == 0) return;
     if (row1 < 0) row1 = H;
     if (row1 <= row0) return;
     const unsigned blocks = (F + 32 * kRasterWarps - 1) / (32 * kRasterWarps);
+    if (wide_list) cudaMemsetAsync(wide_list, 0, sizeof(uint32_t), s);
     k_raster<false, false><<<blocks, 32 * kRasterWarps, 0, s>>>(faces, F, vproj, vfix, W, row0, row1, counts, nullptr,
-                                                                nullptr, nullptr);
-    k_raster<false, true><<<blocks, 32 * kRasterWarps, 0, s>>>(faces, F, vproj, vfix, W, row0, row1, counts, nullptr,
-                                                               nullptr, nullptr);
+                                                                nullptr, nullptr, wide_list);
+    if (wide_list)
+        k_raster_listed<false><<<kListedBlocks, 32 * kRasterWarps, 0, s>>>(faces, vproj, vfix, W, row0, row1, counts,
+                                                                           nullptr, nullptr, wide_list);
+    else
+        k_raster<false, true><<<blocks, 32 * kRasterWarps, 0, s>>>(faces, F, vproj, vfix, W, row0, row1, counts,
+                                                                   nullptr, nullptr, nullptr, nullptr);
     k_row_prefix<<<unsigned(row1 - row0 + 7) / 8, 256, 0, s>>>(counts, W, row0, row1);
 }
 
 void launch_raster_fill(const uint4* faces, uint32_t F, const float4* vproj, const int2* vfix, int W, int H,
                         uint32_t* counts, const u64* offsets, u64* records, cudaStream_t s, int row0, int row1,
-                        const uint32_t* order) {
+                        const uint32_t* order, const uint32_t* wide_list) {
     if (F == 0) return;
     if (row1 < 0) row1 = H;
     const unsigned blocks = (F + 32 * kRasterWarps - 1) / (32 * kRasterWarps);
     k_raster<true, false><<<blocks, 32 * kRasterWarps, 0, s>>>(faces, F, vproj, vfix, W, row0, row1, counts, offsets,
-                                                               records, order);
-    k_raster<true, true><<<blocks, 32 * kRasterWarps, 0, s>>>(faces, F, vproj, vfix, W, row0, row1, counts, offsets,
-                                                              records, order);
+                                                               records, order, nullptr);
+    if (wide_list)
+        k_raster_listed<true><<<kListedBlocks, 32 * kRasterWarps, 0, s>>>(faces, vproj, vfix, W, row0, row1, counts,
+                                                                          offsets, records, wide_list);
+    else
+        k_raster<true, true><<<blocks, 32 * kRasterWarps, 0, s>>>(faces, F, vproj, vfix, W, row0, row1, counts,
+                                                                  offsets, records, order, nullptr);
 }
 
 // ---------------------------------------------------------------------------
