@@ -58,8 +58,8 @@ def parse_args():
     ap.add_argument("--no-scale", action="store_true")
     ap.add_argument("--scale-n", type=int, default=128)
     ap.add_argument("--scale-res", type=int, default=2048)
-    ap.add_argument("--scale-steps", type=int, default=3)
-    ap.add_argument("--scale-warmup", type=int, default=1)
+    ap.add_argument("--scale-steps", type=int, default=5)
+    ap.add_argument("--scale-warmup", type=int, default=3)
     ap.add_argument("--scale-cap-gb", type=float, default=40.0)
     ap.add_argument("--scale-recompute-gb", type=float, default=4.0)
     ap.add_argument("--batched-res", type=str, default="512,1024")
