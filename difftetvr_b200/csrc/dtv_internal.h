@@ -61,7 +61,7 @@ void launch_scan(const uint32_t* counts, uint64_t n, unsigned long long* offsets
 // sort_scratch_elems(P) u32 (length-class counts and lists).  With a non-null
 // `ok`, the sort does nothing when *ok == 0 (batched steps whose records
 // overflowed the buffer).
-constexpr int kSortClasses = 8;  // list-length classes (dtv_kernels.cu)
+constexpr int kSortClasses = 9;  // list-length classes (dtv_kernels.cu)
 constexpr size_t sort_scratch_elems(uint64_t P) { return 16 + size_t(kSortClasses) * size_t(P); }
 // surrogate_classes: bit c set = list-length class c (1..4: up to 64, 128,
 // 256, 512 records) is sorted through 32-bit surrogate keys, else through the

@@ -555,13 +555,17 @@ constexpr int kSortWarps = 8;
 // Length classes of the per-pixel lists.  A classification pass appends each
 // pixel with n >= 2 records to the list of its class (warp-aggregated
 // atomics); one kernel per class then sorts its lists, so each is compiled
-// with only the registers its class needs.  Classes 0..4: one warp per list,
-// 32 K records in registers (K = 1, 2, 4, 8, 16); class 5: one warp per list,
-// bitonic in shared memory (<= kSortWarpCap); class 6: one block per list
+// with only the registers its class needs.  Class 8: lists of 2..kSortTinyMax
+// records, one thread per list (sorting network in registers).  Classes 0..4:
+// one warp per list, 32 K records in registers (K = 1, 2, 4, 8, 16; class 0
+// from kSortTinyMax + 1 records); class 5: one warp per list, bitonic in
+// shared memory (<= kSortWarpCap); class 6: one block per list
 // (<= kSortBlockCap); class 7: one block per longer list, in place (merge
 // stages over global memory), so no list length is refused.
 // Scratch layout (u32): [0, 16) class counts, then kSortClasses lists of P.
 constexpr int kSortGridBlocks = 148 * 8;
+constexpr uint32_t kSortTinyMax = 8;
+constexpr int kSortTinyClass = 8;
 
 __device__ __forceinline__ int sort_class(uint32_t n) {
     if (n <= 32) return 0;
@@ -583,8 +587,10 @@ __global__ void __launch_bounds__(256) k_sort_classify(const u64* __restrict__ o
         const u64 n = offsets[p + 1] - offsets[p];
         if (n > kSortBlockCap)
             c = 7;
-        else if (n > 1)
+        else if (n > kSortTinyMax)
             c = sort_class(uint32_t(n));
+        else if (n > 1)
+            c = kSortTinyClass;
     }
     const unsigned act = __ballot_sync(kFull, c >= 0);
     if (c < 0) return;
@@ -596,6 +602,45 @@ __global__ void __launch_bounds__(256) k_sort_classify(const u64* __restrict__ o
     base = __shfl_sync(peers, base, leader);
     const uint32_t rank = uint32_t(__popc(peers & ((1u << lane) - 1u)));
     scratch[16 + size_t(c) * P + base + rank] = p;
+}
+
+// Class 8: one thread per list of 2..8 records.  The records (padded with
+// ~0, above every record) go through Batcher's odd-even merge network for
+// eight inputs (19 compare-exchanges of the 64-bit values, depth 6), and the
+// first n are stored back.  Lists this short are what the ray-tet path's
+// boundary lists and the silhouettes of the list path hold; one warp each
+// (class 0) spends a 32-lane bitonic network on two or four records.
+__device__ __forceinline__ void cmp_exch(u64& a, u64& b) {
+    const u64 lo = a < b ? a : b, hi = a < b ? b : a;
+    a = lo;
+    b = hi;
+}
+
+__global__ void __launch_bounds__(256) k_sort_class_tiny(const u64* __restrict__ offsets, u64* records,
+                                                         const uint32_t* __restrict__ items,
+                                                         const uint32_t* __restrict__ count,
+                                                         const uint32_t* __restrict__ ok) {
+    static_assert(kSortTinyMax == 8, "the network below sorts eight values");
+    if (ok && *ok == 0u) return;
+    const uint32_t num = *count;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < num; i += gridDim.x * blockDim.x) {
+        const uint32_t p = items[i];
+        const u64 beg = offsets[p];
+        const int n = int(offsets[p + 1] - beg);
+        u64* r = records + beg;
+        u64 v[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) v[q] = q < n ? r[q] : ~0ull;
+        cmp_exch(v[0], v[1]); cmp_exch(v[2], v[3]); cmp_exch(v[4], v[5]); cmp_exch(v[6], v[7]);
+        cmp_exch(v[0], v[2]); cmp_exch(v[1], v[3]); cmp_exch(v[4], v[6]); cmp_exch(v[5], v[7]);
+        cmp_exch(v[1], v[2]); cmp_exch(v[5], v[6]);
+        cmp_exch(v[0], v[4]); cmp_exch(v[1], v[5]); cmp_exch(v[2], v[6]); cmp_exch(v[3], v[7]);
+        cmp_exch(v[2], v[4]); cmp_exch(v[3], v[5]);
+        cmp_exch(v[1], v[2]); cmp_exch(v[3], v[4]); cmp_exch(v[5], v[6]);
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+            if (q < n) r[q] = v[q];
+    }
 }
 
 // Classes 0..4: K records per lane in registers (K = 1: bitonic over shuffles).
@@ -973,7 +1018,7 @@ __global__ void __launch_bounds__(1024) k_sort_class_long(const u64* __restrict_
     }
 }
 
-static_assert(kSortClasses == 8, "k_sort_classify assigns classes 0..7");
+static_assert(kSortClasses == 9, "k_sort_classify assigns classes 0..8");
 
 template <int K>
 void sort_class(int method, unsigned g, const u64* offsets, u64* records, const uint32_t* items,
@@ -1012,6 +1057,8 @@ void launch_sort(const u64* offsets, u64* records, uint32_t P, uint32_t* scratch
     auto q = [&](int c) {
         return ((bucket_classes >> c) & 1u) ? 2 : (((surrogate_classes >> c) & 1u) ? 1 : 0);
     };
+    k_sort_class_tiny<<<kSortGridBlocks / 2, 256, 0, s>>>(offsets, records, items(kSortTinyClass),
+                                                          scratch + kSortTinyClass, ok);
     k_sort_class_regs<1, false><<<g, kSortWarps * 32, 0, s>>>(offsets, records, items(0), scratch + 0, redo_n, redo,
                                                               ok);
     sort_class<2>(q(1), g, offsets, records, items(1), scratch + 1, redo_n, redo, ok, s);
