@@ -174,13 +174,19 @@ __device__ __forceinline__ float ray_scale(const CamDev& cam, float qx, float qy
     return sqrtf(1.f + dx * dx + dy * dy);
 }
 
-__global__ void __launch_bounds__(kTile * kTile, 2) k_walk_composite(
+// The forward walk in 16 x 8 pixel blocks, five per SM (96 registers): the
+// walk is bound by the latency of its tet -> faces -> vertices chain, and 20
+// warps per SM hide more of it than 16 at 110 registers (3.59 -> 3.22 ms at
+// 64^3 / 1024^2).
+constexpr int kWalkRows = 8;
+constexpr int kWalkThreads = kTile * kWalkRows;
+__global__ void __launch_bounds__(kWalkThreads, 5) k_walk_composite(
     const u64* __restrict__ b_offsets, const u64* __restrict__ b_records, const uint32_t* __restrict__ bf_global,
     const uint4* __restrict__ faces, const uint32_t* __restrict__ f2t, TetTopo tt, uint32_t num_tets, const int2* __restrict__ vfix, const VGeo* __restrict__ vgeo,
     const float4* __restrict__ colors, CamDev cam, ShadeDev sh, float4* __restrict__ image,
     float* __restrict__ tfinal, uint4* __restrict__ wstate) {
     const int px = blockIdx.x * kTile + (threadIdx.x % kTile);
-    const int py = blockIdx.y * kTile + (threadIdx.x / kTile);
+    const int py = blockIdx.y * kWalkRows + (threadIdx.x / kTile);
     if (px >= cam.W || py >= cam.H) return;
     const size_t p = size_t(py) * cam.W + px;
     const u64 beg = b_offsets[p];
@@ -396,9 +402,9 @@ void launch_walk_composite(const u64* b_offsets, const u64* b_records, const uin
                            const uint32_t* cells, const uint8_t* tet_flip, uint32_t num_tets, const int2* vfix, const VGeo* vgeo, const float4* colors,
                            const CamDev& cam, const ShadeDev& sh, float4* image, float* tfinal, uint4* wstate,
                            cudaStream_t s) {
-    dim3 grid((cam.W + kTile - 1) / kTile, (cam.H + kTile - 1) / kTile);
+    dim3 grid((cam.W + kTile - 1) / kTile, (cam.H + kWalkRows - 1) / kWalkRows);
     const TetTopo tt{reinterpret_cast<const uint4*>(tet_faces), reinterpret_cast<const uint4*>(cells), tet_flip};
-    k_walk_composite<<<grid, kTile * kTile, 0, s>>>(b_offsets, b_records, bf_global, faces, face_to_tet, tt,
+    k_walk_composite<<<grid, kWalkThreads, 0, s>>>(b_offsets, b_records, bf_global, faces, face_to_tet, tt,
                                                     num_tets, vfix, vgeo, colors, cam, sh, image, tfinal, wstate);
 }
 
