@@ -51,7 +51,7 @@ class BatchRenderer:
 
     def __del__(self):
         h = getattr(self, "_handle", None)
-        if h is not None and h.value and _lib._lib is not None:
+        if h is not None and h.value and _lib is not None and getattr(_lib, "_lib", None) is not None:
             _lib.load().dtv_batch_destroy(h)
             self._handle = None
 

@@ -70,7 +70,8 @@ class Renderer:
 
     def __del__(self):
         h = getattr(self, "_handle", None)
-        if h is not None and getattr(self, "_owner", False) and h.value and _lib._lib is not None:
+        if (h is not None and getattr(self, "_owner", False) and h.value and _lib is not None
+                and getattr(_lib, "_lib", None) is not None):
             _lib.load().dtv_renderer_destroy(h)
             self._handle = None
 

@@ -129,7 +129,7 @@ class NativeMesh:
 
     def __del__(self):
         h = getattr(self, "handle", None)
-        if h is not None and h.value and _lib._lib is not None:
+        if h is not None and h.value and _lib is not None and getattr(_lib, "_lib", None) is not None:
             _lib.load().dtv_mesh_destroy(h)
             self.handle = None
 
