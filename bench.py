@@ -56,6 +56,7 @@ def parse_args():
     ap.add_argument("--profile", choices=["ppll", "intersection"], default=None,
                     help="profiling case: Kuhn --n^3 at --res^2, one warm-up and one render + adjoint, no timing")
     ap.add_argument("--no-scale", action="store_true")
+    ap.add_argument("--no-next", action="store_true", help="skip the per-cell and regularizer sections")
     ap.add_argument("--scale-n", type=int, default=128)
     ap.add_argument("--scale-res", type=int, default=2048)
     ap.add_argument("--scale-steps", type=int, default=5)
@@ -522,6 +523,100 @@ def run_raytet(args):
     del sc
     torch.cuda.empty_cache()
     return out
+
+
+def run_cells_and_regularizer(args):
+    """The path's next rows on the plain workload: per-cell colours (the same
+    Kuhn mesh with one RGBA per tet, the cell mean of the vertex colours; step
+    = render, fused L2 loss, adjoint, Adam on positions and cell colours) and
+    the tet-quality regularizer's gradient over all tets (lambda 0.1, softplus
+    beta 100: the reference training script's defaults)."""
+    import numpy as np
+    import torch
+
+    import difftetvr_b200 as d
+    from difftetvr_b200 import _lib
+    from difftetvr_b200 import synthetic as S
+    from difftetvr_b200.optim import CLAMP_NONNEGATIVE, Adam
+
+    device = torch.device("cuda", torch.cuda.current_device())
+    cells, pos = S.kuhn_mesh(args.n, seed=0)
+    _, pos_t = S.kuhn_mesh(args.n, seed=1)
+    views = [S.sphere_camera(100 + i) for i in range(args.views)]
+
+    def cell_colors(p, seed):
+        return S.gaussian_colors(p, seed=seed)[cells].mean(axis=1).astype(np.float32)
+
+    def make(p, cc):
+        m = d.TetMesh()
+        m.set_use_gradients(True)
+        m.set_tet_mesh_data_cell(cells, p, cc)
+        r = d.Renderer(d.RendererType.PPLL)
+        r.set_tet_mesh(m)
+        r.set_viewport_size(args.res, args.res)
+        r.set_camera_fovy(S.FOVY_45)
+        r.set_attenuation(1.0)
+        r.set_clear_color(d.vec4(0, 0, 0, 0))
+        return m, r
+
+    m_t, r_t = make(pos_t, cell_colors(pos_t, 1))
+    targets = []
+    with torch.no_grad():
+        for v in views:
+            r_t.set_view_matrix(v)
+            targets.append(r_t.render().clone())
+    del r_t, m_t
+    mesh, r = make(pos, cell_colors(pos, 0))
+    p, cc = mesh.get_vertex_positions(), mesh.get_cell_colors()
+    opt = Adam([{"params": [cc], "lr": LR_COL, "clamp": CLAMP_NONNEGATIVE},
+                {"params": [p], "lr": LR_POS}], betas=(0.9, 0.999), eps=1e-8)
+    n_img = targets[0].numel()
+    adj = torch.empty_like(targets[0])
+    loss_acc = torch.zeros(1, device=device)
+    stream = torch.cuda.current_stream(device)
+
+    def step(i):
+        p.grad.zero_()
+        cc.grad.zero_()
+        r.set_view_matrix(views[i % len(views)])
+        image = r.render()
+        _lib.call("dtv_loss_l2", image.data_ptr(), targets[i % len(views)].data_ptr(), n_img,
+                  1.0 / n_img, adj.data_ptr(), loss_acc.data_ptr(), stream.cuda_stream)
+        r.render_adjoint(adj)
+        opt.step()
+
+    def timed(fn, warmup, n):
+        for i in range(warmup):
+            fn(i)
+        torch.cuda.synchronize()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        for i in range(n):
+            fn(warmup + i)
+        t1.record(stream)
+        torch.cuda.synchronize()
+        return t0.elapsed_time(t1) / n
+
+    ms = timed(step, max(args.warmup, 3), args.steps)
+    r.set_stage_timing(True)
+    stage_sum = {k: 0.0 for k in r.STAGES}
+    n_st = min(args.steps, 5)
+    for i in range(n_st):
+        step(i)
+        for k, v in r.get_stage_times().items():
+            stage_sum[k] += v
+    r.set_stage_timing(False)
+    cells_out = {"iter_per_s": 1e3 / ms, "ms_per_step": ms, "fragments_per_step": r.get_num_fragments(),
+                 "stage_ms": {k: round(v / n_st, 4) for k, v in stage_sum.items()},
+                 "workload": f"Kuhn {args.n}^3 with per-cell RGBA at {args.res}x{args.res}, one camera per step"}
+    reg = d.TetRegularizer(mesh, 0.1, 100.0)
+    reg_ms = timed(lambda i: reg.compute_grad(), 3, 20)
+    T = int(cells.shape[0])
+    reg_out = {"ms_per_call": reg_ms, "tets_per_s": T / (reg_ms / 1e3), "tets": T,
+               "note": "gradient of the tet-quality penalty added into the position .grad (float atomics)"}
+    del r, mesh
+    torch.cuda.empty_cache()
+    return cells_out, reg_out
 
 
 def run_scale(args):
@@ -1019,6 +1114,8 @@ def main():
     result, sc = run_ours(args, rank, world)
     if not args.no_raytet:
         result["raytet"] = run_raytet(args)
+    if not args.no_next:
+        result["cells"], result["regularizer"] = run_cells_and_regularizer(args)
     if not args.no_scale:
         result["scale"] = run_scale(args)
     if not args.no_batched:

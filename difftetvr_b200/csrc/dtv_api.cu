@@ -201,7 +201,8 @@ void adjoint_rows(dtv_renderer* r, const dtv_mesh* mesh, const float* d_colors, 
 void scatter_rows(dtv_renderer* r, const dtv::ShadeDev& sh, float* d_grad_positions, float* d_grad_colors,
                   cudaStream_t s) {
     if (r->cells)
-        dtv::launch_scatter_positions(r->grad_rows.ptr, uint32_t(r->V), d_grad_positions, s);
+        dtv::launch_scatter_positions(r->grad_rows.ptr, uint32_t(r->V), d_grad_positions, s,
+                                      sh.use_abs_grad ? nullptr : r->vgeo.ptr, &r->cam);
     else
         dtv::launch_scatter_grads(r->grad_rows.ptr, uint32_t(r->V), d_grad_positions,
                                   reinterpret_cast<float4*>(d_grad_colors), s,

@@ -109,8 +109,12 @@ void launch_adjoint_cells_rows(const unsigned long long* offsets, const unsigned
                                const float4* cell_colors, const CamDev& cam, const ShadeDev& sh, const float4* dimage,
                                const float* tfinal, const uint32_t* term, int row0, int row1, float4* grad_rows,
                                float4* grad_cells, cudaStream_t s);
-// Adds the position part of the [V][2] gradient rows into grad_pos [V,3].
-void launch_scatter_positions(const float4* grad_rows, uint32_t V, float* grad_pos, cudaStream_t s);
+// Adds the position part of the [V][2] gradient rows into grad_pos [V,3]
+// (vgeo non-null: the rows hold screen-space adjoints, converted per vertex
+// with the render's camera, as the per-cell adjoint leaves them without
+// absolute gradients).
+void launch_scatter_positions(const float4* grad_rows, uint32_t V, float* grad_pos, cudaStream_t s,
+                              const VGeo* vgeo = nullptr, const CamDev* cam = nullptr);
 
 // Ray-tet path (dtv_raytet.cu).
 void launch_walk_composite(const unsigned long long* b_offsets, const unsigned long long* b_records,

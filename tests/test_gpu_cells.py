@@ -66,6 +66,29 @@ def test_image_and_gradients_match_fp64_oracle(oracle, kind, n, res, ert):
     assert rel_err(c.grad.cpu().numpy(), gc_o) < 1e-4, rel_err(c.grad.cpu().numpy(), gc_o)
 
 
+@pytest.mark.parametrize("kind,n,res", [("cube", 8, 128), ("two_blocks", 4, 128)])
+def test_absolute_gradients_match_fp64_oracle(oracle, kind, n, res):
+    """render_adjoint(use_abs_grad=True) on per-cell colours: |.| of each
+    fragment's contribution per vertex and per cell, world-space rows (the
+    other path of the per-cell adjoint)."""
+    sc = two_block_scene(n, res, seed=50 + n) if kind == "two_blocks" else Scene(n, res, seed=50 + n)
+    ccol = _ccol(sc, n + 1)
+    m, r = _cells_renderer(sc, ccol)
+    r.render()
+    w = np.random.default_rng(8).normal(size=(res, res, 4)).astype(np.float32)
+    p, c = m.get_vertex_positions(), m.get_cell_colors()
+    p.grad.zero_()
+    c.grad.zero_()
+    r.render_adjoint(torch.from_numpy(w).cuda(), use_abs_grad=True)
+    fa = oracle.Faces(sc.cells, sc.pos.shape[0])
+    prm = oracle.make_params(attenuation=2.0, use_abs_grad=True)
+    _, _, _, _, gp_o, gc_o = oracle.render_cells(fa, sc.pos, ccol, sc.oracle_camera(oracle), prm,
+                                                 image_adjoint=w.astype(np.float64))
+    gp, gc = p.grad.cpu().numpy(), c.grad.cpu().numpy()
+    assert (gc >= 0).all()
+    assert rel_err(gp, gp_o) < 1e-4 and rel_err(gc, gc_o) < 1e-4, (rel_err(gp, gp_o), rel_err(gc, gc_o))
+
+
 def test_banded_per_cell_equals_stored():
     sc = Scene(12, 192, seed=4)
     m, r = _cells_renderer(sc, _ccol(sc, 1))
