@@ -181,14 +181,17 @@ __device__ __forceinline__ float cell_segment_adjoint(uint2 pf, uint2 pb, float 
     return gA * (-a * A);
 }
 
+// 16 x 8 pixel blocks: the carried screen-space variant fits five per SM
+// (at most 102 registers, no spills).
+constexpr int kCellRows = 8;
 template <bool SCREEN>
-__global__ void __launch_bounds__(kTile * kTile) k_adjoint_cells(
+__global__ void __launch_bounds__(kTile * kCellRows, SCREEN ? 5 : 4) k_adjoint_cells(
     const u64* __restrict__ offsets, const u64* __restrict__ records, const uint4* __restrict__ faces,
     const uint2* __restrict__ f2t, const VGeo* __restrict__ vgeo, const float4* __restrict__ cell_colors, int W,
     int row0, int row1, CamDev cam, ShadeDev sh, const float4* __restrict__ dimage, const float* __restrict__ tfinal,
     const uint32_t* __restrict__ term, float4* __restrict__ grad_rows, float4* __restrict__ grad_cells) {
     const int px = blockIdx.x * kTile + (threadIdx.x % kTile);
-    const int py = row0 + int(blockIdx.y) * kTile + int(threadIdx.x / kTile);
+    const int py = row0 + int(blockIdx.y) * kCellRows + int(threadIdx.x / kTile);
     if (px >= W || py >= row1) return;
     const size_t p = size_t(py) * W + px;
     const u64 beg = offsets[p];
@@ -288,14 +291,14 @@ void launch_adjoint_cells_rows(const u64* offsets, const u64* records, const uin
                                const uint32_t* term, int row0, int row1, float4* grad_rows, float4* grad_cells,
                                cudaStream_t s) {
     if (row1 <= row0) return;
-    dim3 grid((cam.W + kTile - 1) / kTile, (row1 - row0 + kTile - 1) / kTile);
+    dim3 grid((cam.W + kTile - 1) / kTile, (row1 - row0 + kCellRows - 1) / kCellRows);
     if (sh.use_abs_grad)
-        k_adjoint_cells<false><<<grid, kTile * kTile, 0, s>>>(offsets, records, faces,
+        k_adjoint_cells<false><<<grid, kTile * kCellRows, 0, s>>>(offsets, records, faces,
                                                               reinterpret_cast<const uint2*>(face_to_tet), vgeo,
                                                               cell_colors, cam.W, row0, row1, cam, sh, dimage, tfinal,
                                                               term, grad_rows, grad_cells);
     else
-        k_adjoint_cells<true><<<grid, kTile * kTile, 0, s>>>(offsets, records, faces,
+        k_adjoint_cells<true><<<grid, kTile * kCellRows, 0, s>>>(offsets, records, faces,
                                                              reinterpret_cast<const uint2*>(face_to_tet), vgeo,
                                                              cell_colors, cam.W, row0, row1, cam, sh, dimage, tfinal,
                                                              term, grad_rows, grad_cells);
