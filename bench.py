@@ -53,8 +53,9 @@ def parse_args():
     ap.add_argument("--no-autotune", action="store_true", help="keep the default kernel configuration")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-raytet", action="store_true")
-    ap.add_argument("--profile", choices=["ppll", "intersection"], default=None,
-                    help="profiling case: Kuhn --n^3 at --res^2, one warm-up and one render + adjoint, no timing")
+    ap.add_argument("--profile", choices=["ppll", "intersection", "cells"], default=None,
+                    help="profiling case: Kuhn --n^3 at --res^2, one warm-up and one render + adjoint, no timing "
+                         "(cells: one RGBA per tet, the cell mean of the vertex colours)")
     ap.add_argument("--no-scale", action="store_true")
     ap.add_argument("--no-next", action="store_true", help="skip the per-cell and regularizer sections")
     ap.add_argument("--scale-n", type=int, default=128)
@@ -1060,7 +1061,8 @@ def run_reference(args, rank, world):
 
 def run_profile_case(args):
     """A small fixed case for ncu: one warm-up and one render + adjoint of the
-    Kuhn n^3 mesh (seed 0) from sphere camera 100 at res x res."""
+    Kuhn n^3 mesh (seed 0) from sphere camera 100 at res x res (per-cell
+    colours for `cells`)."""
     import torch
 
     import difftetvr_b200 as d
@@ -1069,7 +1071,10 @@ def run_profile_case(args):
     col = S.gaussian_colors(pos, seed=0)
     mesh = d.TetMesh()
     mesh.set_use_gradients(True)
-    mesh.set_tet_mesh_data(cells, pos, col)
+    if args.profile == "cells":
+        mesh.set_tet_mesh_data_cell(cells, pos, col[cells].mean(axis=1).astype(col.dtype))
+    else:
+        mesh.set_tet_mesh_data(cells, pos, col)
     rt = d.RendererType.INTERSECTION if args.profile == "intersection" else d.RendererType.PPLL
     r = d.Renderer(rt)
     r.set_tet_mesh(mesh)
