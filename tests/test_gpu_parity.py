@@ -39,6 +39,11 @@ def test_fragment_lists_bit_exact(oracle, n, res):
     assert np.array_equal(off_g.astype(np.int64), off_o)
     assert rec_g.shape == rec_o.shape
     assert np.array_equal(rec_g, rec_o)
+    if (n, res) == (16, 512):
+        # Every length of the one-thread class (2..8) and the first of the
+        # warp classes (9) occurs here.
+        lens = np.diff(off_o)
+        assert all((lens == k).any() for k in range(2, 10))
 
 
 def test_long_lists_bit_exact_and_composited(oracle):
