@@ -167,28 +167,81 @@ __global__ void __launch_bounds__(128) kb_raster(const BatchView* __restrict__ v
                                                  const float4* __restrict__ vproj, const int2* __restrict__ vfix,
                                                  uint32_t* __restrict__ counts, const u64* __restrict__ offsets,
                                                  u64* __restrict__ records, const uint32_t* __restrict__ ok,
-                                                 const uint32_t* __restrict__ order) {
+                                                 const uint32_t* __restrict__ order,
+                                                 uint32_t* __restrict__ wide_list) {
     if (FILL && !batch_ok(ok)) return;
     const u64 first = u64(blockIdx.x) * blockDim.x;
     const u64 i = first + threadIdx.x;
-    bool live = false;
+    bool set = false, live = false;
     RasterJob J;
+    u64 g = 0;
     if (i < total) {
-        const u64 g = order ? u64(order[i]) : i;
+        g = order ? u64(order[i]) : i;
         const int v = order ? find_index(g, nviews, [&](int k) { return views[k].face_base; })
                             : view_of_item(g, first, nviews, [&](int k) { return views[k].face_base; });
         const BatchView& bv = views[v];
-        live = raster_setup(uint32_t(g - bv.face_base), bv.faces, vfix + bv.vert_base, uint32_t(bv.vert_base),
-                            int(bv.W), 0, int(bv.H), bv.pix_base, J) &&
-               (J.wide != 0) == WIDE;
+        set = raster_setup(uint32_t(g - bv.face_base), bv.faces, vfix + bv.vert_base, uint32_t(bv.vert_base),
+                           int(bv.W), 0, int(bv.H), bv.pix_base, J);
+        live = set && (J.wide != 0) == WIDE;
     }
     if constexpr (!FILL) {
         if (live) count_face<typename std::conditional<WIDE, long long, int>::type>(J, counts);
+        if (!WIDE && wide_list) {
+            // The items of the 64-bit path, for its count and fill launches
+            // (wide_list[0] = how many, then the items).
+            const bool wide = set && J.wide != 0;
+            const unsigned m = __ballot_sync(0xffffffffu, wide);
+            if (m) {
+                const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
+                uint32_t base = 0;
+                if (lane == leader) base = atomicAdd(wide_list, uint32_t(__popc(m)));
+                base = __shfl_sync(0xffffffffu, base, leader);
+                if (wide) wide_list[1 + base + __popc(m & ((1u << lane) - 1u))] = uint32_t(g);
+            }
+        }
     } else {
         __shared__ RasterJob jobs[4][32];
         const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
         if (live) jobs[w][lane] = J;
         raster_warp<FILL, WIDE>(jobs[w], __ballot_sync(0xffffffffu, live), lane, vproj, counts, offsets, records);
+    }
+}
+
+// The 64-bit items listed by the count (wide_list), 32 per warp and step over
+// a fixed grid: the count (one thread per face) or the fill (raster_warp).
+template <bool FILL>
+__global__ void __launch_bounds__(128) kb_raster_listed(const BatchView* __restrict__ views, int nviews,
+                                                        const float4* __restrict__ vproj,
+                                                        const int2* __restrict__ vfix,
+                                                        uint32_t* __restrict__ counts,
+                                                        const u64* __restrict__ offsets, u64* __restrict__ records,
+                                                        const uint32_t* __restrict__ ok,
+                                                        const uint32_t* __restrict__ wide_list) {
+    if (FILL && !batch_ok(ok)) return;
+    __shared__ RasterJob jobs[4][32];
+    const uint32_t n = wide_list[0];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x + uint32_t(w) * 32u; base < n; base += stride) {
+        const uint32_t i = base + uint32_t(lane);
+        RasterJob J;
+        bool live = false;
+        if (i < n) {
+            const u64 g = wide_list[1 + i];
+            const int v = find_index(g, nviews, [&](int k) { return views[k].face_base; });
+            const BatchView& bv = views[v];
+            live = raster_setup(uint32_t(g - bv.face_base), bv.faces, vfix + bv.vert_base, uint32_t(bv.vert_base),
+                                int(bv.W), 0, int(bv.H), bv.pix_base, J) &&
+                   J.wide != 0;
+        }
+        if constexpr (!FILL) {
+            if (live) count_face<long long>(J, counts);
+        } else {
+            if (live) jobs[w][lane] = J;
+            raster_warp<FILL, true>(jobs[w], __ballot_sync(0xffffffffu, live), lane, vproj, counts, offsets,
+                                    records);
+            __syncwarp();  // every lane is done with this step's jobs before the next step writes them
+        }
     }
 }
 
@@ -454,6 +507,7 @@ struct dtv_batch {
     DevBuf<float4> grad_rows;
     DevBuf<uint32_t> fill_order;    // items (view faces) in row-band order for the fill
     DevBuf<uint32_t> band_scratch;  // band counts and cursors of fill_order
+    DevBuf<uint32_t> wide_list;     // [0] = n, then the items of the 64-bit raster path (count -> fill)
     DevBuf<float4> view_rows;  // [tot_verts][2]: screen-space adjoint rows of each view (at its vert_base)
     DevBuf<float4> dimage_internal;
     DevBuf<float> loss;
@@ -550,6 +604,7 @@ void ensure_scratch(dtv_batch* b, cudaStream_t s) {
     b->view_rows.ensure(2 * (b->tot_verts ? b->tot_verts : 1), s);
     b->fill_order.ensure(b->tot_faces ? b->tot_faces : 1, s);
     b->band_scratch.ensure(2 * dtv::kFillBands, s);
+    b->wide_list.ensure(b->tot_faces + 1, s);
     b->counts.ensure(b->tot_pixels, s, /*zero_new=*/true);
     b->offsets.ensure(b->tot_pixels + 1, s);
     b->scan.ensure(dtv::scan_scratch_elems(b->tot_pixels), s);
@@ -590,12 +645,16 @@ void launch_kb_raster(dtv_batch* b, const uint32_t* okp, cudaStream_t s) {
                                            b->tot_pixels, b->band_scratch.ptr + kFillBands, b->fill_order.ptr);
         order = b->fill_order.ptr;
     }
+    // The count lists the 64-bit items; the 64-bit count and the fill that
+    // follows walk that list instead of setting up every item again.
+    if (!FILL) DTV_CK(cudaMemsetAsync(b->wide_list.ptr, 0, sizeof(uint32_t), s));
     kb_raster<FILL, false><<<blocks, 128, 0, s>>>(b->d_views.ptr, b->nviews, b->tot_faces, b->vproj.ptr,
                                                   b->vfix.ptr, b->counts.ptr, FILL ? b->offsets.ptr : nullptr,
-                                                  FILL ? b->records.ptr : nullptr, okp, order);
-    kb_raster<FILL, true><<<blocks, 128, 0, s>>>(b->d_views.ptr, b->nviews, b->tot_faces, b->vproj.ptr,
-                                                 b->vfix.ptr, b->counts.ptr, FILL ? b->offsets.ptr : nullptr,
-                                                 FILL ? b->records.ptr : nullptr, okp, order);
+                                                  FILL ? b->records.ptr : nullptr, okp, order,
+                                                  FILL ? nullptr : b->wide_list.ptr);
+    kb_raster_listed<FILL><<<148, 128, 0, s>>>(b->d_views.ptr, b->nviews, b->vproj.ptr, b->vfix.ptr, b->counts.ptr,
+                                               FILL ? b->offsets.ptr : nullptr, FILL ? b->records.ptr : nullptr, okp,
+                                               b->wide_list.ptr);
     if (!FILL) {
         dim3 grid(unsigned(b->max_height + 7) / 8, unsigned(b->nviews));
         kb_row_prefix<<<grid, 256, 0, s>>>(b->d_views.ptr, b->counts.ptr);
@@ -697,6 +756,7 @@ int32_t dtv_batch_reserve(dtv_batch* b, uint64_t max_views, uint64_t max_vertice
         // batch with more faces grows it at its first render.
         b->fill_order.ensure(13 * V, s);
         b->band_scratch.ensure(2 * dtv::kFillBands, s);
+        b->wide_list.ensure(13 * V + 1, s);
         b->counts.ensure(P, s, /*zero_new=*/true);
         b->offsets.ensure(P + 1, s);
         b->scan.ensure(dtv::scan_scratch_elems(P), s);
@@ -745,6 +805,7 @@ int32_t dtv_batch_destroy(dtv_batch* b) {
     b->view_rows.release();
     b->fill_order.release();
     b->band_scratch.release();
+    b->wide_list.release();
     b->dimage_internal.release();
     b->loss.release();
     b->step.release();
@@ -963,7 +1024,7 @@ std::vector<u64> train_signature(const dtv_batch* b, const dtv::AdamConst& ac, i
                             u64(b->max_height),
                             b->capacity, u64(nslots), u64(uintptr_t(b->records.ptr)),
                             u64(uintptr_t(b->dimage_internal.ptr)), u64(uintptr_t(b->grad_rows.ptr)),
-                            u64(uintptr_t(b->view_rows.ptr))};
+                            u64(uintptr_t(b->view_rows.ptr)), u64(uintptr_t(b->wide_list.ptr))};
     const uint32_t* shw = reinterpret_cast<const uint32_t*>(&b->sh);
     for (size_t i = 0; i < sizeof(b->sh) / 4; ++i) sig.push_back(shw[i]);
     const uint32_t* acw = reinterpret_cast<const uint32_t*>(&ac);

@@ -49,6 +49,23 @@ def test_batch_render_matches_plain_views():
         assert float((img - ref).abs().max()) <= 1e-6
 
 
+def test_batch_wide_faces_match_plain_views():
+    """Meshes of 1 and 2 cubes per axis at 512^2: face boxes over 64 px take the
+    64-bit raster path (listed by the count), beside an ordinary 8^3 view."""
+    meshes = [make_mesh(1, 6), make_mesh(2, 7), make_mesh(8, 8)]
+    br = BatchRenderer(meshes, attenuation=1.0)
+    views = views_for([0, 1, 2, 1], [(512, 512), (512, 384), (96, 96), (300, 512)])
+    imgs = br.render(views)
+    torch.cuda.synchronize()
+    nf = 0
+    for v, img in zip(views, imgs):
+        r = plain_renderer(meshes[v.mesh], v)
+        ref = r.render()
+        nf += r.get_num_fragments()
+        assert float((img - ref).abs().max()) <= 1e-6
+    assert br.info()["fragments"] == nf
+
+
 def test_batch_adjoint_matches_sum_of_plain_adjoints():
     meshes = [make_mesh(8, 4), make_mesh(6, 5)]
     br = BatchRenderer(meshes, attenuation=2.0)
